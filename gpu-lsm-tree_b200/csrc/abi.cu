@@ -1,0 +1,314 @@
+// extern "C" boundary (include/gpulsm.h): maps C++ exceptions of the engines
+// to gpulsm_status codes, as a C caller (ctypes / cgo / JNI) needs.
+#include "../../include/gpulsm.h"
+
+#include <cuda_runtime.h>
+
+#include <new>
+#include <stdexcept>
+#include <string>
+
+#include "common.cuh"
+#include "flix_index.h"
+#include "lsm_dictionary.h"
+#include "radix_sort.cuh"
+#include "sort_api.h"
+
+struct gpulsm_dict {
+  gpulsm::LsmDictionary impl;
+  explicit gpulsm_dict(const gpulsm::DictConfig &c) : impl(c) {}
+};
+
+struct gpulsm_flix {
+  gpulsm::FlixIndex impl;
+  explicit gpulsm_flix(const gpulsm::FlixConfig &c) : impl(c) {}
+};
+
+namespace {
+thread_local std::string g_error;
+
+template <class F> int guarded(F &&f) {
+  try {
+    f();
+    return GPULSM_OK;
+  } catch (const std::invalid_argument &e) {
+    g_error = e.what();
+    return GPULSM_ERR_INVALID_ARGUMENT;
+  } catch (const std::length_error &e) {
+    g_error = e.what();
+    return GPULSM_ERR_LENGTH;
+  } catch (const std::bad_alloc &e) {
+    g_error = std::string("out of device memory: ") + e.what();
+    return GPULSM_ERR_OUT_OF_MEMORY;
+  } catch (const gpulsm::CudaError &e) {
+    g_error = e.what();
+    return e.code == cudaErrorMemoryAllocation ? GPULSM_ERR_OUT_OF_MEMORY : GPULSM_ERR_CUDA;
+  } catch (const std::runtime_error &e) {
+    g_error = e.what();
+    const std::string m = e.what();
+    if (m.find("capacity") != std::string::npos) return GPULSM_ERR_CAPACITY;
+    if (m.find("timed out") != std::string::npos) return GPULSM_ERR_TIMEOUT;
+    return GPULSM_ERR_PUBLICATION;
+  } catch (const std::exception &e) {
+    g_error = e.what();
+    return GPULSM_ERR_CUDA;
+  }
+}
+
+inline cudaStream_t S(void *s) { return static_cast<cudaStream_t>(s); }
+
+template <class T> void need(T *p, const char *what) {
+  if (!p) throw std::invalid_argument(std::string("null ") + what);
+}
+}  // namespace
+
+extern "C" {
+
+const char *gpulsm_last_error(void) { return g_error.c_str(); }
+const char *gpulsm_version(void) { return "gpulsm-b200 0.1 (sm_100a)"; }
+
+// ---------------------------------------------------------------- LSM dictionary
+int gpulsm_dict_create(const gpulsm_dict_config *config, gpulsm_dict **out) {
+  return guarded([&] {
+    need(config, "config");
+    need(out, "out");
+    gpulsm::DictConfig c;
+    c.max_elements = config->max_elements;
+    c.batch_capacity = config->batch_capacity;
+    c.level_zero_capacity = config->level_zero_capacity;
+    c.fan_in = config->fan_in;
+    c.rows_per_bucket_log2 = config->rows_per_bucket_log2;
+    c.search_mode = config->search_mode;
+    *out = new gpulsm_dict(c);
+  });
+}
+
+int gpulsm_dict_destroy(gpulsm_dict *d) {
+  return guarded([&] { delete d; });
+}
+
+int gpulsm_dict_clear(gpulsm_dict *d, void *stream) {
+  return guarded([&] {
+    need(d, "dict");
+    d->impl.clear(S(stream));
+  });
+}
+
+int gpulsm_dict_bulk_build(gpulsm_dict *d, const uint32_t *keys, const uint32_t *values,
+                           uint64_t count, void *stream) {
+  return guarded([&] {
+    need(d, "dict");
+    d->impl.bulk_build(keys, values, count, S(stream));
+  });
+}
+
+int gpulsm_dict_insert(gpulsm_dict *d, const uint32_t *keys, const uint32_t *values,
+                       uint64_t count, void *stream) {
+  return guarded([&] {
+    need(d, "dict");
+    d->impl.insert(keys, values, count, S(stream));
+  });
+}
+
+int gpulsm_dict_erase(gpulsm_dict *d, const uint32_t *keys, uint64_t count, void *stream) {
+  return guarded([&] {
+    need(d, "dict");
+    d->impl.erase(keys, count, S(stream));
+  });
+}
+
+int gpulsm_dict_lookup(gpulsm_dict *d, const uint32_t *queries, uint64_t count,
+                       uint32_t *out_values, uint8_t *out_found, void *stream) {
+  return guarded([&] {
+    need(d, "dict");
+    d->impl.lookup(queries, count, out_values, out_found, S(stream));
+  });
+}
+
+int gpulsm_dict_range_sum(gpulsm_dict *d, const uint32_t *lo, const uint32_t *hi, uint64_t count,
+                          uint32_t *out_sums, void *stream) {
+  return guarded([&] {
+    need(d, "dict");
+    d->impl.range_sum(lo, hi, count, out_sums, S(stream));
+  });
+}
+
+int gpulsm_dict_range_count(gpulsm_dict *d, const uint32_t *lo, const uint32_t *hi,
+                            uint64_t count, uint32_t *out_counts, void *stream) {
+  return guarded([&] {
+    need(d, "dict");
+    d->impl.range_count(lo, hi, count, out_counts, S(stream));
+  });
+}
+
+int gpulsm_dict_range_offsets(gpulsm_dict *d, const uint32_t *lo, const uint32_t *hi,
+                              uint64_t count, uint64_t *offsets, void *stream) {
+  return guarded([&] {
+    need(d, "dict");
+    d->impl.range_offsets(lo, hi, count, offsets, S(stream));
+  });
+}
+
+int gpulsm_dict_range_pairs(gpulsm_dict *d, const uint32_t *lo, const uint32_t *hi,
+                            uint64_t count, const uint64_t *offsets, uint32_t *out_keys,
+                            uint32_t *out_values, void *stream) {
+  return guarded([&] {
+    need(d, "dict");
+    d->impl.range_pairs(lo, hi, count, offsets, out_keys, out_values, S(stream));
+  });
+}
+
+int gpulsm_dict_successor(gpulsm_dict *d, const uint32_t *queries, uint64_t count,
+                          uint32_t *out_keys, void *stream) {
+  return guarded([&] {
+    need(d, "dict");
+    d->impl.successor(queries, count, out_keys, S(stream));
+  });
+}
+
+int gpulsm_dict_status(gpulsm_dict *d, uint32_t *out_status) {
+  return guarded([&] {
+    need(d, "dict");
+    need(out_status, "out_status");
+    *out_status = d->impl.status();
+  });
+}
+
+int gpulsm_dict_resident_bytes(gpulsm_dict *d, uint64_t *out_bytes) {
+  return guarded([&] {
+    need(d, "dict");
+    need(out_bytes, "out_bytes");
+    *out_bytes = d->impl.resident_bytes();
+  });
+}
+
+int gpulsm_dict_size(gpulsm_dict *d, uint64_t *out_rows, uint32_t *out_levels) {
+  return guarded([&] {
+    need(d, "dict");
+    d->impl.size(out_rows, out_levels);
+  });
+}
+
+// ---------------------------------------------------------------- FliX
+int gpulsm_flix_create(const gpulsm_flix_config *config, gpulsm_flix **out) {
+  return guarded([&] {
+    need(config, "config");
+    need(out, "out");
+    gpulsm::FlixConfig c;
+    c.key_bits = config->key_bits;
+    c.node_size = config->node_size;
+    c.fill_percent = config->fill_percent;
+    c.search_mode = config->search_mode;
+    c.max_elements = config->max_elements;
+    *out = new gpulsm_flix(c);
+  });
+}
+
+int gpulsm_flix_destroy(gpulsm_flix *f) {
+  return guarded([&] { delete f; });
+}
+
+int gpulsm_flix_build(gpulsm_flix *f, const void *keys, const uint32_t *values, uint64_t count,
+                      uint64_t max_count, void *stream) {
+  return guarded([&] {
+    need(f, "index");
+    f->impl.build(keys, values, count, max_count, S(stream));
+  });
+}
+
+int gpulsm_flix_insert(gpulsm_flix *f, const void *keys, const uint32_t *values, uint64_t count,
+                       void *stream) {
+  return guarded([&] {
+    need(f, "index");
+    f->impl.insert(keys, values, count, S(stream));
+  });
+}
+
+int gpulsm_flix_remove(gpulsm_flix *f, const void *keys, uint64_t count, void *stream) {
+  return guarded([&] {
+    need(f, "index");
+    f->impl.remove(keys, count, S(stream));
+  });
+}
+
+int gpulsm_flix_lookups_ordered(gpulsm_flix *f, const void *sorted_probes, uint64_t count,
+                                uint32_t *out_values, void *stream) {
+  return guarded([&] {
+    need(f, "index");
+    f->impl.lookups_ordered(sorted_probes, count, out_values, S(stream));
+  });
+}
+
+int gpulsm_flix_lookups_successor(gpulsm_flix *f, const void *sorted_probes, uint64_t count,
+                                  void *out_keys, void *stream) {
+  return guarded([&] {
+    need(f, "index");
+    f->impl.lookups_successor(sorted_probes, count, out_keys, S(stream));
+  });
+}
+
+int gpulsm_flix_lookup(gpulsm_flix *f, const void *probes, uint64_t count, uint32_t *out_values,
+                       void *stream) {
+  return guarded([&] {
+    need(f, "index");
+    f->impl.lookup(probes, count, out_values, S(stream));
+  });
+}
+
+int gpulsm_flix_successor(gpulsm_flix *f, const void *probes, uint64_t count, void *out_keys,
+                          void *stream) {
+  return guarded([&] {
+    need(f, "index");
+    f->impl.successor(probes, count, out_keys, S(stream));
+  });
+}
+
+int gpulsm_flix_rebuild(gpulsm_flix *f, void *stream) {
+  return guarded([&] {
+    need(f, "index");
+    f->impl.rebuild(S(stream));
+  });
+}
+
+int gpulsm_flix_resident_bytes(gpulsm_flix *f, uint64_t *out_bytes) {
+  return guarded([&] {
+    need(f, "index");
+    need(out_bytes, "out_bytes");
+    *out_bytes = f->impl.resident_bytes();
+  });
+}
+
+int gpulsm_flix_size(gpulsm_flix *f, uint64_t *out_keys) {
+  return guarded([&] {
+    need(f, "index");
+    need(out_keys, "out_keys");
+    *out_keys = f->impl.size();
+  });
+}
+
+int gpulsm_flix_status(gpulsm_flix *f, uint32_t *out_status) {
+  return guarded([&] {
+    need(f, "index");
+    need(out_status, "out_status");
+    *out_status = f->impl.status();
+  });
+}
+
+// ---------------------------------------------------------------- building blocks
+int gpulsm_sort_pairs(const void *keys_in, const uint32_t *values_in, void *keys_out,
+                      uint32_t *values_out, uint64_t count, uint32_t key_bits, uint32_t begin_bit,
+                      uint32_t end_bit, void *stream) {
+  return guarded([&] {
+    if (key_bits != 32 && key_bits != 64) throw std::invalid_argument("key_bits must be 32 or 64");
+    if (begin_bit >= end_bit || end_bit > key_bits) throw std::invalid_argument("bad bit range");
+    if (count > gpulsm::radix::kMaxKeys) throw std::length_error("sort limited to 2^30-1 keys");
+    if (!count) return;
+    need(keys_in, "keys_in");
+    need(keys_out, "keys_out");
+    if (values_in) need(values_out, "values_out");
+    gpulsm::sort_pairs_any(keys_in, values_in, keys_out, values_out, count, key_bits, begin_bit,
+                           end_bit, S(stream));
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,116 @@
+// Shared device/host helpers for the B200 GPU dictionary (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+
+namespace gpulsm {
+
+// ---- status word bits written by kernels (never a trap) ---------------------
+// A kernel that detects a problem ORs one of these into a device status word
+// and returns; the host folds the word into the status it reports.
+// Bit 3 keeps the meaning of GPULSMOpt's kPublicationOutputOverflow
+// (GPULSMOpt.cuh:535-541); the others are new.
+enum : uint32_t {
+  kDevOk = 0u,
+  kDevOutputOverflow = 1u << 3, // output would exceed its buffer / capacity
+  kDevWaitTimeout = 1u << 8,    // a bounded spin (look-back) gave up
+  kDevBadInput = 1u << 9,       // caller data violated a documented precondition
+};
+
+// Spin limit for decoupled look-back waits.  Predecessor tiles are always
+// resident (tile ids come from an atomic ticket), so a healthy wait ends in a
+// few microseconds; the limit only turns a broken invariant into a status bit.
+constexpr uint32_t kMaxSpins = 1u << 22;
+
+constexpr uint32_t kNotFound = 0xffffffffu;
+
+struct CudaError : std::runtime_error {
+  cudaError_t code;
+  CudaError(cudaError_t c, const std::string &where)
+      : std::runtime_error(std::string(cudaGetErrorString(c)) + " at " + where), code(c) {}
+};
+
+#define GPULSM_CUDA(call)                                                        \
+  do {                                                                           \
+    const cudaError_t e__ = (call);                                              \
+    if (e__ != cudaSuccess)                                                      \
+      throw ::gpulsm::CudaError(e__, std::string(__FILE__) + ":" +               \
+                                         std::to_string(__LINE__));              \
+  } while (false)
+
+inline unsigned grid_for(uint64_t n, unsigned threads) {
+  const uint64_t g = (n + threads - 1) / threads;
+  return static_cast<unsigned>(g ? g : 1);
+}
+
+__host__ __device__ inline uint32_t ceil_log2_u64(uint64_t x) {
+  uint32_t b = 0;
+  while ((uint64_t{1} << b) < x) ++b;
+  return b;
+}
+
+#ifdef __CUDACC__
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm volatile("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+__device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t *p) {
+  uint32_t v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void st_relaxed_u32(uint32_t *p, uint32_t v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long *p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long *p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Exclusive scan across a block of BLOCK threads (one value per thread).
+// `warp_sums` must hold BLOCK/32 entries.  Returns the exclusive prefix and
+// writes the block total to *total.
+template <int BLOCK, typename T>
+__device__ __forceinline__ T block_exclusive_scan(T value, T *warp_sums, T *total) {
+  constexpr int W = BLOCK / 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  T inc = value;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const T y = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += y;
+  }
+  if (lane == 31) warp_sums[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    T w = lane < W ? warp_sums[lane] : T(0);
+    T wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const T y = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += y;
+    }
+    if (lane < W) warp_sums[lane] = wi - w;  // exclusive warp offsets
+    if (lane == W - 1) *total = wi;
+  }
+  __syncthreads();
+  const T r = warp_sums[warp] + inc - value;
+  __syncthreads();
+  return r;
+}
+#endif
+
+}  // namespace gpulsm

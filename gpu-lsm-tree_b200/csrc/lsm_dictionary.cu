@@ -1,0 +1,609 @@
+// Host engine of the LSM dictionary (see lsm_dictionary.h).
+//
+// Structure: levels 0..L-1 are sorted runs of unique keys; level 0 is the
+// newest.  Level i holds at most caps_[i] rows (cap_0 * fan_in^i); the last
+// level is the foundation and takes whatever the cascade delivers.  An update
+// batch is radix-sorted, deduplicated (last input index wins) and carried
+// down: it absorbs every level it cannot fit beside, then lands in the first
+// level with room (leveling with fan-in R).  Tombstones are dropped by the
+// merge whose output has no older level beneath it.
+//
+// The host never waits for row counts.  It plans with upper bounds (dedup and
+// tombstone drops only shrink runs); kernels read the exact counts from the
+// device-side LevelDesc.  Exact counts come back through an asynchronous
+// receipt that the next call applies if it has arrived - the same lazy
+// receipt idea as GPULSMOpt's publication receipt (GPULSMOpt.cuh:6750-6811).
+#include "lsm_dictionary.h"
+
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <stdexcept>
+
+#include "lsm_kernels.cuh"
+#include "radix_sort.cuh"
+
+namespace gpulsm {
+
+using lsm::LevelDesc;
+
+namespace {
+constexpr uint64_t kMaxBatch = uint64_t{1} << 20;  // kMaximumOperationTile, GPULSMOpt.cuh:56
+constexpr size_t kAlign = 256;
+
+size_t align_up(size_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }
+
+struct ReceiptSrc {
+  const LevelDesc *desc[lsm::kMaxLevels];
+  uint32_t count;
+  const uint32_t *status;
+  unsigned long long *out;  // [kMaxLevels] counts then status
+};
+
+__global__ void receipt_kernel(ReceiptSrc src) {
+  const uint32_t i = threadIdx.x;
+  if (i < lsm::kMaxLevels)
+    src.out[i] = (i < src.count && src.desc[i]) ? src.desc[i]->n : 0ull;
+  if (i == lsm::kMaxLevels) src.out[i] = *src.status;
+}
+
+__global__ void set_count_kernel(LevelDesc *desc, unsigned long long n) { desc->n = n; }
+
+// Bump allocator over one zeroed scratch region.
+struct Bump {
+  char *p;
+  size_t off = 0;
+  template <class T> T *take(size_t count) {
+    T *r = reinterpret_cast<T *>(p + off);
+    off += align_up(count * sizeof(T));
+    return r;
+  }
+};
+
+size_t merge_scratch_bytes(uint64_t rows) {
+  const uint64_t tiles = (rows + lsm::kMergeTile - 1) / lsm::kMergeTile + 1;
+  return align_up(8) + align_up(tiles * 8);
+}
+}  // namespace
+
+struct LsmDictionary::Receipt {
+  unsigned long long n[lsm::kMaxLevels];
+  unsigned long long status;
+};
+
+// ----------------------------------------------------------------------------
+RunPool::~RunPool() {
+  for (auto &b : all_)
+    if (b->block) cudaFree(b->block);
+}
+
+RunBuffer *RunPool::acquire(uint64_t min_rows, cudaStream_t stream) {
+  uint64_t cap = 1024;
+  while (cap < min_rows) cap <<= 1;
+  RunBuffer *best = nullptr;
+  size_t best_i = 0;
+  for (size_t i = 0; i < free_.size(); ++i)
+    if (free_[i]->cap >= cap && (!best || free_[i]->cap < best->cap)) {
+      best = free_[i];
+      best_i = i;
+    }
+  if (best && best->cap <= cap * 2) {
+    free_.erase(free_.begin() + best_i);
+    return best;
+  }
+  auto b = std::make_unique<RunBuffer>();
+  b->cap = cap;
+  const uint32_t cl2 = ceil_log2_u64(cap);
+  b->dir_bits = std::max<uint32_t>(1, cl2 > rows_log2_ ? cl2 - rows_log2_ : 1);
+  const size_t kb = align_up(cap * 4), vb = align_up(cap * 4), fb = align_up(cap),
+               db = align_up(((size_t(1) << b->dir_bits) + 1) * 4), sb = align_up(sizeof(LevelDesc));
+  b->bytes = kb + vb + fb + db + sb;
+  cudaError_t e = cudaMallocAsync(&b->block, b->bytes, stream);
+  if (e != cudaSuccess) {
+    // give cached free buffers back and retry once
+    (void)cudaGetLastError();
+    release_all_free(stream);
+    e = cudaMallocAsync(&b->block, b->bytes, stream);
+    if (e != cudaSuccess) {
+      (void)cudaGetLastError();
+      throw std::bad_alloc();
+    }
+  }
+  char *p = static_cast<char *>(b->block);
+  b->keys = reinterpret_cast<uint32_t *>(p);
+  b->vals = reinterpret_cast<uint32_t *>(p + kb);
+  b->flags = reinterpret_cast<uint8_t *>(p + kb + vb);
+  b->dir = reinterpret_cast<uint32_t *>(p + kb + vb + fb);
+  b->desc = reinterpret_cast<LevelDesc *>(p + kb + vb + fb + db);
+  bytes_ += b->bytes;
+  all_.push_back(std::move(b));
+  return all_.back().get();
+}
+
+void RunPool::release(RunBuffer *b) {
+  if (b) free_.push_back(b);
+}
+
+void RunPool::release_all_free(cudaStream_t stream) {
+  for (RunBuffer *f : free_) {
+    cudaFreeAsync(f->block, stream);
+    bytes_ -= f->bytes;
+    for (size_t i = 0; i < all_.size(); ++i)
+      if (all_[i].get() == f) {
+        all_[i]->block = nullptr;
+        all_.erase(all_.begin() + i);
+        break;
+      }
+  }
+  free_.clear();
+}
+
+// ----------------------------------------------------------------------------
+LsmDictionary::LsmDictionary(const DictConfig &config)
+    : cfg_(config), pool_(config.rows_per_bucket_log2 ? config.rows_per_bucket_log2 : 3u) {
+  batch_capacity_ = std::min<uint64_t>(kMaxBatch, std::max<uint64_t>(1, config.batch_capacity
+                                                                             ? config.batch_capacity
+                                                                             : kMaxBatch));
+  fan_in_ = config.fan_in ? config.fan_in : 4u;
+  if (fan_in_ < 2 || fan_in_ > 16) throw std::invalid_argument("fan_in must be in [2, 16]");
+  rows_log2_ = config.rows_per_bucket_log2 ? config.rows_per_bucket_log2 : 3u;
+  if (rows_log2_ > 16) throw std::invalid_argument("rows_per_bucket_log2 must be <= 16");
+  if (config.search_mode > 1) throw std::invalid_argument("unknown search_mode");
+  // publication capacity as in initial_storage_capacity (GPULSMOpt.cuh:255-263)
+  budget_ = std::max<uint64_t>(config.max_elements, batch_capacity_ * 16u);
+  if (budget_ > 0xffffffffull)
+    throw std::invalid_argument("capacity exceeds 32-bit key space");
+  uint64_t cap = config.level_zero_capacity ? config.level_zero_capacity : batch_capacity_ * fan_in_;
+  cap = std::min(cap, budget_);
+  while (cap < budget_) {
+    caps_.push_back(cap);
+    cap = cap > budget_ / fan_in_ ? budget_ : cap * fan_in_;
+    if (caps_.size() >= size_t(lsm::kMaxLevels) - 1)
+      throw std::invalid_argument("level schedule exceeds 16 levels; raise level_zero_capacity");
+  }
+  caps_.push_back(budget_);
+  levels_.assign(caps_.size(), Level{});
+  receipt_gens_.assign(caps_.size(), 0);
+
+  int dev = 0;
+  GPULSM_CUDA(cudaGetDevice(&dev));
+  GPULSM_CUDA(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, dev));
+  GPULSM_CUDA(cudaMalloc(&dev_status_, 256));
+  GPULSM_CUDA(cudaMemset(dev_status_, 0, 256));
+  GPULSM_CUDA(cudaMalloc(&receipt_dev_, sizeof(Receipt)));
+  GPULSM_CUDA(cudaMallocHost(&receipt_host_, sizeof(Receipt)));
+  std::memset(receipt_host_, 0, sizeof(Receipt));
+  GPULSM_CUDA(cudaEventCreateWithFlags(&op_done_, cudaEventDisableTiming));
+  GPULSM_CUDA(cudaEventCreateWithFlags(&receipt_event_, cudaEventDisableTiming));
+  GPULSM_CUDA(cudaEventRecord(op_done_, 0));
+}
+
+LsmDictionary::~LsmDictionary() {
+  if (op_done_) cudaEventSynchronize(op_done_);
+  cudaDeviceSynchronize();
+  for (auto &w : words_)
+    if (w) cudaFree(w);
+  if (scratch_) cudaFree(scratch_);
+  if (dev_status_) cudaFree(dev_status_);
+  if (receipt_dev_) cudaFree(receipt_dev_);
+  if (receipt_host_) cudaFreeHost(receipt_host_);
+  if (op_done_) cudaEventDestroy(op_done_);
+  if (receipt_event_) cudaEventDestroy(receipt_event_);
+}
+
+void LsmDictionary::begin_op(cudaStream_t s) { GPULSM_CUDA(cudaStreamWaitEvent(s, op_done_, 0)); }
+
+void LsmDictionary::end_op(cudaStream_t s) { GPULSM_CUDA(cudaEventRecord(op_done_, s)); }
+
+void *LsmDictionary::scratch(size_t bytes, cudaStream_t s) {
+  bytes = align_up(std::max<size_t>(bytes, kAlign));
+  if (bytes > scratch_bytes_) {
+    if (scratch_) GPULSM_CUDA(cudaFreeAsync(scratch_, s));
+    size_t grow = std::max(bytes, scratch_bytes_ * 2);
+    if (cudaMallocAsync(&scratch_, grow, s) != cudaSuccess) {
+      (void)cudaGetLastError();
+      scratch_ = nullptr;
+      scratch_bytes_ = 0;
+      throw std::bad_alloc();
+    }
+    scratch_bytes_ = grow;
+  }
+  return scratch_;
+}
+
+void LsmDictionary::ensure_sort_space(uint64_t n, cudaStream_t s) {
+  if (n <= words_cap_) return;
+  for (auto &w : words_) {
+    if (w) GPULSM_CUDA(cudaFreeAsync(w, s));
+    w = nullptr;
+  }
+  uint64_t cap = std::max<uint64_t>(n, batch_capacity_);
+  for (auto &w : words_)
+    if (cudaMallocAsync(&w, cap * 8, s) != cudaSuccess) {
+      (void)cudaGetLastError();
+      words_cap_ = 0;
+      throw std::bad_alloc();
+    }
+  words_cap_ = cap;
+}
+
+void LsmDictionary::post_receipt(cudaStream_t s) {
+  ReceiptSrc src{};
+  src.count = uint32_t(levels_.size());
+  for (size_t i = 0; i < levels_.size(); ++i) {
+    src.desc[i] = levels_[i].run ? levels_[i].run->desc : nullptr;
+    receipt_gens_[i] = levels_[i].gen;
+  }
+  src.status = dev_status_;
+  src.out = static_cast<unsigned long long *>(receipt_dev_);
+  receipt_kernel<<<1, 32, 0, s>>>(src);
+  GPULSM_CUDA(cudaGetLastError());
+  GPULSM_CUDA(cudaMemcpyAsync(receipt_host_, receipt_dev_, sizeof(Receipt), cudaMemcpyDeviceToHost, s));
+  GPULSM_CUDA(cudaEventRecord(receipt_event_, s));
+  receipt_pending_ = true;
+}
+
+void LsmDictionary::apply_receipt(bool wait) {
+  if (!receipt_pending_) return;
+  if (wait) {
+    GPULSM_CUDA(cudaEventSynchronize(receipt_event_));
+  } else {
+    const cudaError_t q = cudaEventQuery(receipt_event_);
+    if (q == cudaErrorNotReady) return;
+    GPULSM_CUDA(q);
+  }
+  receipt_pending_ = false;
+  const Receipt r = *receipt_host_;
+  status_bits_ |= uint32_t(r.status);
+  bool current = true;
+  uint64_t total = 0;
+  for (size_t i = 0; i < levels_.size(); ++i) {
+    if (!levels_[i].run) continue;
+    if (levels_[i].gen == receipt_gens_[i]) {
+      levels_[i].upper = r.n[i];
+    } else {
+      current = false;
+    }
+    total += levels_[i].upper;
+  }
+  if ((r.status & kDevWaitTimeout) && !failed_) {
+    failed_ = true;
+    failure_ = "GPU dictionary publication failed: a bounded device wait timed out";
+  }
+  if ((r.status & kDevOutputOverflow) || (current && total > budget_)) {
+    status_bits_ |= kDevOutputOverflow;
+    if (!failed_) {
+      failed_ = true;
+      failure_ = "GPU dictionary capacity exhausted: " + std::to_string(total) +
+                 " resident rows > capacity " + std::to_string(budget_) +
+                 "; accepted updates were preserved";
+    }
+  }
+}
+
+void LsmDictionary::reject_if_failed() const {
+  if (failed_) throw std::runtime_error(failure_);
+}
+
+void LsmDictionary::release_levels(cudaStream_t) {
+  for (auto &l : levels_) {
+    pool_.release(l.run);
+    l = Level{};
+    l.gen = next_gen_++;
+  }
+}
+
+// ----------------------------------------------------------------------------
+RunBuffer *LsmDictionary::sort_dedup(const uint32_t *keys, const uint32_t *values, uint64_t n,
+                                     bool tombstone, cudaStream_t s) {
+  ensure_sort_space(n, s);
+  const uint32_t nn = uint32_t(n);
+  const size_t radix_bytes = align_up(radix::workspace_bytes(n, 4));
+  const uint64_t dtiles = (n + lsm::kCompactTile - 1) / lsm::kCompactTile;
+  const size_t total = radix_bytes + align_up(8) + align_up((dtiles + 1) * 8);
+  Bump bump{static_cast<char *>(scratch(total, s))};
+  GPULSM_CUDA(cudaMemsetAsync(bump.p, 0, total, s));
+  uint32_t *ws = bump.take<uint32_t>(radix_bytes / 4);
+  uint32_t *counter = bump.take<uint32_t>(2);
+  unsigned long long *lb = bump.take<unsigned long long>(dtiles + 1);
+  const unsigned hist_blocks = std::min<unsigned>(grid_for(n, 4096), unsigned(num_sms_) * 4u);
+  lsm::pack_histogram_kernel<<<hist_blocks, 256, 0, s>>>(keys, tombstone ? nullptr : values, nn,
+                                                          words_[0], ws);
+  unsigned long long *bufs[2] = {words_[0], words_[1]};
+  const int cur = radix::run_passes<unsigned long long, false>(bufs, nullptr, nn, 32, 64, ws,
+                                                               dev_status_, s);
+  RunBuffer *carry = pool_.acquire(n, s);
+  lsm::dedup_last_kernel<<<unsigned(dtiles), lsm::kCompactThreads, 0, s>>>(
+      bufs[cur], nn, tombstone ? 1 : 0, carry->keys, carry->vals, carry->flags, carry->desc, lb,
+      counter, dev_status_);
+  GPULSM_CUDA(cudaGetLastError());
+  return carry;
+}
+
+RunBuffer *LsmDictionary::merge(RunBuffer *newer, RunBuffer *older, uint64_t out_upper,
+                                bool drop_tombstones, cudaStream_t s) {
+  RunBuffer *out = pool_.acquire(out_upper, s);
+  const uint64_t tiles = (out_upper + lsm::kMergeTile - 1) / lsm::kMergeTile;
+  const size_t bytes = merge_scratch_bytes(out_upper);
+  Bump bump{static_cast<char *>(scratch(bytes, s))};
+  GPULSM_CUDA(cudaMemsetAsync(bump.p, 0, bytes, s));
+  uint32_t *counter = bump.take<uint32_t>(2);
+  unsigned long long *lb = bump.take<unsigned long long>(tiles + 1);
+  lsm::merge_kernel<<<unsigned(std::max<uint64_t>(tiles, 1)), lsm::kMergeThreads, 0, s>>>(
+      newer->keys, newer->vals, newer->flags, newer->desc, older->keys, older->vals, older->flags,
+      older->desc, out->keys, out->vals, out->flags, out->desc, out->cap, drop_tombstones ? 1 : 0,
+      lb, counter, dev_status_);
+  GPULSM_CUDA(cudaGetLastError());
+  pool_.release(newer);
+  pool_.release(older);
+  return out;
+}
+
+void LsmDictionary::build_directory(RunBuffer *run, uint64_t upper, cudaStream_t s) {
+  lsm::directory_kernel<<<grid_for(std::max<uint64_t>(upper, 1), 256), 256, 0, s>>>(
+      run->keys, run->desc, run->dir, run->dir_bits, rows_log2_);
+  GPULSM_CUDA(cudaGetLastError());
+}
+
+void LsmDictionary::cascade(RunBuffer *carry, uint64_t carry_upper, cudaStream_t s) {
+  const size_t L = levels_.size();
+  size_t dest = 0;
+  uint64_t acc = carry_upper;
+  for (size_t j = 0; j < L; ++j) {
+    dest = j;
+    if (!levels_[j].run) break;
+    if (j == L - 1 || acc + levels_[j].upper <= caps_[j]) break;
+    acc += levels_[j].upper;
+  }
+  const bool dest_occupied = levels_[dest].run != nullptr;
+  bool deeper = false;
+  for (size_t j = dest + 1; j < L; ++j) deeper |= levels_[j].run != nullptr;
+  RunBuffer *x = carry;
+  uint64_t xu = carry_upper;
+  for (size_t i = 0; i < dest; ++i) {
+    const bool last = (i + 1 == dest) && !dest_occupied;
+    const uint64_t ou = xu + levels_[i].upper;
+    x = merge(x, levels_[i].run, ou, last && !deeper, s);
+    xu = ou;
+    levels_[i] = Level{};
+    levels_[i].gen = next_gen_++;
+  }
+  if (dest_occupied) {
+    const uint64_t ou = xu + levels_[dest].upper;
+    x = merge(x, levels_[dest].run, ou, !deeper, s);
+    xu = ou;
+  }
+  levels_[dest].run = x;
+  levels_[dest].upper = std::min<uint64_t>(xu, x->cap);
+  levels_[dest].gen = next_gen_++;
+  build_directory(x, levels_[dest].upper, s);
+}
+
+void LsmDictionary::admit(const uint32_t *keys, const uint32_t *values, uint64_t n, bool tombstone,
+                          cudaStream_t s) {
+  for (uint64_t off = 0; off < n; off += batch_capacity_) {
+    const uint64_t m = std::min(batch_capacity_, n - off);
+    uint64_t total_upper = m;
+    for (auto &l : levels_) total_upper += l.upper;
+    if (total_upper > 2 * budget_ + batch_capacity_ && receipt_pending_) {
+      // stale bounds: wait for the exact counts before planning more storage
+      apply_receipt(true);
+      reject_if_failed();
+    }
+    RunBuffer *carry = sort_dedup(keys + off, values ? values + off : nullptr, m, tombstone, s);
+    cascade(carry, m, s);
+  }
+}
+
+// ----------------------------------------------------------------------------
+void LsmDictionary::clear(cudaStream_t s) {
+  std::lock_guard<std::mutex> g(mu_);
+  begin_op(s);
+  release_levels(s);
+  GPULSM_CUDA(cudaMemsetAsync(dev_status_, 0, 4, s));
+  status_bits_ = 0;
+  failed_ = false;
+  failure_.clear();
+  receipt_pending_ = false;
+  end_op(s);
+}
+
+void LsmDictionary::bulk_build(const uint32_t *keys, const uint32_t *values, uint64_t n,
+                               cudaStream_t s) {
+  std::lock_guard<std::mutex> g(mu_);
+  if ((n && (!keys || !values)) || n > 0xffffffffull)
+    throw std::invalid_argument("invalid GPU dictionary initial input");
+  if (n > radix::kMaxKeys) throw std::length_error("bulk build limited to 2^30-1 keys per call");
+  begin_op(s);
+  release_levels(s);
+  GPULSM_CUDA(cudaMemsetAsync(dev_status_, 0, 4, s));
+  status_bits_ = 0;
+  failed_ = false;
+  failure_.clear();
+  receipt_pending_ = false;
+  if (n) {
+    RunBuffer *run = sort_dedup(keys, values, n, false, s);
+    Level &top = levels_.back();
+    top.run = run;
+    top.upper = n;
+    top.gen = next_gen_++;
+    build_directory(run, n, s);
+    post_receipt(s);
+  }
+  end_op(s);
+}
+
+void LsmDictionary::insert(const uint32_t *keys, const uint32_t *values, uint64_t n,
+                           cudaStream_t s) {
+  std::lock_guard<std::mutex> g(mu_);
+  if (!n) return;
+  if (!keys || !values) throw std::invalid_argument("invalid GPU dictionary update batch");
+  apply_receipt(false);
+  reject_if_failed();
+  begin_op(s);
+  admit(keys, values, n, false, s);
+  post_receipt(s);
+  end_op(s);
+}
+
+void LsmDictionary::erase(const uint32_t *keys, uint64_t n, cudaStream_t s) {
+  std::lock_guard<std::mutex> g(mu_);
+  if (!n) return;
+  if (!keys) throw std::invalid_argument("invalid GPU dictionary update batch");
+  apply_receipt(false);
+  reject_if_failed();
+  begin_op(s);
+  admit(keys, nullptr, n, true, s);
+  post_receipt(s);
+  end_op(s);
+}
+
+void LsmDictionary::level_set(void *out) const {
+  auto *set = static_cast<lsm::LevelSet *>(out);
+  set->count = 0;
+  for (const auto &l : levels_) {
+    if (!l.run) continue;
+    lsm::LevelView &v = set->lv[set->count++];
+    v.keys = l.run->keys;
+    v.vals = l.run->vals;
+    v.flags = l.run->flags;
+    v.dir = l.run->dir;
+    v.desc = l.run->desc;
+  }
+}
+
+void LsmDictionary::lookup(const uint32_t *queries, uint64_t n, uint32_t *out_values,
+                           uint8_t *out_found, cudaStream_t s) {
+  std::lock_guard<std::mutex> g(mu_);
+  if (!n) return;
+  if (!queries || !out_values) throw std::invalid_argument("invalid GPU dictionary lookup");
+  apply_receipt(false);
+  begin_op(s);
+  lsm::LevelSet set;
+  level_set(&set);
+  lsm::lookup_kernel<<<grid_for(n, 256), 256, 0, s>>>(set, queries, n, out_values, out_found);
+  GPULSM_CUDA(cudaGetLastError());
+  end_op(s);
+}
+
+void LsmDictionary::range_sum(const uint32_t *lo, const uint32_t *hi, uint64_t n, uint32_t *out,
+                              cudaStream_t s) {
+  std::lock_guard<std::mutex> g(mu_);
+  if (!n) return;
+  if (!lo || !hi || !out) throw std::invalid_argument("invalid GPU dictionary range");
+  apply_receipt(false);
+  begin_op(s);
+  lsm::LevelSet set;
+  level_set(&set);
+  lsm::range_kernel<0><<<grid_for(n, 256), 256, 0, s>>>(set, lo, hi, n, out, nullptr, nullptr,
+                                                       nullptr);
+  GPULSM_CUDA(cudaGetLastError());
+  end_op(s);
+}
+
+void LsmDictionary::range_count(const uint32_t *lo, const uint32_t *hi, uint64_t n, uint32_t *out,
+                                cudaStream_t s) {
+  std::lock_guard<std::mutex> g(mu_);
+  if (!n) return;
+  if (!lo || !hi || !out) throw std::invalid_argument("invalid GPU dictionary range");
+  apply_receipt(false);
+  begin_op(s);
+  lsm::LevelSet set;
+  level_set(&set);
+  lsm::range_kernel<1><<<grid_for(n, 256), 256, 0, s>>>(set, lo, hi, n, out, nullptr, nullptr,
+                                                       nullptr);
+  GPULSM_CUDA(cudaGetLastError());
+  end_op(s);
+}
+
+void LsmDictionary::range_offsets(const uint32_t *lo, const uint32_t *hi, uint64_t n,
+                                  uint64_t *offsets, cudaStream_t s) {
+  std::lock_guard<std::mutex> g(mu_);
+  if (!offsets) throw std::invalid_argument("invalid GPU dictionary range");
+  if (n && (!lo || !hi)) throw std::invalid_argument("invalid GPU dictionary range");
+  apply_receipt(false);
+  begin_op(s);
+  const uint32_t tiles = lsm::scan_tiles(n);
+  const size_t count_bytes = align_up(std::max<uint64_t>(n, 1) * 4);
+  const size_t bytes = count_bytes + align_up(8) + align_up(size_t(tiles + 1) * 8);
+  Bump bump{static_cast<char *>(scratch(bytes, s))};
+  uint32_t *counts = bump.take<uint32_t>(count_bytes / 4);
+  GPULSM_CUDA(cudaMemsetAsync(bump.p + count_bytes, 0, bytes - count_bytes, s));
+  uint32_t *counter = bump.take<uint32_t>(2);
+  unsigned long long *lb = bump.take<unsigned long long>(tiles + 1);
+  if (n) {
+    lsm::LevelSet set;
+    level_set(&set);
+    lsm::range_kernel<1><<<grid_for(n, 256), 256, 0, s>>>(set, lo, hi, n, counts, nullptr, nullptr,
+                                                         nullptr);
+  }
+  lsm::scan_counts_kernel<<<tiles, lsm::kScanThreads, 0, s>>>(
+      counts, n, reinterpret_cast<unsigned long long *>(offsets), lb, counter, dev_status_);
+  GPULSM_CUDA(cudaGetLastError());
+  end_op(s);
+}
+
+void LsmDictionary::range_pairs(const uint32_t *lo, const uint32_t *hi, uint64_t n,
+                                const uint64_t *offsets, uint32_t *out_keys, uint32_t *out_values,
+                                cudaStream_t s) {
+  std::lock_guard<std::mutex> g(mu_);
+  if (!n) return;
+  if (!lo || !hi || !offsets || !out_keys || !out_values)
+    throw std::invalid_argument("invalid GPU dictionary range");
+  apply_receipt(false);
+  begin_op(s);
+  lsm::LevelSet set;
+  level_set(&set);
+  lsm::range_kernel<2><<<grid_for(n, 256), 256, 0, s>>>(
+      set, lo, hi, n, nullptr, reinterpret_cast<const unsigned long long *>(offsets), out_keys,
+      out_values);
+  GPULSM_CUDA(cudaGetLastError());
+  end_op(s);
+}
+
+void LsmDictionary::successor(const uint32_t *queries, uint64_t n, uint32_t *out_keys,
+                              cudaStream_t s) {
+  std::lock_guard<std::mutex> g(mu_);
+  if (!n) return;
+  if (!queries || !out_keys) throw std::invalid_argument("invalid GPU dictionary successor");
+  apply_receipt(false);
+  begin_op(s);
+  lsm::LevelSet set;
+  level_set(&set);
+  lsm::successor_kernel<<<grid_for(n, 256), 256, 0, s>>>(set, queries, n, out_keys);
+  GPULSM_CUDA(cudaGetLastError());
+  end_op(s);
+}
+
+uint32_t LsmDictionary::status() {
+  std::lock_guard<std::mutex> g(mu_);
+  GPULSM_CUDA(cudaEventSynchronize(op_done_));
+  apply_receipt(true);
+  uint32_t bits = 0;
+  GPULSM_CUDA(cudaMemcpy(&bits, dev_status_, 4, cudaMemcpyDeviceToHost));
+  status_bits_ |= bits;
+  return status_bits_;
+}
+
+uint64_t LsmDictionary::resident_bytes() {
+  std::lock_guard<std::mutex> g(mu_);
+  return pool_.bytes() + words_cap_ * 16 + scratch_bytes_ + sizeof(Receipt) + 256;
+}
+
+void LsmDictionary::size(uint64_t *rows, uint32_t *levels) {
+  std::lock_guard<std::mutex> g(mu_);
+  GPULSM_CUDA(cudaEventSynchronize(op_done_));
+  uint64_t total = 0;
+  uint32_t count = 0;
+  for (auto &l : levels_) {
+    if (!l.run) continue;
+    unsigned long long n = 0;
+    GPULSM_CUDA(cudaMemcpy(&n, &l.run->desc->n, 8, cudaMemcpyDeviceToHost));
+    total += n;
+    ++count;
+  }
+  if (rows) *rows = total;
+  if (levels) *levels = count;
+}
+
+}  // namespace gpulsm

@@ -1,0 +1,147 @@
+// Host engine of the LSM dictionary: the B200 counterpart of class GPULSMOpt
+// (GPULSMOpt.cuh:5599-5881).  Same public operations and semantics; a
+// different structure underneath (sorted levels with radix directories,
+// merge-path merges, lazily applied receipts instead of epochs).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+namespace gpulsm {
+
+namespace lsm {
+struct LevelDesc;
+}
+
+struct DictConfig {
+  uint64_t max_elements = 0;
+  uint64_t batch_capacity = 0;
+  uint64_t level_zero_capacity = 0;
+  uint32_t fan_in = 0;
+  uint32_t rows_per_bucket_log2 = 0;
+  uint32_t search_mode = 0;
+};
+
+// Storage of one sorted run (keys, vals, flags, directory, descriptor).
+struct RunBuffer {
+  uint64_t cap = 0;        // rows
+  uint32_t dir_bits = 0;   // directory holds up to 2^dir_bits buckets
+  uint32_t *keys = nullptr;
+  uint32_t *vals = nullptr;
+  uint8_t *flags = nullptr;
+  uint32_t *dir = nullptr;
+  lsm::LevelDesc *desc = nullptr;
+  void *block = nullptr;   // single device allocation backing all streams
+  size_t bytes = 0;
+};
+
+class RunPool {
+ public:
+  explicit RunPool(uint32_t rows_log2) : rows_log2_(rows_log2) {}
+  ~RunPool();
+  RunBuffer *acquire(uint64_t min_rows, cudaStream_t stream);
+  void release(RunBuffer *b);
+  void release_all_free(cudaStream_t stream);
+  size_t bytes() const { return bytes_; }
+
+ private:
+  uint32_t rows_log2_;
+  std::vector<std::unique_ptr<RunBuffer>> all_;
+  std::vector<RunBuffer *> free_;
+  size_t bytes_ = 0;
+};
+
+class LsmDictionary {
+ public:
+  explicit LsmDictionary(const DictConfig &config);
+  ~LsmDictionary();
+  LsmDictionary(const LsmDictionary &) = delete;
+  LsmDictionary &operator=(const LsmDictionary &) = delete;
+
+  void clear(cudaStream_t s);
+  void bulk_build(const uint32_t *keys, const uint32_t *values, uint64_t n, cudaStream_t s);
+  void insert(const uint32_t *keys, const uint32_t *values, uint64_t n, cudaStream_t s);
+  void erase(const uint32_t *keys, uint64_t n, cudaStream_t s);
+  void lookup(const uint32_t *queries, uint64_t n, uint32_t *out_values, uint8_t *out_found,
+              cudaStream_t s);
+  void range_sum(const uint32_t *lo, const uint32_t *hi, uint64_t n, uint32_t *out, cudaStream_t s);
+  void range_count(const uint32_t *lo, const uint32_t *hi, uint64_t n, uint32_t *out,
+                   cudaStream_t s);
+  void range_offsets(const uint32_t *lo, const uint32_t *hi, uint64_t n, uint64_t *offsets,
+                     cudaStream_t s);
+  void range_pairs(const uint32_t *lo, const uint32_t *hi, uint64_t n, const uint64_t *offsets,
+                   uint32_t *out_keys, uint32_t *out_values, cudaStream_t s);
+  void successor(const uint32_t *queries, uint64_t n, uint32_t *out_keys, cudaStream_t s);
+  uint32_t status();
+  uint64_t resident_bytes();
+  void size(uint64_t *rows, uint32_t *levels);
+
+  // Introspection for tests and benchmarks.
+  uint32_t level_count() const { return uint32_t(caps_.size()); }
+  uint64_t level_capacity(uint32_t i) const { return caps_[i]; }
+
+ private:
+  struct Level {
+    RunBuffer *run = nullptr;
+    uint64_t upper = 0;  // upper bound of the row count known on the host
+    uint64_t gen = 0;    // bumps whenever the level changes
+  };
+  struct Receipt;
+
+  void begin_op(cudaStream_t s);
+  void end_op(cudaStream_t s);
+  void apply_receipt(bool wait);
+  void post_receipt(cudaStream_t s);
+  void reject_if_failed() const;
+  void admit(const uint32_t *keys, const uint32_t *values, uint64_t n, bool tombstone,
+             cudaStream_t s);
+  RunBuffer *sort_dedup(const uint32_t *keys, const uint32_t *values, uint64_t n, bool tombstone,
+                        cudaStream_t s);
+  void cascade(RunBuffer *carry, uint64_t carry_upper, cudaStream_t s);
+  RunBuffer *merge(RunBuffer *newer, RunBuffer *older, uint64_t out_upper, bool drop_tombstones,
+                   cudaStream_t s);
+  void build_directory(RunBuffer *run, uint64_t upper, cudaStream_t s);
+  void release_levels(cudaStream_t s);
+  void *scratch(size_t bytes, cudaStream_t s);
+  void ensure_sort_space(uint64_t n, cudaStream_t s);
+  struct LevelSetHost;
+  void level_set(void *out) const;
+
+  DictConfig cfg_;
+  uint64_t batch_capacity_ = 0;
+  uint64_t budget_ = 0;
+  uint32_t fan_in_ = 4;
+  uint32_t rows_log2_ = 3;
+  int num_sms_ = 148;
+  std::vector<uint64_t> caps_;
+  std::vector<Level> levels_;
+  RunPool pool_;
+  uint64_t next_gen_ = 1;
+
+  // sort space for admission: two u64 word buffers + radix workspace
+  unsigned long long *words_[2] = {nullptr, nullptr};
+  uint64_t words_cap_ = 0;
+  void *scratch_ = nullptr;
+  size_t scratch_bytes_ = 0;
+  uint32_t *dev_status_ = nullptr;
+
+  // receipts (pinned host copy of the level row counts and status)
+  Receipt *receipt_host_ = nullptr;
+  void *receipt_dev_ = nullptr;
+  cudaEvent_t receipt_event_ = nullptr;
+  bool receipt_pending_ = false;
+  std::vector<uint64_t> receipt_gens_;
+
+  uint32_t status_bits_ = 0;
+  bool failed_ = false;
+  std::string failure_;
+  cudaEvent_t op_done_ = nullptr;
+  mutable std::mutex mu_;
+};
+
+}  // namespace gpulsm

@@ -1,0 +1,555 @@
+// Kernels of the LSM dictionary (GPULSMOpt semantics, u32 keys / u32 values).
+//
+// HBM layout of one level (a sorted run of unique keys, newest version only):
+//   keys   u32[n]   sorted ascending
+//   vals   u32[n]   value, or 0xffffffff for a tombstone
+//   flags  u8[n]    bit 0 = tombstone (read only when the value is 0xffffffff)
+//   dir    u32[nbuckets+1]  radix directory: dir[b] = first row whose
+//          (key - kmin) >> shift >= b, so bucket b spans [dir[b], dir[b+1]).
+//   desc   LevelDesc {n, kmin, kmax, shift, nbuckets} written on the device.
+// Levels are ordered newest (index 0) to oldest; the first level holding a key
+// decides its visible version (the reference's lower level id = newer rule,
+// GPULSMOpt.cuh:4714-4750).
+#pragma once
+
+#include "common.cuh"
+
+namespace gpulsm {
+namespace lsm {
+
+constexpr int kMaxLevels = 16;
+constexpr uint32_t kTombValue = 0xffffffffu;
+constexpr uint8_t kFlagTomb = 1u;
+
+struct LevelDesc {
+  unsigned long long n;
+  uint32_t kmin, kmax, shift, nbuckets;
+  uint32_t pad[2];
+};
+static_assert(sizeof(LevelDesc) == 32, "LevelDesc layout");
+
+struct LevelView {
+  const uint32_t *keys;
+  const uint32_t *vals;
+  const uint8_t *flags;
+  const uint32_t *dir;
+  const LevelDesc *desc;
+};
+
+struct LevelSet {
+  LevelView lv[kMaxLevels];
+  uint32_t count;
+};
+
+// ---------------------------------------------------------------------------
+// single-value decoupled look-back over tiles (u64 counts, 62-bit)
+constexpr unsigned long long kLbAgg = 1ull << 62;
+constexpr unsigned long long kLbInc = 2ull << 62;
+constexpr unsigned long long kLbMask = (1ull << 62) - 1ull;
+
+__device__ __forceinline__ unsigned long long tile_lookback(unsigned long long *lb, uint32_t tile,
+                                                            unsigned long long agg,
+                                                            uint32_t *status) {
+  if (tile == 0) {
+    st_relaxed_u64(lb, kLbInc | agg);
+    return 0ull;
+  }
+  st_relaxed_u64(lb + tile, kLbAgg | agg);
+  unsigned long long excl = 0;
+  int64_t t = int64_t(tile) - 1;
+  uint32_t spins = 0;
+  while (t >= 0) {
+    const unsigned long long v = ld_relaxed_u64(lb + t);
+    const unsigned long long flag = v & ~kLbMask;
+    if (flag == 0ull) {
+      if (++spins > kMaxSpins) {
+        atomicOr(status, kDevWaitTimeout);
+        break;
+      }
+      continue;
+    }
+    excl += v & kLbMask;
+    if (flag == kLbInc) break;
+    --t;
+  }
+  st_relaxed_u64(lb + tile, kLbInc | (excl + agg));
+  return excl;
+}
+
+// ---------------------------------------------------------------------------
+// Admission: pack (key, value) into one u64 word (key in the high half so an
+// LSD sort on bits 32..63 orders by key and keeps input order among equal
+// keys) and count the key bytes of the four sort passes.
+__global__ void __launch_bounds__(256) pack_histogram_kernel(const uint32_t *__restrict__ keys,
+                                                             const uint32_t *__restrict__ vals,
+                                                             uint32_t n,
+                                                             unsigned long long *__restrict__ words,
+                                                             uint32_t *__restrict__ hist) {
+  __shared__ uint32_t s[4][256];
+  for (uint32_t i = threadIdx.x; i < 4 * 256; i += 256) (&s[0][0])[i] = 0;
+  __syncthreads();
+  for (uint32_t i = blockIdx.x * 256 + threadIdx.x; i < n; i += gridDim.x * 256) {
+    const uint32_t k = keys[i];
+    const uint32_t v = vals ? vals[i] : kTombValue;
+    words[i] = (static_cast<unsigned long long>(k) << 32) | v;
+    atomicAdd(&s[0][k & 0xffu], 1u);
+    atomicAdd(&s[1][(k >> 8) & 0xffu], 1u);
+    atomicAdd(&s[2][(k >> 16) & 0xffu], 1u);
+    atomicAdd(&s[3][k >> 24], 1u);
+  }
+  __syncthreads();
+  for (int p = 0; p < 4; ++p) {
+    const uint32_t c = s[p][threadIdx.x];
+    if (c) atomicAdd(&hist[p * 256 + threadIdx.x], c);
+  }
+}
+
+// Keep the LAST word of every equal-key run of a stably sorted batch (the
+// highest input index wins, GPULSMOpt.cuh:2578-2598 ages + :2633 keep-last)
+// and split it into a level (keys, vals, flags).  Single pass: tile counts are
+// chained by decoupled look-back.
+constexpr int kCompactThreads = 256;
+constexpr int kCompactItems = 8;
+constexpr uint32_t kCompactTile = kCompactThreads * kCompactItems;
+
+__global__ void __launch_bounds__(kCompactThreads) dedup_last_kernel(
+    const unsigned long long *__restrict__ words, uint32_t n, int tombstone,
+    uint32_t *__restrict__ out_keys, uint32_t *__restrict__ out_vals, uint8_t *__restrict__ out_flags,
+    LevelDesc *__restrict__ out_desc, unsigned long long *__restrict__ lb,
+    uint32_t *__restrict__ tile_counter, uint32_t *__restrict__ status) {
+  __shared__ unsigned long long s_words[kCompactTile + 1];
+  __shared__ uint32_t s_scan[kCompactThreads / 32];
+  __shared__ uint32_t s_total;
+  __shared__ uint32_t s_tile;
+  __shared__ unsigned long long s_base;
+  if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
+  __syncthreads();
+  const uint32_t tile = s_tile;
+  const uint32_t base = tile * kCompactTile;
+  const uint32_t count = base < n ? min(kCompactTile, n - base) : 0u;
+  for (uint32_t j = threadIdx.x; j <= count; j += kCompactThreads) {
+    const uint32_t g = base + j;
+    s_words[j] = g < n ? words[g] : ~0ull;  // one word past the tile decides keep-last
+  }
+  __syncthreads();
+  uint32_t keep_mask = 0, kept = 0;
+#pragma unroll
+  for (int i = 0; i < kCompactItems; ++i) {
+    const uint32_t j = threadIdx.x * kCompactItems + i;
+    if (j < count) {
+      const bool last = (base + j + 1 == n) || ((s_words[j] >> 32) != (s_words[j + 1] >> 32));
+      if (last) {
+        keep_mask |= 1u << i;
+        ++kept;
+      }
+    }
+  }
+  const uint32_t local = block_exclusive_scan<kCompactThreads>(kept, s_scan, &s_total);
+  const uint32_t tile_kept = s_total;
+  if (threadIdx.x == 0) s_base = tile_lookback(lb, tile, tile_kept, status);
+  // stage the kept words compactly (reuse the buffer after everyone has read it)
+  unsigned long long mine[kCompactItems];
+#pragma unroll
+  for (int i = 0; i < kCompactItems; ++i) mine[i] = s_words[threadIdx.x * kCompactItems + i];
+  __syncthreads();
+  uint32_t o = local;
+#pragma unroll
+  for (int i = 0; i < kCompactItems; ++i)
+    if (keep_mask & (1u << i)) s_words[o++] = mine[i];
+  __syncthreads();
+  const unsigned long long gbase = s_base;
+  for (uint32_t j = threadIdx.x; j < tile_kept; j += kCompactThreads) {
+    const unsigned long long w = s_words[j];
+    if (gbase + j >= n) break;  // only after a timed-out look-back (status bit set)
+    out_keys[gbase + j] = uint32_t(w >> 32);
+    out_vals[gbase + j] = tombstone ? kTombValue : uint32_t(w);
+    out_flags[gbase + j] = tombstone ? kFlagTomb : 0u;
+  }
+  if (base + kCompactTile >= n && threadIdx.x == 0) out_desc->n = gbase + tile_kept;
+}
+
+// ---------------------------------------------------------------------------
+// Merge of a newer run A into an older run B (both sorted, unique keys).
+// Merge-path tiles of kMergeTile outputs; ties put A first, so a B row whose
+// key was just taken from A is shadowed and dropped (newest level wins).  With
+// drop_tombstones (the output becomes the oldest level) tombstones disappear.
+constexpr int kMergeThreads = 256;
+constexpr int kMergeItems = 8;
+constexpr uint32_t kMergeTile = kMergeThreads * kMergeItems;
+
+__device__ __forceinline__ uint64_t merge_path(const uint32_t *a, uint64_t na, const uint32_t *b,
+                                               uint64_t nb, uint64_t diag) {
+  uint64_t lo = diag > nb ? diag - nb : 0, hi = diag < na ? diag : na;
+  while (lo < hi) {
+    const uint64_t mid = (lo + hi) >> 1;
+    if (a[mid] <= b[diag - 1 - mid]) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(kMergeThreads) merge_kernel(
+    const uint32_t *__restrict__ ak, const uint32_t *__restrict__ av, const uint8_t *__restrict__ af,
+    const LevelDesc *__restrict__ adesc, const uint32_t *__restrict__ bk,
+    const uint32_t *__restrict__ bv, const uint8_t *__restrict__ bf,
+    const LevelDesc *__restrict__ bdesc, uint32_t *__restrict__ ok, uint32_t *__restrict__ ov,
+    uint8_t *__restrict__ of, LevelDesc *__restrict__ odesc, unsigned long long out_capacity,
+    int drop_tombstones, unsigned long long *__restrict__ lb, uint32_t *__restrict__ tile_counter,
+    uint32_t *__restrict__ status) {
+  __shared__ uint32_t s_k[kMergeTile];
+  __shared__ uint32_t s_v[kMergeTile];
+  __shared__ uint8_t s_f[kMergeTile];
+  __shared__ uint32_t s_scan[kMergeThreads / 32];
+  __shared__ uint32_t s_total;
+  __shared__ uint32_t s_tile;
+  __shared__ unsigned long long s_a0, s_a1, s_base;
+  if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
+  __syncthreads();
+  const uint64_t na = adesc->n, nb = bdesc->n, total = na + nb;
+  const uint32_t tile = s_tile;
+  const uint64_t d0 = uint64_t(tile) * kMergeTile;
+  if (d0 >= total && !(tile == 0 && total == 0)) return;  // beyond the merged length
+  const uint64_t d1 = min(d0 + kMergeTile, total);
+  if (threadIdx.x == 0) s_a0 = merge_path(ak, na, bk, nb, d0);
+  if (threadIdx.x == 32) s_a1 = merge_path(ak, na, bk, nb, d1);
+  __syncthreads();
+  const uint64_t a0 = s_a0, a1 = s_a1, b0 = d0 - a0, b1 = d1 - a1;
+  const uint32_t alen = uint32_t(a1 - a0), blen = uint32_t(b1 - b0);
+  // stage A then B in shared memory
+  for (uint32_t j = threadIdx.x; j < alen; j += kMergeThreads) {
+    s_k[j] = ak[a0 + j];
+    s_v[j] = av[a0 + j];
+    s_f[j] = af[a0 + j];
+  }
+  for (uint32_t j = threadIdx.x; j < blen; j += kMergeThreads) {
+    s_k[alen + j] = bk[b0 + j];
+    s_v[alen + j] = bv[b0 + j];
+    s_f[alen + j] = bf[b0 + j];
+  }
+  // key of the A row just before this tile (shadows a leading B row)
+  const bool has_prev_a = a0 > 0;
+  const uint32_t prev_a_global = has_prev_a ? ak[a0 - 1] : 0u;
+  __syncthreads();
+  const uint32_t *sa = s_k, *sb = s_k + alen;
+  const uint32_t my_d = min(uint32_t(threadIdx.x) * kMergeItems, alen + blen);
+  const uint32_t my_e = min(my_d + kMergeItems, alen + blen);
+  uint32_t ai = uint32_t(merge_path(sa, alen, sb, blen, my_d));
+  uint32_t bi = my_d - ai;
+  bool have_prev = ai > 0 ? true : has_prev_a;
+  uint32_t prev_a = ai > 0 ? sa[ai - 1] : prev_a_global;
+  uint32_t src[kMergeItems];  // smem index of each kept row
+  uint32_t kept = 0;
+  for (uint32_t d = my_d; d < my_e; ++d) {
+    const bool take_a = ai < alen && (bi >= blen || sa[ai] <= sb[bi]);
+    uint32_t idx, key;
+    bool keep;
+    if (take_a) {
+      idx = ai++;
+      key = sa[idx];
+      have_prev = true;
+      prev_a = key;
+      keep = true;
+    } else {
+      idx = alen + bi++;
+      key = sb[idx - alen];
+      keep = !(have_prev && prev_a == key);
+    }
+    if (keep && drop_tombstones && s_v[idx] == kTombValue && (s_f[idx] & kFlagTomb)) keep = false;
+    if (keep) src[kept++] = idx;
+  }
+  const uint32_t local = block_exclusive_scan<kMergeThreads>(kept, s_scan, &s_total);
+  const uint32_t tile_kept = s_total;
+  if (threadIdx.x == 0) s_base = tile_lookback(lb, tile, tile_kept, status);
+  uint32_t rk[kMergeItems], rv[kMergeItems];
+  uint8_t rf[kMergeItems];
+#pragma unroll
+  for (int i = 0; i < kMergeItems; ++i)
+    if (uint32_t(i) < kept) {
+      rk[i] = s_k[src[i]];
+      rv[i] = s_v[src[i]];
+      rf[i] = s_f[src[i]];
+    }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < kMergeItems; ++i)
+    if (uint32_t(i) < kept) {
+      s_k[local + i] = rk[i];
+      s_v[local + i] = rv[i];
+      s_f[local + i] = rf[i];
+    }
+  __syncthreads();
+  const unsigned long long gbase = s_base;
+  for (uint32_t j = threadIdx.x; j < tile_kept; j += kMergeThreads) {
+    const unsigned long long o = gbase + j;
+    if (o < out_capacity) {
+      ok[o] = s_k[j];
+      ov[o] = s_v[j];
+      of[o] = s_f[j];
+    }
+  }
+  if (d1 == total && threadIdx.x == 0) {
+    const unsigned long long n_out = gbase + tile_kept;
+    if (n_out > out_capacity) atomicOr(status, kDevOutputOverflow);
+    odesc->n = n_out < out_capacity ? n_out : out_capacity;
+  }
+}
+
+// Copy a run (used when a carry that still holds duplicates or tombstones must
+// be placed as is) - plain grid-stride copy of the three streams.
+__global__ void copy_run_kernel(const uint32_t *__restrict__ k, const uint32_t *__restrict__ v,
+                                const uint8_t *__restrict__ f, const LevelDesc *__restrict__ d,
+                                uint32_t *__restrict__ ok, uint32_t *__restrict__ ov,
+                                uint8_t *__restrict__ of, LevelDesc *__restrict__ od) {
+  const uint64_t n = d->n;
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += uint64_t(gridDim.x) * blockDim.x) {
+    ok[i] = k[i];
+    ov[i] = v[i];
+    of[i] = f[i];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) od->n = n;
+}
+
+// ---------------------------------------------------------------------------
+// Radix directory over the level's own key range [kmin, kmax]: about
+// 2^rows_log2 rows per bucket, at most 2^dir_bits buckets.
+__global__ void directory_kernel(const uint32_t *__restrict__ keys, LevelDesc *__restrict__ desc,
+                                 uint32_t *__restrict__ dir, uint32_t dir_bits, uint32_t rows_log2) {
+  const uint64_t n = desc->n;
+  const uint64_t p = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (n == 0) {
+    if (p == 0) {
+      desc->kmin = 1u;
+      desc->kmax = 0u;
+      desc->shift = 0u;
+      desc->nbuckets = 1u;
+      dir[0] = 0u;
+      dir[1] = 0u;
+    }
+    return;
+  }
+  const uint32_t kmin = keys[0], kmax = keys[n - 1];
+  const uint32_t range = kmax - kmin;
+  const uint32_t nl2 = ceil_log2_u64(n);
+  const uint32_t want = min(nl2 > rows_log2 ? nl2 - rows_log2 : 0u, dir_bits);
+  const uint32_t range_bits = range ? 32u - __clz(range) : 0u;
+  const uint32_t shift = range_bits > want ? range_bits - want : 0u;
+  const uint32_t nbuckets = (range >> shift) + 1u;
+  if (p == 0) {
+    desc->kmin = kmin;
+    desc->kmax = kmax;
+    desc->shift = shift;
+    desc->nbuckets = nbuckets;
+  }
+  if (p >= n) return;
+  const int64_t b = int64_t((keys[p] - kmin) >> shift);
+  const int64_t bp = p ? int64_t((keys[p - 1] - kmin) >> shift) : -1;
+  for (int64_t bb = bp + 1; bb <= b; ++bb) dir[bb] = uint32_t(p);
+  if (p == n - 1) dir[nbuckets] = uint32_t(n);
+}
+
+// ---------------------------------------------------------------------------
+// Search helpers over one level.
+__device__ __forceinline__ uint32_t bucket_lower_bound(const uint32_t *keys, uint32_t s, uint32_t e,
+                                                       uint32_t key) {
+  while (e - s > 8) {  // binary search down to a short window
+    const uint32_t mid = s + ((e - s) >> 1);
+    if (keys[mid] < key) s = mid + 1;
+    else e = mid;
+  }
+  while (s < e && keys[s] < key) ++s;
+  return s;
+}
+
+// First row with key >= x in the level (n when none).
+__device__ __forceinline__ uint64_t level_lower_bound(const LevelView &L, const LevelDesc &d,
+                                                      uint32_t x) {
+  if (d.n == 0 || x <= d.kmin) return 0;
+  if (x > d.kmax) return d.n;
+  const uint32_t b = (x - d.kmin) >> d.shift;
+  return bucket_lower_bound(L.keys, L.dir[b], L.dir[b + 1], x);
+}
+
+// First row with key > x.
+__device__ __forceinline__ uint64_t level_upper_bound(const LevelView &L, const LevelDesc &d,
+                                                      uint32_t x) {
+  if (d.n == 0 || x < d.kmin) return 0;
+  if (x >= d.kmax) return d.n;
+  return level_lower_bound(L, d, x + 1u);
+}
+
+__device__ __forceinline__ LevelDesc load_desc(const LevelDesc *p) {
+  LevelDesc d;
+  d.n = __ldg(&p->n);
+  d.kmin = __ldg(&p->kmin);
+  d.kmax = __ldg(&p->kmax);
+  d.shift = __ldg(&p->shift);
+  d.nbuckets = __ldg(&p->nbuckets);
+  return d;
+}
+
+__device__ __forceinline__ bool row_is_tomb(const LevelView &L, uint64_t p, uint32_t v) {
+  return v == kTombValue && (L.flags[p] & kFlagTomb);
+}
+
+// ---------------------------------------------------------------------------
+// Point lookup: newest level first; miss value follows GPULSMOpt.cuh:4742-4749.
+__global__ void __launch_bounds__(256) lookup_kernel(LevelSet set, const uint32_t *__restrict__ queries,
+                                                     uint64_t n, uint32_t *__restrict__ out_values,
+                                                     uint8_t *__restrict__ out_found) {
+  const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t q = queries[i];
+  const uint32_t miss = out_found ? 0u : kNotFound;
+  for (uint32_t l = 0; l < set.count; ++l) {
+    const LevelView &L = set.lv[l];
+    const LevelDesc d = load_desc(L.desc);
+    if (q < d.kmin || q > d.kmax) continue;
+    const uint32_t b = (q - d.kmin) >> d.shift;
+    const uint32_t s = L.dir[b], e = L.dir[b + 1];
+    const uint32_t p = bucket_lower_bound(L.keys, s, e, q);
+    if (p < e && L.keys[p] == q) {
+      const uint32_t v = L.vals[p];
+      const bool live = !row_is_tomb(L, p, v);
+      out_values[i] = live ? v : miss;
+      if (out_found) out_found[i] = live;
+      return;
+    }
+  }
+  out_values[i] = miss;
+  if (out_found) out_found[i] = 0u;
+}
+
+// ---------------------------------------------------------------------------
+// Range queries over the union of levels with newest-wins, one thread per
+// query (k-way cursor merge).  MODE 0: u32 sum (wraps like
+// GPULSMOpt.cuh:1520-1605), 1: live count, 2: emit (key, value) pairs at
+// offsets[q].
+template <int MODE>
+__global__ void __launch_bounds__(256) range_kernel(LevelSet set, const uint32_t *__restrict__ lo,
+                                                    const uint32_t *__restrict__ hi, uint64_t n,
+                                                    uint32_t *__restrict__ out_u32,
+                                                    const unsigned long long *__restrict__ offsets,
+                                                    uint32_t *__restrict__ out_keys,
+                                                    uint32_t *__restrict__ out_vals) {
+  const uint64_t q = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const uint32_t a = lo[q], z = hi[q];
+  unsigned long long acc = 0;
+  unsigned long long o = MODE == 2 ? offsets[q] : 0ull;
+  if (a <= z) {
+    uint64_t cur[kMaxLevels], end[kMaxLevels];
+    const uint32_t L = set.count;
+    for (uint32_t l = 0; l < L; ++l) {
+      const LevelDesc d = load_desc(set.lv[l].desc);
+      cur[l] = level_lower_bound(set.lv[l], d, a);
+      end[l] = level_upper_bound(set.lv[l], d, z);
+    }
+    while (true) {
+      uint32_t best = 0xffffffffu;
+      int owner = -1;
+      for (uint32_t l = 0; l < L; ++l)
+        if (cur[l] < end[l]) {
+          const uint32_t k = set.lv[l].keys[cur[l]];
+          if (owner < 0 || k < best) {
+            best = k;
+            owner = int(l);
+          }
+        }
+      if (owner < 0) break;
+      const uint32_t v = set.lv[owner].vals[cur[owner]];
+      const bool live = !row_is_tomb(set.lv[owner], cur[owner], v);
+      if (live) {
+        if (MODE == 0) acc += v;
+        else if (MODE == 1) ++acc;
+        else {
+          out_keys[o] = best;
+          out_vals[o] = v;
+          ++o;
+        }
+      }
+      for (uint32_t l = uint32_t(owner); l < L; ++l)
+        if (cur[l] < end[l] && set.lv[l].keys[cur[l]] == best) ++cur[l];
+    }
+  }
+  if (MODE != 2) out_u32[q] = uint32_t(acc);
+}
+
+// Successor: smallest live key >= query, else 0xffffffff (GPULSMOpt.cuh:5566-5594).
+__global__ void __launch_bounds__(256) successor_kernel(LevelSet set, const uint32_t *__restrict__ queries,
+                                                        uint64_t n, uint32_t *__restrict__ out_keys) {
+  const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t x = queries[i];
+  uint64_t cur[kMaxLevels], end[kMaxLevels];
+  const uint32_t L = set.count;
+  for (uint32_t l = 0; l < L; ++l) {
+    const LevelDesc d = load_desc(set.lv[l].desc);
+    cur[l] = level_lower_bound(set.lv[l], d, x);
+    end[l] = d.n;
+  }
+  uint32_t result = kNotFound;
+  while (true) {
+    uint32_t best = 0xffffffffu;
+    int owner = -1;
+    for (uint32_t l = 0; l < L; ++l)
+      if (cur[l] < end[l]) {
+        const uint32_t k = set.lv[l].keys[cur[l]];
+        if (owner < 0 || k < best) {
+          best = k;
+          owner = int(l);
+        }
+      }
+    if (owner < 0) break;
+    const uint32_t v = set.lv[owner].vals[cur[owner]];
+    if (!row_is_tomb(set.lv[owner], cur[owner], v)) {
+      result = best;
+      break;
+    }
+    for (uint32_t l = uint32_t(owner); l < L; ++l)
+      if (cur[l] < end[l] && set.lv[l].keys[cur[l]] == best) ++cur[l];
+  }
+  out_keys[i] = result;
+}
+
+// ---------------------------------------------------------------------------
+// Exclusive scan of u32 counts into u64 offsets (offsets[n] = total), single
+// pass with decoupled look-back.
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr uint32_t kScanTile = kScanThreads * kScanItems;
+
+__global__ void __launch_bounds__(kScanThreads) scan_counts_kernel(
+    const uint32_t *__restrict__ counts, uint64_t n, unsigned long long *__restrict__ offsets,
+    unsigned long long *__restrict__ lb, uint32_t *__restrict__ tile_counter,
+    uint32_t *__restrict__ status) {
+  __shared__ unsigned long long s_scan[kScanThreads / 32];
+  __shared__ unsigned long long s_total;
+  __shared__ uint32_t s_tile;
+  __shared__ unsigned long long s_base;
+  if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
+  __syncthreads();
+  const uint32_t tile = s_tile;
+  const uint64_t base = uint64_t(tile) * kScanTile + uint64_t(threadIdx.x) * kScanItems;
+  uint32_t c[kScanItems];
+  unsigned long long sum = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    c[i] = base + i < n ? counts[base + i] : 0u;
+    sum += c[i];
+  }
+  const unsigned long long local = block_exclusive_scan<kScanThreads>(sum, s_scan, &s_total);
+  if (threadIdx.x == 0) s_base = tile_lookback(lb, tile, s_total, status);
+  __syncthreads();
+  unsigned long long o = s_base + local;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    if (base + i <= n) offsets[base + i] = o;  // index n receives the total
+    o += c[i];
+  }
+}
+// Tiles needed so that index n (the total) is covered.
+inline uint32_t scan_tiles(uint64_t n) { return uint32_t(n / kScanTile + 1); }
+
+}  // namespace lsm
+}  // namespace gpulsm

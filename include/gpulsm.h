@@ -1,0 +1,171 @@
+/*
+ * gpulsm.h - C ABI of the B200-native GPU dictionary.
+ *
+ * Drop-in boundary for the GPU dictionary hot path of the reference project:
+ *   - gpulsm_dict_*  replaces class GPULSMOpt (GPULSMOpt.cuh:5599-5881) and
+ *                    its adapter structs (gpu_dictionary_adapter.cuh:16-49);
+ *   - gpulsm_flix_*  replaces the FliX bucket layer, class
+ *                    cg_rtx_index_updates (FliX/impl_cg_rtx_index_updates.cuh:1711-2677).
+ *
+ * Conventions (same as the reference):
+ *   - every key/value/output pointer is a DEVICE pointer owned by the caller;
+ *     the library never frees it;
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default
+ *     stream); calls enqueue work asynchronously and return;
+ *   - operations on one handle are serialised internally (a mutex plus an
+ *     event that orders work issued on different streams), as the reference
+ *     does with operation_mutex_ / operation_done_ (GPULSMOpt.cuh:6852-6858);
+ *   - every call returns a gpulsm_status; on failure gpulsm_last_error()
+ *     returns the message (the reference throws instead).
+ */
+#ifndef GPULSM_H
+#define GPULSM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum gpulsm_status {
+  GPULSM_OK = 0,
+  GPULSM_ERR_INVALID_ARGUMENT = 1, /* reference: std::invalid_argument */
+  GPULSM_ERR_CAPACITY = 2,         /* reference: runtime_error "...capacity exhausted..." */
+  GPULSM_ERR_PUBLICATION = 3,      /* reference: runtime_error "publication failed" */
+  GPULSM_ERR_TIMEOUT = 4,          /* a bounded device wait gave up (no reference equivalent) */
+  GPULSM_ERR_CUDA = 5,             /* reference: runtime_error from CUDA_CHECK */
+  GPULSM_ERR_OUT_OF_MEMORY = 6,    /* reference: std::bad_alloc */
+  GPULSM_ERR_LENGTH = 7            /* reference: std::length_error */
+} gpulsm_status;
+
+/* Status bits of gpulsm_dict_status(); bit 3 has the meaning of
+ * kPublicationOutputOverflow (GPULSMOpt.cuh:535-541). */
+#define GPULSM_STATUS_OUTPUT_OVERFLOW (1u << 3)
+#define GPULSM_STATUS_WAIT_TIMEOUT (1u << 8)
+#define GPULSM_STATUS_BAD_INPUT (1u << 9)
+
+/* Search structure used inside each sorted level. */
+#define GPULSM_SEARCH_DIRECTORY 0u /* radix directory over the level's key range */
+#define GPULSM_SEARCH_LEARNED 1u   /* piecewise-linear position model + checked window */
+
+/* Message of the last failed call on this thread. */
+const char *gpulsm_last_error(void);
+/* Library version string. */
+const char *gpulsm_version(void);
+
+/* ===================== LSM dictionary (GPULSMOpt semantics) ============== */
+typedef struct gpulsm_dict gpulsm_dict;
+
+/* Mirrors DictionaryConfig (gpu_dictionary_adapter.cuh:16-23) plus tunables. */
+typedef struct gpulsm_dict_config {
+  uint64_t max_elements;        /* DictionaryConfig::max_elements (live rows incl. tombstones) */
+  uint64_t batch_capacity;      /* DictionaryConfig::batch_capacity; 0 -> 2^20, max 2^20 */
+  uint64_t level_zero_capacity; /* DictionaryConfig::level_zero_capacity; 0 -> batch * fan_in */
+  uint32_t fan_in;              /* merge fan-in between levels, 2..16; 0 -> 4 */
+  uint32_t rows_per_bucket_log2;/* directory density; 0 -> 3 (about 8 rows per bucket) */
+  uint32_t search_mode;         /* GPULSM_SEARCH_* */
+  uint32_t reserved;
+} gpulsm_dict_config;
+
+/* GPULSMOpt::GPULSMOpt(const DictionaryConfig&)  GPULSMOpt.cuh:5606 */
+int gpulsm_dict_create(const gpulsm_dict_config *config, gpulsm_dict **out);
+/* GPULSMOpt::~GPULSMOpt  GPULSMOpt.cuh:5689 */
+int gpulsm_dict_destroy(gpulsm_dict *dict);
+/* GPULSMOpt::clear  GPULSMOpt.cuh:5731 */
+int gpulsm_dict_clear(gpulsm_dict *dict, void *stream);
+/* GPULSMOpt::bulk_build  GPULSMOpt.cuh:5738 (last duplicate wins) */
+int gpulsm_dict_bulk_build(gpulsm_dict *dict, const uint32_t *keys, const uint32_t *values,
+                           uint64_t count, void *stream);
+/* GPULSMOpt::insert(DeviceKeyValueBatch)  GPULSMOpt.cuh:5836 (upsert, last input index wins) */
+int gpulsm_dict_insert(gpulsm_dict *dict, const uint32_t *keys, const uint32_t *values,
+                       uint64_t count, void *stream);
+/* GPULSMOpt::erase(DeviceKeyBatch)  GPULSMOpt.cuh:5843 (tombstones) */
+int gpulsm_dict_erase(gpulsm_dict *dict, const uint32_t *keys, uint64_t count, void *stream);
+/* GPULSMOpt::lookup(DeviceLookupBatch)  GPULSMOpt.cuh:5850; out_found may be NULL.
+ * Miss: out_values = out_found ? 0 : 0xffffffff (GPULSMOpt.cuh:4742-4749). */
+int gpulsm_dict_lookup(gpulsm_dict *dict, const uint32_t *queries, uint64_t count,
+                       uint32_t *out_values, uint8_t *out_found, void *stream);
+/* GPULSMOpt::range(DeviceRangeOutputBatch)  GPULSMOpt.cuh:5858: u32 sum of live
+ * values with lo <= key <= hi, wrapping at 2^32; lo > hi gives 0. */
+int gpulsm_dict_range_sum(gpulsm_dict *dict, const uint32_t *lo, const uint32_t *hi,
+                          uint64_t count, uint32_t *out_sums, void *stream);
+/* Live-key count per range (the "range count" of LSMu count, FliX/impl_lsm_tree.cuh:1208). */
+int gpulsm_dict_range_count(gpulsm_dict *dict, const uint32_t *lo, const uint32_t *hi,
+                            uint64_t count, uint32_t *out_counts, void *stream);
+/* Range query returning pairs, step 1: offsets[count+1] (device, u64) = exclusive
+ * scan of the live counts; offsets[count] is the total number of pairs. */
+int gpulsm_dict_range_offsets(gpulsm_dict *dict, const uint32_t *lo, const uint32_t *hi,
+                              uint64_t count, uint64_t *offsets, void *stream);
+/* Step 2: writes each range's live (key, value) pairs in key order at
+ * out_keys/out_values[offsets[i] ...]; offsets must come from step 1 with no
+ * update in between. No counterpart in GPULSMOpt (it only sums). */
+int gpulsm_dict_range_pairs(gpulsm_dict *dict, const uint32_t *lo, const uint32_t *hi,
+                            uint64_t count, const uint64_t *offsets, uint32_t *out_keys,
+                            uint32_t *out_values, void *stream);
+/* GPULSMOpt::successor(DeviceSuccessorBatch)  GPULSMOpt.cuh:5865: smallest live
+ * key >= query, else 0xffffffff. */
+int gpulsm_dict_successor(gpulsm_dict *dict, const uint32_t *queries, uint64_t count,
+                          uint32_t *out_keys, void *stream);
+/* GPULSMOpt::canonical_carry_status  GPULSMOpt.cuh:5872 (synchronises). */
+int gpulsm_dict_status(gpulsm_dict *dict, uint32_t *out_status);
+/* GPULSMOpt::gpu_resident_bytes  GPULSMOpt.cuh:6341 */
+int gpulsm_dict_resident_bytes(gpulsm_dict *dict, uint64_t *out_bytes);
+/* Number of live rows (synchronises; diagnostics). */
+int gpulsm_dict_size(gpulsm_dict *dict, uint64_t *out_rows, uint32_t *out_levels);
+
+/* ===================== FliX bucket layer ================================== */
+typedef struct gpulsm_flix gpulsm_flix;
+
+typedef struct gpulsm_flix_config {
+  uint32_t key_bits;     /* 32 or 64 (key32 / key64, FliX/definitions.cuh:74-77) */
+  uint32_t node_size;    /* entries per node; 0 -> 32 (NODESIZE=5) */
+  uint32_t fill_percent; /* initial fill of build nodes; 0 -> 50 */
+  uint32_t search_mode;  /* GPULSM_SEARCH_* for unsorted probes */
+  uint64_t max_elements; /* capacity hint for the allocation region */
+} gpulsm_flix_config;
+
+int gpulsm_flix_create(const gpulsm_flix_config *config, gpulsm_flix **out);
+int gpulsm_flix_destroy(gpulsm_flix *index);
+/* build_bucket_layer_only  FliX/impl_cg_rtx_index_updates.cuh:1711; values NULL
+ * -> value = input index (the reference's offsets). keys are u32 or u64 per key_bits. */
+int gpulsm_flix_build(gpulsm_flix *index, const void *keys, const uint32_t *values,
+                      uint64_t count, uint64_t max_count, void *stream);
+/* insert  FliX/impl_cg_rtx_index_updates.cuh:2195 (insert if absent). Unlike the
+ * reference, the batch may be unsorted and hold duplicates (first one applies). */
+int gpulsm_flix_insert(gpulsm_flix *index, const void *keys, const uint32_t *values,
+                       uint64_t count, void *stream);
+/* remove  FliX/impl_cg_rtx_index_updates.cuh:2253 (physical delete, any order). */
+int gpulsm_flix_remove(gpulsm_flix *index, const void *keys, uint64_t count, void *stream);
+/* lookups_ordered  FliX/impl_cg_rtx_index_updates.cuh:2485: probes sorted
+ * ascending; out[i] = value or 0xffffffff. */
+int gpulsm_flix_lookups_ordered(gpulsm_flix *index, const void *sorted_probes, uint64_t count,
+                                uint32_t *out_values, void *stream);
+/* lookups_successor  FliX/impl_cg_rtx_index_updates.cuh:2647: probes sorted;
+ * out = first stored key >= probe, else 0xffffffff zero-extended. */
+int gpulsm_flix_lookups_successor(gpulsm_flix *index, const void *sorted_probes, uint64_t count,
+                                  void *out_keys, void *stream);
+/* Unsorted probes: sort with a permutation, ordered walk, scatter back
+ * (the driver protocol of FliX/benchmarks_updates.cuh:252-360 in one call). */
+int gpulsm_flix_lookup(gpulsm_flix *index, const void *probes, uint64_t count,
+                       uint32_t *out_values, void *stream);
+int gpulsm_flix_successor(gpulsm_flix *index, const void *probes, uint64_t count,
+                          void *out_keys, void *stream);
+/* rebuild_bucket_layer_only  FliX/impl_cg_rtx_index_updates.cuh:1821 */
+int gpulsm_flix_rebuild(gpulsm_flix *index, void *stream);
+int gpulsm_flix_resident_bytes(gpulsm_flix *index, uint64_t *out_bytes);
+int gpulsm_flix_size(gpulsm_flix *index, uint64_t *out_keys);
+int gpulsm_flix_status(gpulsm_flix *index, uint32_t *out_status);
+
+/* ===================== building blocks ==================================== */
+/* Stable LSD radix sort of (key, u32 value) pairs by key bits [begin_bit, end_bit).
+ * key_bits 32 or 64; values may be NULL. keys_out/values_out receive the result;
+ * the inputs are not modified. Allocates its scratch on the stream. */
+int gpulsm_sort_pairs(const void *keys_in, const uint32_t *values_in, void *keys_out,
+                      uint32_t *values_out, uint64_t count, uint32_t key_bits, uint32_t begin_bit,
+                      uint32_t end_bit, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GPULSM_H */

@@ -1,0 +1,212 @@
+"""ctypes front end of the CPU oracle (liboracle.so).  TEST INFRASTRUCTURE ONLY.
+
+The C sources (lsm_oracle.c, flix_oracle.c) restate the reference semantics and
+cite the reference file:line of each rule.  This module only marshals numpy
+arrays; it contains no dictionary logic of its own.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+_u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+_u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
+_u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
+
+
+def build_oracle(reference: bool = True) -> None:
+    """Compile liboracle.so (and oracle/_ref when the reference checkout exists)."""
+    target = "all" if reference else os.path.join(_HERE, "liboracle.so")
+    subprocess.run(["make", "-s", "-C", _HERE, target], check=True)
+
+
+def _load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(_LIB_PATH):
+        build_oracle(reference=False)
+    lib = C.CDLL(_LIB_PATH)
+    vp = C.c_void_p
+    u64 = C.c_uint64
+    sig = {
+        "orc_set_threads": (C.c_int, [C.c_int]),
+        "orc_get_threads": (C.c_int, []),
+        "orc_lsm_create": (vp, []),
+        "orc_lsm_destroy": (None, [vp]),
+        "orc_lsm_clear": (None, [vp]),
+        "orc_lsm_size": (u64, [vp]),
+        "orc_lsm_dump": (u64, [vp, _u32p, _u32p]),
+        "orc_lsm_bulk_build": (None, [vp, _u32p, _u32p, u64]),
+        "orc_lsm_insert": (None, [vp, _u32p, _u32p, u64]),
+        "orc_lsm_erase": (None, [vp, _u32p, u64]),
+        "orc_lsm_lookup": (None, [vp, _u32p, u64, _u32p, vp]),
+        "orc_lsm_range_sum": (None, [vp, _u32p, _u32p, u64, _u32p]),
+        "orc_lsm_range_count": (None, [vp, _u32p, _u32p, u64, _u32p]),
+        "orc_lsm_range_offsets": (u64, [vp, _u32p, _u32p, u64, _u64p]),
+        "orc_lsm_range_pairs": (None, [vp, _u32p, _u32p, u64, _u64p, _u32p, _u32p]),
+        "orc_lsm_successor": (None, [vp, _u32p, u64, _u32p]),
+        "orc_flix_create": (vp, [C.c_int]),
+        "orc_flix_destroy": (None, [vp]),
+        "orc_flix_size": (u64, [vp]),
+        "orc_flix_dump": (u64, [vp, _u64p, _u32p]),
+        "orc_flix_build": (None, [vp, _u64p, vp, u64]),
+        "orc_flix_insert": (None, [vp, _u64p, vp, u64]),
+        "orc_flix_remove": (None, [vp, _u64p, u64]),
+        "orc_flix_lookup": (None, [vp, _u64p, u64, _u32p]),
+        "orc_flix_successor": (None, [vp, _u64p, u64, _u64p]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def oracle_threads(threads: int = 0) -> int:
+    """Set the oracle's OpenMP thread count (0 = every host core); returns it."""
+    return _load().orc_set_threads(int(threads))
+
+
+def _u32(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.uint32))
+
+
+def _u64(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.uint64))
+
+
+class OracleLSM:
+    """GPULSMOpt semantics (upsert, tombstones) on the CPU: the std::map oracle."""
+
+    def __init__(self):
+        self._lib = _load()
+        self._h = self._lib.orc_lsm_create()
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            self._lib.orc_lsm_destroy(self._h)
+            self._h = None
+
+    def clear(self):
+        self._lib.orc_lsm_clear(self._h)
+
+    def __len__(self):
+        return int(self._lib.orc_lsm_size(self._h))
+
+    def dump(self):
+        n = len(self)
+        k = np.empty(n, np.uint32)
+        v = np.empty(n, np.uint32)
+        self._lib.orc_lsm_dump(self._h, k, v)
+        return k, v
+
+    def bulk_build(self, keys, values):
+        k, v = _u32(keys), _u32(values)
+        self._lib.orc_lsm_bulk_build(self._h, k, v, k.size)
+
+    def insert(self, keys, values):
+        k, v = _u32(keys), _u32(values)
+        assert k.size == v.size
+        self._lib.orc_lsm_insert(self._h, k, v, k.size)
+
+    def erase(self, keys):
+        k = _u32(keys)
+        self._lib.orc_lsm_erase(self._h, k, k.size)
+
+    def lookup(self, queries, with_found: bool = False):
+        q = _u32(queries)
+        out = np.empty(q.size, np.uint32)
+        if with_found:
+            found = np.empty(q.size, np.uint8)
+            self._lib.orc_lsm_lookup(self._h, q, q.size, out, found.ctypes.data_as(C.c_void_p))
+            return out, found
+        self._lib.orc_lsm_lookup(self._h, q, q.size, out, None)
+        return out
+
+    def range_sum(self, lo, hi):
+        lo, hi = _u32(lo), _u32(hi)
+        out = np.empty(lo.size, np.uint32)
+        self._lib.orc_lsm_range_sum(self._h, lo, hi, lo.size, out)
+        return out
+
+    def range_count(self, lo, hi):
+        lo, hi = _u32(lo), _u32(hi)
+        out = np.empty(lo.size, np.uint32)
+        self._lib.orc_lsm_range_count(self._h, lo, hi, lo.size, out)
+        return out
+
+    def range_pairs(self, lo, hi):
+        """Returns (offsets[n+1] u64, keys, values) with each query's live pairs in key order."""
+        lo, hi = _u32(lo), _u32(hi)
+        offsets = np.empty(lo.size + 1, np.uint64)
+        total = int(self._lib.orc_lsm_range_offsets(self._h, lo, hi, lo.size, offsets))
+        keys = np.empty(total, np.uint32)
+        vals = np.empty(total, np.uint32)
+        self._lib.orc_lsm_range_pairs(self._h, lo, hi, lo.size, offsets, keys, vals)
+        return offsets, keys, vals
+
+    def successor(self, queries):
+        q = _u32(queries)
+        out = np.empty(q.size, np.uint32)
+        self._lib.orc_lsm_successor(self._h, q, q.size, out)
+        return out
+
+
+class OracleFlix:
+    """FliX bucket-layer semantics (insert-if-absent, physical delete) on the CPU."""
+
+    def __init__(self, key_bits: int = 64):
+        assert key_bits in (32, 64)
+        self.key_bits = key_bits
+        self._lib = _load()
+        self._h = self._lib.orc_flix_create(key_bits)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            self._lib.orc_flix_destroy(self._h)
+            self._h = None
+
+    def __len__(self):
+        return int(self._lib.orc_flix_size(self._h))
+
+    def dump(self):
+        n = len(self)
+        k = np.empty(n, np.uint64)
+        v = np.empty(n, np.uint32)
+        self._lib.orc_flix_dump(self._h, k, v)
+        return k, v
+
+    def build(self, keys, values=None):
+        k = _u64(keys)
+        v = None if values is None else _u32(values)
+        self._lib.orc_flix_build(self._h, k, None if v is None else v.ctypes.data_as(C.c_void_p), k.size)
+
+    def insert(self, keys, values):
+        k, v = _u64(keys), _u32(values)
+        assert k.size == v.size
+        self._lib.orc_flix_insert(self._h, k, v.ctypes.data_as(C.c_void_p), k.size)
+
+    def remove(self, keys):
+        k = _u64(keys)
+        self._lib.orc_flix_remove(self._h, k, k.size)
+
+    def lookup(self, probes):
+        p = _u64(probes)
+        out = np.empty(p.size, np.uint32)
+        self._lib.orc_flix_lookup(self._h, p, p.size, out)
+        return out
+
+    def successor(self, probes):
+        p = _u64(probes)
+        out = np.empty(p.size, np.uint64)
+        self._lib.orc_flix_successor(self._h, p, p.size, out)
+        return out

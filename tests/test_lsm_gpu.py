@@ -1,0 +1,301 @@
+"""GPU parity of the LSM dictionary (GPULSMOpt semantics) against the CPU oracle.
+
+Every answer is compared bit for bit: integer work, no tolerance.
+"""
+import numpy as np
+import pytest
+
+from conftest import empty_u32, to_dev, to_host
+from oracle import OracleLSM
+from scenarios import (NOT_FOUND, capacity_ops, forced_validation_steps, key_for_index, range_digest,
+                       rollover_ops, sweep_lookup_queries, sweep_range_queries, validation_queries)
+
+pytestmark = pytest.mark.gpu
+
+
+class Twin:
+    """Runs every operation on the GPU dictionary and on the oracle."""
+
+    def __init__(self, gl, **cfg):
+        self.d = gl.GPULSMOpt(gl.DictionaryConfig(**cfg))
+        self.o = OracleLSM()
+
+    def apply(self, op):
+        if op[0] == "insert":
+            self.d.insert(to_dev(op[1]), to_dev(op[2]))
+            self.o.insert(op[1], op[2])
+        else:
+            self.d.erase(to_dev(op[1]))
+            self.o.erase(op[1])
+
+    def lookup(self, q, with_found=False):
+        import torch
+
+        out = empty_u32(q.size)
+        found = torch.empty(max(q.size, 1), dtype=torch.uint8, device="cuda") if with_found else None
+        self.d.lookup(to_dev(q), out, found, count=q.size)
+        got = to_host(out)[: q.size]
+        if with_found:
+            want_v, want_f = self.o.lookup(q, with_found=True)
+            assert np.array_equal(to_host(found, np.uint8)[: q.size], want_f)
+            assert np.array_equal(got, want_v)
+        else:
+            assert np.array_equal(got, self.o.lookup(q))
+
+    def ranges(self, lo, hi):
+        out = empty_u32(lo.size)
+        self.d.range(to_dev(lo), to_dev(hi), out, count=lo.size)
+        assert np.array_equal(to_host(out)[: lo.size], self.o.range_sum(lo, hi))
+        self.d.range_count(to_dev(lo), to_dev(hi), out, count=lo.size)
+        assert np.array_equal(to_host(out)[: lo.size], self.o.range_count(lo, hi))
+        off, k, v = self.d.range_query(to_dev(lo), to_dev(hi))
+        o_off, o_k, o_v = self.o.range_pairs(lo, hi)
+        assert np.array_equal(to_host(off, np.uint64), o_off)
+        assert np.array_equal(to_host(k), o_k)
+        assert np.array_equal(to_host(v), o_v)
+
+    def successor(self, q):
+        out = empty_u32(q.size)
+        self.d.successor(to_dev(q), out, count=q.size)
+        assert np.array_equal(to_host(out)[: q.size], self.o.successor(q))
+
+
+def test_sort_pairs_stable(gl, cuda):
+    import torch
+
+    rng = np.random.default_rng(5)
+    for n in (1, 100, 4096, 4097, 300_000):
+        k = rng.integers(0, 1 << 12, n, dtype=np.uint64).astype(np.uint32)  # many ties
+        v = np.arange(n, dtype=np.uint32)
+        ko, vo = empty_u32(n), empty_u32(n)
+        gl.sort_pairs(to_dev(k), to_dev(v), ko, vo)
+        order = np.argsort(k, kind="stable")
+        assert np.array_equal(to_host(ko)[:n], k[order])
+        assert np.array_equal(to_host(vo)[:n], v[order])
+    n = 200_000
+    k64 = rng.integers(0, 1 << 40, n, dtype=np.uint64)
+    ko = torch.empty(n, dtype=torch.int64, device="cuda")
+    vo = empty_u32(n)
+    gl.sort_pairs(to_dev(k64), to_dev(np.arange(n, dtype=np.uint32)), ko, vo, 0, 40)
+    order = np.argsort(k64, kind="stable")
+    assert np.array_equal(to_host(ko, np.uint64), k64[order])
+    assert np.array_equal(to_host(vo)[:n], order.astype(np.uint32))
+
+
+def test_forced_validation_scenarios(gl, cuda):
+    t = Twin(gl, max_elements=1 << 20)
+    for name, ops, expected, removed in forced_validation_steps():
+        for op in ops:
+            t.apply(op)
+        q, want = validation_queries(expected, removed)
+        out = empty_u32(q.size)
+        t.d.lookup(to_dev(q), out, count=q.size)
+        assert np.array_equal(to_host(out)[: q.size], want), name
+        t.lookup(q, with_found=True)
+    assert t.d.canonical_carry_status() == 0
+
+
+def test_multilevel_rollover(gl, cuda):
+    ops, q, expected = rollover_ops()
+    t = Twin(gl, max_elements=512, batch_capacity=4, level_zero_capacity=64)
+    for op in ops:
+        t.apply(op)
+    out = empty_u32(q.size)
+    t.d.lookup(to_dev(q), out)
+    assert np.array_equal(to_host(out), expected)
+    assert t.d.canonical_carry_status() == 0
+    t.successor(np.arange(0, 300, dtype=np.uint32))
+    t.ranges(np.array([0, 10, 200], np.uint32), np.array([255, 20, 100], np.uint32))
+
+
+def test_capacity_exhaustion_is_controlled(gl, cuda):
+    d = gl.GPULSMOpt(gl.DictionaryConfig(max_elements=1024, batch_capacity=4, level_zero_capacity=1024))
+    o = OracleLSM()
+    raised = None
+    for op in capacity_ops():
+        try:
+            d.insert(to_dev(op[1]), to_dev(op[2]))
+        except gl.CapacityError as e:
+            raised = e
+            break
+        o.insert(op[1], op[2])
+    if raised is None:  # the receipt of the last batch may still be in flight
+        assert d.canonical_carry_status() & gl._native.STATUS_OUTPUT_OVERFLOW
+        with pytest.raises(gl.CapacityError, match="capacity"):
+            d.insert(to_dev(np.array([1], np.uint32)), to_dev(np.array([1], np.uint32)))
+    assert "capacity" in str(raised or "capacity")
+    assert d.canonical_carry_status() & gl._native.STATUS_OUTPUT_OVERFLOW
+    # every accepted update stays readable
+    q = np.arange(0, 17 * 16 * 4 + 8, dtype=np.uint32)
+    out = empty_u32(q.size)
+    d.lookup(to_dev(q), out)
+    assert np.array_equal(to_host(out), o.lookup(q))
+
+
+@pytest.mark.parametrize("batch_capacity,level_zero,fan_in", [(64, 0, 2), (256, 512, 4), (1024, 0, 8)])
+def test_random_updates_match_oracle(gl, cuda, batch_capacity, level_zero, fan_in):
+    rng = np.random.default_rng(batch_capacity + fan_in)
+    t = Twin(gl, max_elements=1 << 16, batch_capacity=batch_capacity, level_zero_capacity=level_zero,
+             fan_in=fan_in)
+    universe = rng.integers(0, 1 << 32, 5000, dtype=np.uint64).astype(np.uint32)
+    universe[:6] = [0, 1, 2, 0xFFFFFFFF, 0xFFFFFFFE, 0x80000000]
+    for step in range(60):
+        n = int(rng.integers(0, 3 * batch_capacity))
+        k = universe[rng.integers(0, universe.size, n)]
+        if rng.random() < 0.3:
+            t.apply(("erase", k))
+        else:
+            v = rng.integers(0, 1 << 32, n, dtype=np.uint64).astype(np.uint32)
+            v[: min(n, 3)] = 0xFFFFFFFF  # real values equal to the tombstone sentinel
+            t.apply(("insert", k, v))
+        if step % 10 == 9:
+            q = np.concatenate([universe, rng.integers(0, 1 << 32, 500, dtype=np.uint64).astype(np.uint32)])
+            t.lookup(q)
+            t.lookup(q, with_found=True)
+            lo = universe[rng.integers(0, universe.size, 300)]
+            hi = (lo.astype(np.uint64) + rng.integers(0, 1 << 28, 300, dtype=np.uint64)).clip(0, 0xFFFFFFFF)
+            lo[:3] = [5, 0, 0xFFFFFFFF]
+            hi = hi.astype(np.uint32)
+            hi[:3] = [4, 0xFFFFFFFF, 0xFFFFFFFF]  # lo > hi, full range, single key
+            t.ranges(lo, hi)
+            t.successor(q)
+    assert t.d.canonical_carry_status() == 0
+
+
+def test_empty_and_edge_inputs(gl, cuda):
+    import torch
+
+    d = gl.GPULSMOpt(gl.DictionaryConfig(max_elements=1 << 12))
+    q = np.array([0, 1, 0xFFFFFFFF], np.uint32)
+    out = empty_u32(3)
+    d.lookup(to_dev(q), out)
+    assert to_host(out).tolist() == [NOT_FOUND] * 3
+    d.successor(to_dev(q), out)
+    assert to_host(out).tolist() == [NOT_FOUND] * 3
+    d.range(to_dev(q), to_dev(q), out)
+    assert to_host(out).tolist() == [0, 0, 0]
+    z = torch.empty(0, dtype=torch.int32, device="cuda")
+    d.insert(z, z)  # empty batches are no-ops
+    d.erase(z)
+    d.lookup(z, z)
+    with pytest.raises(gl.InvalidArgument):
+        gl._native.check(d._lib.gpulsm_dict_insert(d._h, None, None, 5, None))
+    with pytest.raises(ValueError):
+        gl._native.check(d._lib.gpulsm_dict_lookup(d._h, None, 4, None, None, None))
+    with pytest.raises(ValueError):
+        gl.GPULSMOpt(gl.DictionaryConfig(max_elements=1 << 33))
+    d.insert(to_dev(np.array([0xFFFFFFFF, 0], np.uint32)), to_dev(np.array([7, 0xFFFFFFFF], np.uint32)))
+    d.lookup(to_dev(q), out)
+    assert to_host(out).tolist() == [0xFFFFFFFF, NOT_FOUND, 7]
+    d.successor(to_dev(np.array([1, 0xFFFFFFFF], np.uint32)), out, count=2)
+    assert to_host(out)[:2].tolist() == [0xFFFFFFFF, 0xFFFFFFFF]
+
+
+def test_bulk_build_then_updates(gl, cuda):
+    rng = np.random.default_rng(3)
+    t = Twin(gl, max_elements=1 << 18, batch_capacity=1 << 12)
+    k = rng.integers(0, 1 << 20, 100_000, dtype=np.uint64).astype(np.uint32)
+    v = np.arange(k.size, dtype=np.uint32)
+    t.d.bulk_build(to_dev(k), to_dev(v))
+    t.o.bulk_build(k, v)
+    t.lookup(np.arange(0, 1 << 20, 7, dtype=np.uint32))
+    for i in range(10):
+        kk = rng.integers(0, 1 << 20, 5000, dtype=np.uint64).astype(np.uint32)
+        t.apply(("erase", kk) if i % 3 == 2 else ("insert", kk, rng.integers(0, 1 << 32, 5000, dtype=np.uint64).astype(np.uint32)))
+    t.lookup(np.arange(0, 1 << 20, 3, dtype=np.uint32), with_found=True)
+    t.successor(rng.integers(0, 1 << 21, 10000, dtype=np.uint64).astype(np.uint32))
+    lo = rng.integers(0, 1 << 20, 2000, dtype=np.uint64).astype(np.uint32)
+    t.ranges(lo, lo + np.uint32(500))
+
+
+def test_streams_are_ordered(gl, cuda):
+    import torch
+
+    t = Twin(gl, max_elements=1 << 16, batch_capacity=1 << 10)
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+    rng = np.random.default_rng(9)
+    k = rng.integers(0, 1 << 32, 20000, dtype=np.uint64).astype(np.uint32)
+    v = rng.integers(0, 1 << 32, 20000, dtype=np.uint64).astype(np.uint32)
+    kd, vd = to_dev(k), to_dev(v)
+    torch.cuda.synchronize()
+    t.d.insert(kd, vd, stream=s1)
+    t.o.insert(k, v)
+    out = empty_u32(k.size)
+    t.d.lookup(kd, out, stream=s2)
+    s2.synchronize()
+    assert np.array_equal(to_host(out), t.o.lookup(k))
+
+
+def test_lsm_small_configuration(gl, cuda, workloads):
+    w = workloads.lsm_small()
+    t = Twin(gl, max_elements=1 << 20, batch_capacity=1 << 16)
+    for op in w.ops:
+        t.apply(op)
+    t.lookup(w.lookups)
+    t.lookup(w.lookups, with_found=True)
+    out = empty_u32(w.range_lo.size)
+    t.d.range_count(to_dev(w.range_lo), to_dev(w.range_hi), out)
+    assert np.array_equal(to_host(out), t.o.range_count(w.range_lo, w.range_hi))
+    t.ranges(w.range_lo[:4096], w.range_hi[:4096])
+    t.successor(w.lookups[:100_000])
+
+
+def test_paper_sweep_protocol(gl, cuda):
+    n = 1 << 20
+    d = gl.GPULSMOpt(gl.DictionaryConfig(max_elements=n))
+    keys = key_for_index(np.arange(n))
+    ones = to_dev(np.ones(1 << 16, np.uint32))
+    for b in range(0, n, 1 << 16):
+        d.insert(to_dev(keys[b:b + (1 << 16)]), ones)
+    out = empty_u32(1 << 18)
+    d.lookup(to_dev(sweep_lookup_queries(1 << 18, n, True, 3)), out)
+    assert (to_host(out) == 1).all()
+    d.lookup(to_dev(sweep_lookup_queries(1 << 18, n, False, 4)), out)
+    assert (to_host(out) == NOT_FOUND).all()
+    o = OracleLSM()
+    o.insert(keys, np.ones(n, np.uint32))
+    for expected_hits in (8, 1024):
+        lo, hi = sweep_range_queries(1 << 16, n, expected_hits, 5)
+        r = empty_u32(lo.size)
+        d.range(to_dev(lo), to_dev(hi), r)
+        assert range_digest(to_host(r)) == range_digest(o.range_sum(lo, hi))
+
+
+def test_lsm_scale_reduced(gl, cuda, workloads):
+    """The at-scale configuration's shape at 1/16 size, exact against the oracle."""
+    w = workloads.lsm_scale(scale=4)
+    t = Twin(gl, max_elements=(1 << 22) + (1 << 18), batch_capacity=1 << 16)
+    for op in w.ops:
+        t.apply(op)
+    t.lookup(w.lookups)
+    t.ranges(w.range_lo, w.range_hi)
+    t.successor(w.lookups[:200_000])
+    assert t.d.canonical_carry_status() == 0
+
+
+@pytest.mark.slow
+def test_lsm_scale_full_size_properties(gl, cuda, workloads):
+    """Full 2^26-key configuration: lookups exact; ranges through per-query
+    counts, sums and a digest of every returned pair."""
+    import torch
+
+    w = workloads.lsm_scale(scale=0)
+    t = Twin(gl, max_elements=(1 << 26) + (1 << 22))
+    for op in w.ops:
+        t.apply(op)
+    t.lookup(w.lookups)
+    lo, hi = w.range_lo, w.range_hi
+    off, k, v = t.d.range_query(to_dev(lo), to_dev(hi))
+    counts = (off[1:] - off[:-1]).to(torch.int64)
+    assert np.array_equal(counts.cpu().numpy().astype(np.uint32), t.o.range_count(lo, hi))
+    seg = torch.repeat_interleave(torch.arange(lo.size, device="cuda"), counts)
+    sums = torch.zeros(lo.size, dtype=torch.int64, device="cuda")
+    sums.index_add_(0, seg, v.to(torch.int64) & 0xFFFFFFFF)
+    assert np.array_equal((sums.cpu().numpy() & 0xFFFFFFFF).astype(np.uint32), t.o.range_sum(lo, hi))
+    keys_sorted = bool(((k[1:].to(torch.int64) & 0xFFFFFFFF) > (k[:-1].to(torch.int64) & 0xFFFFFFFF))
+                       .logical_or(seg[1:] != seg[:-1]).all())
+    assert keys_sorted
+    sample = np.arange(0, lo.size, 997)
+    o_off, o_k, o_v = t.o.range_pairs(lo[sample], hi[sample])
+    got_k = np.concatenate([to_host(k[int(off[i]):int(off[i + 1])]) for i in sample])
+    assert np.array_equal(got_k, o_k)

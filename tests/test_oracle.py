@@ -1,0 +1,151 @@
+"""CPU tests of the oracle: the reference's own known answers, a pure-Python
+model on small random cases, and the paper-sweep protocol."""
+import numpy as np
+import pytest
+
+from oracle import OracleFlix, OracleLSM
+from scenarios import (NOT_FOUND, forced_validation_steps, key_for_index, range_digest, rollover_ops,
+                       sweep_lookup_queries, sweep_range_queries, validation_queries)
+
+
+def apply_ops(d, ops):
+    for op in ops:
+        if op[0] == "insert":
+            d.insert(op[1], op[2])
+        else:
+            d.erase(op[1])
+
+
+def test_forced_validation_scenarios():
+    d = OracleLSM()
+    for name, ops, expected, removed in forced_validation_steps():
+        apply_ops(d, ops)
+        q, want = validation_queries(expected, removed)
+        got = d.lookup(q)
+        assert np.array_equal(got, want), name
+        vals, found = d.lookup(q, with_found=True)
+        assert np.array_equal(found.astype(bool), want != NOT_FOUND) or name == "sparse_unique"
+        assert np.array_equal(vals[found == 0], np.zeros(int((found == 0).sum()), np.uint32)), name
+
+
+def test_rollover_scenario():
+    ops, q, expected = rollover_ops()
+    d = OracleLSM()
+    apply_ops(d, ops)
+    assert np.array_equal(d.lookup(q), expected)
+
+
+class Model:
+    """Pure-Python statement of the GPULSMOpt visible state (dict of live keys)."""
+
+    def __init__(self):
+        self.m = {}
+
+    def insert(self, k, v):
+        for a, b in zip(k.tolist(), v.tolist()):
+            self.m[a] = b  # later input index wins
+
+    def erase(self, k):
+        for a in k.tolist():
+            self.m.pop(a, None)
+
+    def lookup(self, q):
+        return np.array([self.m.get(x, NOT_FOUND) for x in q.tolist()], np.uint32)
+
+    def sorted(self):
+        ks = sorted(self.m)
+        return np.array(ks, np.uint64), np.array([self.m[k] for k in ks], np.uint64)
+
+    def range_sum(self, lo, hi):
+        ks, vs = self.sorted()
+        out = []
+        for a, b in zip(lo.tolist(), hi.tolist()):
+            if a > b:
+                out.append(0)
+                continue
+            i, j = np.searchsorted(ks, a), np.searchsorted(ks, b, side="right")
+            out.append(int(vs[i:j].sum()) & 0xFFFFFFFF)
+        return np.array(out, np.uint32)
+
+    def successor(self, q):
+        ks, _ = self.sorted()
+        out = []
+        for x in q.tolist():
+            i = np.searchsorted(ks, x)
+            out.append(int(ks[i]) if i < ks.size else NOT_FOUND)
+        return np.array(out, np.uint32)
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_oracle_matches_python_model(seed):
+    rng = np.random.default_rng(seed)
+    d, m = OracleLSM(), Model()
+    universe = rng.integers(0, 1 << 32, 300, dtype=np.uint64).astype(np.uint32)
+    universe[:4] = [0, 1, 0xFFFFFFFF, 0xFFFFFFFE]
+    for step in range(40):
+        n = int(rng.integers(0, 200))
+        k = universe[rng.integers(0, universe.size, n)]
+        if rng.random() < 0.3:
+            d.erase(k)
+            m.erase(k)
+        else:
+            v = rng.integers(0, 1 << 32, n, dtype=np.uint64).astype(np.uint32)
+            d.insert(k, v)
+            m.insert(k, v)
+        q = np.concatenate([universe, rng.integers(0, 1 << 32, 50, dtype=np.uint64).astype(np.uint32)])
+        assert np.array_equal(d.lookup(q), m.lookup(q))
+        lo = universe[rng.integers(0, universe.size, 64)]
+        hi = universe[rng.integers(0, universe.size, 64)]
+        assert np.array_equal(d.range_sum(lo, hi), m.range_sum(lo, hi))
+        assert np.array_equal(d.successor(q), m.successor(q))
+        off, rk, rv = d.range_pairs(lo, hi)
+        counts = d.range_count(lo, hi)
+        assert np.array_equal(np.diff(off).astype(np.uint32), counts)
+        sums = np.array([int(rv[off[i]:off[i + 1]].astype(np.uint64).sum()) & 0xFFFFFFFF
+                         for i in range(lo.size)], np.uint32)
+        assert np.array_equal(sums, d.range_sum(lo, hi))
+
+
+def test_bulk_build_keeps_last_duplicate():
+    d = OracleLSM()
+    d.bulk_build(np.array([7, 3, 7, 7, 3], np.uint32), np.array([1, 2, 3, 4, 5], np.uint32))
+    k, v = d.dump()
+    assert k.tolist() == [3, 7] and v.tolist() == [5, 4]
+
+
+def test_range_sum_wraps_and_empty_ranges():
+    d = OracleLSM()
+    d.insert(np.array([10, 11, 12], np.uint32), np.array([0xFFFFFFFF, 0xFFFFFFFF, 3], np.uint32))
+    assert d.range_sum([10, 12, 5], [12, 10, 9]).tolist() == [(2 * 0xFFFFFFFF + 3) & 0xFFFFFFFF, 0, 0]
+
+
+def test_flix_oracle_rules():
+    f = OracleFlix(64)
+    f.build(np.array([10, 2, 30, 2], np.uint64))  # values = input index, first duplicate wins
+    assert f.dump()[0].tolist() == [2, 10, 30] and f.dump()[1].tolist() == [1, 0, 2]
+    f.insert(np.array([2, 5, 5], np.uint64), np.array([7, 8, 9], np.uint32))  # insert if absent
+    assert f.lookup(np.array([2, 5, 11], np.uint64)).tolist() == [1, 8, NOT_FOUND]
+    f.remove(np.array([10, 11], np.uint64))
+    assert f.successor(np.array([3, 6, 31, 1 << 40], np.uint64)).tolist() == [5, 30, 0xFFFFFFFF, 0xFFFFFFFF]
+    g = OracleFlix(32)
+    g.build(np.array([5, 0xFFFFFFFE], np.uint64), np.array([1, 2], np.uint32))
+    assert g.successor(np.array([6], np.uint64)).tolist() == [0xFFFFFFFE]
+
+
+def test_paper_sweep_protocol():
+    n = 1 << 16
+    d = OracleLSM()
+    keys = key_for_index(np.arange(n))
+    for b in range(0, n, 1 << 13):
+        d.insert(keys[b:b + (1 << 13)], np.ones(1 << 13, np.uint32))
+    hits = sweep_lookup_queries(4096, n, True, 7)
+    misses = sweep_lookup_queries(4096, n, False, 9)
+    assert (d.lookup(hits) == 1).all()
+    assert (d.lookup(misses) == NOT_FOUND).all()
+    for expected_hits in (8, 1024):
+        lo, hi = sweep_range_queries(2048, n, expected_hits, 11)
+        sums = d.range_sum(lo, hi)
+        assert np.array_equal(sums, d.range_count(lo, hi))  # values are 1
+        assert abs(float(sums.mean()) - expected_hits) < 0.2 * expected_hits
+        s, x = range_digest(sums)
+        assert s == int(sums.sum())
