@@ -1,0 +1,435 @@
+"""Benchmark of the GPU dictionary hot path (one JSON line on stdout, rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload lsm_scale|lsm_small] [--no-e2e] [--no-cpu]
+
+A step is one pass of the at-scale LSM workload over a fresh dictionary:
+64 insert batches of 2^20 u32 (key, value) pairs with a 2^18-key delete batch
+after every 4th insert batch (2^26 + 2^22 updates), then 2^24 point lookups
+(70% Zipf s=0.99 over inserted keys, 30% uniform) and 2^20 range queries that
+return (key, value) pairs (offsets pass + pairs pass).  value = all operations
+of the step (updated keys + lookups + range queries) / step time, in M ops/s;
+per-phase rates (inserted keys/s, lookups/s, range queries/s) and per-batch
+p50/p99 latencies ride along.  Inputs live in HBM before the timed region;
+together they exceed the 126 MB L2, so no flush is needed between steps.
+
+--impl reference times the reference path's CPU implementation (the oracle
+restatement, all host threads; the reference has no CPU engine of its own) on
+a bounded sample of the same workload.  Under torchrun (N > 1) each rank runs
+an independent dictionary on its own seeded data (replicas: the path has no
+exchange step), rank 0 prints the aggregate.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "M lookups/s & M inserted keys/s at 2^26 keys vs plain form; p50/p99 request latency"
+LOOKUP_BYTES = 41  # algorithmic bytes per u32 point lookup (query + value + found + one row sector)
+INSERT_BYTES = 16  # per inserted (key, value): read 8 + write 8 into the structure
+DELETE_BYTES = 12
+RANGE_BYTES = 76   # per range query (lo, hi, count + two boundary sectors) + 16 per returned pair
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--workload", default="lsm_scale", choices=["lsm_scale", "lsm_small"])
+    p.add_argument("--scale", type=int, default=0, help="divide sizes by 2^scale (development only)")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(
+        os.environ.get("LOCAL_RANK", 0))
+
+
+def make_workload(W, name, scale, rank):
+    if name == "lsm_small":
+        w = W.lsm_small(scale)
+    else:
+        w = W.lsm_scale(scale)
+    if rank:
+        # replicas: each rank draws its own keys (same shapes, different seed stream)
+        rng = np.random.default_rng(0x5EED + 7919 * rank)
+        perm = rng.integers(0, 1 << 32, 1, dtype=np.uint64).astype(np.uint32)[0]
+        w.ops = [(o[0], o[1] ^ perm, *o[2:]) for o in w.ops]
+        w.lookups = w.lookups ^ perm
+    return w
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for nm, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+    gl = importlib.import_module("gpu-lsm-tree_b200")
+    W = importlib.import_module("gpu-lsm-tree_b200.workloads")
+    lib = gl.load()
+    w = make_workload(W, args.workload, args.scale, rank)
+
+    def to_dev(a):
+        return torch.from_numpy(np.ascontiguousarray(a).view(np.int32)).to(dev)
+
+    ops_dev = [(o[0], to_dev(o[1]), to_dev(o[2]) if o[0] == "insert" else None) for o in w.ops]
+    q = to_dev(w.lookups)
+    lo, hi = to_dev(w.range_lo), to_dev(w.range_hi)
+    nq, nr = w.lookups.size, w.range_lo.size
+    out_v = torch.empty(nq, dtype=torch.int32, device=dev)
+    out_f = torch.empty(nq, dtype=torch.uint8, device=dev)
+    offsets = torch.empty(nr + 1, dtype=torch.int64, device=dev)
+    max_el = w.inserted_keys + w.erased_keys
+    d = gl.GPULSMOpt(gl.DictionaryConfig(max_elements=max_el))
+    stream = torch.cuda.current_stream(dev)
+    pairs = [None, None]
+
+    def step(ev=None):
+        d.clear()
+        if ev is not None:
+            ev["start"].record(stream)
+        for i, (kind, k, v) in enumerate(ops_dev):
+            if kind == "insert":
+                d.insert(k, v)
+            else:
+                d.erase(k)
+            if ev is not None:
+                ev["batch"][i].record(stream)
+        d.lookup(q, out_v, out_f)
+        if ev is not None:
+            ev["lookup"].record(stream)
+        d.range_offsets(lo, hi, offsets)
+        d.range_pairs(lo, hi, offsets, pairs[0], pairs[1])
+        if ev is not None:
+            ev["range"].record(stream)
+
+    # size the range output from one untimed pass
+    d.clear()
+    for kind, k, v in ops_dev:
+        d.insert(k, v) if kind == "insert" else d.erase(k)
+    d.range_offsets(lo, hi, offsets)
+    total_pairs = int(offsets[nr].item())
+    pairs[0] = torch.empty(max(total_pairs, 1), dtype=torch.int32, device=dev)
+    pairs[1] = torch.empty(max(total_pairs, 1), dtype=torch.int32, device=dev)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+
+    def new_events():
+        mk = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+        return {"start": mk(), "batch": [mk() for _ in ops_dev], "lookup": mk(), "range": mk()}
+
+    events = [new_events() for _ in range(args.steps)]
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = lib.gpulsm_launch_count()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    with ClockSampler(local) as clocks:
+        t0.record(stream)
+        for s in range(args.steps):
+            step(events[s])
+        t1.record(stream)
+        torch.cuda.synchronize(dev)
+    launches = lib.gpulsm_launch_count() - launches0
+    total_ms = t0.elapsed_time(t1)
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+
+    # per-phase times (device events on the launching stream)
+    upd_ms, look_ms, range_ms, batch_ms = [], [], [], []
+    n_ops = len(ops_dev)
+    for ev in events:
+        prev = ev["start"]
+        for i in range(n_ops):
+            batch_ms.append((ops_dev[i][0], prev.elapsed_time(ev["batch"][i])))
+            prev = ev["batch"][i]
+        upd_ms.append(ev["start"].elapsed_time(ev["batch"][-1]))
+        look_ms.append(ev["batch"][-1].elapsed_time(ev["lookup"]))
+        range_ms.append(ev["lookup"].elapsed_time(ev["range"]))
+    ms_per_step = total_ms / args.steps
+    upd_keys = w.inserted_keys + w.erased_keys
+    ops_per_step = upd_keys + nq + nr
+    value = ops_per_step * world / (ms_per_step * 1e-3) / 1e6
+    ins_lat = [b for k, b in batch_ms if k == "insert"]
+    upd = float(np.median(upd_ms))
+    look = float(np.median(look_ms))
+    rng_ms = float(np.median(range_ms))
+    peak, peak_kind = peaks()
+    lookup_gbs = nq * LOOKUP_BYTES / (look * 1e-3) / 1e9
+    range_gbs = (nr * RANGE_BYTES + total_pairs * 16) / (rng_ms * 1e-3) / 1e9
+    update_gbs = (w.inserted_keys * INSERT_BYTES + w.erased_keys * DELETE_BYTES) / (upd * 1e-3) / 1e9
+    phases = {"update": (upd, update_gbs), "lookup": (look, lookup_gbs), "range": (rng_ms, range_gbs)}
+    dom = max(phases, key=lambda k: phases[k][0])
+    roofline = {"bound": "hbm", "kernel_phase": dom, "achieved": round(phases[dom][1], 1), "peak": peak,
+                "unit": "GB/s", "frac": round(phases[dom][1] / peak, 4), "peak_source": peak_kind,
+                "traffic": None,
+                "phases_gbs": {k: round(v[1], 1) for k, v in phases.items()}}
+
+    result = {
+        "metric": METRIC, "value": round(value, 2), "unit": "M ops/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic (seeded PCG64; shapes of the at-scale LSM configuration)",
+        "config": {"workload": f"{args.workload}: " + w.name, "global_batch": upd_keys * world,
+                   "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (no flush)",
+                   "value_definition": "(updated keys + lookups + range queries) per step / step time",
+                   "scale": args.scale},
+        "parts": {
+            "insert_mkeys_s": round(upd_keys / (upd * 1e-3) / 1e6, 1),
+            "lookup_mops_s": round(nq / (look * 1e-3) / 1e6, 1),
+            "range_mqueries_s": round(nr / (rng_ms * 1e-3) / 1e6, 2),
+            "range_pairs_per_step": total_pairs,
+            "update_ms": round(upd, 3), "lookup_ms": round(look, 3), "range_ms": round(rng_ms, 3),
+            "insert_batch_ms_p50": round(float(np.percentile(ins_lat, 50)), 4),
+            "insert_batch_ms_p99": round(float(np.percentile(ins_lat, 99)), 4),
+        },
+        "roofline": roofline,
+        "gpu_launches": int(launches),
+        "clocks": clocks.summary(),
+    }
+
+    if not args.no_e2e:
+        result["e2e"] = e2e_ours(args, gl, w, dev, total_pairs, max_el)
+    if rank == 0 and not args.no_cpu:
+        result["cpu_baseline"] = cpu_baseline(args, W)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+
+
+def e2e_ours(args, gl, w, dev, total_pairs, max_el):
+    """Same step through the public API with HOST buffers: every step copies
+    its inputs from pinned host memory and reads every result back."""
+    import torch
+
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.int32)).pin_memory()  # noqa: E731
+    host_ops = [(o[0], pin(o[1]), pin(o[2]) if o[0] == "insert" else None) for o in w.ops]
+    hq, hlo, hhi = pin(w.lookups), pin(w.range_lo), pin(w.range_hi)
+    nq, nr = w.lookups.size, w.range_lo.size
+    h_out_v = torch.empty(nq, dtype=torch.int32).pin_memory()
+    h_out_f = torch.empty(nq, dtype=torch.uint8).pin_memory()
+    h_off = torch.empty(nr + 1, dtype=torch.int64).pin_memory()
+    h_pk = torch.empty(max(total_pairs, 1), dtype=torch.int32).pin_memory()
+    h_pv = torch.empty(max(total_pairs, 1), dtype=torch.int32).pin_memory()
+    d = gl.GPULSMOpt(gl.DictionaryConfig(max_elements=max_el))
+    dk = [(o[0], torch.empty_like(o[1], device=dev), torch.empty_like(o[2], device=dev) if o[2] is not None else None)
+          for o in host_ops]
+    q = torch.empty(nq, dtype=torch.int32, device=dev)
+    lo = torch.empty(nr, dtype=torch.int32, device=dev)
+    hi = torch.empty(nr, dtype=torch.int32, device=dev)
+    ov = torch.empty(nq, dtype=torch.int32, device=dev)
+    of = torch.empty(nq, dtype=torch.uint8, device=dev)
+    off = torch.empty(nr + 1, dtype=torch.int64, device=dev)
+    pk = torch.empty(max(total_pairs, 1), dtype=torch.int32, device=dev)
+    pv = torch.empty(max(total_pairs, 1), dtype=torch.int32, device=dev)
+    h2d = sum(o[1].numel() * 4 + (o[2].numel() * 4 if o[2] is not None else 0) for o in host_ops) + (nq + 2 * nr) * 4
+    d2h = nq * 5 + (nr + 1) * 8 + total_pairs * 8
+
+    def step():
+        d.clear()
+        for (kind, hk, hv), (_, gk, gv) in zip(host_ops, dk):
+            gk.copy_(hk, non_blocking=True)
+            if kind == "insert":
+                gv.copy_(hv, non_blocking=True)
+                d.insert(gk, gv)
+            else:
+                d.erase(gk)
+        q.copy_(hq, non_blocking=True)
+        d.lookup(q, ov, of)
+        h_out_v.copy_(ov, non_blocking=True)
+        h_out_f.copy_(of, non_blocking=True)
+        lo.copy_(hlo, non_blocking=True)
+        hi.copy_(hhi, non_blocking=True)
+        d.range_offsets(lo, hi, off)
+        d.range_pairs(lo, hi, off, pk, pv)
+        h_off.copy_(off, non_blocking=True)
+        h_pk[:total_pairs].copy_(pk[:total_pairs], non_blocking=True)
+        h_pv[:total_pairs].copy_(pv[:total_pairs], non_blocking=True)
+
+    steps = max(1, min(args.steps, 3))
+    step()
+    torch.cuda.synchronize(dev)
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(steps):
+        step()
+    e.record()
+    torch.cuda.synchronize(dev)
+    ms = s.elapsed_time(e) / steps
+    ops = w.inserted_keys + w.erased_keys + nq + nr
+    d.close()
+    return {"value": round(ops / (ms * 1e-3) / 1e6, 2), "unit": "M ops/s", "ms_per_step": round(ms, 3),
+            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": steps}
+
+
+def cpu_baseline(args, W, threads: int = 1, scale_extra: int = 4):
+    """The oracle on a bounded sample of the workload (1/16 of every size)."""
+    from oracle import OracleLSM, oracle_threads
+
+    used = oracle_threads(threads)
+    w = W.lsm_scale(args.scale + scale_extra) if args.workload == "lsm_scale" else W.lsm_small(args.scale + 2)
+    o = OracleLSM()
+    t = time.perf_counter()
+    for op in w.ops:
+        o.insert(op[1], op[2]) if op[0] == "insert" else o.erase(op[1])
+    o.lookup(w.lookups, with_found=True)
+    if w.range_kind == "pairs":
+        o.range_pairs(w.range_lo, w.range_hi)
+    else:
+        o.range_count(w.range_lo, w.range_hi)
+    dt = time.perf_counter() - t
+    ops = w.inserted_keys + w.erased_keys + w.lookups.size + w.range_lo.size
+    return {"value": round(ops / dt / 1e6, 3), "unit": "M ops/s", "cores": used, "kind": "port",
+            "sample": f"same workload shape at 1/{1 << (args.scale + scale_extra)} of every size, one pass, "
+                      f"{dt:.1f} s"}
+
+
+def run_reference(args):
+    """CPU implementation of the path (the oracle restatement on every host core)."""
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from oracle import OracleLSM, oracle_threads
+
+    W = importlib.import_module("gpu-lsm-tree_b200.workloads")
+    used = oracle_threads(0)
+    extra = 2
+    w = W.lsm_scale(args.scale + extra) if args.workload == "lsm_scale" else W.lsm_small(args.scale)
+
+    def step():
+        o = OracleLSM()
+        for op in w.ops:
+            o.insert(op[1], op[2]) if op[0] == "insert" else o.erase(op[1])
+        o.lookup(w.lookups, with_found=True)
+        if w.range_kind == "pairs":
+            o.range_pairs(w.range_lo, w.range_hi)
+        else:
+            o.range_count(w.range_lo, w.range_hi)
+
+    for _ in range(args.warmup):
+        step()
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = (time.perf_counter() - t) / args.steps
+    ops = w.inserted_keys + w.erased_keys + w.lookups.size + w.range_lo.size
+    value = ops / dt / 1e6
+    sample = (f"{args.workload} shape at 1/{1 << (args.scale + extra)} of every size per step "
+              f"(oracle: sorted-array restatement, OpenMP)")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "M ops/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": args.workload, "parallelism": "cpu", "sample": sample},
+        "cpu_baseline": {"value": round(value, 3), "unit": "M ops/s", "cores": used, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": round(value, 3), "unit": "M ops/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+if __name__ == "__main__":
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)

@@ -11,6 +11,7 @@ from . import _native  # noqa: F401
 from ._native import (CapacityError, CudaError, DeviceTimeout, GpuLsmError, InvalidArgument,  # noqa: F401
                       LengthError, OutOfDeviceMemory, PublicationError, load)
 from .dictionary import DictionaryConfig, GPULSMOpt, GpuLsmOptIndex, sort_pairs  # noqa: F401
+from .flix import FlixIndex  # noqa: F401
 
 
 def build(force: bool = False) -> str:

@@ -127,6 +127,7 @@ def load() -> C.CDLL:
     sig = {
         "gpulsm_last_error": (C.c_char_p, []),
         "gpulsm_version": (C.c_char_p, []),
+        "gpulsm_launch_count": (C.c_uint64, []),
         "gpulsm_dict_create": (i32, [C.POINTER(DictConfig), pvp]),
         "gpulsm_dict_destroy": (i32, [vp]),
         "gpulsm_dict_clear": (i32, [vp, vp]),

@@ -60,12 +60,34 @@ inline cudaStream_t S(void *s) { return static_cast<cudaStream_t>(s); }
 template <class T> void need(T *p, const char *what) {
   if (!p) throw std::invalid_argument(std::string("null ") + what);
 }
+
+// Rejects a non-null pointer the GPU cannot dereference (pageable host memory,
+// an integer passed in a pointer slot) before any kernel can touch it, so a
+// caller mistake becomes GPULSM_ERR_INVALID_ARGUMENT instead of a device fault.
+// Null pointers are left to the engines' own argument checks.
+void device_accessible(const void *p, const char *what) {
+  if (!p) return;
+  cudaPointerAttributes a{};
+  const cudaError_t e = cudaPointerGetAttributes(&a, p);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    throw std::invalid_argument(std::string(what) + " is not a CUDA pointer");
+  }
+  if (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) return;
+  if (a.type == cudaMemoryTypeHost && a.devicePointer) return;  // mapped pinned host memory
+  throw std::invalid_argument(std::string(what) + " is not device-accessible memory");
+}
+
+void device_accessible(std::initializer_list<std::pair<const void *, const char *>> ptrs) {
+  for (const auto &p : ptrs) device_accessible(p.first, p.second);
+}
 }  // namespace
 
 extern "C" {
 
 const char *gpulsm_last_error(void) { return g_error.c_str(); }
 const char *gpulsm_version(void) { return "gpulsm-b200 0.1 (sm_100a)"; }
+uint64_t gpulsm_launch_count(void) { return gpulsm::launch_counter().load(); }
 
 // ---------------------------------------------------------------- LSM dictionary
 int gpulsm_dict_create(const gpulsm_dict_config *config, gpulsm_dict **out) {
@@ -98,6 +120,7 @@ int gpulsm_dict_bulk_build(gpulsm_dict *d, const uint32_t *keys, const uint32_t 
                            uint64_t count, void *stream) {
   return guarded([&] {
     need(d, "dict");
+    device_accessible({{keys, "keys"}, {values, "values"}});
     d->impl.bulk_build(keys, values, count, S(stream));
   });
 }
@@ -106,6 +129,7 @@ int gpulsm_dict_insert(gpulsm_dict *d, const uint32_t *keys, const uint32_t *val
                        uint64_t count, void *stream) {
   return guarded([&] {
     need(d, "dict");
+    device_accessible({{keys, "keys"}, {values, "values"}});
     d->impl.insert(keys, values, count, S(stream));
   });
 }
@@ -113,6 +137,7 @@ int gpulsm_dict_insert(gpulsm_dict *d, const uint32_t *keys, const uint32_t *val
 int gpulsm_dict_erase(gpulsm_dict *d, const uint32_t *keys, uint64_t count, void *stream) {
   return guarded([&] {
     need(d, "dict");
+    device_accessible({{keys, "keys"}});
     d->impl.erase(keys, count, S(stream));
   });
 }
@@ -121,6 +146,7 @@ int gpulsm_dict_lookup(gpulsm_dict *d, const uint32_t *queries, uint64_t count,
                        uint32_t *out_values, uint8_t *out_found, void *stream) {
   return guarded([&] {
     need(d, "dict");
+    device_accessible({{queries, "queries"}, {out_values, "out_values"}, {out_found, "out_found"}});
     d->impl.lookup(queries, count, out_values, out_found, S(stream));
   });
 }
@@ -129,6 +155,7 @@ int gpulsm_dict_range_sum(gpulsm_dict *d, const uint32_t *lo, const uint32_t *hi
                           uint32_t *out_sums, void *stream) {
   return guarded([&] {
     need(d, "dict");
+    device_accessible({{lo, "lo"}, {hi, "hi"}, {out_sums, "out_sums"}});
     d->impl.range_sum(lo, hi, count, out_sums, S(stream));
   });
 }
@@ -137,6 +164,7 @@ int gpulsm_dict_range_count(gpulsm_dict *d, const uint32_t *lo, const uint32_t *
                             uint64_t count, uint32_t *out_counts, void *stream) {
   return guarded([&] {
     need(d, "dict");
+    device_accessible({{lo, "lo"}, {hi, "hi"}, {out_counts, "out_counts"}});
     d->impl.range_count(lo, hi, count, out_counts, S(stream));
   });
 }
@@ -145,6 +173,7 @@ int gpulsm_dict_range_offsets(gpulsm_dict *d, const uint32_t *lo, const uint32_t
                               uint64_t count, uint64_t *offsets, void *stream) {
   return guarded([&] {
     need(d, "dict");
+    device_accessible({{lo, "lo"}, {hi, "hi"}, {offsets, "offsets"}});
     d->impl.range_offsets(lo, hi, count, offsets, S(stream));
   });
 }
@@ -154,6 +183,7 @@ int gpulsm_dict_range_pairs(gpulsm_dict *d, const uint32_t *lo, const uint32_t *
                             uint32_t *out_values, void *stream) {
   return guarded([&] {
     need(d, "dict");
+    device_accessible({{lo, "lo"}, {hi, "hi"}, {offsets, "offsets"}, {out_keys, "out_keys"}, {out_values, "out_values"}});
     d->impl.range_pairs(lo, hi, count, offsets, out_keys, out_values, S(stream));
   });
 }
@@ -162,6 +192,7 @@ int gpulsm_dict_successor(gpulsm_dict *d, const uint32_t *queries, uint64_t coun
                           uint32_t *out_keys, void *stream) {
   return guarded([&] {
     need(d, "dict");
+    device_accessible({{queries, "queries"}, {out_keys, "out_keys"}});
     d->impl.successor(queries, count, out_keys, S(stream));
   });
 }
@@ -212,6 +243,7 @@ int gpulsm_flix_build(gpulsm_flix *f, const void *keys, const uint32_t *values, 
                       uint64_t max_count, void *stream) {
   return guarded([&] {
     need(f, "index");
+    device_accessible({{keys, "keys"}, {values, "values"}});
     f->impl.build(keys, values, count, max_count, S(stream));
   });
 }
@@ -220,6 +252,7 @@ int gpulsm_flix_insert(gpulsm_flix *f, const void *keys, const uint32_t *values,
                        void *stream) {
   return guarded([&] {
     need(f, "index");
+    device_accessible({{keys, "keys"}, {values, "values"}});
     f->impl.insert(keys, values, count, S(stream));
   });
 }
@@ -227,6 +260,7 @@ int gpulsm_flix_insert(gpulsm_flix *f, const void *keys, const uint32_t *values,
 int gpulsm_flix_remove(gpulsm_flix *f, const void *keys, uint64_t count, void *stream) {
   return guarded([&] {
     need(f, "index");
+    device_accessible({{keys, "keys"}});
     f->impl.remove(keys, count, S(stream));
   });
 }
@@ -235,6 +269,7 @@ int gpulsm_flix_lookups_ordered(gpulsm_flix *f, const void *sorted_probes, uint6
                                 uint32_t *out_values, void *stream) {
   return guarded([&] {
     need(f, "index");
+    device_accessible({{sorted_probes, "probes"}, {out_values, "out_values"}});
     f->impl.lookups_ordered(sorted_probes, count, out_values, S(stream));
   });
 }
@@ -243,6 +278,7 @@ int gpulsm_flix_lookups_successor(gpulsm_flix *f, const void *sorted_probes, uin
                                   void *out_keys, void *stream) {
   return guarded([&] {
     need(f, "index");
+    device_accessible({{sorted_probes, "probes"}, {out_keys, "out_keys"}});
     f->impl.lookups_successor(sorted_probes, count, out_keys, S(stream));
   });
 }
@@ -251,6 +287,7 @@ int gpulsm_flix_lookup(gpulsm_flix *f, const void *probes, uint64_t count, uint3
                        void *stream) {
   return guarded([&] {
     need(f, "index");
+    device_accessible({{probes, "probes"}, {out_values, "out_values"}});
     f->impl.lookup(probes, count, out_values, S(stream));
   });
 }
@@ -259,6 +296,7 @@ int gpulsm_flix_successor(gpulsm_flix *f, const void *probes, uint64_t count, vo
                           void *stream) {
   return guarded([&] {
     need(f, "index");
+    device_accessible({{probes, "probes"}, {out_keys, "out_keys"}});
     f->impl.successor(probes, count, out_keys, S(stream));
   });
 }
@@ -306,6 +344,7 @@ int gpulsm_sort_pairs(const void *keys_in, const uint32_t *values_in, void *keys
     need(keys_in, "keys_in");
     need(keys_out, "keys_out");
     if (values_in) need(values_out, "values_out");
+    device_accessible({{keys_in, "keys_in"}, {values_in, "values_in"}, {keys_out, "keys_out"}, {values_out, "values_out"}});
     gpulsm::sort_pairs_any(keys_in, values_in, keys_out, values_out, count, key_bits, begin_bit,
                            end_bit, S(stream));
   });

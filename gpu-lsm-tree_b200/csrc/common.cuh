@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <stdexcept>
 #include <string>
@@ -41,6 +42,14 @@ struct CudaError : std::runtime_error {
       throw ::gpulsm::CudaError(e__, std::string(__FILE__) + ":" +               \
                                          std::to_string(__LINE__));              \
   } while (false)
+
+// Number of kernels this library has launched (all devices, all handles);
+// read through gpulsm_launch_count() to attribute work to our own kernels.
+inline std::atomic<unsigned long long> &launch_counter() {
+  static std::atomic<unsigned long long> c{0};
+  return c;
+}
+inline void note_launch() { launch_counter().fetch_add(1, std::memory_order_relaxed); }
 
 inline unsigned grid_for(uint64_t n, unsigned threads) {
   const uint64_t g = (n + threads - 1) / threads;

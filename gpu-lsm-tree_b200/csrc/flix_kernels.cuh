@@ -1,0 +1,638 @@
+// Kernels of the FliX-style bucket layer (32- or 64-bit keys, u32 values).
+//
+// HBM layout.  A node is one 16-byte aligned record:
+//   keys[32]  sorted ascending in slots [0, count)
+//   vals[32]  u32 value of each key (FliX "offset")
+//   max       largest key this node covers: node i of a chain covers
+//             (previous node's max, max]; the last node of bucket b covers up
+//             to bmax[b]
+//   count     live entries
+//   next      index of the next node of the chain, kNone at the end
+// Node<u64> is 400 bytes, the stride of FliX's node_size 32 layout
+// (FliX/definitions_updates.cuh:259-329); a warp loads the 32 keys of a node
+// with one coalesced 256-byte read (lane j holds slot j).
+// nodes[0, B) are the bucket heads in key order; nodes[B, cap) form the
+// allocation region for split nodes (FliX/tile_utils.cuh:306-392).
+// bmax[b] is the fixed upper key of bucket b (FliX maxvalues,
+// FliX/impl_cg_rtx_index_updates.cuh:208-238); bucket b covers
+// (bmax[b-1], bmax[b]] and bmax[B-1] is the largest key value.
+//
+// Every update/query batch is sorted first; a batch is split into runs of
+// keys that fall into the same bucket and ONE warp owns a run, so a chain is
+// only ever touched by one warp (the tile-per-bucket rule of
+// FliX/coarse_granular_inserts_tiles.cuh:571-643) - no locks, no atomics on
+// nodes.
+#pragma once
+
+#include "common.cuh"
+
+namespace gpulsm {
+namespace flix {
+
+constexpr uint32_t kNodeSize = 32;
+constexpr uint32_t kNone = 0xffffffffu;
+
+template <typename K>
+struct alignas(16) Node {
+  K keys[kNodeSize];
+  uint32_t vals[kNodeSize];
+  K max;
+  uint32_t count;
+  uint32_t next;
+};
+static_assert(sizeof(Node<unsigned long long>) == 400, "u64 node stride");
+
+template <typename K>
+__host__ __device__ constexpr K key_max() {
+  return ~K(0);
+}
+
+// not_found cast to the key type (FliX/coarse_granular_lookups_tile_bulk.cuh:672,917,946)
+template <typename K>
+__host__ __device__ constexpr K successor_miss() {
+  return K(0xffffffffu);
+}
+
+struct Run {
+  uint32_t bucket;
+  uint32_t start;
+};
+
+struct PoolView {
+  uint32_t *alloc_top;   // next free node index (bump)
+  uint32_t capacity;     // total nodes (heads + region)
+  uint32_t *status;
+};
+
+// ---------------------------------------------------------------------------
+// build: lay sorted unique (key, value) pairs into bucket heads at `fill`
+// entries per node (FliX/impl_cg_rtx_index_updates.cuh:443-528).
+template <typename K>
+__global__ void build_layout_kernel(const K *__restrict__ keys, const uint32_t *__restrict__ vals,
+                                    uint64_t n, uint32_t fill, uint32_t buckets,
+                                    Node<K> *__restrict__ nodes, K *__restrict__ bmax) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t b = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  if (b >= buckets) return;
+  Node<K> *node = nodes + b;
+  const uint64_t first = b * fill;
+  const uint64_t idx = first + lane;
+  const bool has = lane < fill && idx < n;
+  node->keys[lane] = has ? keys[idx] : K(0);
+  node->vals[lane] = has ? (vals ? vals[idx] : uint32_t(idx)) : 0u;
+  if (lane == 0) {
+    const uint64_t end = first + fill < n ? first + fill : n;
+    const uint32_t count = first < n ? uint32_t(end - first) : 0u;
+    const K mx = (b + 1 == buckets) ? key_max<K>() : keys[end - 1];
+    node->max = mx;
+    node->count = count;
+    node->next = kNone;
+    bmax[b] = mx;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// bucket of a key: first b with bmax[b] >= key
+template <typename K>
+__device__ __forceinline__ uint32_t bucket_of(const K *__restrict__ bmax, uint32_t buckets, K key) {
+  uint32_t lo = 0, hi = buckets - 1;  // bmax[buckets-1] is key_max, always >= key
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (bmax[mid] < key) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Routes a sorted key list to buckets and emits one Run per maximal group of
+// consecutive keys in the same bucket (compacted with decoupled look-back).
+constexpr int kRouteThreads = 256;
+constexpr int kRouteItems = 8;
+constexpr uint32_t kRouteTile = kRouteThreads * kRouteItems;
+
+constexpr unsigned long long kLbAgg = 1ull << 62;
+constexpr unsigned long long kLbInc = 2ull << 62;
+constexpr unsigned long long kLbMask = (1ull << 62) - 1ull;
+
+__device__ __forceinline__ unsigned long long lookback(unsigned long long *lb, uint32_t tile,
+                                                       unsigned long long agg, uint32_t *status) {
+  if (tile == 0) {
+    st_relaxed_u64(lb, kLbInc | agg);
+    return 0ull;
+  }
+  st_relaxed_u64(lb + tile, kLbAgg | agg);
+  unsigned long long excl = 0;
+  int64_t t = int64_t(tile) - 1;
+  uint32_t spins = 0;
+  while (t >= 0) {
+    const unsigned long long v = ld_relaxed_u64(lb + t);
+    const unsigned long long flag = v & ~kLbMask;
+    if (flag == 0ull) {
+      if (++spins > kMaxSpins) {
+        atomicOr(status, kDevWaitTimeout);
+        break;
+      }
+      continue;
+    }
+    excl += v & kLbMask;
+    if (flag == kLbInc) break;
+    --t;
+  }
+  st_relaxed_u64(lb + tile, kLbInc | (excl + agg));
+  return excl;
+}
+
+template <typename K>
+__global__ void __launch_bounds__(kRouteThreads) route_runs_kernel(
+    const K *__restrict__ keys, const uint32_t *__restrict__ n_ptr, const K *__restrict__ bmax,
+    uint32_t buckets, Run *__restrict__ runs, uint32_t *__restrict__ run_count,
+    unsigned long long *__restrict__ lb, uint32_t *__restrict__ tile_counter,
+    uint32_t *__restrict__ status) {
+  const uint32_t n = *n_ptr;
+  __shared__ uint32_t s_scan[kRouteThreads / 32];
+  __shared__ uint32_t s_total;
+  __shared__ uint32_t s_tile;
+  __shared__ unsigned long long s_base;
+  __shared__ uint32_t s_prev_bucket;
+  if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
+  __syncthreads();
+  const uint32_t tile = s_tile;
+  const uint64_t base = uint64_t(tile) * kRouteTile;
+  if (base >= n && !(tile == 0 && n == 0)) return;  // grid sized for an upper bound
+  if (threadIdx.x == 0)
+    s_prev_bucket = (base > 0 && base <= n) ? bucket_of(bmax, buckets, keys[base - 1]) : kNone;
+  __syncthreads();
+  const uint64_t mine = base + uint64_t(threadIdx.x) * kRouteItems;
+  uint32_t bk[kRouteItems];
+  uint32_t starts = 0, cnt = 0;
+#pragma unroll
+  for (int i = 0; i < kRouteItems; ++i) {
+    const uint64_t g = mine + i;
+    bk[i] = g < n ? bucket_of(bmax, buckets, keys[g]) : kNone;
+  }
+  // previous key's bucket for item 0 of this thread
+  uint32_t prev = __shfl_up_sync(0xffffffffu, bk[kRouteItems - 1], 1);
+  if ((threadIdx.x & 31) == 0) prev = kNone;
+  __shared__ uint32_t s_last[kRouteThreads / 32];
+  if ((threadIdx.x & 31) == 31) s_last[threadIdx.x >> 5] = bk[kRouteItems - 1];
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) prev = (threadIdx.x == 0) ? s_prev_bucket : s_last[(threadIdx.x >> 5) - 1];
+#pragma unroll
+  for (int i = 0; i < kRouteItems; ++i) {
+    const uint64_t g = mine + i;
+    const uint32_t p = i == 0 ? prev : bk[i - 1];
+    if (g < n && bk[i] != p) {
+      starts |= 1u << i;
+      ++cnt;
+    }
+  }
+  const uint32_t local = block_exclusive_scan<kRouteThreads>(cnt, s_scan, &s_total);
+  if (threadIdx.x == 0) s_base = lookback(lb, tile, s_total, status);
+  __syncthreads();
+  uint64_t o = s_base + local;
+#pragma unroll
+  for (int i = 0; i < kRouteItems; ++i)
+    if (starts & (1u << i)) {
+      if (o < n) runs[o] = Run{bk[i], uint32_t(mine + i)};  // o < n unless a wait timed out
+      ++o;
+    }
+  if (base + kRouteTile >= n && threadIdx.x == 0) *run_count = uint32_t(min(s_base + s_total, (unsigned long long)n));
+}
+
+// ---------------------------------------------------------------------------
+// Warp-resident node: lane j holds slot j.
+template <typename K>
+struct WarpNode {
+  uint32_t id;
+  K key;
+  uint32_t val;
+  K max;
+  uint32_t count;
+  uint32_t next;
+};
+
+template <typename K>
+__device__ __forceinline__ void load_node(const Node<K> *nodes, uint32_t id, uint32_t lane,
+                                          WarpNode<K> &w) {
+  const Node<K> *p = nodes + id;
+  w.id = id;
+  w.key = p->keys[lane];
+  w.val = p->vals[lane];
+  w.max = p->max;
+  w.count = p->count;
+  w.next = p->next;
+}
+
+template <typename K>
+__device__ __forceinline__ void store_node(Node<K> *nodes, uint32_t lane, const WarpNode<K> &w) {
+  Node<K> *p = nodes + w.id;
+  if (lane < w.count) {
+    p->keys[lane] = w.key;
+    p->vals[lane] = w.val;
+  }
+  if (lane == 0) {
+    p->count = w.count;
+    p->max = w.max;
+    p->next = w.next;
+  }
+}
+
+__device__ __forceinline__ uint32_t run_end(const Run *runs, uint32_t r, uint32_t run_count, uint32_t n) {
+  return r + 1 < run_count ? runs[r + 1].start : n;
+}
+
+// Insert if absent (FliX/coarse_granular_inserts_tiles_bulk.cuh:1307-1602):
+// the run's keys are sorted and unique; an existing key keeps its value.  A
+// full node splits: the lower half keeps 16 entries, the upper half moves to
+// a fresh node linked after it (FliX/tile_utils.cuh:306-392).  An exhausted
+// allocation region sets kDevOutputOverflow and the key is reported, not
+// silently dropped.
+template <typename K>
+__global__ void __launch_bounds__(256) insert_runs_kernel(
+    const K *__restrict__ keys, const uint32_t *__restrict__ vals, const uint32_t *__restrict__ n_ptr,
+    const Run *__restrict__ runs, const uint32_t *__restrict__ run_count_ptr, Node<K> *nodes,
+    PoolView pool, unsigned long long *__restrict__ inserted) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t n = *n_ptr;
+  const uint32_t r = (uint32_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t run_count = *run_count_ptr;
+  if (r >= run_count) return;
+  const Run run = runs[r];
+  const uint32_t end = run_end(runs, r, run_count, n);
+  WarpNode<K> w;
+  load_node(nodes, run.bucket, lane, w);
+  bool dirty = false;
+  uint32_t added = 0;
+  for (uint32_t i = run.start; i < end; ++i) {
+    const K k = keys[i];
+    const uint32_t v = vals[i];
+    while (k > w.max && w.next != kNone) {
+      if (dirty) store_node(nodes, lane, w);
+      dirty = false;
+      load_node(nodes, w.next, lane, w);
+    }
+    if (k > w.max) {  // chain ends below the key: broken invariant, report and skip
+      if (lane == 0) atomicOr(pool.status, kDevBadInput);
+      continue;
+    }
+    if (__ballot_sync(0xffffffffu, lane < w.count && w.key == k)) continue;  // present: keep
+    if (w.count == kNodeSize) {
+      uint32_t fresh = 0;
+      if (lane == 0) fresh = atomicAdd(pool.alloc_top, 1u);
+      fresh = __shfl_sync(0xffffffffu, fresh, 0);
+      if (fresh >= pool.capacity) {
+        if (lane == 0) atomicOr(pool.status, kDevOutputOverflow);
+        continue;
+      }
+      constexpr uint32_t half = kNodeSize / 2;
+      const K lower_max = __shfl_sync(0xffffffffu, w.key, half - 1);
+      // upper half -> fresh node (slots 0..15)
+      WarpNode<K> up;
+      up.id = fresh;
+      up.key = __shfl_down_sync(0xffffffffu, w.key, half);
+      up.val = __shfl_down_sync(0xffffffffu, w.val, half);
+      up.max = w.max;
+      up.count = kNodeSize - half;
+      up.next = w.next;
+      w.max = lower_max;
+      w.count = half;
+      w.next = fresh;
+      if (k > lower_max) {
+        store_node(nodes, lane, w);
+        w = up;
+      } else {
+        store_node(nodes, lane, up);
+      }
+      dirty = true;
+    }
+    const uint32_t pos = __popc(__ballot_sync(0xffffffffu, lane < w.count && w.key < k));
+    const K sk = __shfl_up_sync(0xffffffffu, w.key, 1);
+    const uint32_t sv = __shfl_up_sync(0xffffffffu, w.val, 1);
+    if (lane > pos && lane <= w.count) {
+      w.key = sk;
+      w.val = sv;
+    }
+    if (lane == pos) {
+      w.key = k;
+      w.val = v;
+    }
+    ++w.count;
+    ++added;
+    dirty = true;
+  }
+  if (dirty) store_node(nodes, lane, w);
+  if (lane == 0 && added) atomicAdd(inserted, (unsigned long long)added);
+}
+
+// Physical delete (FliX/coarse_granular_deletes_tiles.cuh:1128-1320): matches
+// are removed and survivors compacted left; an emptied non-head node is
+// unlinked from its chain (its range passes to its neighbour).
+template <typename K>
+__global__ void __launch_bounds__(256) delete_runs_kernel(
+    const K *__restrict__ keys, const uint32_t *__restrict__ n_ptr, const Run *__restrict__ runs,
+    const uint32_t *__restrict__ run_count_ptr, Node<K> *nodes,
+    unsigned long long *__restrict__ removed) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t n = *n_ptr;
+  const uint32_t r = (uint32_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t run_count = *run_count_ptr;
+  if (r >= run_count) return;
+  const Run run = runs[r];
+  const uint32_t end = run_end(runs, r, run_count, n);
+  WarpNode<K> w;
+  load_node(nodes, run.bucket, lane, w);
+  uint32_t prev = kNone;
+  bool dirty = false;
+  uint32_t gone = 0;
+  auto flush = [&]() {
+    if (!dirty) return;
+    if (w.count == 0 && prev != kNone) {
+      // unlink the emptied node; the predecessor inherits its key range
+      if (lane == 0) {
+        nodes[prev].next = w.next;
+        if (w.next == kNone) nodes[prev].max = w.max;
+      }
+    } else {
+      store_node(nodes, lane, w);
+    }
+    dirty = false;
+  };
+  for (uint32_t i = run.start; i < end; ++i) {
+    const K k = keys[i];
+    while (k > w.max && w.next != kNone) {
+      const bool unlinked = dirty && w.count == 0 && prev != kNone;
+      flush();
+      if (!unlinked) prev = w.id;
+      load_node(nodes, w.next, lane, w);
+    }
+    const uint32_t match = __ballot_sync(0xffffffffu, lane < w.count && w.key == k);
+    if (!match) continue;
+    const uint32_t p = __ffs(match) - 1;
+    const K sk = __shfl_down_sync(0xffffffffu, w.key, 1);
+    const uint32_t sv = __shfl_down_sync(0xffffffffu, w.val, 1);
+    if (lane >= p && lane + 1 < w.count) {
+      w.key = sk;
+      w.val = sv;
+    }
+    --w.count;
+    ++gone;
+    dirty = true;
+  }
+  flush();
+  if (lane == 0 && gone) atomicAdd(removed, (unsigned long long)gone);
+}
+
+// Ordered lookup (FliX/coarse_granular_lookups_tile_bulk.cuh:312-470): value
+// or not_found per probe; results go to out[perm ? perm[i] : i].
+template <typename K>
+__global__ void __launch_bounds__(256) lookup_runs_kernel(
+    const K *__restrict__ probes, const uint32_t *__restrict__ n_ptr, const Run *__restrict__ runs,
+    const uint32_t *__restrict__ run_count_ptr, const Node<K> *__restrict__ nodes,
+    const uint32_t *__restrict__ perm, uint32_t *__restrict__ out) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t n = *n_ptr;
+  const uint32_t r = (uint32_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t run_count = *run_count_ptr;
+  if (r >= run_count) return;
+  const Run run = runs[r];
+  const uint32_t end = run_end(runs, r, run_count, n);
+  WarpNode<K> w;
+  load_node(nodes, run.bucket, lane, w);
+  for (uint32_t base = run.start; base < end; base += 32) {
+    // lanes take 32 consecutive probes; the node walk is shared (probes sorted)
+    const uint32_t i = base + lane;
+    const K k = i < end ? probes[i] : K(0);
+    uint32_t result = kNotFound;
+    uint32_t pending = __ballot_sync(0xffffffffu, i < end);
+    while (pending) {
+      // lanes whose probe is covered by the current node resolve now
+      const bool here = (pending >> lane & 1u) && k <= w.max;
+      uint32_t todo = __ballot_sync(0xffffffffu, here);
+      while (todo) {
+        const uint32_t src = __ffs(todo) - 1;
+        const K kk = __shfl_sync(0xffffffffu, k, src);
+        const uint32_t m = __ballot_sync(0xffffffffu, lane < w.count && w.key == kk);
+        const uint32_t v = __shfl_sync(0xffffffffu, w.val, m ? __ffs(m) - 1 : 0);
+        if (lane == src) result = m ? v : kNotFound;
+        todo &= todo - 1;
+      }
+      pending &= ~__ballot_sync(0xffffffffu, here);
+      if (pending && w.next == kNone) break;  // chain covers every routed probe; defensive
+      if (pending) load_node(nodes, w.next, lane, w);
+    }
+    if (i < end) out[perm ? perm[i] : i] = result;
+  }
+}
+
+// First stored key >= k in bucket b or any later bucket.
+template <typename K>
+__device__ K first_key_from_bucket(const Node<K> *nodes, uint32_t b, uint32_t buckets) {
+  for (; b < buckets; ++b) {
+    uint32_t id = b;
+    while (id != kNone) {
+      const Node<K> *p = nodes + id;
+      if (p->count) return p->keys[0];
+      id = p->next;
+    }
+  }
+  return successor_miss<K>();
+}
+
+// Ordered successor (FliX/coarse_granular_lookups_tile_bulk.cuh:630-972).
+template <typename K>
+__global__ void __launch_bounds__(256) successor_runs_kernel(
+    const K *__restrict__ probes, const uint32_t *__restrict__ n_ptr, const Run *__restrict__ runs,
+    const uint32_t *__restrict__ run_count_ptr, const Node<K> *__restrict__ nodes,
+    uint32_t buckets, const uint32_t *__restrict__ perm, K *__restrict__ out) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t n = *n_ptr;
+  const uint32_t r = (uint32_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t run_count = *run_count_ptr;
+  if (r >= run_count) return;
+  const Run run = runs[r];
+  const uint32_t end = run_end(runs, r, run_count, n);
+  WarpNode<K> w;
+  load_node(nodes, run.bucket, lane, w);
+  bool next_known = false;
+  K next_first = successor_miss<K>();
+  bool chain_done = false;
+  for (uint32_t i = run.start; i < end; ++i) {
+    const K k = probes[i];
+    K result;
+    while (true) {
+      if (!chain_done) {
+        while (k > w.max && w.next != kNone) load_node(nodes, w.next, lane, w);
+        const uint32_t c = __ballot_sync(0xffffffffu, lane < w.count && w.key >= k);
+        if (c) {
+          result = __shfl_sync(0xffffffffu, w.key, __ffs(c) - 1);
+          break;
+        }
+        if (w.next != kNone) {
+          load_node(nodes, w.next, lane, w);
+          continue;
+        }
+        chain_done = true;  // nothing >= k left in this bucket
+      }
+      if (!next_known) {
+        if (lane == 0) next_first = first_key_from_bucket(nodes, run.bucket + 1, buckets);
+        next_first = __shfl_sync(0xffffffffu, next_first, 0);
+        next_known = true;
+      }
+      result = next_first;
+      break;
+    }
+    if (lane == 0) out[perm ? perm[i] : i] = result;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// helpers for sorting / dedup of batches
+template <typename K>
+__global__ void set_u32_kernel(uint32_t *__restrict__ p, uint32_t v) {
+  *p = v;
+}
+
+template <typename K>
+__global__ void iota_kernel(uint32_t *__restrict__ v, uint32_t n) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) v[i] = i;
+}
+
+// keep the FIRST of each run of equal keys (insert-if-absent in input order)
+constexpr int kDedupThreads = 256;
+constexpr int kDedupItems = 8;
+constexpr uint32_t kDedupTile = kDedupThreads * kDedupItems;
+
+template <typename K>
+__global__ void __launch_bounds__(kDedupThreads) dedup_first_kernel(
+    const K *__restrict__ kin, const uint32_t *__restrict__ vin, uint32_t n, K *__restrict__ kout,
+    uint32_t *__restrict__ vout, uint32_t *__restrict__ out_n, unsigned long long *__restrict__ lb,
+    uint32_t *__restrict__ tile_counter, uint32_t *__restrict__ status) {
+  __shared__ uint32_t s_scan[kDedupThreads / 32];
+  __shared__ uint32_t s_total;
+  __shared__ uint32_t s_tile;
+  __shared__ unsigned long long s_base;
+  if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
+  __syncthreads();
+  const uint64_t base = uint64_t(s_tile) * kDedupTile + uint64_t(threadIdx.x) * kDedupItems;
+  K k[kDedupItems];
+  uint32_t keep = 0, cnt = 0;
+  K prev = base > 0 && base <= n ? kin[base - 1] : K(0);
+#pragma unroll
+  for (int i = 0; i < kDedupItems; ++i) {
+    const uint64_t g = base + i;
+    k[i] = g < n ? kin[g] : K(0);
+    if (g < n && (g == 0 || k[i] != prev)) {
+      keep |= 1u << i;
+      ++cnt;
+    }
+    prev = k[i];
+  }
+  const uint32_t local = block_exclusive_scan<kDedupThreads>(cnt, s_scan, &s_total);
+  if (threadIdx.x == 0) s_base = lookback(lb, s_tile, s_total, status);
+  __syncthreads();
+  uint64_t o = s_base + local;
+#pragma unroll
+  for (int i = 0; i < kDedupItems; ++i)
+    if (keep & (1u << i)) {
+      if (o < n) {
+        kout[o] = k[i];
+        if (vout) vout[o] = vin ? vin[base + i] : 0u;
+      }
+      ++o;
+    }
+  if (uint64_t(s_tile + 1) * kDedupTile >= n && threadIdx.x == 0) *out_n = uint32_t(s_base + s_total);
+}
+
+// sortedness / max probe of a key array: flags bit0 = not sorted ascending,
+// bit1 = has equal neighbours; max key via atomicMax
+template <typename K>
+__global__ void inspect_keys_kernel(const K *__restrict__ keys, uint64_t n, uint32_t *__restrict__ flags,
+                                    unsigned long long *__restrict__ max_key) {
+  unsigned long long local_max = 0;
+  uint32_t f = 0;
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += uint64_t(gridDim.x) * blockDim.x) {
+    const K k = keys[i];
+    local_max = max(local_max, (unsigned long long)k);
+    if (i + 1 < n) {
+      const K nx = keys[i + 1];
+      if (nx < k) f |= 1u;
+      if (nx == k) f |= 2u;
+    }
+  }
+  f = __reduce_or_sync(0xffffffffu, f);
+  for (int o = 16; o; o >>= 1) local_max = max(local_max, __shfl_down_sync(0xffffffffu, local_max, o));
+  if ((threadIdx.x & 31) == 0) {
+    if (f) atomicOr(flags, f);
+    atomicMax(max_key, local_max);
+  }
+}
+
+// Exclusive scan of u32 counts into u64 offsets (offsets[n] = total).
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr uint32_t kScanTile = kScanThreads * kScanItems;
+template <typename K>
+__global__ void __launch_bounds__(kScanThreads) scan_counts_kernel(
+    const uint32_t *__restrict__ counts, uint64_t n, unsigned long long *__restrict__ offsets,
+    unsigned long long *__restrict__ lb, uint32_t *__restrict__ tile_counter,
+    uint32_t *__restrict__ status) {
+  __shared__ unsigned long long s_scan[kScanThreads / 32];
+  __shared__ unsigned long long s_total;
+  __shared__ uint32_t s_tile;
+  __shared__ unsigned long long s_base;
+  if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
+  __syncthreads();
+  const uint64_t base = uint64_t(s_tile) * kScanTile + uint64_t(threadIdx.x) * kScanItems;
+  uint32_t c[kScanItems];
+  unsigned long long sum = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    c[i] = base + i < n ? counts[base + i] : 0u;
+    sum += c[i];
+  }
+  const unsigned long long local = block_exclusive_scan<kScanThreads>(sum, s_scan, &s_total);
+  if (threadIdx.x == 0) s_base = lookback(lb, s_tile, s_total, status);
+  __syncthreads();
+  unsigned long long o = s_base + local;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    if (base + i <= n) offsets[base + i] = o;
+    o += c[i];
+  }
+}
+
+// Per-bucket live counts (rebuild step 1) - one warp per bucket chain.
+template <typename K>
+__global__ void chain_counts_kernel(const Node<K> *__restrict__ nodes, uint32_t buckets,
+                                    uint32_t *__restrict__ counts) {
+  const uint32_t b = (uint32_t(blockIdx.x) * blockDim.x + threadIdx.x);
+  if (b >= buckets) return;
+  uint32_t c = 0;
+  for (uint32_t id = b; id != kNone; id = nodes[id].next) c += nodes[id].count;
+  counts[b] = c;
+}
+
+// Rebuild step 2: copy every chain's entries, in key order, into a dense
+// sorted array at offsets[b] (FliX/coarse_granular_rebuild.cuh:219-397).
+template <typename K>
+__global__ void gather_chains_kernel(const Node<K> *__restrict__ nodes, uint32_t buckets,
+                                     const unsigned long long *__restrict__ offsets, K *__restrict__ keys,
+                                     uint32_t *__restrict__ vals) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t b = (uint32_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  if (b >= buckets) return;
+  unsigned long long o = offsets[b];
+  for (uint32_t id = b; id != kNone; id = nodes[id].next) {
+    const uint32_t c = nodes[id].count;
+    if (lane < c) {
+      keys[o + lane] = nodes[id].keys[lane];
+      vals[o + lane] = nodes[id].vals[lane];
+    }
+    o += c;
+  }
+}
+
+}  // namespace flix
+}  // namespace gpulsm

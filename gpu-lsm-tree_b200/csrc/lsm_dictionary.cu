@@ -47,8 +47,6 @@ __global__ void receipt_kernel(ReceiptSrc src) {
   if (i == lsm::kMaxLevels) src.out[i] = *src.status;
 }
 
-__global__ void set_count_kernel(LevelDesc *desc, unsigned long long n) { desc->n = n; }
-
 // Bump allocator over one zeroed scratch region.
 struct Bump {
   char *p;
@@ -236,7 +234,7 @@ void LsmDictionary::post_receipt(cudaStream_t s) {
   }
   src.status = dev_status_;
   src.out = static_cast<unsigned long long *>(receipt_dev_);
-  receipt_kernel<<<1, 32, 0, s>>>(src);
+  receipt_kernel<<<1, 32, 0, s>>>(src); note_launch();
   GPULSM_CUDA(cudaGetLastError());
   GPULSM_CUDA(cudaMemcpyAsync(receipt_host_, receipt_dev_, sizeof(Receipt), cudaMemcpyDeviceToHost, s));
   GPULSM_CUDA(cudaEventRecord(receipt_event_, s));
@@ -308,14 +306,14 @@ RunBuffer *LsmDictionary::sort_dedup(const uint32_t *keys, const uint32_t *value
   unsigned long long *lb = bump.take<unsigned long long>(dtiles + 1);
   const unsigned hist_blocks = std::min<unsigned>(grid_for(n, 4096), unsigned(num_sms_) * 4u);
   lsm::pack_histogram_kernel<<<hist_blocks, 256, 0, s>>>(keys, tombstone ? nullptr : values, nn,
-                                                          words_[0], ws);
+                                                          words_[0], ws); note_launch();
   unsigned long long *bufs[2] = {words_[0], words_[1]};
   const int cur = radix::run_passes<unsigned long long, false>(bufs, nullptr, nn, 32, 64, ws,
                                                                dev_status_, s);
   RunBuffer *carry = pool_.acquire(n, s);
   lsm::dedup_last_kernel<<<unsigned(dtiles), lsm::kCompactThreads, 0, s>>>(
       bufs[cur], nn, tombstone ? 1 : 0, carry->keys, carry->vals, carry->flags, carry->desc, lb,
-      counter, dev_status_);
+      counter, dev_status_); note_launch();
   GPULSM_CUDA(cudaGetLastError());
   return carry;
 }
@@ -332,7 +330,7 @@ RunBuffer *LsmDictionary::merge(RunBuffer *newer, RunBuffer *older, uint64_t out
   lsm::merge_kernel<<<unsigned(std::max<uint64_t>(tiles, 1)), lsm::kMergeThreads, 0, s>>>(
       newer->keys, newer->vals, newer->flags, newer->desc, older->keys, older->vals, older->flags,
       older->desc, out->keys, out->vals, out->flags, out->desc, out->cap, drop_tombstones ? 1 : 0,
-      lb, counter, dev_status_);
+      lb, counter, dev_status_); note_launch();
   GPULSM_CUDA(cudaGetLastError());
   pool_.release(newer);
   pool_.release(older);
@@ -341,7 +339,7 @@ RunBuffer *LsmDictionary::merge(RunBuffer *newer, RunBuffer *older, uint64_t out
 
 void LsmDictionary::build_directory(RunBuffer *run, uint64_t upper, cudaStream_t s) {
   lsm::directory_kernel<<<grid_for(std::max<uint64_t>(upper, 1), 256), 256, 0, s>>>(
-      run->keys, run->desc, run->dir, run->dir_bits, rows_log2_);
+      run->keys, run->desc, run->dir, run->dir_bits, rows_log2_); note_launch();
   GPULSM_CUDA(cudaGetLastError());
 }
 
@@ -481,7 +479,7 @@ void LsmDictionary::lookup(const uint32_t *queries, uint64_t n, uint32_t *out_va
   begin_op(s);
   lsm::LevelSet set;
   level_set(&set);
-  lsm::lookup_kernel<<<grid_for(n, 256), 256, 0, s>>>(set, queries, n, out_values, out_found);
+  lsm::lookup_kernel<<<grid_for(n, 256), 256, 0, s>>>(set, queries, n, out_values, out_found); note_launch();
   GPULSM_CUDA(cudaGetLastError());
   end_op(s);
 }
@@ -496,7 +494,7 @@ void LsmDictionary::range_sum(const uint32_t *lo, const uint32_t *hi, uint64_t n
   lsm::LevelSet set;
   level_set(&set);
   lsm::range_kernel<0><<<grid_for(n, 256), 256, 0, s>>>(set, lo, hi, n, out, nullptr, nullptr,
-                                                       nullptr);
+                                                       nullptr); note_launch();
   GPULSM_CUDA(cudaGetLastError());
   end_op(s);
 }
@@ -511,7 +509,7 @@ void LsmDictionary::range_count(const uint32_t *lo, const uint32_t *hi, uint64_t
   lsm::LevelSet set;
   level_set(&set);
   lsm::range_kernel<1><<<grid_for(n, 256), 256, 0, s>>>(set, lo, hi, n, out, nullptr, nullptr,
-                                                       nullptr);
+                                                       nullptr); note_launch();
   GPULSM_CUDA(cudaGetLastError());
   end_op(s);
 }
@@ -535,10 +533,10 @@ void LsmDictionary::range_offsets(const uint32_t *lo, const uint32_t *hi, uint64
     lsm::LevelSet set;
     level_set(&set);
     lsm::range_kernel<1><<<grid_for(n, 256), 256, 0, s>>>(set, lo, hi, n, counts, nullptr, nullptr,
-                                                         nullptr);
+                                                         nullptr); note_launch();
   }
   lsm::scan_counts_kernel<<<tiles, lsm::kScanThreads, 0, s>>>(
-      counts, n, reinterpret_cast<unsigned long long *>(offsets), lb, counter, dev_status_);
+      counts, n, reinterpret_cast<unsigned long long *>(offsets), lb, counter, dev_status_); note_launch();
   GPULSM_CUDA(cudaGetLastError());
   end_op(s);
 }
@@ -556,7 +554,7 @@ void LsmDictionary::range_pairs(const uint32_t *lo, const uint32_t *hi, uint64_t
   level_set(&set);
   lsm::range_kernel<2><<<grid_for(n, 256), 256, 0, s>>>(
       set, lo, hi, n, nullptr, reinterpret_cast<const unsigned long long *>(offsets), out_keys,
-      out_values);
+      out_values); note_launch();
   GPULSM_CUDA(cudaGetLastError());
   end_op(s);
 }
@@ -570,7 +568,7 @@ void LsmDictionary::successor(const uint32_t *queries, uint64_t n, uint32_t *out
   begin_op(s);
   lsm::LevelSet set;
   level_set(&set);
-  lsm::successor_kernel<<<grid_for(n, 256), 256, 0, s>>>(set, queries, n, out_keys);
+  lsm::successor_kernel<<<grid_for(n, 256), 256, 0, s>>>(set, queries, n, out_keys); note_launch();
   GPULSM_CUDA(cudaGetLastError());
   end_op(s);
 }

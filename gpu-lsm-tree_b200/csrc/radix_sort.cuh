@@ -190,7 +190,7 @@ int run_passes(KeyT *keys[2], uint32_t *vals[2], uint32_t n, int begin_bit, int 
     onesweep_kernel<KeyT, kValues><<<tiles, kThreads, smem, stream>>>(
         keys[cur], kValues ? vals[cur] : nullptr, keys[cur ^ 1], kValues ? vals[cur ^ 1] : nullptr,
         n, uint32_t(begin_bit + 8 * p), hist + p * kDigits, lookback + size_t(p) * tiles * kDigits,
-        counters + p, status);
+        counters + p, status); note_launch();
     cur ^= 1;
   }
   GPULSM_CUDA(cudaGetLastError());
@@ -206,7 +206,7 @@ int sort(KeyT *keys[2], uint32_t *vals[2], uint32_t n, int begin_bit, int end_bi
   GPULSM_CUDA(cudaMemsetAsync(workspace, 0, workspace_bytes(n, passes), stream));
   const unsigned blocks = std::min<unsigned>(grid_for(n, kTile), unsigned(num_sms) * 4u);
   histogram_kernel<KeyT><<<blocks, kThreads, 0, stream>>>(keys[0], n, uint32_t(begin_bit),
-                                                          uint32_t(passes), workspace);
+                                                          uint32_t(passes), workspace); note_launch();
   return run_passes<KeyT, kValues>(keys, vals, n, begin_bit, end_bit, workspace, status, stream);
 }
 

@@ -98,8 +98,8 @@ class GPULSMOpt:
     def lookup(self, queries, out_values, out_found=None, count: int | None = None, stream=None):
         n = queries.numel() if count is None else count
         N.check(self._lib.gpulsm_dict_lookup(
-            self._h, _ptr(queries, "queries", count=n), _ptr(out_values, "out_values", count=n),
-            _ptr(out_found, "out_found", 1, n), n, _stream(stream)))
+            self._h, _ptr(queries, "queries", count=n), n, _ptr(out_values, "out_values", count=n),
+            _ptr(out_found, "out_found", 1, n), _stream(stream)))
 
     def range(self, lo, hi, out_sums, count: int | None = None, stream=None):
         """GPULSMOpt::range: u32 sum of live values in [lo, hi] (wraps at 2^32)."""
@@ -139,8 +139,8 @@ class GPULSMOpt:
 
     def successor(self, queries, out_keys, count: int | None = None, stream=None):
         n = queries.numel() if count is None else count
-        N.check(self._lib.gpulsm_dict_successor(self._h, _ptr(queries, "queries", count=n),
-                                                _ptr(out_keys, "out_keys", count=n), n, _stream(stream)))
+        N.check(self._lib.gpulsm_dict_successor(self._h, _ptr(queries, "queries", count=n), n,
+                                                _ptr(out_keys, "out_keys", count=n), _stream(stream)))
 
     # --- introspection ------------------------------------------------------
     def canonical_carry_status(self) -> int:

@@ -53,6 +53,9 @@ typedef enum gpulsm_status {
 const char *gpulsm_last_error(void);
 /* Library version string. */
 const char *gpulsm_version(void);
+/* Number of CUDA kernels this library has launched in this process (all
+ * handles); a diagnostic so callers can attribute device work to it. */
+uint64_t gpulsm_launch_count(void);
 
 /* ===================== LSM dictionary (GPULSMOpt semantics) ============== */
 typedef struct gpulsm_dict gpulsm_dict;

@@ -182,6 +182,13 @@ def test_empty_and_edge_inputs(gl, cuda):
         gl._native.check(d._lib.gpulsm_dict_insert(d._h, None, None, 5, None))
     with pytest.raises(ValueError):
         gl._native.check(d._lib.gpulsm_dict_lookup(d._h, None, 4, None, None, None))
+    # pointers the GPU cannot dereference are refused before any kernel runs
+    host_buf = np.zeros(16, np.uint32)
+    qd = to_dev(q)
+    with pytest.raises(gl.InvalidArgument, match="device-accessible|CUDA pointer"):
+        gl._native.check(d._lib.gpulsm_dict_lookup(d._h, qd.data_ptr(), 3, host_buf.ctypes.data, None, None))
+    with pytest.raises(gl.InvalidArgument):
+        gl._native.check(d._lib.gpulsm_dict_lookup(d._h, qd.data_ptr(), 3, out.data_ptr(), 1 << 24, None))
     with pytest.raises(ValueError):
         gl.GPULSMOpt(gl.DictionaryConfig(max_elements=1 << 33))
     d.insert(to_dev(np.array([0xFFFFFFFF, 0], np.uint32)), to_dev(np.array([7, 0xFFFFFFFF], np.uint32)))
