@@ -157,6 +157,11 @@ def load() -> C.CDLL:
         "gpulsm_flix_size": (i32, [vp, C.POINTER(u64)]),
         "gpulsm_flix_status": (i32, [vp, C.POINTER(u32)]),
         "gpulsm_sort_pairs": (i32, [vp, vp, vp, vp, u64, u32, u32, u32, vp]),
+        "gpulsm_model_bytes": (u64, [u32]),
+        "gpulsm_model_fit": (i32, [vp, u64, u32, u32, u32, vp, vp, vp]),
+        "gpulsm_model_gradients": (i32, [vp, u64, u32, u32, vp, vp, vp, vp]),
+        "gpulsm_model_lower_bound": (i32, [vp, u64, u32, u32, vp, vp, u64, vp, vp]),
+        "gpulsm_binary_lower_bound": (i32, [vp, u64, u32, vp, u64, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

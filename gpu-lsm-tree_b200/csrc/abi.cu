@@ -12,6 +12,7 @@
 #include "flix_index.h"
 #include "lsm_dictionary.h"
 #include "radix_sort.cuh"
+#include "model_api.h"
 #include "sort_api.h"
 
 struct gpulsm_dict {
@@ -329,6 +330,82 @@ int gpulsm_flix_status(gpulsm_flix *f, uint32_t *out_status) {
     need(f, "index");
     need(out_status, "out_status");
     *out_status = f->impl.status();
+  });
+}
+
+// ---------------------------------------------------------------- learned model
+uint64_t gpulsm_model_bytes(uint32_t segments) { return gpulsm::learned::bytes_for(segments); }
+
+int gpulsm_model_fit(const void *sorted_keys, uint64_t count, uint32_t key_bits, uint32_t segments,
+                     uint32_t iters, void *model, float *loss_history, void *stream) {
+  return guarded([&] {
+    if (key_bits != 32 && key_bits != 64) throw std::invalid_argument("key_bits must be 32 or 64");
+    if (count && !sorted_keys) throw std::invalid_argument("null keys");
+    need(model, "model");
+    if (!segments || segments > (1u << 24)) throw std::invalid_argument("segments must be in [1, 2^24]");
+    if (count > 0xffffffffull) throw std::length_error("model fit limited to 2^32-1 keys");
+    device_accessible({{sorted_keys, "sorted_keys"}, {model, "model"}, {loss_history, "loss_history"}});
+    if (key_bits == 32)
+      gpulsm::learned::fit(static_cast<const uint32_t *>(sorted_keys), count, segments, iters, model,
+                           loss_history, S(stream));
+    else
+      gpulsm::learned::fit(static_cast<const unsigned long long *>(sorted_keys), count, segments, iters, model,
+                           loss_history, S(stream));
+  });
+}
+
+int gpulsm_model_gradients(const void *sorted_keys, uint64_t count, uint32_t key_bits, uint32_t segments,
+                           void *model, float *grad, float *loss, void *stream) {
+  return guarded([&] {
+    if (key_bits != 32 && key_bits != 64) throw std::invalid_argument("key_bits must be 32 or 64");
+    need(model, "model");
+    need(grad, "grad");
+    device_accessible({{sorted_keys, "sorted_keys"}, {model, "model"}, {grad, "grad"}, {loss, "loss"}});
+    if (key_bits == 32)
+      gpulsm::learned::gradients(static_cast<const uint32_t *>(sorted_keys), count, segments, model, grad, loss,
+                                 S(stream));
+    else
+      gpulsm::learned::gradients(static_cast<const unsigned long long *>(sorted_keys), count, segments, model,
+                                 grad, loss, S(stream));
+  });
+}
+
+int gpulsm_model_lower_bound(const void *sorted_keys, uint64_t count, uint32_t key_bits, uint32_t segments,
+                             const void *model, const void *queries, uint64_t query_count, uint64_t *out,
+                             void *stream) {
+  return guarded([&] {
+    if (key_bits != 32 && key_bits != 64) throw std::invalid_argument("key_bits must be 32 or 64");
+    if (!query_count) return;
+    need(model, "model");
+    need(queries, "queries");
+    need(out, "out");
+    device_accessible({{sorted_keys, "sorted_keys"}, {model, "model"}, {queries, "queries"}, {out, "out"}});
+    auto *o = reinterpret_cast<unsigned long long *>(out);
+    if (key_bits == 32)
+      gpulsm::learned::lower_bound(static_cast<const uint32_t *>(sorted_keys), count, segments, model,
+                                   static_cast<const uint32_t *>(queries), query_count, o, S(stream));
+    else
+      gpulsm::learned::lower_bound(static_cast<const unsigned long long *>(sorted_keys), count, segments, model,
+                                   static_cast<const unsigned long long *>(queries), query_count, o, S(stream));
+  });
+}
+
+int gpulsm_binary_lower_bound(const void *sorted_keys, uint64_t count, uint32_t key_bits, const void *queries,
+                              uint64_t query_count, uint64_t *out, void *stream) {
+  return guarded([&] {
+    if (key_bits != 32 && key_bits != 64) throw std::invalid_argument("key_bits must be 32 or 64");
+    if (!query_count) return;
+    need(queries, "queries");
+    need(out, "out");
+    device_accessible({{sorted_keys, "sorted_keys"}, {queries, "queries"}, {out, "out"}});
+    auto *o = reinterpret_cast<unsigned long long *>(out);
+    if (key_bits == 32)
+      gpulsm::learned::binary_lower_bound(static_cast<const uint32_t *>(sorted_keys), count,
+                                          static_cast<const uint32_t *>(queries), query_count, o, S(stream));
+    else
+      gpulsm::learned::binary_lower_bound(static_cast<const unsigned long long *>(sorted_keys), count,
+                                          static_cast<const unsigned long long *>(queries), query_count, o,
+                                          S(stream));
   });
 }
 

@@ -151,8 +151,10 @@ class FlixImpl final : public FlixIndex::Impl {
     // 2. allocate the node pool: heads + allocation region
     const uint64_t buckets = std::max<uint64_t>(1, (unique + fill_ - 1) / fill_);
     const uint64_t hint = std::max<uint64_t>({max_n, cfg_.max_elements, unique});
+    // Splits create at most one node per 16 inserted keys plus one per node
+    // that was already full; size for the hint with that slack (grown on demand).
     const uint64_t region = std::max<uint64_t>(
-        1024, (hint - unique) / (flix::kNodeSize / 2) + buckets / 8 + 1024);
+        {min_region_, 1024, (hint - unique) / (flix::kNodeSize / 4) + buckets / 4 + 1024});
     if (buckets + region >= 0xffffffffull) throw std::length_error("FliX node pool exceeds 2^32 nodes");
     release_pool(s);
     buckets_ = uint32_t(buckets);
@@ -370,35 +372,58 @@ class FlixImpl final : public FlixIndex::Impl {
     return out;
   }
 
+  // Compacts the chains into a fresh layout whose allocation region holds at
+  // least `need` more nodes (FliX's rebuild, plus growth).
+  void grow(uint64_t need, cudaStream_t s) {
+    min_region_ = std::max<uint64_t>({min_region_, 2ull * (capacity_ - buckets_), need + 1024});
+    rebuild(s);
+  }
+
   void update(const K *keys, const uint32_t *vals, uint64_t n, bool is_insert, cudaStream_t s) {
     require_built();
-    begin(s);
-    if (is_insert) {
-      // worst case every key splits a node: make sure the region can take it
-      if (uint64_t(used_upper_) + n > capacity_) {
-        read_counters(s);
-        used_upper_ = ctr_host_->alloc_top;
-        if (uint64_t(used_upper_) + n > capacity_) {
-          end(s);
-          rebuild(s);
+    for (int attempt = 0;; ++attempt) {
+      if (is_insert) {
+        // expected new nodes: one per 16 inserted keys plus slack; a shortfall
+        // is reported by the kernel (status bit 3) and handled below
+        const uint64_t need = n / 8 + 1024;
+        if (uint64_t(used_upper_) + need > capacity_) {
           begin(s);
-          if (uint64_t(buckets_) + n > capacity_) throw std::runtime_error("FliX allocation region capacity exhausted");
+          read_counters(s);
+          end(s);
+          used_upper_ = ctr_host_->alloc_top;
+          if (uint64_t(used_upper_) + need > capacity_) grow(need, s);
         }
       }
-      used_upper_ = uint32_t(std::min<uint64_t>(uint64_t(used_upper_) + n, capacity_));
+      begin(s);
+      Sorted st = prepare(keys, vals, n, is_insert, false, true, s);
+      const unsigned grid = grid_for(n * 32, 256);
+      flix::PoolView pool{&ctr_->alloc_top, capacity_, &ctr_->status};
+      if (is_insert) {
+        flix::insert_runs_kernel<K><<<grid, 256, 0, s>>>(st.keys, st.vals, st.n_dev, st.runs, st.run_count,
+                                                         nodes_, pool, &ctr_->inserted); note_launch();
+      } else {
+        flix::delete_runs_kernel<K><<<grid, 256, 0, s>>>(st.keys, st.n_dev, st.runs, st.run_count, nodes_,
+                                                         &ctr_->removed); note_launch();
+      }
+      GPULSM_CUDA(cudaGetLastError());
+      if (!is_insert) {
+        end(s);
+        return;
+      }
+      // the region fill and overflow bit come back with one small read
+      read_counters(s);
+      end(s);
+      used_upper_ = uint32_t(std::min<uint64_t>(ctr_host_->alloc_top, capacity_));
+      if (!(ctr_host_->status & kDevOutputOverflow)) return;
+      // keys that found no free node were skipped, not dropped: grow and
+      // re-run the batch (insert-if-absent makes the retry idempotent)
+      if (attempt == 3) throw std::runtime_error("FliX allocation region capacity exhausted");
+      begin(s);
+      flix::set_u32_kernel<K><<<1, 1, 0, s>>>(&ctr_->status, ctr_host_->status & ~kDevOutputOverflow);
+      note_launch();
+      end(s);
+      grow(n / 4 + 1024, s);
     }
-    Sorted st = prepare(keys, vals, n, is_insert, false, true, s);
-    const unsigned grid = grid_for(n * 32, 256);
-    flix::PoolView pool{&ctr_->alloc_top, capacity_, &ctr_->status};
-    if (is_insert) {
-      flix::insert_runs_kernel<K><<<grid, 256, 0, s>>>(st.keys, st.vals, st.n_dev, st.runs, st.run_count, nodes_,
-                                                       pool, &ctr_->inserted); note_launch();
-    } else {
-      flix::delete_runs_kernel<K><<<grid, 256, 0, s>>>(st.keys, st.n_dev, st.runs, st.run_count, nodes_,
-                                                       &ctr_->removed); note_launch();
-    }
-    GPULSM_CUDA(cudaGetLastError());
-    end(s);
   }
 
   // sorted probes: route, then one warp per run
@@ -453,6 +478,7 @@ class FlixImpl final : public FlixIndex::Impl {
   uint32_t buckets_ = 0;
   uint32_t capacity_ = 0;
   uint32_t used_upper_ = 0;
+  uint64_t min_region_ = 0;
   bool built_ = false;
   DevCounters *ctr_ = nullptr;
   DevCounters *ctr_host_ = nullptr;

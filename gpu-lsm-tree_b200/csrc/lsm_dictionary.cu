@@ -171,6 +171,8 @@ LsmDictionary::LsmDictionary(const DictConfig &config)
   GPULSM_CUDA(cudaMalloc(&receipt_dev_, sizeof(Receipt)));
   GPULSM_CUDA(cudaMallocHost(&receipt_host_, sizeof(Receipt)));
   std::memset(receipt_host_, 0, sizeof(Receipt));
+  GPULSM_CUDA(cudaMalloc(&width_, 8));
+  GPULSM_CUDA(cudaMallocHost(&width_host_, 8));
   GPULSM_CUDA(cudaEventCreateWithFlags(&op_done_, cudaEventDisableTiming));
   GPULSM_CUDA(cudaEventCreateWithFlags(&receipt_event_, cudaEventDisableTiming));
   GPULSM_CUDA(cudaEventRecord(op_done_, 0));
@@ -185,6 +187,9 @@ LsmDictionary::~LsmDictionary() {
   if (dev_status_) cudaFree(dev_status_);
   if (receipt_dev_) cudaFree(receipt_dev_);
   if (receipt_host_) cudaFreeHost(receipt_host_);
+  if (prefix_) cudaFree(prefix_);
+  if (width_) cudaFree(width_);
+  if (width_host_) cudaFreeHost(width_host_);
   if (op_done_) cudaEventDestroy(op_done_);
   if (receipt_event_) cudaEventDestroy(receipt_event_);
 }
@@ -343,7 +348,7 @@ void LsmDictionary::build_directory(RunBuffer *run, uint64_t upper, cudaStream_t
   GPULSM_CUDA(cudaGetLastError());
 }
 
-void LsmDictionary::cascade(RunBuffer *carry, uint64_t carry_upper, cudaStream_t s) {
+void LsmDictionary::cascade(RunBuffer *carry, uint64_t carry_upper, bool carry_tombs, cudaStream_t s) {
   const size_t L = levels_.size();
   size_t dest = 0;
   uint64_t acc = carry_upper;
@@ -358,11 +363,14 @@ void LsmDictionary::cascade(RunBuffer *carry, uint64_t carry_upper, cudaStream_t
   for (size_t j = dest + 1; j < L; ++j) deeper |= levels_[j].run != nullptr;
   RunBuffer *x = carry;
   uint64_t xu = carry_upper;
+  bool xt = carry_tombs;
   for (size_t i = 0; i < dest; ++i) {
     const bool last = (i + 1 == dest) && !dest_occupied;
     const uint64_t ou = xu + levels_[i].upper;
-    x = merge(x, levels_[i].run, ou, last && !deeper, s);
+    const bool drop = last && !deeper;
+    x = merge(x, levels_[i].run, ou, drop, s);
     xu = ou;
+    xt = !drop && (xt || levels_[i].tombs);
     levels_[i] = Level{};
     levels_[i].gen = next_gen_++;
   }
@@ -370,11 +378,104 @@ void LsmDictionary::cascade(RunBuffer *carry, uint64_t carry_upper, cudaStream_t
     const uint64_t ou = xu + levels_[dest].upper;
     x = merge(x, levels_[dest].run, ou, !deeper, s);
     xu = ou;
+    xt = deeper && (xt || levels_[dest].tombs);
   }
   levels_[dest].run = x;
   levels_[dest].upper = std::min<uint64_t>(xu, x->cap);
   levels_[dest].gen = next_gen_++;
+  levels_[dest].tombs = xt;
   build_directory(x, levels_[dest].upper, s);
+}
+
+// Merge every occupied level, newest first, into one tombstone-free run at
+// the position of the oldest one (a full compaction).
+void LsmDictionary::compact_all(cudaStream_t s) {
+  std::vector<size_t> occ;
+  for (size_t i = 0; i < levels_.size(); ++i)
+    if (levels_[i].run) occ.push_back(i);
+  if (occ.empty()) return;
+  if (occ.size() == 1 && !levels_[occ[0]].tombs) return;
+  const size_t dest = occ.back();
+  RunBuffer *x = levels_[occ[0]].run;
+  uint64_t xu = levels_[occ[0]].upper;
+  if (occ.size() == 1) {
+    // a lone level that may hold tombstones: merge with an empty run to drop them
+    RunBuffer *empty = pool_.acquire(1, s);
+    GPULSM_CUDA(cudaMemsetAsync(empty->desc, 0, sizeof(LevelDesc), s));
+    x = merge(x, empty, xu, true, s);
+  } else {
+    for (size_t k = 1; k < occ.size(); ++k) {
+      const uint64_t ou = xu + levels_[occ[k]].upper;
+      x = merge(x, levels_[occ[k]].run, ou, k + 1 == occ.size(), s);
+      xu = ou;
+    }
+  }
+  for (size_t i : occ) {
+    levels_[i] = Level{};
+    levels_[i].gen = next_gen_++;
+  }
+  levels_[dest].run = x;
+  levels_[dest].upper = std::min<uint64_t>(xu, x->cap);
+  levels_[dest].gen = next_gen_++;
+  levels_[dest].tombs = false;
+  build_directory(x, levels_[dest].upper, s);
+}
+
+int LsmDictionary::ranges_on_single_level(const uint32_t *lo, const uint32_t *hi, uint64_t n, cudaStream_t s) {
+  int occupied = 0, only = -1;
+  uint64_t rows = 0;
+  for (size_t i = 0; i < levels_.size(); ++i)
+    if (levels_[i].run) {
+      ++occupied;
+      only = int(i);
+      rows += levels_[i].upper;
+    }
+  if (occupied == 0) return -1;
+  if (occupied == 1 && !levels_[only].tombs) return only;
+  if (n < 1024) return -1;  // small batches: the per-query merge is cheaper
+  // estimate the rows the batch covers from its total key width (one 8-byte read)
+  GPULSM_CUDA(cudaMemsetAsync(width_, 0, 8, s));
+  lsm::range_width_kernel<<<std::min<unsigned>(grid_for(n, 256), unsigned(num_sms_) * 8u), 256, 0, s>>>(
+      lo, hi, n, width_); note_launch();
+  GPULSM_CUDA(cudaMemcpyAsync(width_host_, width_, 8, cudaMemcpyDeviceToHost, s));
+  GPULSM_CUDA(cudaStreamSynchronize(s));
+  const double covered = double(*width_host_) / 4294967296.0 * double(rows);
+  // per-query merging touches every covered row once per level; a compaction
+  // streams every row about twice
+  if (covered * double(occupied) < 2.0 * double(rows)) return -1;
+  compact_all(s);
+  for (size_t i = 0; i < levels_.size(); ++i)
+    if (levels_[i].run) return int(i);
+  return -1;
+}
+
+const unsigned long long *LsmDictionary::value_prefix(int level, cudaStream_t s) {
+  const Level &l = levels_[level];
+  if (prefix_gen_ == l.gen && prefix_) return prefix_;
+  const uint64_t n = l.upper;
+  if (n + 1 > prefix_cap_) {
+    if (prefix_) GPULSM_CUDA(cudaFreeAsync(prefix_, s));
+    prefix_cap_ = std::max<uint64_t>(n + 1, prefix_cap_ * 3 / 2);
+    if (cudaMallocAsync(reinterpret_cast<void **>(&prefix_), prefix_cap_ * 8, s) != cudaSuccess) {
+      (void)cudaGetLastError();
+      prefix_ = nullptr;
+      prefix_cap_ = 0;
+      throw std::bad_alloc();
+    }
+  }
+  // exclusive scan of the values; the count comes from the device descriptor,
+  // so scan the host upper bound of rows (rows past n read as values of a
+  // stale buffer tail are never used: queries stop at n)
+  const uint32_t tiles = lsm::scan_tiles(n);
+  const size_t bytes = align_up(8) + align_up(size_t(tiles + 1) * 8);
+  Bump bump{static_cast<char *>(scratch(bytes, s))};
+  GPULSM_CUDA(cudaMemsetAsync(bump.p, 0, bytes, s));
+  uint32_t *counter = bump.take<uint32_t>(2);
+  unsigned long long *lb = bump.take<unsigned long long>(tiles + 1);
+  lsm::scan_counts_kernel<<<tiles, lsm::kScanThreads, 0, s>>>(l.run->vals, n, prefix_, lb, counter, dev_status_);
+  note_launch();
+  prefix_gen_ = l.gen;
+  return prefix_;
 }
 
 void LsmDictionary::admit(const uint32_t *keys, const uint32_t *values, uint64_t n, bool tombstone,
@@ -389,7 +490,7 @@ void LsmDictionary::admit(const uint32_t *keys, const uint32_t *values, uint64_t
       reject_if_failed();
     }
     RunBuffer *carry = sort_dedup(keys + off, values ? values + off : nullptr, m, tombstone, s);
-    cascade(carry, m, s);
+    cascade(carry, m, tombstone, s);
   }
 }
 
@@ -425,6 +526,7 @@ void LsmDictionary::bulk_build(const uint32_t *keys, const uint32_t *values, uin
     top.run = run;
     top.upper = n;
     top.gen = next_gen_++;
+    top.tombs = false;
     build_directory(run, n, s);
     post_receipt(s);
   }
@@ -454,6 +556,11 @@ void LsmDictionary::erase(const uint32_t *keys, uint64_t n, cudaStream_t s) {
   admit(keys, nullptr, n, true, s);
   post_receipt(s);
   end_op(s);
+}
+
+lsm::LevelView LsmDictionary::view_of(int level) const {
+  const RunBuffer *r = levels_[level].run;
+  return lsm::LevelView{r->keys, r->vals, r->flags, r->dir, r->desc};
 }
 
 void LsmDictionary::level_set(void *out) const {
@@ -491,10 +598,17 @@ void LsmDictionary::range_sum(const uint32_t *lo, const uint32_t *hi, uint64_t n
   if (!lo || !hi || !out) throw std::invalid_argument("invalid GPU dictionary range");
   apply_receipt(false);
   begin_op(s);
-  lsm::LevelSet set;
-  level_set(&set);
-  lsm::range_kernel<0><<<grid_for(n, 256), 256, 0, s>>>(set, lo, hi, n, out, nullptr, nullptr,
-                                                       nullptr); note_launch();
+  const int single = ranges_on_single_level(lo, hi, n, s);
+  if (single >= 0) {
+    const unsigned long long *prefix = value_prefix(single, s);
+    lsm::single_level_range_kernel<0><<<grid_for(n, 256), 256, 0, s>>>(view_of(single), lo, hi, n, prefix, out);
+    note_launch();
+  } else {
+    lsm::LevelSet set;
+    level_set(&set);
+    lsm::range_kernel<0><<<grid_for(n, 256), 256, 0, s>>>(set, lo, hi, n, out, nullptr, nullptr,
+                                                         nullptr); note_launch();
+  }
   GPULSM_CUDA(cudaGetLastError());
   end_op(s);
 }
@@ -506,10 +620,16 @@ void LsmDictionary::range_count(const uint32_t *lo, const uint32_t *hi, uint64_t
   if (!lo || !hi || !out) throw std::invalid_argument("invalid GPU dictionary range");
   apply_receipt(false);
   begin_op(s);
-  lsm::LevelSet set;
-  level_set(&set);
-  lsm::range_kernel<1><<<grid_for(n, 256), 256, 0, s>>>(set, lo, hi, n, out, nullptr, nullptr,
-                                                       nullptr); note_launch();
+  const int single = ranges_on_single_level(lo, hi, n, s);
+  if (single >= 0) {
+    lsm::single_level_range_kernel<1><<<grid_for(n, 256), 256, 0, s>>>(view_of(single), lo, hi, n, nullptr, out);
+    note_launch();
+  } else {
+    lsm::LevelSet set;
+    level_set(&set);
+    lsm::range_kernel<1><<<grid_for(n, 256), 256, 0, s>>>(set, lo, hi, n, out, nullptr, nullptr,
+                                                         nullptr); note_launch();
+  }
   GPULSM_CUDA(cudaGetLastError());
   end_op(s);
 }
@@ -530,10 +650,17 @@ void LsmDictionary::range_offsets(const uint32_t *lo, const uint32_t *hi, uint64
   uint32_t *counter = bump.take<uint32_t>(2);
   unsigned long long *lb = bump.take<unsigned long long>(tiles + 1);
   if (n) {
-    lsm::LevelSet set;
-    level_set(&set);
-    lsm::range_kernel<1><<<grid_for(n, 256), 256, 0, s>>>(set, lo, hi, n, counts, nullptr, nullptr,
-                                                         nullptr); note_launch();
+    const int single = ranges_on_single_level(lo, hi, n, s);
+    if (single >= 0) {
+      lsm::single_level_range_kernel<1><<<grid_for(n, 256), 256, 0, s>>>(view_of(single), lo, hi, n, nullptr,
+                                                                          counts);
+      note_launch();
+    } else {
+      lsm::LevelSet set;
+      level_set(&set);
+      lsm::range_kernel<1><<<grid_for(n, 256), 256, 0, s>>>(set, lo, hi, n, counts, nullptr, nullptr,
+                                                           nullptr); note_launch();
+    }
   }
   lsm::scan_counts_kernel<<<tiles, lsm::kScanThreads, 0, s>>>(
       counts, n, reinterpret_cast<unsigned long long *>(offsets), lb, counter, dev_status_); note_launch();
@@ -550,11 +677,19 @@ void LsmDictionary::range_pairs(const uint32_t *lo, const uint32_t *hi, uint64_t
     throw std::invalid_argument("invalid GPU dictionary range");
   apply_receipt(false);
   begin_op(s);
-  lsm::LevelSet set;
-  level_set(&set);
-  lsm::range_kernel<2><<<grid_for(n, 256), 256, 0, s>>>(
-      set, lo, hi, n, nullptr, reinterpret_cast<const unsigned long long *>(offsets), out_keys,
-      out_values); note_launch();
+  const int single = ranges_on_single_level(lo, hi, n, s);
+  if (single >= 0) {
+    const unsigned grid = std::min<unsigned>(grid_for(n * 32, 256), unsigned(num_sms_) * 64u);
+    lsm::single_level_pairs_kernel<<<grid, 256, 0, s>>>(
+        view_of(single), lo, hi, n, reinterpret_cast<const unsigned long long *>(offsets), out_keys, out_values);
+    note_launch();
+  } else {
+    lsm::LevelSet set;
+    level_set(&set);
+    lsm::range_kernel<2><<<grid_for(n, 256), 256, 0, s>>>(
+        set, lo, hi, n, nullptr, reinterpret_cast<const unsigned long long *>(offsets), out_keys,
+        out_values); note_launch();
+  }
   GPULSM_CUDA(cudaGetLastError());
   end_op(s);
 }

@@ -16,6 +16,7 @@ namespace gpulsm {
 
 namespace lsm {
 struct LevelDesc;
+struct LevelView;
 }
 
 struct DictConfig {
@@ -90,6 +91,7 @@ class LsmDictionary {
     RunBuffer *run = nullptr;
     uint64_t upper = 0;  // upper bound of the row count known on the host
     uint64_t gen = 0;    // bumps whenever the level changes
+    bool tombs = false;  // may hold tombstone rows
   };
   struct Receipt;
 
@@ -102,15 +104,21 @@ class LsmDictionary {
              cudaStream_t s);
   RunBuffer *sort_dedup(const uint32_t *keys, const uint32_t *values, uint64_t n, bool tombstone,
                         cudaStream_t s);
-  void cascade(RunBuffer *carry, uint64_t carry_upper, cudaStream_t s);
+  void cascade(RunBuffer *carry, uint64_t carry_upper, bool carry_tombs, cudaStream_t s);
   RunBuffer *merge(RunBuffer *newer, RunBuffer *older, uint64_t out_upper, bool drop_tombstones,
                    cudaStream_t s);
   void build_directory(RunBuffer *run, uint64_t upper, cudaStream_t s);
+  // Range batches: merge every level into one tombstone-free run when the
+  // rows the batch covers outweigh the merge; returns the single level to
+  // answer from, or -1 to use the per-query k-way merge.
+  int ranges_on_single_level(const uint32_t *lo, const uint32_t *hi, uint64_t n, cudaStream_t s);
+  void compact_all(cudaStream_t s);
+  const unsigned long long *value_prefix(int level, cudaStream_t s);
   void release_levels(cudaStream_t s);
   void *scratch(size_t bytes, cudaStream_t s);
   void ensure_sort_space(uint64_t n, cudaStream_t s);
-  struct LevelSetHost;
   void level_set(void *out) const;
+  lsm::LevelView view_of(int level) const;
 
   DictConfig cfg_;
   uint64_t batch_capacity_ = 0;
@@ -136,6 +144,13 @@ class LsmDictionary {
   cudaEvent_t receipt_event_ = nullptr;
   bool receipt_pending_ = false;
   std::vector<uint64_t> receipt_gens_;
+
+  // u64 prefix sums of a single level's values (range sums after compaction)
+  unsigned long long *prefix_ = nullptr;
+  uint64_t prefix_cap_ = 0;
+  uint64_t prefix_gen_ = 0;
+  unsigned long long *width_ = nullptr;  // device word for the range-width estimate
+  unsigned long long *width_host_ = nullptr;
 
   uint32_t status_bits_ = 0;
   bool failed_ = false;

@@ -475,6 +475,79 @@ __global__ void __launch_bounds__(256) range_kernel(LevelSet set, const uint32_t
   if (MODE != 2) out_u32[q] = uint32_t(acc);
 }
 
+// ---------------------------------------------------------------------------
+// Ranges over ONE tombstone-free level (after a compaction): the answer of a
+// query is the contiguous row slice [lower_bound(lo), upper_bound(hi)).
+
+// sum over queries of the covered key width (decides whether to compact)
+__global__ void __launch_bounds__(256) range_width_kernel(const uint32_t *__restrict__ lo,
+                                                          const uint32_t *__restrict__ hi, uint64_t n,
+                                                          unsigned long long *__restrict__ total) {
+  unsigned long long w = 0;
+  for (uint64_t q = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n; q += uint64_t(gridDim.x) * blockDim.x)
+    if (lo[q] <= hi[q]) w += (unsigned long long)(hi[q] - lo[q]) + 1ull;
+#pragma unroll
+  for (int o = 16; o; o >>= 1) w += __shfl_down_sync(0xffffffffu, w, o);
+  if ((threadIdx.x & 31) == 0 && w) atomicAdd(total, w);
+}
+
+// MODE 1: live count (u32), MODE 0: u32 sum from the level's value prefix P
+template <int MODE>
+__global__ void __launch_bounds__(256) single_level_range_kernel(
+    LevelView L, const uint32_t *__restrict__ lo, const uint32_t *__restrict__ hi, uint64_t n,
+    const unsigned long long *__restrict__ prefix, uint32_t *__restrict__ out) {
+  const uint64_t q = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const uint32_t a = lo[q], z = hi[q];
+  uint32_t r = 0;
+  if (a <= z) {
+    const LevelDesc d = load_desc(L.desc);
+    const uint64_t b = level_lower_bound(L, d, a), e = level_upper_bound(L, d, z);
+    if (e > b) r = MODE == 1 ? uint32_t(e - b) : uint32_t(prefix[e] - prefix[b]);
+  }
+  out[q] = r;
+}
+
+// pairs: one warp per query copies its row slice (coalesced, 4 rows in flight per lane)
+__global__ void __launch_bounds__(256) single_level_pairs_kernel(
+    LevelView L, const uint32_t *__restrict__ lo, const uint32_t *__restrict__ hi, uint64_t n,
+    const unsigned long long *__restrict__ offsets, uint32_t *__restrict__ out_keys,
+    uint32_t *__restrict__ out_vals) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t warps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+  const LevelDesc d = load_desc(L.desc);
+  for (uint64_t q = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; q < n; q += warps) {
+    const uint32_t a = lo[q], z = hi[q];
+    if (a > z) continue;
+    uint64_t b = 0, e = 0;
+    if (lane == 0) {
+      b = level_lower_bound(L, d, a);
+      e = level_upper_bound(L, d, z);
+    }
+    b = __shfl_sync(0xffffffffu, b, 0);
+    e = __shfl_sync(0xffffffffu, e, 0);
+    const unsigned long long o = offsets[q];
+    const uint64_t len = e > b ? e - b : 0;
+    uint64_t j = lane;
+    for (; j + 96 < len; j += 128) {
+      const uint32_t k0 = L.keys[b + j], k1 = L.keys[b + j + 32], k2 = L.keys[b + j + 64], k3 = L.keys[b + j + 96];
+      const uint32_t v0 = L.vals[b + j], v1 = L.vals[b + j + 32], v2 = L.vals[b + j + 64], v3 = L.vals[b + j + 96];
+      out_keys[o + j] = k0;
+      out_keys[o + j + 32] = k1;
+      out_keys[o + j + 64] = k2;
+      out_keys[o + j + 96] = k3;
+      out_vals[o + j] = v0;
+      out_vals[o + j + 32] = v1;
+      out_vals[o + j + 64] = v2;
+      out_vals[o + j + 96] = v3;
+    }
+    for (; j < len; j += 32) {
+      out_keys[o + j] = L.keys[b + j];
+      out_vals[o + j] = L.vals[b + j];
+    }
+  }
+}
+
 // Successor: smallest live key >= query, else 0xffffffff (GPULSMOpt.cuh:5566-5594).
 __global__ void __launch_bounds__(256) successor_kernel(LevelSet set, const uint32_t *__restrict__ queries,
                                                         uint64_t n, uint32_t *__restrict__ out_keys) {

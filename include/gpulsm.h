@@ -160,6 +160,30 @@ int gpulsm_flix_resident_bytes(gpulsm_flix *index, uint64_t *out_bytes);
 int gpulsm_flix_size(gpulsm_flix *index, uint64_t *out_keys);
 int gpulsm_flix_status(gpulsm_flix *index, uint32_t *out_status);
 
+/* ===================== learned position model ============================ */
+/* A piecewise-linear CDF over one sorted key array (no reference counterpart:
+ * the reference narrows searches with 128-cell rank directories,
+ * GPULSMOpt.cuh:4605-4646).  Equal-width key segments (count rounded up to a
+ * power of two), fp32 slope/intercept per segment trained on the GPU by
+ * forward/backward kernels, exact through a per-segment maximum error.
+ * `model` is caller-owned device memory of gpulsm_model_bytes(segments). */
+uint64_t gpulsm_model_bytes(uint32_t segments);
+/* Fit: interpolation init, `iters` preconditioned gradient steps, error bounds.
+ * loss_history (device, iters + 1 floats, may be NULL) = mean squared error. */
+int gpulsm_model_fit(const void *sorted_keys, uint64_t count, uint32_t key_bits, uint32_t segments,
+                     uint32_t iters, void *model, float *loss_history, void *stream);
+/* Gradients of the mean squared error for the current parameters:
+ * grad[2s] = dL/da_s, grad[2s+1] = dL/db_s (device, 2 * segments floats). */
+int gpulsm_model_gradients(const void *sorted_keys, uint64_t count, uint32_t key_bits, uint32_t segments,
+                           void *model, float *grad, float *loss, void *stream);
+/* Exact lower bounds (first index with key >= query) through the model. */
+int gpulsm_model_lower_bound(const void *sorted_keys, uint64_t count, uint32_t key_bits, uint32_t segments,
+                             const void *model, const void *queries, uint64_t query_count, uint64_t *out,
+                             void *stream);
+/* The same lower bounds by plain binary search (the method without the model). */
+int gpulsm_binary_lower_bound(const void *sorted_keys, uint64_t count, uint32_t key_bits, const void *queries,
+                              uint64_t query_count, uint64_t *out, void *stream);
+
 /* ===================== building blocks ==================================== */
 /* Stable LSD radix sort of (key, u32 value) pairs by key bits [begin_bit, end_bit).
  * key_bits 32 or 64; values may be NULL. keys_out/values_out receive the result;

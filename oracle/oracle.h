@@ -76,6 +76,10 @@ void orc_flix_remove(orc_flix *f, const uint64_t *keys, uint64_t n);
 void orc_flix_lookup(const orc_flix *f, const uint64_t *probes, uint64_t n, uint32_t *out);
 void orc_flix_successor(const orc_flix *f, const uint64_t *probes, uint64_t n, uint64_t *out);
 
+/* ---- learned position model (restated for gradient checks) ------------ */
+void orc_model_gradients(const uint64_t *keys, uint64_t n, uint64_t kmin, uint32_t shift, uint32_t nseg,
+                         const float *a, const float *b, double *ga, double *gb, double *loss);
+
 #ifdef __cplusplus
 }
 #endif

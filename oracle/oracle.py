@@ -210,3 +210,22 @@ class OracleFlix:
         out = np.empty(p.size, np.uint64)
         self._lib.orc_flix_successor(self._h, p, p.size, out)
         return out
+
+
+def model_gradients(keys, kmin: int, shift: int, nseg: int, a, b):
+    """float64 gradients of the learned model's mean squared error (model_oracle.c)."""
+    lib = _load()
+    fn = lib.orc_model_gradients
+    fn.restype = None
+    fn.argtypes = [_u64p, C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint32,
+                   np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS"),
+                   np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS"),
+                   np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS"),
+                   np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS"), C.POINTER(C.c_double)]
+    k = _u64(keys)
+    ga = np.zeros(nseg, np.float64)
+    gb = np.zeros(nseg, np.float64)
+    loss = C.c_double()
+    fn(k, k.size, kmin, shift, nseg, np.ascontiguousarray(a, np.float32), np.ascontiguousarray(b, np.float32),
+       ga, gb, C.byref(loss))
+    return ga, gb, loss.value
