@@ -14,6 +14,7 @@
 #include <string>
 
 #include "flix_kernels.cuh"
+#include "model_api.h"
 #include "radix_sort.cuh"
 
 namespace gpulsm {
@@ -95,6 +96,7 @@ class FlixImpl final : public FlixIndex::Impl {
     if (nodes_) cudaFree(nodes_);
     if (bmax_) cudaFree(bmax_);
     if (scratch_) cudaFree(scratch_);
+    if (model_) cudaFree(model_);
     if (ctr_) cudaFree(ctr_);
     if (ctr_host_) cudaFreeHost(ctr_host_);
     if (op_done_) cudaEventDestroy(op_done_);
@@ -172,6 +174,7 @@ class FlixImpl final : public FlixIndex::Impl {
     GPULSM_CUDA(cudaStreamSynchronize(s));  // ctr_host_ is reused as the staging buffer
     if (tmp) GPULSM_CUDA(cudaFreeAsync(tmp, s));
     used_upper_ = buckets_;
+    fit_routing_model(s);
     built_ = true;
     end(s);
   }
@@ -309,6 +312,24 @@ class FlixImpl final : public FlixIndex::Impl {
     return scratch_;
   }
 
+  // search_mode 1: a piecewise-linear model over bmax[0, B-1) routes keys to
+  // buckets instead of a full binary search (learned.cuh)
+  static constexpr uint32_t kModelSegments = 4096;
+  static constexpr uint32_t kModelIters = 8;
+  void fit_routing_model(cudaStream_t s) {
+    model_ready_ = false;
+    if (cfg_.search_mode != 1 || buckets_ < 2) return;
+    if (!model_) model_ = static_cast<char *>(dmalloc(learned::bytes_for(kModelSegments), s));
+    learned::fit<K>(bmax_, uint64_t(buckets_) - 1, kModelSegments, kModelIters, model_, nullptr, s);
+    model_ready_ = true;
+  }
+  const learned::ModelHeader *model_header() const {
+    return model_ready_ ? reinterpret_cast<const learned::ModelHeader *>(model_) : nullptr;
+  }
+  const learned::Segment *model_segments() const {
+    return model_ready_ ? reinterpret_cast<const learned::Segment *>(model_ + sizeof(learned::ModelHeader)) : nullptr;
+  }
+
   struct Sorted {
     K *keys;
     uint32_t *vals;
@@ -368,7 +389,8 @@ class FlixImpl final : public FlixIndex::Impl {
       flix::set_u32_kernel<K><<<1, 1, 0, s>>>(n_dev, nn); note_launch();
     }
     flix::route_runs_kernel<K><<<unsigned(std::max<uint64_t>(rtiles, 1)), flix::kRouteThreads, 0, s>>>(
-        out.keys, n_dev, bmax_, buckets_, runs, run_count, rlb, rctr, &ctr_->status); note_launch();
+        out.keys, n_dev, bmax_, buckets_, runs, run_count, rlb, rctr, &ctr_->status, model_header(),
+        model_segments()); note_launch();
     return out;
   }
 
@@ -444,7 +466,8 @@ class FlixImpl final : public FlixIndex::Impl {
     const uint32_t nn = uint32_t(n);
     flix::set_u32_kernel<K><<<1, 1, 0, s>>>(n_dev, nn); note_launch();
     flix::route_runs_kernel<K><<<unsigned(std::max<uint64_t>(rtiles, 1)), flix::kRouteThreads, 0, s>>>(
-        probes, n_dev, bmax_, buckets_, runs, run_count, rlb, rctr, &ctr_->status); note_launch();
+        probes, n_dev, bmax_, buckets_, runs, run_count, rlb, rctr, &ctr_->status, model_header(),
+        model_segments()); note_launch();
     run_queries(probes, n_dev, runs, run_count, n, perm, out_v, out_k, s);
     end(s);
   }
@@ -481,6 +504,8 @@ class FlixImpl final : public FlixIndex::Impl {
   uint64_t min_region_ = 0;
   bool built_ = false;
   DevCounters *ctr_ = nullptr;
+  char *model_ = nullptr;  // learned routing model over bmax (search_mode 1)
+  bool model_ready_ = false;
   DevCounters *ctr_host_ = nullptr;
   void *scratch_ = nullptr;
   size_t scratch_bytes_ = 0;

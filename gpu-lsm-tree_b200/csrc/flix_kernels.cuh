@@ -25,6 +25,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "learned.cuh"
 
 namespace gpulsm {
 namespace flix {
@@ -104,6 +105,15 @@ __device__ __forceinline__ uint32_t bucket_of(const K *__restrict__ bmax, uint32
   return lo;
 }
 
+// Same answer through the learned model fitted on bmax[0, buckets-1): the
+// model narrows the search to its error window (learned.cuh); keys above
+// bmax[buckets-2] fall into the last bucket.
+template <typename K>
+__device__ __forceinline__ uint32_t bucket_of_model(const learned::ModelHeader &h, const learned::Segment *seg,
+                                                    const K *__restrict__ bmax, K key) {
+  return uint32_t(learned::model_lower_bound<K>(h, seg, bmax, key));
+}
+
 // Routes a sorted key list to buckets and emits one Run per maximal group of
 // consecutive keys in the same bucket (compacted with decoupled look-back).
 constexpr int kRouteThreads = 256;
@@ -147,8 +157,14 @@ __global__ void __launch_bounds__(kRouteThreads) route_runs_kernel(
     const K *__restrict__ keys, const uint32_t *__restrict__ n_ptr, const K *__restrict__ bmax,
     uint32_t buckets, Run *__restrict__ runs, uint32_t *__restrict__ run_count,
     unsigned long long *__restrict__ lb, uint32_t *__restrict__ tile_counter,
-    uint32_t *__restrict__ status) {
+    uint32_t *__restrict__ status, const learned::ModelHeader *__restrict__ model,
+    const learned::Segment *__restrict__ segs) {
   const uint32_t n = *n_ptr;
+  learned::ModelHeader mh{};
+  if (model) mh = *model;
+  auto route = [&](K key) -> uint32_t {
+    return model ? bucket_of_model<K>(mh, segs, bmax, key) : bucket_of(bmax, buckets, key);
+  };
   __shared__ uint32_t s_scan[kRouteThreads / 32];
   __shared__ uint32_t s_total;
   __shared__ uint32_t s_tile;
@@ -160,7 +176,7 @@ __global__ void __launch_bounds__(kRouteThreads) route_runs_kernel(
   const uint64_t base = uint64_t(tile) * kRouteTile;
   if (base >= n && !(tile == 0 && n == 0)) return;  // grid sized for an upper bound
   if (threadIdx.x == 0)
-    s_prev_bucket = (base > 0 && base <= n) ? bucket_of(bmax, buckets, keys[base - 1]) : kNone;
+    s_prev_bucket = (base > 0 && base <= n) ? route(keys[base - 1]) : kNone;
   __syncthreads();
   const uint64_t mine = base + uint64_t(threadIdx.x) * kRouteItems;
   uint32_t bk[kRouteItems];
@@ -168,7 +184,7 @@ __global__ void __launch_bounds__(kRouteThreads) route_runs_kernel(
 #pragma unroll
   for (int i = 0; i < kRouteItems; ++i) {
     const uint64_t g = mine + i;
-    bk[i] = g < n ? bucket_of(bmax, buckets, keys[g]) : kNone;
+    bk[i] = g < n ? route(keys[g]) : kNone;
   }
   // previous key's bucket for item 0 of this thread
   uint32_t prev = __shfl_up_sync(0xffffffffu, bk[kRouteItems - 1], 1);

@@ -258,28 +258,27 @@ void LsmDictionary::apply_receipt(bool wait) {
   receipt_pending_ = false;
   const Receipt r = *receipt_host_;
   status_bits_ |= uint32_t(r.status);
-  bool current = true;
-  uint64_t total = 0;
+  // A level holds each key once, so one level with more rows than the
+  // capacity means more live keys (tombstones included) than the capacity;
+  // rows summed across levels would count stale versions of a key twice.
+  uint64_t largest = 0;
   for (size_t i = 0; i < levels_.size(); ++i) {
     if (!levels_[i].run) continue;
     if (levels_[i].gen == receipt_gens_[i]) {
       levels_[i].upper = r.n[i];
-    } else {
-      current = false;
+      largest = std::max<uint64_t>(largest, r.n[i]);
     }
-    total += levels_[i].upper;
   }
   if ((r.status & kDevWaitTimeout) && !failed_) {
     failed_ = true;
     failure_ = "GPU dictionary publication failed: a bounded device wait timed out";
   }
-  if ((r.status & kDevOutputOverflow) || (current && total > budget_)) {
+  if ((r.status & kDevOutputOverflow) || largest > budget_) {
     status_bits_ |= kDevOutputOverflow;
     if (!failed_) {
       failed_ = true;
-      failure_ = "GPU dictionary capacity exhausted: " + std::to_string(total) +
-                 " resident rows > capacity " + std::to_string(budget_) +
-                 "; accepted updates were preserved";
+      failure_ = "GPU dictionary capacity exhausted: a level holds " + std::to_string(largest) +
+                 " rows > capacity " + std::to_string(budget_) + "; accepted updates were preserved";
     }
   }
 }

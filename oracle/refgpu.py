@@ -80,6 +80,9 @@ class RefGPULSMOpt:
         except Exception:
             pass
 
+    def clear(self, stream=None):
+        _chk(self._lib.ref_clear(self._h, _stream(stream)))
+
     def bulk_build(self, keys, values, stream=None):
         _chk(self._lib.ref_bulk_build(self._h, keys.data_ptr(), values.data_ptr(), keys.numel(), _stream(stream)))
 

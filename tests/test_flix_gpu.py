@@ -58,11 +58,11 @@ class FlixTwin:
         assert self.f.status() == 0
 
 
-@pytest.mark.parametrize("bits", [32, 64])
-def test_build_lookup_successor(gl, cuda, bits):
+@pytest.mark.parametrize("bits,mode", [(32, 0), (64, 0), (64, 1)])
+def test_build_lookup_successor(gl, cuda, bits, mode):
     rng = np.random.default_rng(bits)
     keys = np.unique(rng.integers(2, 1 << (bits - 2), 50_000, dtype=np.uint64))
-    t = FlixTwin(gl, bits)
+    t = FlixTwin(gl, bits, search_mode=mode)
     t.build(keys)  # sorted unique, values = input index
     probes = np.concatenate([keys[::3], rng.integers(0, 1 << (bits - 2), 20_000, dtype=np.uint64),
                              np.array([0, 1, 2, keys[-1], keys[-1] + 1], np.uint64)])
@@ -78,12 +78,12 @@ def test_unsorted_build_keeps_first_duplicate(gl, cuda, bits):
     t.check(np.arange(0, 5100, dtype=np.uint64))
 
 
-@pytest.mark.parametrize("bits", [32, 64])
-def test_insert_delete_rounds(gl, cuda, bits):
+@pytest.mark.parametrize("bits,mode", [(32, 0), (64, 0), (32, 1), (64, 1)])
+def test_insert_delete_rounds(gl, cuda, bits, mode):
     rng = np.random.default_rng(11 + bits)
     hi = (1 << 31) if bits == 32 else (1 << 40)
     keys = np.unique(rng.integers(2, hi, 100_000, dtype=np.uint64))
-    t = FlixTwin(gl, bits, max_elements=400_000)
+    t = FlixTwin(gl, bits, max_elements=400_000, search_mode=mode)
     t.build(keys)
     hot = rng.integers(2, hi - 100_000, 16, dtype=np.uint64)
     for r in range(8):
@@ -115,9 +115,10 @@ def test_delete_everything_then_successor_walks_buckets(gl, cuda):
     t.check(np.array([0, 50, 51, 100, 101], np.uint64))
 
 
-def test_flix_workload_shape_small(gl, cuda, workloads):
+@pytest.mark.parametrize("mode", [0, 1])
+def test_flix_workload_shape_small(gl, cuda, workloads, mode):
     w = workloads.flix(scale=10, rounds=4)
-    t = FlixTwin(gl, 64, max_elements=w.build_keys.size * 2)
+    t = FlixTwin(gl, 64, max_elements=w.build_keys.size * 2, search_mode=mode)
     t.build(w.build_keys)
     for ins, vals, dels, probes in w.rounds:
         t.insert(ins, vals)
