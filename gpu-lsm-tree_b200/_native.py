@@ -157,6 +157,8 @@ def load() -> C.CDLL:
         "gpulsm_flix_size": (i32, [vp, C.POINTER(u64)]),
         "gpulsm_flix_status": (i32, [vp, C.POINTER(u32)]),
         "gpulsm_sort_pairs": (i32, [vp, vp, vp, vp, u64, u32, u32, u32, vp]),
+        "gpulsm_sort_pairs_noalloc": (i32, [vp, vp, vp, vp, u64, u32, u32, u32, vp]),
+        "gpulsm_sort_noalloc_scratch_bytes": (u64, []),
         "gpulsm_model_bytes": (u64, [u32]),
         "gpulsm_model_fit": (i32, [vp, u64, u32, u32, u32, vp, vp, vp]),
         "gpulsm_model_gradients": (i32, [vp, u64, u32, u32, vp, vp, vp, vp]),

@@ -14,6 +14,7 @@
 #include "radix_sort.cuh"
 #include "model_api.h"
 #include "sort_api.h"
+#include "sort_noalloc.h"
 
 struct gpulsm_dict {
   gpulsm::LsmDictionary impl;
@@ -428,3 +429,25 @@ int gpulsm_sort_pairs(const void *keys_in, const uint32_t *values_in, void *keys
 }
 
 }  // extern "C"
+
+// Allocation-free sort (see sort_noalloc.cu): same checks as gpulsm_sort_pairs.
+extern "C" int gpulsm_sort_pairs_noalloc(const void *keys_in, const uint32_t *values_in, void *keys_out,
+                                         uint32_t *values_out, uint64_t count, uint32_t key_bits,
+                                         uint32_t begin_bit, uint32_t end_bit, void *stream) {
+  return guarded([&] {
+    if (key_bits != 32 && key_bits != 64) throw std::invalid_argument("key_bits must be 32 or 64");
+    if (begin_bit >= end_bit || end_bit > key_bits) throw std::invalid_argument("bad bit range");
+    if (count > gpulsm::kNoallocMaxKeys)
+      throw std::length_error("gpulsm_sort_pairs_noalloc sorts at most 2^20 keys per call");
+    if (!count) return;
+    need(keys_in, "keys_in");
+    need(keys_out, "keys_out");
+    if (values_in) need(values_out, "values_out");
+    device_accessible({{keys_in, "keys_in"}, {values_in, "values_in"}, {keys_out, "keys_out"},
+                       {values_out, "values_out"}});
+    gpulsm::sort_pairs_noalloc(keys_in, values_in, keys_out, values_out, count, key_bits, begin_bit, end_bit,
+                               S(stream));
+  });
+}
+
+extern "C" uint64_t gpulsm_sort_noalloc_scratch_bytes(void) { return gpulsm::noalloc_scratch_bytes(); }

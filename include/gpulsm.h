@@ -191,6 +191,20 @@ int gpulsm_binary_lower_bound(const void *sorted_keys, uint64_t count, uint32_t 
 int gpulsm_sort_pairs(const void *keys_in, const uint32_t *values_in, void *keys_out,
                       uint32_t *values_out, uint64_t count, uint32_t key_bits, uint32_t begin_bit,
                       uint32_t end_bit, void *stream);
+/* No counterpart in the reference.  The same sort for callers that must not
+ * allocate device memory (e.g. a process whose device memory is owned by
+ * another allocator under a fixed budget, or a latency-critical path that
+ * cannot risk a blocking or failing allocation): it calls no cudaMalloc,
+ * cudaFree or allocating library routine.  Its scratch is one static device
+ * array (about 14 MiB, see gpulsm_sort_noalloc_scratch_bytes) that every GPU
+ * loading the library holds until exit.  At most 2^20 keys per call; more
+ * gives GPULSM_ERR_LENGTH.  All calls on a device share that array: calls that
+ * overlap on the GPU race, so serialise them.  The first call on a device
+ * resolves the array's address - make it before any stream capture. */
+int gpulsm_sort_pairs_noalloc(const void *keys_in, const uint32_t *values_in, void *keys_out,
+                              uint32_t *values_out, uint64_t count, uint32_t key_bits, uint32_t begin_bit,
+                              uint32_t end_bit, void *stream);
+uint64_t gpulsm_sort_noalloc_scratch_bytes(void);
 
 #ifdef __cplusplus
 }
