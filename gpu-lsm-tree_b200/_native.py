@@ -159,6 +159,15 @@ def load() -> C.CDLL:
         "gpulsm_sort_pairs": (i32, [vp, vp, vp, vp, u64, u32, u32, u32, vp]),
         "gpulsm_sort_pairs_noalloc": (i32, [vp, vp, vp, vp, u64, u32, u32, u32, vp]),
         "gpulsm_sort_noalloc_scratch_bytes": (u64, []),
+        "gpulsm_tenants_create": (i32, [u32, vp, u64, u32, u32, u32, pvp]),
+        "gpulsm_tenants_destroy": (i32, [vp]),
+        "gpulsm_tenants_set_tuning": (i32, [vp, u32, u32, u32]),
+        "gpulsm_tenants_insert_round": (i32, [vp, vp, vp, vp, vp]),
+        "gpulsm_tenants_round_graph": (i32, [vp, vp, vp, vp, vp]),
+        "gpulsm_tenants_lookup": (i32, [vp, vp, vp, u64, vp, vp, vp]),
+        "gpulsm_tenants_sizes": (i32, [vp, vp]),
+        "gpulsm_tenants_status": (i32, [vp, C.POINTER(u32)]),
+        "gpulsm_tenants_resident_bytes": (i32, [vp, C.POINTER(u64)]),
         "gpulsm_model_bytes": (u64, [u32]),
         "gpulsm_model_fit": (i32, [vp, u64, u32, u32, u32, vp, vp, vp]),
         "gpulsm_model_gradients": (i32, [vp, u64, u32, u32, vp, vp, vp, vp]),

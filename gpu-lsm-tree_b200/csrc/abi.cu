@@ -15,6 +15,7 @@
 #include "model_api.h"
 #include "sort_api.h"
 #include "sort_noalloc.h"
+#include "tenants.h"
 
 struct gpulsm_dict {
   gpulsm::LsmDictionary impl;
@@ -24,6 +25,13 @@ struct gpulsm_dict {
 struct gpulsm_flix {
   gpulsm::FlixIndex impl;
   explicit gpulsm_flix(const gpulsm::FlixConfig &c) : impl(c) {}
+};
+
+struct gpulsm_tenants {
+  gpulsm::TenantPool impl;
+  gpulsm_tenants(uint32_t t, const uint64_t *caps, uint64_t max_round, uint32_t tile, uint32_t fan_in,
+                 uint32_t fanout)
+      : impl(t, caps, max_round, tile, fan_in, fanout) {}
 };
 
 namespace {
@@ -331,6 +339,79 @@ int gpulsm_flix_status(gpulsm_flix *f, uint32_t *out_status) {
     need(f, "index");
     need(out_status, "out_status");
     *out_status = f->impl.status();
+  });
+}
+
+// ---------------------------------------------------------------- tenants
+int gpulsm_tenants_create(uint32_t tenants, const uint64_t *capacities, uint64_t max_round_keys, uint32_t tile,
+                          uint32_t fan_in, uint32_t fanout, gpulsm_tenants **out) {
+  return guarded([&] {
+    need(out, "out");
+    need(capacities, "capacities");
+    *out = new gpulsm_tenants(tenants, capacities, max_round_keys, tile, fan_in, fanout);
+  });
+}
+
+int gpulsm_tenants_destroy(gpulsm_tenants *p) {
+  return guarded([&] { delete p; });
+}
+
+int gpulsm_tenants_set_tuning(gpulsm_tenants *p, uint32_t tile, uint32_t fan_in, uint32_t fanout) {
+  return guarded([&] {
+    need(p, "pool");
+    p->impl.set_tuning(tile, fan_in, fanout);
+  });
+}
+
+int gpulsm_tenants_insert_round(gpulsm_tenants *p, const uint32_t *keys, const uint32_t *values,
+                                const uint64_t *offsets, void *stream) {
+  return guarded([&] {
+    need(p, "pool");
+    device_accessible({{keys, "keys"}, {values, "values"}, {offsets, "offsets"}});
+    p->impl.insert_round(keys, values, offsets, S(stream));
+  });
+}
+
+int gpulsm_tenants_round_graph(gpulsm_tenants *p, const uint32_t *keys, const uint32_t *values,
+                               const uint64_t *offsets, void *stream) {
+  return guarded([&] {
+    need(p, "pool");
+    device_accessible({{keys, "keys"}, {values, "values"}, {offsets, "offsets"}});
+    p->impl.round_graph(keys, values, offsets, S(stream));
+  });
+}
+
+int gpulsm_tenants_lookup(gpulsm_tenants *p, const uint32_t *tenant_ids, const uint32_t *keys, uint64_t count,
+                          uint32_t *out_values, uint8_t *out_found, void *stream) {
+  return guarded([&] {
+    need(p, "pool");
+    device_accessible({{tenant_ids, "tenant_ids"}, {keys, "keys"}, {out_values, "out_values"},
+                       {out_found, "out_found"}});
+    p->impl.lookup(tenant_ids, keys, count, out_values, out_found, S(stream));
+  });
+}
+
+int gpulsm_tenants_sizes(gpulsm_tenants *p, uint64_t *out_rows) {
+  return guarded([&] {
+    need(p, "pool");
+    need(out_rows, "out_rows");
+    p->impl.sizes(out_rows);
+  });
+}
+
+int gpulsm_tenants_status(gpulsm_tenants *p, uint32_t *out_status) {
+  return guarded([&] {
+    need(p, "pool");
+    need(out_status, "out_status");
+    *out_status = p->impl.status();
+  });
+}
+
+int gpulsm_tenants_resident_bytes(gpulsm_tenants *p, uint64_t *out_bytes) {
+  return guarded([&] {
+    need(p, "pool");
+    need(out_bytes, "out_bytes");
+    *out_bytes = p->impl.resident_bytes();
   });
 }
 

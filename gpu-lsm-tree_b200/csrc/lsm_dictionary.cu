@@ -316,8 +316,8 @@ RunBuffer *LsmDictionary::sort_dedup(const uint32_t *keys, const uint32_t *value
                                                                dev_status_, s);
   RunBuffer *carry = pool_.acquire(n, s);
   lsm::dedup_last_kernel<<<unsigned(dtiles), lsm::kCompactThreads, 0, s>>>(
-      bufs[cur], nn, tombstone ? 1 : 0, carry->keys, carry->vals, carry->flags, carry->desc, lb,
-      counter, dev_status_); note_launch();
+      bufs[cur], nn, tombstone ? 1 : 0, carry->keys, carry->vals, carry->flags, carry->desc, carry->dir,
+      carry->dir_bits, rows_log2_, lb, counter, dev_status_); note_launch();
   GPULSM_CUDA(cudaGetLastError());
   return carry;
 }
@@ -325,27 +325,30 @@ RunBuffer *LsmDictionary::sort_dedup(const uint32_t *keys, const uint32_t *value
 RunBuffer *LsmDictionary::merge(RunBuffer *newer, RunBuffer *older, uint64_t out_upper,
                                 bool drop_tombstones, cudaStream_t s) {
   RunBuffer *out = pool_.acquire(out_upper, s);
-  const uint64_t tiles = (out_upper + lsm::kMergeTile - 1) / lsm::kMergeTile;
-  const size_t bytes = merge_scratch_bytes(out_upper);
+  const uint64_t tiles = std::max<uint64_t>(1, (out_upper + lsm::kMergeTile - 1) / lsm::kMergeTile);
+  const size_t zero_bytes = merge_scratch_bytes(out_upper);
+  const size_t bytes = zero_bytes + align_up((tiles + 2) * 8);
   Bump bump{static_cast<char *>(scratch(bytes, s))};
-  GPULSM_CUDA(cudaMemsetAsync(bump.p, 0, bytes, s));
+  GPULSM_CUDA(cudaMemsetAsync(bump.p, 0, zero_bytes, s));
   uint32_t *counter = bump.take<uint32_t>(2);
   unsigned long long *lb = bump.take<unsigned long long>(tiles + 1);
-  lsm::merge_kernel<<<unsigned(std::max<uint64_t>(tiles, 1)), lsm::kMergeThreads, 0, s>>>(
+  bump.off = zero_bytes;
+  unsigned long long *parts = bump.take<unsigned long long>(tiles + 2);
+  lsm::merge_partition_kernel<<<grid_for(tiles + 1, 256), 256, 0, s>>>(newer->keys, newer->desc, older->keys,
+                                                                         older->desc, parts, uint32_t(tiles + 1));
+  note_launch();
+  lsm::merge_kernel<<<unsigned(tiles), lsm::kMergeThreads, 0, s>>>(
       newer->keys, newer->vals, newer->flags, newer->desc, older->keys, older->vals, older->flags,
-      older->desc, out->keys, out->vals, out->flags, out->desc, out->cap, drop_tombstones ? 1 : 0,
-      lb, counter, dev_status_); note_launch();
+      older->desc, out->keys, out->vals, out->flags, out->desc, out->dir, out->dir_bits, rows_log2_,
+      std::min<uint64_t>(out_upper, out->cap), out->cap, drop_tombstones ? 1 : 0, parts, lb, counter,
+      dev_status_);
+  note_launch();
   GPULSM_CUDA(cudaGetLastError());
   pool_.release(newer);
   pool_.release(older);
   return out;
 }
 
-void LsmDictionary::build_directory(RunBuffer *run, uint64_t upper, cudaStream_t s) {
-  lsm::directory_kernel<<<grid_for(std::max<uint64_t>(upper, 1), 256), 256, 0, s>>>(
-      run->keys, run->desc, run->dir, run->dir_bits, rows_log2_); note_launch();
-  GPULSM_CUDA(cudaGetLastError());
-}
 
 void LsmDictionary::cascade(RunBuffer *carry, uint64_t carry_upper, bool carry_tombs, cudaStream_t s) {
   const size_t L = levels_.size();
@@ -382,8 +385,7 @@ void LsmDictionary::cascade(RunBuffer *carry, uint64_t carry_upper, bool carry_t
   levels_[dest].run = x;
   levels_[dest].upper = std::min<uint64_t>(xu, x->cap);
   levels_[dest].gen = next_gen_++;
-  levels_[dest].tombs = xt;
-  build_directory(x, levels_[dest].upper, s);
+  levels_[dest].tombs = xt;  // its directory was written by the kernel that wrote its rows
 }
 
 // Merge every occupied level, newest first, into one tombstone-free run at
@@ -417,7 +419,6 @@ void LsmDictionary::compact_all(cudaStream_t s) {
   levels_[dest].upper = std::min<uint64_t>(xu, x->cap);
   levels_[dest].gen = next_gen_++;
   levels_[dest].tombs = false;
-  build_directory(x, levels_[dest].upper, s);
 }
 
 int LsmDictionary::ranges_on_single_level(const uint32_t *lo, const uint32_t *hi, uint64_t n, cudaStream_t s) {
@@ -526,7 +527,6 @@ void LsmDictionary::bulk_build(const uint32_t *keys, const uint32_t *values, uin
     top.upper = n;
     top.gen = next_gen_++;
     top.tombs = false;
-    build_directory(run, n, s);
     post_receipt(s);
   }
   end_op(s);

@@ -107,7 +107,6 @@ class LsmDictionary {
   void cascade(RunBuffer *carry, uint64_t carry_upper, bool carry_tombs, cudaStream_t s);
   RunBuffer *merge(RunBuffer *newer, RunBuffer *older, uint64_t out_upper, bool drop_tombstones,
                    cudaStream_t s);
-  void build_directory(RunBuffer *run, uint64_t upper, cudaStream_t s);
   // Range batches: merge every level into one tombstone-free run when the
   // rows the batch covers outweigh the merge; returns the single level to
   // answer from, or -1 to use the per-query k-way merge.

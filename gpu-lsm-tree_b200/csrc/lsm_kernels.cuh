@@ -104,10 +104,66 @@ __global__ void __launch_bounds__(256) pack_histogram_kernel(const uint32_t *__r
   }
 }
 
+// ---------------------------------------------------------------------------
+// Radix directory built by the kernel that writes the run.  Its geometry is
+// fixed before the rows exist from a key range [kmin, kmax] that bounds every
+// output row (dedup and tombstone drops only remove rows) and the host's upper
+// bound of the row count: about 2^rows_log2 rows per bucket, at most
+// 2^dir_bits buckets.
+struct DirGeom {
+  uint32_t kmin, kmax, shift, nbuckets;
+};
+
+__device__ __forceinline__ DirGeom dir_geometry(uint32_t kmin, uint32_t kmax, unsigned long long n_upper,
+                                                uint32_t dir_bits, uint32_t rows_log2) {
+  const uint32_t range = kmax - kmin;
+  const uint32_t nl2 = ceil_log2_u64(n_upper ? n_upper : 1);
+  const uint32_t want = min(nl2 > rows_log2 ? nl2 - rows_log2 : 0u, dir_bits);
+  const uint32_t range_bits = range ? 32u - __clz(range) : 0u;
+  const uint32_t shift = range_bits > want ? range_bits - want : 0u;
+  return DirGeom{kmin, kmax, shift, (range >> shift) + 1u};
+}
+
+// A tile that consumed the input keys in (prev_key, last_key] (no prev for the
+// first tile) and kept `cnt` rows - keys key_at(0..cnt) at global positions
+// g0.. - owns the directory buckets (bucket(prev_key), bucket(last_key)]: each
+// gets the position of the tile's first kept row in or after it, or g0 + cnt
+// (where the next tile's rows start) when no kept row of the tile reaches it.
+// Consecutive tiles own consecutive bucket ranges, so every entry is written
+// exactly once; the last tile also closes the range and writes dir[nbuckets].
+template <typename KeyAt>
+__device__ __forceinline__ void fill_directory(uint32_t *__restrict__ dir, const DirGeom &g, bool has_prev,
+                                               uint32_t prev_key, uint32_t last_key, bool last_tile,
+                                               unsigned long long g0, uint32_t cnt, unsigned long long n_out,
+                                               KeyAt key_at) {
+  const int64_t bp = has_prev ? int64_t((prev_key - g.kmin) >> g.shift) : -1;
+  const int64_t bl = last_tile ? int64_t(g.nbuckets) - 1 : int64_t((last_key - g.kmin) >> g.shift);
+  for (uint32_t j = threadIdx.x; j < cnt; j += blockDim.x) {
+    const int64_t bj = int64_t((key_at(j) - g.kmin) >> g.shift);
+    const int64_t bprev = j ? int64_t((key_at(j - 1) - g.kmin) >> g.shift) : bp;
+    for (int64_t b = bprev + 1; b <= bj; ++b) dir[b] = uint32_t(g0 + j);
+  }
+  if (threadIdx.x == 0) {
+    const int64_t blast = cnt ? int64_t((key_at(cnt - 1) - g.kmin) >> g.shift) : bp;
+    for (int64_t b = blast + 1; b <= bl; ++b) dir[b] = uint32_t(g0 + cnt);
+    if (last_tile) dir[g.nbuckets] = uint32_t(n_out);
+  }
+}
+
+__device__ __forceinline__ void write_empty_desc(LevelDesc *d, uint32_t *dir) {
+  d->n = 0;
+  d->kmin = 1u;
+  d->kmax = 0u;
+  d->shift = 0u;
+  d->nbuckets = 1u;
+  dir[0] = 0u;
+  dir[1] = 0u;
+}
+
 // Keep the LAST word of every equal-key run of a stably sorted batch (the
 // highest input index wins, GPULSMOpt.cuh:2578-2598 ages + :2633 keep-last)
-// and split it into a level (keys, vals, flags).  Single pass: tile counts are
-// chained by decoupled look-back.
+// and split it into a level (keys, vals, flags, directory).  Single pass: tile
+// counts are chained by decoupled look-back.
 constexpr int kCompactThreads = 256;
 constexpr int kCompactItems = 8;
 constexpr uint32_t kCompactTile = kCompactThreads * kCompactItems;
@@ -115,8 +171,8 @@ constexpr uint32_t kCompactTile = kCompactThreads * kCompactItems;
 __global__ void __launch_bounds__(kCompactThreads) dedup_last_kernel(
     const unsigned long long *__restrict__ words, uint32_t n, int tombstone,
     uint32_t *__restrict__ out_keys, uint32_t *__restrict__ out_vals, uint8_t *__restrict__ out_flags,
-    LevelDesc *__restrict__ out_desc, unsigned long long *__restrict__ lb,
-    uint32_t *__restrict__ tile_counter, uint32_t *__restrict__ status) {
+    LevelDesc *__restrict__ out_desc, uint32_t *__restrict__ out_dir, uint32_t dir_bits, uint32_t rows_log2,
+    unsigned long long *__restrict__ lb, uint32_t *__restrict__ tile_counter, uint32_t *__restrict__ status) {
   __shared__ unsigned long long s_words[kCompactTile + 1];
   __shared__ uint32_t s_scan[kCompactThreads / 32];
   __shared__ uint32_t s_total;
@@ -165,7 +221,20 @@ __global__ void __launch_bounds__(kCompactThreads) dedup_last_kernel(
     out_vals[gbase + j] = tombstone ? kTombValue : uint32_t(w);
     out_flags[gbase + j] = tombstone ? kFlagTomb : 0u;
   }
-  if (base + kCompactTile >= n && threadIdx.x == 0) out_desc->n = gbase + tile_kept;
+  // directory over the batch's key range (the sorted input's first and last key)
+  const DirGeom g = dir_geometry(uint32_t(words[0] >> 32), uint32_t(words[n - 1] >> 32), n, dir_bits, rows_log2);
+  const bool last_tile = base + kCompactTile >= n;
+  const unsigned long long kept_total = gbase + tile_kept;
+  fill_directory(out_dir, g, base > 0, base > 0 ? uint32_t(words[base - 1] >> 32) : 0u,
+                 uint32_t(words[base + count - 1] >> 32), last_tile, gbase, tile_kept, kept_total,
+                 [&](uint32_t j) { return uint32_t(s_words[j] >> 32); });
+  if (tile == 0 && threadIdx.x == 0) {
+    out_desc->kmin = g.kmin;
+    out_desc->kmax = g.kmax;
+    out_desc->shift = g.shift;
+    out_desc->nbuckets = g.nbuckets;
+  }
+  if (last_tile && threadIdx.x == 0) out_desc->n = kept_total;
 }
 
 // ---------------------------------------------------------------------------
@@ -174,7 +243,7 @@ __global__ void __launch_bounds__(kCompactThreads) dedup_last_kernel(
 // key was just taken from A is shadowed and dropped (newest level wins).  With
 // drop_tombstones (the output becomes the oldest level) tombstones disappear.
 constexpr int kMergeThreads = 256;
-constexpr int kMergeItems = 8;
+constexpr int kMergeItems = 16;
 constexpr uint32_t kMergeTile = kMergeThreads * kMergeItems;
 
 __device__ __forceinline__ uint64_t merge_path(const uint32_t *a, uint64_t na, const uint32_t *b,
@@ -188,32 +257,55 @@ __device__ __forceinline__ uint64_t merge_path(const uint32_t *a, uint64_t na, c
   return lo;
 }
 
+// Split points of every merge tile, one thread per tile boundary: the
+// dependent binary searches run in parallel here instead of serialising each
+// merge tile behind one searching thread.  parts[i] = A rows before diagonal
+// min(i * kMergeTile, na + nb).
+__global__ void __launch_bounds__(256) merge_partition_kernel(const uint32_t *__restrict__ ak,
+                                                              const LevelDesc *__restrict__ adesc,
+                                                              const uint32_t *__restrict__ bk,
+                                                              const LevelDesc *__restrict__ bdesc,
+                                                              unsigned long long *__restrict__ parts,
+                                                              uint32_t max_parts) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= max_parts) return;
+  const uint64_t na = adesc->n, nb = bdesc->n, total = na + nb;
+  const uint64_t d = min(uint64_t(i) * kMergeTile, total);
+  parts[i] = merge_path(ak, na, bk, nb, d);
+}
+
 __global__ void __launch_bounds__(kMergeThreads) merge_kernel(
     const uint32_t *__restrict__ ak, const uint32_t *__restrict__ av, const uint8_t *__restrict__ af,
     const LevelDesc *__restrict__ adesc, const uint32_t *__restrict__ bk,
     const uint32_t *__restrict__ bv, const uint8_t *__restrict__ bf,
     const LevelDesc *__restrict__ bdesc, uint32_t *__restrict__ ok, uint32_t *__restrict__ ov,
-    uint8_t *__restrict__ of, LevelDesc *__restrict__ odesc, unsigned long long out_capacity,
-    int drop_tombstones, unsigned long long *__restrict__ lb, uint32_t *__restrict__ tile_counter,
-    uint32_t *__restrict__ status) {
+    uint8_t *__restrict__ of, LevelDesc *__restrict__ odesc, uint32_t *__restrict__ odir, uint32_t dir_bits,
+    uint32_t rows_log2, unsigned long long out_upper, unsigned long long out_capacity, int drop_tombstones,
+    const unsigned long long *__restrict__ parts, unsigned long long *__restrict__ lb,
+    uint32_t *__restrict__ tile_counter, uint32_t *__restrict__ status) {
   __shared__ uint32_t s_k[kMergeTile];
   __shared__ uint32_t s_v[kMergeTile];
   __shared__ uint8_t s_f[kMergeTile];
   __shared__ uint32_t s_scan[kMergeThreads / 32];
   __shared__ uint32_t s_total;
   __shared__ uint32_t s_tile;
-  __shared__ unsigned long long s_a0, s_a1, s_base;
+  __shared__ unsigned long long s_base;
   if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
   __syncthreads();
   const uint64_t na = adesc->n, nb = bdesc->n, total = na + nb;
   const uint32_t tile = s_tile;
   const uint64_t d0 = uint64_t(tile) * kMergeTile;
-  if (d0 >= total && !(tile == 0 && total == 0)) return;  // beyond the merged length
+  if (total == 0) {
+    if (tile == 0 && threadIdx.x == 0) write_empty_desc(odesc, odir);
+    return;
+  }
+  if (d0 >= total) return;  // beyond the merged length (grid sized for an upper bound)
   const uint64_t d1 = min(d0 + kMergeTile, total);
-  if (threadIdx.x == 0) s_a0 = merge_path(ak, na, bk, nb, d0);
-  if (threadIdx.x == 32) s_a1 = merge_path(ak, na, bk, nb, d1);
-  __syncthreads();
-  const uint64_t a0 = s_a0, a1 = s_a1, b0 = d0 - a0, b1 = d1 - a1;
+  // every output key lies in the union of the inputs' key ranges
+  const uint32_t kmin = na == 0 ? bdesc->kmin : nb == 0 ? adesc->kmin : min(adesc->kmin, bdesc->kmin);
+  const uint32_t kmax = na == 0 ? bdesc->kmax : nb == 0 ? adesc->kmax : max(adesc->kmax, bdesc->kmax);
+  const DirGeom geom = dir_geometry(kmin, kmax, out_upper, dir_bits, rows_log2);
+  const uint64_t a0 = parts[tile], a1 = parts[tile + 1], b0 = d0 - a0, b1 = d1 - a1;
   const uint32_t alen = uint32_t(a1 - a0), blen = uint32_t(b1 - b0);
   // stage A then B in shared memory
   for (uint32_t j = threadIdx.x; j < alen; j += kMergeThreads) {
@@ -226,9 +318,13 @@ __global__ void __launch_bounds__(kMergeThreads) merge_kernel(
     s_v[alen + j] = bv[b0 + j];
     s_f[alen + j] = bf[b0 + j];
   }
-  // key of the A row just before this tile (shadows a leading B row)
+  // key of the A row just before this tile (shadows a leading B row); the
+  // largest key consumed before / by this tile bounds its directory buckets
   const bool has_prev_a = a0 > 0;
   const uint32_t prev_a_global = has_prev_a ? ak[a0 - 1] : 0u;
+  const bool has_prev = a0 > 0 || b0 > 0;
+  const uint32_t prev_key = max(has_prev_a ? prev_a_global : 0u, b0 > 0 ? bk[b0 - 1] : 0u);
+  const uint32_t last_key = max(a1 > 0 ? ak[a1 - 1] : 0u, b1 > 0 ? bk[b1 - 1] : 0u);
   __syncthreads();
   const uint32_t *sa = s_k, *sb = s_k + alen;
   const uint32_t my_d = min(uint32_t(threadIdx.x) * kMergeItems, alen + blen);
@@ -237,45 +333,51 @@ __global__ void __launch_bounds__(kMergeThreads) merge_kernel(
   uint32_t bi = my_d - ai;
   bool have_prev = ai > 0 ? true : has_prev_a;
   uint32_t prev_a = ai > 0 ? sa[ai - 1] : prev_a_global;
-  uint32_t src[kMergeItems];  // smem index of each kept row
-  uint32_t kept = 0;
-  for (uint32_t d = my_d; d < my_e; ++d) {
-    const bool take_a = ai < alen && (bi >= blen || sa[ai] <= sb[bi]);
-    uint32_t idx, key;
-    bool keep;
-    if (take_a) {
-      idx = ai++;
-      key = sa[idx];
-      have_prev = true;
-      prev_a = key;
-      keep = true;
-    } else {
-      idx = alen + bi++;
-      key = sb[idx - alen];
-      keep = !(have_prev && prev_a == key);
+  uint32_t src[kMergeItems];  // smem index of each item, kept ones flagged in keep_mask
+  uint32_t keep_mask = 0;
+#pragma unroll
+  for (int i = 0; i < kMergeItems; ++i) {
+    src[i] = 0;
+    if (my_d + i < my_e) {
+      const bool take_a = ai < alen && (bi >= blen || sa[ai] <= sb[bi]);
+      uint32_t idx, key;
+      bool keep;
+      if (take_a) {
+        idx = ai++;
+        key = sa[idx];
+        have_prev = true;
+        prev_a = key;
+        keep = true;
+      } else {
+        idx = alen + bi++;
+        key = sb[idx - alen];
+        keep = !(have_prev && prev_a == key);
+      }
+      if (keep && drop_tombstones && s_v[idx] == kTombValue && (s_f[idx] & kFlagTomb)) keep = false;
+      src[i] = idx;
+      if (keep) keep_mask |= 1u << i;
     }
-    if (keep && drop_tombstones && s_v[idx] == kTombValue && (s_f[idx] & kFlagTomb)) keep = false;
-    if (keep) src[kept++] = idx;
   }
+  const uint32_t kept = __popc(keep_mask);
   const uint32_t local = block_exclusive_scan<kMergeThreads>(kept, s_scan, &s_total);
   const uint32_t tile_kept = s_total;
   if (threadIdx.x == 0) s_base = tile_lookback(lb, tile, tile_kept, status);
   uint32_t rk[kMergeItems], rv[kMergeItems];
   uint8_t rf[kMergeItems];
 #pragma unroll
-  for (int i = 0; i < kMergeItems; ++i)
-    if (uint32_t(i) < kept) {
-      rk[i] = s_k[src[i]];
-      rv[i] = s_v[src[i]];
-      rf[i] = s_f[src[i]];
-    }
+  for (int i = 0; i < kMergeItems; ++i) {
+    rk[i] = s_k[src[i]];
+    rv[i] = s_v[src[i]];
+    rf[i] = s_f[src[i]];
+  }
   __syncthreads();
 #pragma unroll
   for (int i = 0; i < kMergeItems; ++i)
-    if (uint32_t(i) < kept) {
-      s_k[local + i] = rk[i];
-      s_v[local + i] = rv[i];
-      s_f[local + i] = rf[i];
+    if (keep_mask & (1u << i)) {
+      const uint32_t o = local + __popc(keep_mask & ((1u << i) - 1u));
+      s_k[o] = rk[i];
+      s_v[o] = rv[i];
+      s_f[o] = rf[i];
     }
   __syncthreads();
   const unsigned long long gbase = s_base;
@@ -287,65 +389,20 @@ __global__ void __launch_bounds__(kMergeThreads) merge_kernel(
       of[o] = s_f[j];
     }
   }
-  if (d1 == total && threadIdx.x == 0) {
-    const unsigned long long n_out = gbase + tile_kept;
+  const bool last_tile = d1 == total;
+  const unsigned long long n_out = gbase + tile_kept;
+  fill_directory(odir, geom, has_prev, prev_key, last_key, last_tile, gbase, tile_kept,
+                 n_out < out_capacity ? n_out : out_capacity, [&](uint32_t j) { return s_k[j]; });
+  if (tile == 0 && threadIdx.x == 0) {
+    odesc->kmin = geom.kmin;
+    odesc->kmax = geom.kmax;
+    odesc->shift = geom.shift;
+    odesc->nbuckets = geom.nbuckets;
+  }
+  if (last_tile && threadIdx.x == 0) {
     if (n_out > out_capacity) atomicOr(status, kDevOutputOverflow);
     odesc->n = n_out < out_capacity ? n_out : out_capacity;
   }
-}
-
-// Copy a run (used when a carry that still holds duplicates or tombstones must
-// be placed as is) - plain grid-stride copy of the three streams.
-__global__ void copy_run_kernel(const uint32_t *__restrict__ k, const uint32_t *__restrict__ v,
-                                const uint8_t *__restrict__ f, const LevelDesc *__restrict__ d,
-                                uint32_t *__restrict__ ok, uint32_t *__restrict__ ov,
-                                uint8_t *__restrict__ of, LevelDesc *__restrict__ od) {
-  const uint64_t n = d->n;
-  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-       i += uint64_t(gridDim.x) * blockDim.x) {
-    ok[i] = k[i];
-    ov[i] = v[i];
-    of[i] = f[i];
-  }
-  if (blockIdx.x == 0 && threadIdx.x == 0) od->n = n;
-}
-
-// ---------------------------------------------------------------------------
-// Radix directory over the level's own key range [kmin, kmax]: about
-// 2^rows_log2 rows per bucket, at most 2^dir_bits buckets.
-__global__ void directory_kernel(const uint32_t *__restrict__ keys, LevelDesc *__restrict__ desc,
-                                 uint32_t *__restrict__ dir, uint32_t dir_bits, uint32_t rows_log2) {
-  const uint64_t n = desc->n;
-  const uint64_t p = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (n == 0) {
-    if (p == 0) {
-      desc->kmin = 1u;
-      desc->kmax = 0u;
-      desc->shift = 0u;
-      desc->nbuckets = 1u;
-      dir[0] = 0u;
-      dir[1] = 0u;
-    }
-    return;
-  }
-  const uint32_t kmin = keys[0], kmax = keys[n - 1];
-  const uint32_t range = kmax - kmin;
-  const uint32_t nl2 = ceil_log2_u64(n);
-  const uint32_t want = min(nl2 > rows_log2 ? nl2 - rows_log2 : 0u, dir_bits);
-  const uint32_t range_bits = range ? 32u - __clz(range) : 0u;
-  const uint32_t shift = range_bits > want ? range_bits - want : 0u;
-  const uint32_t nbuckets = (range >> shift) + 1u;
-  if (p == 0) {
-    desc->kmin = kmin;
-    desc->kmax = kmax;
-    desc->shift = shift;
-    desc->nbuckets = nbuckets;
-  }
-  if (p >= n) return;
-  const int64_t b = int64_t((keys[p] - kmin) >> shift);
-  const int64_t bp = p ? int64_t((keys[p - 1] - kmin) >> shift) : -1;
-  for (int64_t bb = bp + 1; bb <= b; ++bb) dir[bb] = uint32_t(p);
-  if (p == n - 1) dir[nbuckets] = uint32_t(n);
 }
 
 // ---------------------------------------------------------------------------

@@ -59,9 +59,12 @@ struct OnesweepSmem {
 template <typename KeyT, bool kValues>
 __global__ void __launch_bounds__(kThreads) onesweep_kernel(
     const KeyT *__restrict__ kin, const uint32_t *__restrict__ vin, KeyT *__restrict__ kout,
-    uint32_t *__restrict__ vout, uint32_t n, uint32_t shift, const uint32_t *__restrict__ pass_hist,
+    uint32_t *__restrict__ vout, uint32_t n_host, uint32_t shift, const uint32_t *__restrict__ pass_hist,
     uint32_t *__restrict__ lookback, uint32_t *__restrict__ tile_counter,
-    uint32_t *__restrict__ status) {
+    uint32_t *__restrict__ status, const uint32_t *__restrict__ n_dev) {
+  // n_dev (optional) carries a count produced on the device; the grid is then
+  // sized for n_host, an upper bound, and tiles past the count leave at once
+  const uint32_t n = n_dev ? *n_dev : n_host;
   extern __shared__ __align__(16) unsigned char dyn[];
   KeyT *s_keys = reinterpret_cast<KeyT *>(dyn);
   uint32_t *s_vals = reinterpret_cast<uint32_t *>(dyn + size_t(kTile) * sizeof(KeyT));
@@ -78,6 +81,7 @@ __global__ void __launch_bounds__(kThreads) onesweep_kernel(
   const uint32_t tile = s_tile;
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t tile_base = tile * kTile;
+  if (tile_base >= n) return;  // past a device-side count: no later tile waits on this one
   const uint32_t warp_base = tile_base + warp * 32 * kItems;
 
   KeyT keys[kItems];
@@ -176,7 +180,8 @@ __global__ void __launch_bounds__(kThreads) onesweep_kernel(
 // buffer that holds the sorted output.
 template <typename KeyT, bool kValues>
 int run_passes(KeyT *keys[2], uint32_t *vals[2], uint32_t n, int begin_bit, int end_bit,
-               uint32_t *workspace, uint32_t *status, cudaStream_t stream) {
+               uint32_t *workspace, uint32_t *status, cudaStream_t stream,
+               const uint32_t *n_dev = nullptr) {
   const int passes = (end_bit - begin_bit + 7) / 8;
   const uint32_t tiles = tiles_for(n);
   const size_t smem = OnesweepSmem<KeyT, kValues>::bytes;
@@ -190,7 +195,7 @@ int run_passes(KeyT *keys[2], uint32_t *vals[2], uint32_t n, int begin_bit, int 
     onesweep_kernel<KeyT, kValues><<<tiles, kThreads, smem, stream>>>(
         keys[cur], kValues ? vals[cur] : nullptr, keys[cur ^ 1], kValues ? vals[cur ^ 1] : nullptr,
         n, uint32_t(begin_bit + 8 * p), hist + p * kDigits, lookback + size_t(p) * tiles * kDigits,
-        counters + p, status); note_launch();
+        counters + p, status, n_dev); note_launch();
     cur ^= 1;
   }
   GPULSM_CUDA(cudaGetLastError());

@@ -160,6 +160,37 @@ int gpulsm_flix_resident_bytes(gpulsm_flix *index, uint64_t *out_bytes);
 int gpulsm_flix_size(gpulsm_flix *index, uint64_t *out_keys);
 int gpulsm_flix_status(gpulsm_flix *index, uint32_t *out_status);
 
+/* ===================== multi-tenant batched dictionary ==================== */
+/* Many independent u32 dictionaries (GPULSMOpt upsert semantics, inserts and
+ * lookups) updated in rounds.  No reference counterpart: the reference would
+ * need one GPULSMOpt per tenant, each with its fixed directories
+ * (GPULSMOpt.cuh:5640-5702).  A round passes one batch per tenant as CSR:
+ * keys/values concatenated in tenant order and offsets[tenants + 1] (u64), all
+ * device memory; per-tenant answers equal one GPULSMOpt per tenant. */
+typedef struct gpulsm_tenants gpulsm_tenants;
+/* capacities: HOST array of per-tenant maximum live keys; max_round_keys bounds
+ * one round's total batch; tile (256..4096), fan_in (1..16: rounds gathered in
+ * a tenant's delta run before it merges into its main run) and fanout (8, 16,
+ * 32: B-ary fence tree) are the tunables, 0 = defaults 2048 / 4 / 16. */
+int gpulsm_tenants_create(uint32_t tenants, const uint64_t *capacities, uint64_t max_round_keys, uint32_t tile,
+                          uint32_t fan_in, uint32_t fanout, gpulsm_tenants **out);
+int gpulsm_tenants_destroy(gpulsm_tenants *pool);
+int gpulsm_tenants_set_tuning(gpulsm_tenants *pool, uint32_t tile, uint32_t fan_in, uint32_t fanout);
+/* One round: everything sized on the device, no host wait. */
+int gpulsm_tenants_insert_round(gpulsm_tenants *pool, const uint32_t *keys, const uint32_t *values,
+                                const uint64_t *offsets, void *stream);
+/* The same round replayed from a CUDA graph captured once per (buffers, round
+ * kind); stream must not be the legacy default stream. */
+int gpulsm_tenants_round_graph(gpulsm_tenants *pool, const uint32_t *keys, const uint32_t *values,
+                               const uint64_t *offsets, void *stream);
+/* (tenant, key) lookups; out_found may be NULL (misses then read 0xffffffff). */
+int gpulsm_tenants_lookup(gpulsm_tenants *pool, const uint32_t *tenant_ids, const uint32_t *keys, uint64_t count,
+                          uint32_t *out_values, uint8_t *out_found, void *stream);
+/* Rows held per tenant (main + delta runs; a key may appear in both), host array. */
+int gpulsm_tenants_sizes(gpulsm_tenants *pool, uint64_t *out_rows);
+int gpulsm_tenants_status(gpulsm_tenants *pool, uint32_t *out_status);
+int gpulsm_tenants_resident_bytes(gpulsm_tenants *pool, uint64_t *out_bytes);
+
 /* ===================== learned position model ============================ */
 /* A piecewise-linear CDF over one sorted key array (no reference counterpart:
  * the reference narrows searches with 128-cell rank directories,
