@@ -36,12 +36,13 @@ __host__ __device__ __forceinline__ unsigned long long fence_level_size(unsigned
 // (tenant << 32 | key) and histograms for the sort passes.
 __global__ void __launch_bounds__(256) pack_tenant_words_kernel(
     const uint32_t *__restrict__ keys, const uint32_t *__restrict__ vals,
-    const unsigned long long *__restrict__ batch_off, uint32_t tenants, unsigned long long *__restrict__ words,
-    uint32_t *__restrict__ wvals, uint32_t passes, uint32_t *__restrict__ hist) {
+    const unsigned long long *__restrict__ batch_off, uint32_t tenants, const uint32_t *__restrict__ count,
+    unsigned long long *__restrict__ words, uint32_t *__restrict__ wvals, uint32_t passes,
+    uint32_t *__restrict__ hist) {
   __shared__ uint32_t s[8][256];
   for (uint32_t i = threadIdx.x; i < 8 * 256; i += 256) (&s[0][0])[i] = 0;
   __syncthreads();
-  const unsigned long long n = batch_off[tenants];
+  const unsigned long long n = *count;
   for (unsigned long long i = uint64_t(blockIdx.x) * 256 + threadIdx.x; i < n; i += uint64_t(gridDim.x) * 256) {
     uint32_t lo = 0, hi = tenants;  // last t with batch_off[t] <= i
     while (hi - lo > 1) {
@@ -61,10 +62,19 @@ __global__ void __launch_bounds__(256) pack_tenant_words_kernel(
   }
 }
 
-// the round's batch total (device CSR offsets) as the sort passes' u32 count
+// the round's batch total (device CSR offsets) as the u32 count every later
+// step reads; a round larger than the configured maximum is refused (status
+// bit, nothing applied) instead of overrunning the round buffers
 __global__ void set_count_kernel(const unsigned long long *__restrict__ batch_off, uint32_t tenants,
-                                 uint32_t *__restrict__ count) {
-  *count = uint32_t(batch_off[tenants]);
+                                 unsigned long long max_round, uint32_t *__restrict__ count,
+                                 uint32_t *__restrict__ status) {
+  const unsigned long long n = batch_off[tenants];
+  if (n > max_round || batch_off[0] != 0) {
+    *count = 0;
+    atomicOr(status, kDevBadInput);
+  } else {
+    *count = uint32_t(n);
+  }
 }
 
 // Round step 3: keep the last update of each (tenant, key) (stable sort keeps
@@ -108,14 +118,14 @@ __device__ __forceinline__ unsigned long long lookback(unsigned long long *lb, u
 
 __global__ void __launch_bounds__(kDedupThreads) dedup_tenant_words_kernel(
     const unsigned long long *__restrict__ words, const uint32_t *__restrict__ wvals,
-    const unsigned long long *__restrict__ batch_off, uint32_t tenants, uint32_t *__restrict__ out_keys,
+    const uint32_t *__restrict__ count, uint32_t tenants, uint32_t *__restrict__ out_keys,
     uint32_t *__restrict__ out_vals, uint32_t *__restrict__ out_tenant, unsigned long long *__restrict__ bstart,
     unsigned long long *__restrict__ lb, uint32_t *__restrict__ tile_counter, uint32_t *__restrict__ status) {
   __shared__ uint32_t s_scan[kDedupThreads / 32];
   __shared__ uint32_t s_total;
   __shared__ uint32_t s_tile;
   __shared__ unsigned long long s_base;
-  const unsigned long long n = batch_off[tenants];
+  const unsigned long long n = *count;
   if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
   __syncthreads();
   const unsigned long long base = uint64_t(s_tile) * kDedupTile + uint64_t(threadIdx.x) * kDedupItems;
@@ -212,6 +222,11 @@ __global__ void tenant_tiles_kernel(MergeArgs m, unsigned long long *__restrict_
   const unsigned long long nx = m.kind == kBatchIntoDelta ? m.bstart[t + 1] - m.bstart[t] : mt.delta_n;
   const unsigned long long ny = m.kind == kBatchIntoDelta ? mt.delta_n : mt.main_n;
   const unsigned long long total = nx + ny;
+  if (nx > mt.cap) {  // a batch larger than the tenant's capacity cannot fit: refuse it
+    atomicOr(m.status, kDevBadInput);
+    tiles[t] = 0;
+    return;
+  }
   tiles[t] = nx ? (total + m.tile - 1) / m.tile : 0ull;  // nothing newer: the run stays as it is
 }
 

@@ -188,18 +188,18 @@ void TenantPool::enqueue_round(const uint32_t *keys, const uint32_t *values, con
   const auto *off = reinterpret_cast<const unsigned long long *>(offsets);
   const uint32_t passes = (32 + tenant_bits() + 7) / 8;
   GPULSM_CUDA(cudaMemsetAsync(zero_, 0, zero_bytes_, s));
+  // the device-side batch total (checked against max_round_keys) read by every step below
+  tenants::set_count_kernel<<<1, 1, 0, s>>>(off, tenants_, max_round_, misc_, misc_ + 1); note_launch();
   const unsigned pack_blocks = std::min<unsigned>(grid_for(max_round_, 4096), unsigned(num_sms_) * 4u);
-  tenants::pack_tenant_words_kernel<<<pack_blocks, 256, 0, s>>>(keys, values, off, tenants_, words_[0], wvals_[0],
-                                                                 passes, radix_ws_); note_launch();
-  // the device-side batch total as u32 for the sort passes
-  tenants::set_count_kernel<<<1, 1, 0, s>>>(off, tenants_, misc_); note_launch();
+  tenants::pack_tenant_words_kernel<<<pack_blocks, 256, 0, s>>>(keys, values, off, tenants_, misc_, words_[0],
+                                                                 wvals_[0], passes, radix_ws_); note_launch();
   unsigned long long *kk[2] = {words_[0], words_[1]};
   uint32_t *vv[2] = {wvals_[0], wvals_[1]};
   const int cur = radix::run_passes<unsigned long long, true>(kk, vv, uint32_t(max_round_), 0, int(passes * 8),
                                                               radix_ws_, misc_ + 1, s, misc_);
   const uint64_t dtiles = (max_round_ + tenants::kDedupTile - 1) / tenants::kDedupTile;
   tenants::dedup_tenant_words_kernel<<<unsigned(std::max<uint64_t>(dtiles, 1)), tenants::kDedupThreads, 0, s>>>(
-      kk[cur], vv[cur], off, tenants_, bkeys_, bvals_, btenant_, bstart_, dedup_lb_, dedup_ctr_, misc_ + 1);
+      kk[cur], vv[cur], misc_, tenants_, bkeys_, bvals_, btenant_, bstart_, dedup_lb_, dedup_ctr_, misc_ + 1);
   note_launch();
   tenants::tenant_slices_kernel<<<grid_for(std::max<uint64_t>(max_round_, tenants_), 256), 256, 0, s>>>(
       btenant_, bstart_, tenants_); note_launch();
