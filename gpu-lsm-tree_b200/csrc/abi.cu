@@ -532,3 +532,4 @@ extern "C" int gpulsm_sort_pairs_noalloc(const void *keys_in, const uint32_t *va
 }
 
 extern "C" uint64_t gpulsm_sort_noalloc_scratch_bytes(void) { return gpulsm::noalloc_scratch_bytes(); }
+

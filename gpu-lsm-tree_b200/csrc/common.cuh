@@ -89,6 +89,22 @@ __device__ __forceinline__ void st_relaxed_u64(unsigned long long *p, unsigned l
   asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
+// Index checks compiled in only for diagnostic builds (-DGPULSM_CHECKED):
+// a failed check records (site, value) of the first failure and the access
+// is skipped.  Product builds compile GPULSM_OK(...) to true.
+#ifdef GPULSM_CHECKED
+static __device__ unsigned long long g_check_fail[2];
+__device__ __forceinline__ bool gpulsm_check(bool ok, uint32_t site, unsigned long long v) {
+  if (!ok && atomicCAS(reinterpret_cast<unsigned long long *>(&g_check_fail[0]), 0ull,
+                       static_cast<unsigned long long>(site)) == 0ull)
+    g_check_fail[1] = v;
+  return ok;
+}
+#define GPULSM_OK(cond, site, v) ::gpulsm::gpulsm_check((cond), (site), (unsigned long long)(v))
+#else
+#define GPULSM_OK(cond, site, v) true
+#endif
+
 // Exclusive scan across a block of BLOCK threads (one value per thread).
 // `warp_sums` must hold BLOCK/32 entries.  Returns the exclusive prefix and
 // writes the block total to *total.
@@ -119,6 +135,51 @@ __device__ __forceinline__ T block_exclusive_scan(T value, T *warp_sums, T *tota
   const T r = warp_sums[warp] + inc - value;
   __syncthreads();
   return r;
+}
+// Decoupled look-back over per-tile counts (u64: flag in the top two bits,
+// 62-bit value).  Tile ids come from an atomic ticket, so every predecessor
+// is resident or done.  Run by one full warp: each round trip reads 32
+// predecessors, so the walk to the nearest inclusive prefix takes
+// distance / 32 dependent loads instead of distance.  Returns the exclusive
+// prefix on every lane; lb[] must be zeroed before the launch.
+constexpr unsigned long long kLbAgg = 1ull << 62;
+constexpr unsigned long long kLbInc = 2ull << 62;
+constexpr unsigned long long kLbMask = (1ull << 62) - 1ull;
+
+__device__ __forceinline__ unsigned long long warp_lookback(unsigned long long *lb, uint32_t tile,
+                                                            unsigned long long agg, uint32_t *status) {
+  const uint32_t lane = threadIdx.x & 31u;
+  if (tile == 0) {
+    if (lane == 0) st_relaxed_u64(lb, kLbInc | agg);
+    return 0ull;
+  }
+  if (lane == 0) st_relaxed_u64(lb + tile, kLbAgg | agg);
+  unsigned long long excl = 0;
+  int64_t end = int64_t(tile);  // window [end - 32, end); slots before tile 0 read as inclusive 0
+  uint32_t spins = 0;
+  while (true) {
+    const int64_t t = end - 32 + int64_t(lane);
+    const unsigned long long v = t >= 0 ? ld_relaxed_u64(lb + t) : kLbInc;
+    const unsigned long long flag = v & ~kLbMask;
+    if (__any_sync(0xffffffffu, flag == 0ull)) {
+      if (++spins > kMaxSpins) {
+        if (lane == 0) atomicOr(status, kDevWaitTimeout);
+        break;
+      }
+      continue;
+    }
+    // a published inclusive prefix implies every earlier slot is published
+    const uint32_t inc = __ballot_sync(0xffffffffu, flag == kLbInc);
+    const int hi = inc ? 31 - __clz(int(inc)) : 0;
+    unsigned long long s = int(lane) >= hi ? (v & kLbMask) : 0ull;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    excl += s;
+    if (inc) break;
+    end -= 32;
+  }
+  if (lane == 0) st_relaxed_u64(lb + tile, kLbInc | (excl + agg));
+  return excl;
 }
 #endif
 

@@ -120,37 +120,6 @@ constexpr int kRouteThreads = 256;
 constexpr int kRouteItems = 8;
 constexpr uint32_t kRouteTile = kRouteThreads * kRouteItems;
 
-constexpr unsigned long long kLbAgg = 1ull << 62;
-constexpr unsigned long long kLbInc = 2ull << 62;
-constexpr unsigned long long kLbMask = (1ull << 62) - 1ull;
-
-__device__ __forceinline__ unsigned long long lookback(unsigned long long *lb, uint32_t tile,
-                                                       unsigned long long agg, uint32_t *status) {
-  if (tile == 0) {
-    st_relaxed_u64(lb, kLbInc | agg);
-    return 0ull;
-  }
-  st_relaxed_u64(lb + tile, kLbAgg | agg);
-  unsigned long long excl = 0;
-  int64_t t = int64_t(tile) - 1;
-  uint32_t spins = 0;
-  while (t >= 0) {
-    const unsigned long long v = ld_relaxed_u64(lb + t);
-    const unsigned long long flag = v & ~kLbMask;
-    if (flag == 0ull) {
-      if (++spins > kMaxSpins) {
-        atomicOr(status, kDevWaitTimeout);
-        break;
-      }
-      continue;
-    }
-    excl += v & kLbMask;
-    if (flag == kLbInc) break;
-    --t;
-  }
-  st_relaxed_u64(lb + tile, kLbInc | (excl + agg));
-  return excl;
-}
 
 template <typename K>
 __global__ void __launch_bounds__(kRouteThreads) route_runs_kernel(
@@ -203,7 +172,10 @@ __global__ void __launch_bounds__(kRouteThreads) route_runs_kernel(
     }
   }
   const uint32_t local = block_exclusive_scan<kRouteThreads>(cnt, s_scan, &s_total);
-  if (threadIdx.x == 0) s_base = lookback(lb, tile, s_total, status);
+  if (threadIdx.x < 32) {
+    const unsigned long long lb_excl = warp_lookback(lb, tile, s_total, status);
+    if (threadIdx.x == 0) s_base = lb_excl;
+  }
   __syncthreads();
   uint64_t o = s_base + local;
 #pragma unroll
@@ -545,7 +517,10 @@ __global__ void __launch_bounds__(kDedupThreads) dedup_first_kernel(
     prev = k[i];
   }
   const uint32_t local = block_exclusive_scan<kDedupThreads>(cnt, s_scan, &s_total);
-  if (threadIdx.x == 0) s_base = lookback(lb, s_tile, s_total, status);
+  if (threadIdx.x < 32) {
+    const unsigned long long lb_excl = warp_lookback(lb, s_tile, s_total, status);
+    if (threadIdx.x == 0) s_base = lb_excl;
+  }
   __syncthreads();
   uint64_t o = s_base + local;
 #pragma unroll
@@ -609,7 +584,10 @@ __global__ void __launch_bounds__(kScanThreads) scan_counts_kernel(
     sum += c[i];
   }
   const unsigned long long local = block_exclusive_scan<kScanThreads>(sum, s_scan, &s_total);
-  if (threadIdx.x == 0) s_base = lookback(lb, s_tile, s_total, status);
+  if (threadIdx.x < 32) {
+    const unsigned long long lb_excl = warp_lookback(lb, s_tile, s_total, status);
+    if (threadIdx.x == 0) s_base = lb_excl;
+  }
   __syncthreads();
   unsigned long long o = s_base + local;
 #pragma unroll

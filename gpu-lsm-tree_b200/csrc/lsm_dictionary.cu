@@ -20,6 +20,7 @@
 #include <new>
 #include <stdexcept>
 
+#include "lsm_admit.cuh"
 #include "lsm_kernels.cuh"
 #include "radix_sort.cuh"
 
@@ -166,6 +167,8 @@ LsmDictionary::LsmDictionary(const DictConfig &config)
   int dev = 0;
   GPULSM_CUDA(cudaGetDevice(&dev));
   GPULSM_CUDA(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, dev));
+  GPULSM_CUDA(cudaFuncSetAttribute(lsm::admit::admit_bucket_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   int(lsm::admit::kBucketSmemBytes)));
   GPULSM_CUDA(cudaMalloc(&dev_status_, 256));
   GPULSM_CUDA(cudaMemset(dev_status_, 0, 256));
   GPULSM_CUDA(cudaMalloc(&receipt_dev_, sizeof(Receipt)));
@@ -299,6 +302,7 @@ void LsmDictionary::release_levels(cudaStream_t) {
 RunBuffer *LsmDictionary::sort_dedup(const uint32_t *keys, const uint32_t *values, uint64_t n,
                                      bool tombstone, cudaStream_t s) {
   ensure_sort_space(n, s);
+  if (n <= lsm::admit::kMaxKeys) return bucket_admit(keys, values, n, tombstone, s);
   const uint32_t nn = uint32_t(n);
   const size_t radix_bytes = align_up(radix::workspace_bytes(n, 4));
   const uint64_t dtiles = (n + lsm::kCompactTile - 1) / lsm::kCompactTile;
@@ -318,6 +322,36 @@ RunBuffer *LsmDictionary::sort_dedup(const uint32_t *keys, const uint32_t *value
   lsm::dedup_last_kernel<<<unsigned(dtiles), lsm::kCompactThreads, 0, s>>>(
       bufs[cur], nn, tombstone ? 1 : 0, carry->keys, carry->vals, carry->flags, carry->desc, carry->dir,
       carry->dir_bits, rows_log2_, lb, counter, dev_status_); note_launch();
+  GPULSM_CUDA(cudaGetLastError());
+  return carry;
+}
+
+// Batches up to 2^20 rows: pack, one stable pass on the key's top byte, then
+// one CTA per top-byte bucket sorts, deduplicates and writes the level rows
+// (lsm_admit.cuh).
+RunBuffer *LsmDictionary::bucket_admit(const uint32_t *keys, const uint32_t *values, uint64_t n,
+                                       bool tombstone, cudaStream_t s) {
+  namespace ad = lsm::admit;
+  const uint32_t nn = uint32_t(n);
+  // [key-byte histograms 0..2][top-byte histogram | onesweep counters | onesweep look-back]
+  const size_t hist_words = 3 * 256 + radix::workspace_words(n, 1);
+  const size_t total = align_up(hist_words * 4) + align_up(8) + align_up((ad::kBuckets + 1) * 8);
+  Bump bump{static_cast<char *>(scratch(total, s))};
+  GPULSM_CUDA(cudaMemsetAsync(bump.p, 0, total, s));
+  uint32_t *hist = bump.take<uint32_t>(hist_words);
+  uint32_t *counter = bump.take<uint32_t>(2);
+  unsigned long long *lb = bump.take<unsigned long long>(ad::kBuckets + 1);
+  const unsigned hist_blocks = std::min<unsigned>(grid_for(n, 4096), unsigned(num_sms_) * 4u);
+  lsm::pack_histogram_kernel<<<hist_blocks, 256, 0, s>>>(keys, tombstone ? nullptr : values, nn, words_[0], hist);
+  note_launch();
+  unsigned long long *bufs[2] = {words_[0], words_[1]};
+  const int cur = radix::run_passes<unsigned long long, false>(bufs, nullptr, nn, 56, 64, hist + 3 * 256,
+                                                               dev_status_, s);
+  RunBuffer *carry = pool_.acquire(n, s);
+  ad::admit_bucket_kernel<<<ad::kBuckets, ad::kThreads, ad::kBucketSmemBytes, s>>>(
+      bufs[cur], bufs[cur ^ 1], hist + 3 * 256, nn, tombstone ? 1 : 0, carry->keys, carry->vals, carry->flags,
+      carry->desc, carry->dir, carry->dir_bits, rows_log2_, lb, counter, dev_status_);
+  note_launch();
   GPULSM_CUDA(cudaGetLastError());
   return carry;
 }
@@ -739,3 +773,4 @@ void LsmDictionary::size(uint64_t *rows, uint32_t *levels) {
 }
 
 }  // namespace gpulsm
+

@@ -104,6 +104,8 @@ class LsmDictionary {
              cudaStream_t s);
   RunBuffer *sort_dedup(const uint32_t *keys, const uint32_t *values, uint64_t n, bool tombstone,
                         cudaStream_t s);
+  RunBuffer *bucket_admit(const uint32_t *keys, const uint32_t *values, uint64_t n, bool tombstone,
+                          cudaStream_t s);
   void cascade(RunBuffer *carry, uint64_t carry_upper, bool carry_tombs, cudaStream_t s);
   RunBuffer *merge(RunBuffer *newer, RunBuffer *older, uint64_t out_upper, bool drop_tombstones,
                    cudaStream_t s);

@@ -42,41 +42,6 @@ struct LevelSet {
 };
 
 // ---------------------------------------------------------------------------
-// single-value decoupled look-back over tiles (u64 counts, 62-bit)
-constexpr unsigned long long kLbAgg = 1ull << 62;
-constexpr unsigned long long kLbInc = 2ull << 62;
-constexpr unsigned long long kLbMask = (1ull << 62) - 1ull;
-
-__device__ __forceinline__ unsigned long long tile_lookback(unsigned long long *lb, uint32_t tile,
-                                                            unsigned long long agg,
-                                                            uint32_t *status) {
-  if (tile == 0) {
-    st_relaxed_u64(lb, kLbInc | agg);
-    return 0ull;
-  }
-  st_relaxed_u64(lb + tile, kLbAgg | agg);
-  unsigned long long excl = 0;
-  int64_t t = int64_t(tile) - 1;
-  uint32_t spins = 0;
-  while (t >= 0) {
-    const unsigned long long v = ld_relaxed_u64(lb + t);
-    const unsigned long long flag = v & ~kLbMask;
-    if (flag == 0ull) {
-      if (++spins > kMaxSpins) {
-        atomicOr(status, kDevWaitTimeout);
-        break;
-      }
-      continue;
-    }
-    excl += v & kLbMask;
-    if (flag == kLbInc) break;
-    --t;
-  }
-  st_relaxed_u64(lb + tile, kLbInc | (excl + agg));
-  return excl;
-}
-
-// ---------------------------------------------------------------------------
 // Admission: pack (key, value) into one u64 word (key in the high half so an
 // LSD sort on bits 32..63 orders by key and keeps input order among equal
 // keys) and count the key bytes of the four sort passes.
@@ -141,11 +106,13 @@ __device__ __forceinline__ void fill_directory(uint32_t *__restrict__ dir, const
   for (uint32_t j = threadIdx.x; j < cnt; j += blockDim.x) {
     const int64_t bj = int64_t((key_at(j) - g.kmin) >> g.shift);
     const int64_t bprev = j ? int64_t((key_at(j - 1) - g.kmin) >> g.shift) : bp;
-    for (int64_t b = bprev + 1; b <= bj; ++b) dir[b] = uint32_t(g0 + j);
+    for (int64_t b = bprev + 1; b <= bj; ++b)
+      if (GPULSM_OK(b >= 0 && b < int64_t(g.nbuckets), 10, b)) dir[b] = uint32_t(g0 + j);
   }
   if (threadIdx.x == 0) {
     const int64_t blast = cnt ? int64_t((key_at(cnt - 1) - g.kmin) >> g.shift) : bp;
-    for (int64_t b = blast + 1; b <= bl; ++b) dir[b] = uint32_t(g0 + cnt);
+    for (int64_t b = blast + 1; b <= bl; ++b)
+      if (GPULSM_OK(b >= 0 && b < int64_t(g.nbuckets), 13, b)) dir[b] = uint32_t(g0 + cnt);
     if (last_tile) dir[g.nbuckets] = uint32_t(n_out);
   }
 }
@@ -202,7 +169,10 @@ __global__ void __launch_bounds__(kCompactThreads) dedup_last_kernel(
   }
   const uint32_t local = block_exclusive_scan<kCompactThreads>(kept, s_scan, &s_total);
   const uint32_t tile_kept = s_total;
-  if (threadIdx.x == 0) s_base = tile_lookback(lb, tile, tile_kept, status);
+  if (threadIdx.x < 32) {
+    const unsigned long long lb_excl = warp_lookback(lb, tile, tile_kept, status);
+    if (threadIdx.x == 0) s_base = lb_excl;
+  }
   // stage the kept words compactly (reuse the buffer after everyone has read it)
   unsigned long long mine[kCompactItems];
 #pragma unroll
@@ -361,7 +331,10 @@ __global__ void __launch_bounds__(kMergeThreads) merge_kernel(
   const uint32_t kept = __popc(keep_mask);
   const uint32_t local = block_exclusive_scan<kMergeThreads>(kept, s_scan, &s_total);
   const uint32_t tile_kept = s_total;
-  if (threadIdx.x == 0) s_base = tile_lookback(lb, tile, tile_kept, status);
+  if (threadIdx.x < 32) {
+    const unsigned long long lb_excl = warp_lookback(lb, tile, tile_kept, status);
+    if (threadIdx.x == 0) s_base = lb_excl;
+  }
   uint32_t rk[kMergeItems], rv[kMergeItems];
   uint8_t rf[kMergeItems];
 #pragma unroll
@@ -669,7 +642,10 @@ __global__ void __launch_bounds__(kScanThreads) scan_counts_kernel(
     sum += c[i];
   }
   const unsigned long long local = block_exclusive_scan<kScanThreads>(sum, s_scan, &s_total);
-  if (threadIdx.x == 0) s_base = tile_lookback(lb, tile, s_total, status);
+  if (threadIdx.x < 32) {
+    const unsigned long long lb_excl = warp_lookback(lb, tile, s_total, status);
+    if (threadIdx.x == 0) s_base = lb_excl;
+  }
   __syncthreads();
   unsigned long long o = s_base + local;
 #pragma unroll

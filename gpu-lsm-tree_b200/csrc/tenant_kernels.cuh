@@ -84,37 +84,6 @@ constexpr int kDedupThreads = 256;
 constexpr int kDedupItems = 8;
 constexpr uint32_t kDedupTile = kDedupThreads * kDedupItems;
 
-constexpr unsigned long long kLbAgg = 1ull << 62;
-constexpr unsigned long long kLbInc = 2ull << 62;
-constexpr unsigned long long kLbMask = (1ull << 62) - 1ull;
-
-__device__ __forceinline__ unsigned long long lookback(unsigned long long *lb, uint32_t tile,
-                                                       unsigned long long agg, uint32_t *status) {
-  if (tile == 0) {
-    st_relaxed_u64(lb, kLbInc | agg);
-    return 0ull;
-  }
-  st_relaxed_u64(lb + tile, kLbAgg | agg);
-  unsigned long long excl = 0;
-  int64_t t = int64_t(tile) - 1;
-  uint32_t spins = 0;
-  while (t >= 0) {
-    const unsigned long long v = ld_relaxed_u64(lb + t);
-    const unsigned long long flag = v & ~kLbMask;
-    if (flag == 0ull) {
-      if (++spins > kMaxSpins) {
-        atomicOr(status, kDevWaitTimeout);
-        break;
-      }
-      continue;
-    }
-    excl += v & kLbMask;
-    if (flag == kLbInc) break;
-    --t;
-  }
-  st_relaxed_u64(lb + tile, kLbInc | (excl + agg));
-  return excl;
-}
 
 __global__ void __launch_bounds__(kDedupThreads) dedup_tenant_words_kernel(
     const unsigned long long *__restrict__ words, const uint32_t *__restrict__ wvals,
@@ -148,7 +117,10 @@ __global__ void __launch_bounds__(kDedupThreads) dedup_tenant_words_kernel(
     }
   }
   const uint32_t local = block_exclusive_scan<kDedupThreads>(cnt, s_scan, &s_total);
-  if (threadIdx.x == 0) s_base = lookback(lb, s_tile, s_total, status);
+  if (threadIdx.x < 32) {
+    const unsigned long long lb_excl = warp_lookback(lb, s_tile, s_total, status);
+    if (threadIdx.x == 0) s_base = lb_excl;
+  }
   __syncthreads();
   unsigned long long o = s_base + local;
 #pragma unroll
@@ -350,8 +322,10 @@ __global__ void __launch_bounds__(kMergeThreads) tenant_merge_kernel(MergeArgs m
     }
     const uint32_t local = block_exclusive_scan<kMergeThreads>(kept, s_scan, &s_total);
     const uint32_t tile_kept = s_total;
-    if (threadIdx.x == 0)
-      s_base = lookback(m.lb + m.tile_off[t], local_tile, tile_kept, m.status);
+    if (threadIdx.x < 32) {
+      const unsigned long long lb_excl = warp_lookback(m.lb + m.tile_off[t], local_tile, tile_kept, m.status);
+      if (threadIdx.x == 0) s_base = lb_excl;
+    }
     // pass 2: write kept rows compactly into shared memory
     uint32_t o = local;
     for (uint32_t d = my_d; d < my_e; ++d) {

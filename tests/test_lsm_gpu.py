@@ -162,6 +162,46 @@ def test_random_updates_match_oracle(gl, cuda, batch_capacity, level_zero, fan_i
     assert t.d.canonical_carry_status() == 0
 
 
+def skewed_batches(rng):
+    """Update batches shaped to exercise every admission route: batch sizes
+    around the 4096-row bucket limit, all-equal keys, few distinct keys
+    repeated (buckets of one key larger than shared memory), a dense cluster
+    inside a wide range (one bucket sorted through global memory) and a
+    normal distribution (uneven buckets)."""
+    u32 = lambda a: np.asarray(a, np.uint64).astype(np.uint32)
+    full = lambda n: u32(rng.integers(0, 1 << 32, n, dtype=np.uint64))
+    yield "sizes", [full(n) for n in (1, 2, 3, 4095, 4096, 4097, 3 * 2048 + 1, 100_000)]
+    yield "all_equal", [np.full(1 << 20, 0x9E3779B9, np.uint32), np.full(5000, 0, np.uint32)]
+    yield "few_keys", [u32(rng.integers(0, 100, 1 << 20)), u32(rng.integers(0, 1000, 300_000))]
+    cluster = u32(rng.integers(500_000_000, 500_000_000 + (1 << 14), 1 << 19))
+    yield "cluster", [rng.permutation(np.concatenate([cluster, full(1 << 19)]))]
+    normal = rng.normal(2.0 ** 31, 2.0 ** 26, 1 << 20).clip(0, 2.0 ** 32 - 1)
+    yield "normal", [u32(normal)]
+    yield "top_bits", [u32(rng.integers(0, 1 << 8, 200_000)) << np.uint32(24),
+                       full(50_000) | np.uint32(0xFFFF0000)]
+
+
+def test_admission_skewed_batches(gl, cuda):
+    rng = np.random.default_rng(77)
+    for name, batches in skewed_batches(rng):
+        t = Twin(gl, max_elements=1 << 23)
+        seen = []
+        for i, k in enumerate(batches):
+            v = rng.integers(0, 1 << 32, k.size, dtype=np.uint64).astype(np.uint32)
+            t.apply(("insert", k, v))
+            seen.append(k)
+            if i % 2 == 1:  # erase a skewed sample of what is there
+                t.apply(("erase", k[rng.integers(0, k.size, max(1, k.size // 3))]))
+        keys = np.unique(np.concatenate(seen))
+        probe = np.concatenate([keys, rng.integers(0, 1 << 32, 2000, dtype=np.uint64).astype(np.uint32)])
+        t.lookup(probe, with_found=True)
+        t.successor(probe[rng.integers(0, probe.size, 5000)])
+        lo = probe[rng.integers(0, probe.size, 500)]
+        hi = (lo.astype(np.uint64) + rng.integers(0, 1 << 26, 500, dtype=np.uint64)).clip(0, 0xFFFFFFFF)
+        t.ranges(lo, hi.astype(np.uint32))
+        assert t.d.canonical_carry_status() == 0, name
+
+
 def test_empty_and_edge_inputs(gl, cuda):
     import torch
 
