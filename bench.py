@@ -52,6 +52,10 @@ def parse():
     p.add_argument("--scale", type=int, default=0, help="divide sizes by 2^scale (development only)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-serving", action="store_true")
+    p.add_argument("--no-tenants", action="store_true")
+    p.add_argument("--tenant-rounds", type=int, default=4)
+    p.add_argument("--serving-seconds", type=float, default=2.0)
     return p.parse_args()
 
 
@@ -286,6 +290,12 @@ def run_ours(args):
 
     if not args.no_e2e:
         result["e2e"] = e2e_ours(args, gl, w, dev, total_pairs, max_el)
+    if not args.no_tenants:
+        result["tenants"] = tenants_leg(args, gl, dev)
+    if not args.no_serving:
+        del d, ops_dev, q, lo, hi, out_v, out_f, offsets, pairs
+        torch.cuda.empty_cache()
+        result["serving"] = serving_leg(args, gl, w, dev)
     if rank == 0 and not args.no_cpu:
         result["cpu_baseline"] = cpu_baseline(args, W)
     if world > 1:
@@ -295,6 +305,151 @@ def run_ours(args):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(result), flush=True)
+
+
+def tenant_round(rng, sizes, lo=6, hi=16):
+    """One round of the multi-tenant configuration: per tenant a batch of
+    log-uniform size in [2^lo, 2^hi], keys uniform in the tenant's key span
+    [0, size) (upserts, so a tenant never outgrows its size)."""
+    n = np.exp(rng.uniform(lo * np.log(2), hi * np.log(2), sizes.size)).astype(np.int64)
+    off = np.zeros(sizes.size + 1, np.int64)
+    off[1:] = np.cumsum(n)
+    span = np.repeat(sizes.astype(np.float64), n)
+    keys = (rng.random(int(off[-1])) * span).astype(np.uint32)
+    vals = rng.integers(0, 1 << 32, int(off[-1]), dtype=np.uint64).astype(np.uint32)
+    return keys, vals, off
+
+
+def tenants_leg(args, gl, dev):
+    """Multi-tenant batched mode: 4096 dictionaries of log-uniform size in
+    [2^10, 2^20], per-tenant batches log-uniform in [2^6, 2^16], one persistent
+    merge launch per round replayed from a CUDA graph, tile / fan-in / fanout
+    picked by the autotuner on a 512-tenant sample; against the plain form
+    (one dictionary per tenant, a call per tenant) timed on a 256-tenant sample."""
+    import torch
+
+    tune = importlib.import_module("gpu-lsm-tree_b200.autotune")
+    rng = np.random.default_rng(17)
+    T = 4096
+    sizes = np.exp(rng.uniform(10 * np.log(2), 20 * np.log(2), T)).astype(np.uint64)
+
+    def dev_round(r):
+        k, v, off = r
+        return (torch.from_numpy(k.view(np.int32)).to(dev), torch.from_numpy(v.view(np.int32)).to(dev),
+                torch.from_numpy(off).to(dev))
+
+    # autotune on a sample of the workload (cached by signature)
+    ts = 512
+    s_sizes = sizes[:ts]
+    s_rounds = [dev_round(tenant_round(rng, s_sizes, 6, 12)) for _ in range(2)]
+    s_lookup = (torch.from_numpy(rng.integers(0, ts, 1 << 16).astype(np.int32)).to(dev),
+                torch.from_numpy(rng.integers(0, 1 << 20, 1 << 16).astype(np.int32)).to(dev))
+    best = tune.autotune(s_sizes * 2 + 8, s_rounds, s_lookup, max(int(r[2][-1].item()) for r in s_rounds),
+                         cache_path=None)
+    rounds = [tenant_round(rng, sizes) for _ in range(args.tenant_rounds + 1)]
+    max_round = max(int(r[2][-1]) for r in rounds)
+    pool = gl.TenantPool(sizes * 2 + 8, max_round, best["tile"], best["fan_in"], best["fanout"])
+    kbuf = torch.empty(max_round, dtype=torch.int32, device=dev)
+    vbuf = torch.empty(max_round, dtype=torch.int32, device=dev)
+    obuf = torch.empty(T + 1, dtype=torch.int64, device=dev)
+    stream = torch.cuda.Stream(dev)
+    keys_total, ms_total = 0, 0.0
+    for i, r in enumerate(rounds):
+        k, v, off = dev_round(r)
+        n = int(r[2][-1])
+        with torch.cuda.stream(stream):
+            kbuf[:n].copy_(k)
+            vbuf[:n].copy_(v)
+            obuf.copy_(off)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            pool.insert_round(kbuf, vbuf, obuf, stream=stream, graph=True)
+            e1.record(stream)
+        stream.synchronize()
+        if i > 0:  # round 0 warms up (and captures the graph)
+            keys_total += n
+            ms_total += e0.elapsed_time(e1)
+    nq = 1 << 24
+    tid = torch.from_numpy(rng.integers(0, T, nq).astype(np.int32)).to(dev)
+    qk = torch.from_numpy((rng.random(nq) * sizes[tid.cpu().numpy()].astype(np.float64)).astype(np.uint32).view(np.int32)).to(dev)
+    out = torch.empty(nq, dtype=torch.int32, device=dev)
+    pool.lookup(tid, qk, out)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    pool.lookup(tid, qk, out)
+    e1.record()
+    torch.cuda.synchronize()
+    look_ms = e0.elapsed_time(e1)
+    status = pool.status()
+    resident = pool.gpu_resident_bytes()
+    pool.close()
+    del kbuf, vbuf
+    # plain form: one dictionary per tenant, a call per tenant, on a sample
+    ps = 256
+    plain = [gl.GPULSMOpt(gl.DictionaryConfig(max_elements=int(c) + 8, batch_capacity=1 << 16)) for c in sizes[:ps]]
+    r = rounds[1]
+    k, v, off = dev_round(r)
+    pk = 0
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for t in range(ps):
+        a, b = int(off[t]), int(off[t + 1])
+        plain[t].insert(k[a:b], v[a:b])
+        pk += b - a
+    e1.record()
+    torch.cuda.synchronize()
+    plain_ms = e0.elapsed_time(e1)
+    for d in plain:
+        d.close()
+    return {
+        "tenants": T, "total_size_keys": int(sizes.sum()), "rounds_timed": args.tenant_rounds,
+        "keys_per_round": int(keys_total / max(args.tenant_rounds, 1)),
+        "tuning": {"tile": best["tile"], "fan_in": best["fan_in"], "fanout": best["fanout"]},
+        "insert_mkeys_s": round(keys_total / (ms_total * 1e-3) / 1e6, 1),
+        "round_ms": round(ms_total / max(args.tenant_rounds, 1), 3),
+        "lookup_mops_s": round(nq / (look_ms * 1e-3) / 1e6, 1),
+        "plain_form_insert_mkeys_s": round(pk / (plain_ms * 1e-3) / 1e6, 1),
+        "plain_form_sample_tenants": ps,
+        "speedup_vs_plain_form": round((keys_total / ms_total) / (pk / plain_ms), 2),
+        "resident_gb": round(resident / 1e9, 2), "status": status,
+    }
+
+
+def serving_leg(args, gl, w, dev):
+    """The serving mode over the same dictionary: every inserted key loaded,
+    a 16 GB device budget, requests of log-uniform size in [1, 2^16] keys
+    (60% lookup, 20% insert, 10% erase, 10% range sum; Zipf s=1.1 keys).
+    Peak = closed loop with 64 requests in flight; latency = open-loop Poisson
+    arrivals at half the peak request rate (host submit to results in host
+    buffers)."""
+    import torch
+
+    keys = np.concatenate([o[1] for o in w.ops if o[0] == "insert"])
+    srv = gl.Server(gl.DictionaryConfig(max_elements=keys.size + w.erased_keys + (1 << 24)),
+                    budget_bytes=16 << 30, max_round_keys=1 << 20, depth=3)
+    kd = torch.from_numpy(keys.view(np.int32)).to(dev)
+    vd = torch.arange(keys.size, dtype=torch.int32, device=dev)
+    srv.bulk_build(kd, vd)
+    del kd, vd
+    secs = args.serving_seconds
+    srv.run_load(keys, rate_per_s=0, seconds=0.3, max_outstanding=64, seed=3)  # warm-up
+    peak = srv.run_load(keys, rate_per_s=0, seconds=secs, max_outstanding=64, seed=4)
+    peak_rate = peak["completed"] / max(peak["wall_s"], 1e-9)
+    half = srv.run_load(keys, rate_per_s=0.5 * peak_rate, seconds=secs, seed=5)
+    srv.close()
+    return {
+        "dictionary_keys": int(keys.size), "budget_gb": 16,
+        "peak_mkeys_s": round(peak["keys"] / max(peak["wall_s"], 1e-9) / 1e6, 1),
+        "peak_requests_s": round(peak_rate, 1),
+        "load_requests_s": round(0.5 * peak_rate, 1),
+        "mkeys_s": round(half["keys"] / max(half["wall_s"], 1e-9) / 1e6, 1),
+        "p50_ms": round(half["p50_us"] / 1e3, 4), "p99_ms": round(half["p99_us"] / 1e3, 4),
+        "max_ms": round(half["max_us"] / 1e3, 4),
+        "peak_p50_ms": round(peak["p50_us"] / 1e3, 4), "peak_p99_ms": round(peak["p99_us"] / 1e3, 4),
+        "mean_round_keys": round(half["mean_round_keys"], 1), "requests": int(half["completed"]),
+        "rejected": int(half["rejected"] + peak["rejected"]),
+    }
 
 
 def e2e_ours(args, gl, w, dev, total_pairs, max_el):

@@ -12,6 +12,7 @@ from ._native import (CapacityError, CudaError, DeviceTimeout, GpuLsmError, Inva
                       LengthError, OutOfDeviceMemory, PublicationError, load)
 from .dictionary import DictionaryConfig, GPULSMOpt, GpuLsmOptIndex, sort_pairs  # noqa: F401
 from .flix import FlixIndex  # noqa: F401
+from .serving import Server  # noqa: F401
 from .tenants import TenantPool  # noqa: F401
 
 

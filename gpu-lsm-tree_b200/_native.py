@@ -28,6 +28,7 @@ STATUS_BAD_INPUT = 1 << 9
 
 SEARCH_DIRECTORY = 0
 SEARCH_LEARNED = 1
+SEARCH_BINARY = 2
 
 
 class GpuLsmError(RuntimeError):
@@ -101,6 +102,37 @@ class FlixConfig(C.Structure):
     ]
 
 
+class ServeStats(C.Structure):
+    _fields_ = [
+        ("completed", C.c_uint64),
+        ("rejected", C.c_uint64),
+        ("rounds", C.c_uint64),
+        ("keys", C.c_uint64),
+        ("p50_us", C.c_double),
+        ("p99_us", C.c_double),
+        ("max_us", C.c_double),
+        ("mean_us", C.c_double),
+        ("mean_round_keys", C.c_double),
+        ("wall_s", C.c_double),
+    ]
+
+
+class LoadSpec(C.Structure):
+    _fields_ = [
+        ("rate_per_s", C.c_double),
+        ("seconds", C.c_double),
+        ("mix", C.c_double * 4),
+        ("zipf_s", C.c_double),
+        ("max_outstanding", C.c_uint32),
+        ("min_keys", C.c_uint32),
+        ("max_keys", C.c_uint32),
+        ("range_width_max", C.c_uint32),
+        ("seed", C.c_uint64),
+        ("universe", C.c_void_p),
+        ("universe_n", C.c_uint64),
+    ]
+
+
 _lib = None
 
 
@@ -168,6 +200,17 @@ def load() -> C.CDLL:
         "gpulsm_tenants_sizes": (i32, [vp, vp]),
         "gpulsm_tenants_status": (i32, [vp, C.POINTER(u32)]),
         "gpulsm_tenants_resident_bytes": (i32, [vp, C.POINTER(u64)]),
+        "gpulsm_server_create": (i32, [C.POINTER(DictConfig), u64, u32, u32, pvp]),
+        "gpulsm_server_destroy": (i32, [vp]),
+        "gpulsm_server_bulk_build": (i32, [vp, vp, vp, u64, vp]),
+        "gpulsm_server_submit": (i32, [vp, u32, vp, vp, u64, vp, vp, C.POINTER(u64)]),
+        "gpulsm_server_poll": (i32, [vp, u64, C.POINTER(C.c_int32)]),
+        "gpulsm_server_wait": (i32, [vp, u64, C.POINTER(C.c_int32)]),
+        "gpulsm_server_drain": (i32, [vp]),
+        "gpulsm_server_stats": (i32, [vp, C.POINTER(ServeStats)]),
+        "gpulsm_server_reset_stats": (i32, [vp]),
+        "gpulsm_server_run_load": (i32, [vp, C.POINTER(LoadSpec), C.POINTER(ServeStats)]),
+        "gpulsm_server_resident_bytes": (i32, [vp, C.POINTER(u64)]),
         "gpulsm_model_bytes": (u64, [u32]),
         "gpulsm_model_fit": (i32, [vp, u64, u32, u32, u32, vp, vp, vp]),
         "gpulsm_model_gradients": (i32, [vp, u64, u32, u32, vp, vp, vp, vp]),

@@ -13,6 +13,7 @@
 #include "lsm_dictionary.h"
 #include "radix_sort.cuh"
 #include "model_api.h"
+#include "serving.h"
 #include "sort_api.h"
 #include "sort_noalloc.h"
 #include "tenants.h"
@@ -32,6 +33,12 @@ struct gpulsm_tenants {
   gpulsm_tenants(uint32_t t, const uint64_t *caps, uint64_t max_round, uint32_t tile, uint32_t fan_in,
                  uint32_t fanout)
       : impl(t, caps, max_round, tile, fan_in, fanout) {}
+};
+
+struct gpulsm_server {
+  gpulsm::Server impl;
+  gpulsm_server(const gpulsm::DictConfig &c, uint64_t budget, uint32_t round, uint32_t depth)
+      : impl(c, budget, round, depth) {}
 };
 
 namespace {
@@ -91,6 +98,30 @@ void device_accessible(const void *p, const char *what) {
 void device_accessible(std::initializer_list<std::pair<const void *, const char *>> ptrs) {
   for (const auto &p : ptrs) device_accessible(p.first, p.second);
 }
+
+gpulsm::DictConfig dict_config(const gpulsm_dict_config &config) {
+  gpulsm::DictConfig c;
+  c.max_elements = config.max_elements;
+  c.batch_capacity = config.batch_capacity;
+  c.level_zero_capacity = config.level_zero_capacity;
+  c.fan_in = config.fan_in;
+  c.rows_per_bucket_log2 = config.rows_per_bucket_log2;
+  c.search_mode = config.search_mode;
+  return c;
+}
+
+void copy_stats(const gpulsm::ServeStats &s, gpulsm_serve_stats *o) {
+  o->completed = s.completed;
+  o->rejected = s.rejected;
+  o->rounds = s.rounds;
+  o->keys = s.keys;
+  o->p50_us = s.p50_us;
+  o->p99_us = s.p99_us;
+  o->max_us = s.max_us;
+  o->mean_us = s.mean_us;
+  o->mean_round_keys = s.mean_round_keys;
+  o->wall_s = s.wall_s;
+}
 }  // namespace
 
 extern "C" {
@@ -104,14 +135,7 @@ int gpulsm_dict_create(const gpulsm_dict_config *config, gpulsm_dict **out) {
   return guarded([&] {
     need(config, "config");
     need(out, "out");
-    gpulsm::DictConfig c;
-    c.max_elements = config->max_elements;
-    c.batch_capacity = config->batch_capacity;
-    c.level_zero_capacity = config->level_zero_capacity;
-    c.fan_in = config->fan_in;
-    c.rows_per_bucket_log2 = config->rows_per_bucket_log2;
-    c.search_mode = config->search_mode;
-    *out = new gpulsm_dict(c);
+    *out = new gpulsm_dict(dict_config(*config));
   });
 }
 
@@ -509,6 +533,111 @@ int gpulsm_sort_pairs(const void *keys_in, const uint32_t *values_in, void *keys
   });
 }
 
+}  // extern "C"
+
+// ---------------------------------------------------------------- serving loop
+extern "C" {
+int gpulsm_server_create(const gpulsm_dict_config *config, uint64_t budget_bytes, uint32_t max_round_keys,
+                         uint32_t depth, gpulsm_server **out) {
+  return guarded([&] {
+    need(config, "config");
+    need(out, "out");
+    *out = new gpulsm_server(dict_config(*config), budget_bytes, max_round_keys, depth);
+  });
+}
+
+int gpulsm_server_destroy(gpulsm_server *server) {
+  return guarded([&] { delete server; });
+}
+
+int gpulsm_server_bulk_build(gpulsm_server *server, const uint32_t *keys, const uint32_t *values, uint64_t count,
+                             void *stream) {
+  return guarded([&] {
+    need(server, "server");
+    device_accessible({{keys, "keys"}, {values, "values"}});
+    server->impl.drain();
+    server->impl.dict().bulk_build(keys, values, count, S(stream));
+    GPULSM_CUDA(cudaStreamSynchronize(S(stream)));
+  });
+}
+
+int gpulsm_server_submit(gpulsm_server *server, uint32_t kind, const uint32_t *keys, const uint32_t *aux,
+                         uint64_t count, uint32_t *out, uint8_t *out_found, uint64_t *out_ticket) {
+  return guarded([&] {
+    need(server, "server");
+    need(out_ticket, "out_ticket");
+    *out_ticket = server->impl.submit(kind, keys, aux, count, out, out_found);
+  });
+}
+
+int gpulsm_server_poll(gpulsm_server *server, uint64_t ticket, int32_t *out_state) {
+  return guarded([&] {
+    need(server, "server");
+    need(out_state, "out_state");
+    *out_state = server->impl.poll(ticket);
+  });
+}
+
+int gpulsm_server_wait(gpulsm_server *server, uint64_t ticket, int32_t *out_state) {
+  return guarded([&] {
+    need(server, "server");
+    need(out_state, "out_state");
+    *out_state = server->impl.wait(ticket);
+  });
+}
+
+int gpulsm_server_drain(gpulsm_server *server) {
+  return guarded([&] {
+    need(server, "server");
+    server->impl.drain();
+  });
+}
+
+int gpulsm_server_stats(gpulsm_server *server, gpulsm_serve_stats *out) {
+  return guarded([&] {
+    need(server, "server");
+    need(out, "out");
+    copy_stats(server->impl.stats(), out);
+  });
+}
+
+int gpulsm_server_reset_stats(gpulsm_server *server) {
+  return guarded([&] {
+    need(server, "server");
+    server->impl.reset_stats();
+  });
+}
+
+int gpulsm_server_run_load(gpulsm_server *server, const gpulsm_load_spec *spec, gpulsm_serve_stats *out) {
+  return guarded([&] {
+    need(server, "server");
+    need(spec, "spec");
+    need(out, "out");
+    gpulsm::LoadSpec l;
+    l.rate_per_s = spec->rate_per_s;
+    l.seconds = spec->seconds;
+    for (int i = 0; i < 4; ++i) l.mix[i] = spec->mix[i];
+    l.zipf_s = spec->zipf_s;
+    l.max_outstanding = spec->max_outstanding ? spec->max_outstanding : 64;
+    l.min_keys = spec->min_keys;
+    l.max_keys = spec->max_keys;
+    l.range_width_max = spec->range_width_max ? spec->range_width_max : (1u << 16);
+    l.seed = spec->seed;
+    l.universe = spec->universe;
+    l.universe_n = spec->universe_n;
+    gpulsm::ServeStats st;
+    server->impl.run_load(l, &st);
+    copy_stats(st, out);
+  });
+}
+
+int gpulsm_server_resident_bytes(gpulsm_server *server, uint64_t *out_bytes) {
+  return guarded([&] {
+    need(server, "server");
+    need(out_bytes, "out_bytes");
+    *out_bytes = server->impl.dict().resident_bytes() + server->impl.device_bytes();
+  });
+}
 }  // extern "C"
 
 // Allocation-free sort (see sort_noalloc.cu): same checks as gpulsm_sort_pairs.

@@ -146,14 +146,17 @@ constexpr unsigned long long kLbAgg = 1ull << 62;
 constexpr unsigned long long kLbInc = 2ull << 62;
 constexpr unsigned long long kLbMask = (1ull << 62) - 1ull;
 
-__device__ __forceinline__ unsigned long long warp_lookback(unsigned long long *lb, uint32_t tile,
+// Publish a tile's own count (one thread).  Tile 0 publishes it as inclusive.
+__device__ __forceinline__ void lookback_publish(unsigned long long *lb, uint32_t tile, unsigned long long agg) {
+  st_relaxed_u64(lb + tile, (tile == 0 ? kLbInc : kLbAgg) | agg);
+}
+
+// Walk back from a tile whose count is published; run by one full warp.
+// Returns the exclusive prefix on every lane and publishes the inclusive one.
+__device__ __forceinline__ unsigned long long lookback_walk(unsigned long long *lb, uint32_t tile,
                                                             unsigned long long agg, uint32_t *status) {
   const uint32_t lane = threadIdx.x & 31u;
-  if (tile == 0) {
-    if (lane == 0) st_relaxed_u64(lb, kLbInc | agg);
-    return 0ull;
-  }
-  if (lane == 0) st_relaxed_u64(lb + tile, kLbAgg | agg);
+  if (tile == 0) return 0ull;
   unsigned long long excl = 0;
   int64_t end = int64_t(tile);  // window [end - 32, end); slots before tile 0 read as inclusive 0
   uint32_t spins = 0;
@@ -166,6 +169,7 @@ __device__ __forceinline__ unsigned long long warp_lookback(unsigned long long *
         if (lane == 0) atomicOr(status, kDevWaitTimeout);
         break;
       }
+      __nanosleep(32);
       continue;
     }
     // a published inclusive prefix implies every earlier slot is published
@@ -180,6 +184,12 @@ __device__ __forceinline__ unsigned long long warp_lookback(unsigned long long *
   }
   if (lane == 0) st_relaxed_u64(lb + tile, kLbInc | (excl + agg));
   return excl;
+}
+
+__device__ __forceinline__ unsigned long long warp_lookback(unsigned long long *lb, uint32_t tile,
+                                                            unsigned long long agg, uint32_t *status) {
+  if ((threadIdx.x & 31u) == 0) lookback_publish(lb, tile, agg);
+  return lookback_walk(lb, tile, agg, status);
 }
 #endif
 

@@ -98,8 +98,9 @@ __device__ __forceinline__ uint64_t model_lower_bound(const ModelHeader &h, cons
 // fit, step 0: header (key range, segment width) - one thread
 template <typename K>
 __global__ void model_header_kernel(const K *__restrict__ keys, uint64_t n, uint32_t segments,
-                                    ModelHeader *__restrict__ h) {
+                                    ModelHeader *__restrict__ h, const unsigned long long *__restrict__ n_dev) {
   if (threadIdx.x || blockIdx.x) return;
+  if (n_dev) n = *n_dev;  // a count produced on the device (an LSM level's row count)
   ModelHeader m{};
   m.n = n;
   m.kmin = n ? (unsigned long long)keys[0] : 1ull;

@@ -32,7 +32,7 @@ namespace lsm {
 namespace admit {
 
 constexpr int kThreads = 512;
-constexpr int kItems = 16;
+constexpr int kItems = 12;
 constexpr int kWarps = kThreads / 32;
 constexpr uint32_t kCap = uint32_t(kThreads) * kItems;  // rows one bucket sorts in shared memory
 constexpr uint32_t kBuckets = 256;
@@ -47,13 +47,28 @@ struct RankSmem {
   uint32_t total;
 };
 
+// Lanes of the warp whose 8-bit digit equals this lane's, among the lanes in
+// `valid` (eight ballots instead of match.any, which issues on a slow pipe).
+__device__ __forceinline__ uint32_t digit_peers(uint32_t d, uint32_t valid) {
+  uint32_t peers = valid;
+#pragma unroll
+  for (int b = 0; b < 8; ++b) {
+    const uint32_t m = __ballot_sync(0xffffffffu, (d >> b) & 1u);
+    peers &= ((d >> b) & 1u) ? m : ~m;
+  }
+  return peers;
+}
+
+__device__ __forceinline__ uint32_t digit_of(unsigned long long w, uint32_t bit) {
+  return (word_key(w) >> bit) & 0xffu;
+}
+
 // Stable rank of one chunk of up to kCap words held warp-striped in
 // registers (item i of lane l in warp w is chunk element w*32*keff + i*32 + l)
 // by the 8-bit key digit at `bit`.  pos[i] = the element's position in the
-// chunk sorted by that digit; digit[i] its digit.  keff is block-uniform.
+// chunk sorted by that digit.  keff is block-uniform.
 __device__ __forceinline__ void rank_chunk(const unsigned long long (&it)[kItems], uint32_t keff, uint32_t cnt,
-                                           uint32_t bit, RankSmem &sm, uint32_t (&pos)[kItems],
-                                           uint32_t (&digit)[kItems]) {
+                                           uint32_t bit, RankSmem &sm, uint32_t (&pos)[kItems]) {
   const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
   for (uint32_t d = lane; d < 256; d += 32) sm.cnt[w][d] = 0;
   __syncwarp();
@@ -62,16 +77,14 @@ __device__ __forceinline__ void rank_chunk(const unsigned long long (&it)[kItems
 #pragma unroll
   for (int i = 0; i < kItems; ++i) {
     pos[i] = 0;
-    digit[i] = 0;
     if (uint32_t(i) < keff) {
       const bool valid = wbase + uint32_t(i) * 32u + lane < cnt;
-      const uint32_t d = (word_key(it[i]) >> bit) & 0xffu;
-      const uint32_t peers = __match_any_sync(0xffffffffu, valid ? d : 0x100u);
+      const uint32_t d = digit_of(it[i], bit);
+      const uint32_t peers = digit_peers(d, __ballot_sync(0xffffffffu, valid));
       if (valid) pos[i] = sm.cnt[w][d] + __popc(peers & lt);
       __syncwarp();
       if (valid && (__ffs(peers) - 1) == int(lane)) sm.cnt[w][d] = uint16_t(sm.cnt[w][d] + __popc(peers));
       __syncwarp();
-      digit[i] = d;
     }
   }
   __syncthreads();
@@ -90,8 +103,10 @@ __device__ __forceinline__ void rank_chunk(const unsigned long long (&it)[kItems
   __syncthreads();
 #pragma unroll
   for (int i = 0; i < kItems; ++i)
-    if (uint32_t(i) < keff && wbase + uint32_t(i) * 32u + lane < cnt)
-      pos[i] += sm.dstart[digit[i]] + sm.cnt[w][digit[i]];
+    if (uint32_t(i) < keff && wbase + uint32_t(i) * 32u + lane < cnt) {
+      const uint32_t d = digit_of(it[i], bit);
+      pos[i] += sm.dstart[d] + sm.cnt[w][d];
+    }
 }
 
 __device__ __forceinline__ void load_striped(const unsigned long long *src, uint32_t keff, uint32_t cnt,
@@ -118,28 +133,44 @@ __device__ __forceinline__ uint32_t count_distinct(const unsigned long long *src
 }
 
 // Write the last row of every equal-key run of the sorted sequence
-// src[0, cnt) to out[g0 ...], in chunks of kCap (each thread a blocked span).
+// src[0, cnt) to out[g0 ...], in chunks of kCap read striped (element
+// c0 + i*kThreads + t): per item a warp ballot counts the kept rows, one block
+// scan over the (item, warp) counts gives every warp its output offset, and
+// consecutive lanes store consecutive rows.
 __device__ __forceinline__ void write_rows(const unsigned long long *src, uint32_t cnt, int tombstone,
                                            uint32_t *out_keys, uint32_t *out_vals, uint8_t *out_flags,
                                            unsigned long long g0, RankSmem &rs) {
+  static_assert(kItems * kWarps <= 256, "one scan slot per (item, warp)");
+  const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+  const uint32_t lt = lanemask_lt();
+  uint32_t *slot = rs.dstart;  // kItems * kWarps counts, then their offsets
   unsigned long long written = 0;
   for (uint32_t c0 = 0; c0 < cnt; c0 += kCap) {
     const uint32_t cc = min(kCap, cnt - c0);
-    const uint32_t kb = (cc + kThreads - 1) / kThreads;
-    const uint32_t j0 = c0 + threadIdx.x * kb;
-    const uint32_t jend = min(j0 + kb, c0 + cc);
-    uint32_t nkeep = 0;
-    for (uint32_t j = j0; j < jend; ++j) nkeep += run_end(src, j, cnt) ? 1u : 0u;
-    uint32_t o = block_exclusive_scan<kThreads>(nkeep, rs.scan, &rs.total);
+    uint32_t ends[kItems];
+#pragma unroll
+    for (int i = 0; i < kItems; ++i) {
+      const uint32_t e = c0 + uint32_t(i) * kThreads + threadIdx.x;
+      ends[i] = __ballot_sync(0xffffffffu, e < c0 + cc && run_end(src, e, cnt));
+      if (lane == 0) slot[i * kWarps + w] = __popc(ends[i]);
+    }
+    __syncthreads();
+    const uint32_t v = threadIdx.x < uint32_t(kItems * kWarps) ? slot[threadIdx.x] : 0u;
+    const uint32_t ex = block_exclusive_scan<kThreads>(v, rs.scan, &rs.total);
     const uint32_t chunk_kept = rs.total;
-    for (uint32_t j = j0; j < jend; ++j)
-      if (run_end(src, j, cnt)) {
-        const unsigned long long w = src[j];
-        const unsigned long long r = g0 + written + o++;
-        out_keys[r] = word_key(w);
-        out_vals[r] = uint32_t(w);  // the tombstone value was packed for erase batches
+    if (threadIdx.x < uint32_t(kItems * kWarps)) slot[threadIdx.x] = ex;
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < kItems; ++i)
+      if ((ends[i] >> lane) & 1u) {
+        const uint32_t e = c0 + uint32_t(i) * kThreads + threadIdx.x;
+        const unsigned long long w64 = src[e];
+        const unsigned long long r = g0 + written + slot[i * kWarps + w] + __popc(ends[i] & lt);
+        out_keys[r] = word_key(w64);
+        out_vals[r] = uint32_t(w64);  // the tombstone value was packed for erase batches
         out_flags[r] = tombstone ? kFlagTomb : uint8_t(0);
       }
+    __syncthreads();
     written += chunk_kept;
   }
 }
@@ -195,14 +226,16 @@ __device__ __noinline__ unsigned long long *sort_global(unsigned long long *a, u
       const uint32_t cc = min(kCap, cnt - c0);
       const uint32_t keff = (cc + kThreads - 1) / kThreads;
       unsigned long long it[kItems];
-      uint32_t pos[kItems], dg[kItems];
+      uint32_t pos[kItems];
       load_striped(src + c0, keff, cc, it);
-      rank_chunk(it, keff, cc, bit, sm, pos, dg);
+      rank_chunk(it, keff, cc, bit, sm, pos);
       const uint32_t wbase = (threadIdx.x >> 5) * 32u * keff;
 #pragma unroll
       for (int i = 0; i < kItems; ++i)
-        if (uint32_t(i) < keff && wbase + uint32_t(i) * 32u + (threadIdx.x & 31u) < cc)
-          dst[s_off[dg[i]] + pos[i] - sm.dstart[dg[i]]] = it[i];
+        if (uint32_t(i) < keff && wbase + uint32_t(i) * 32u + (threadIdx.x & 31u) < cc) {
+          const uint32_t d = digit_of(it[i], bit);
+          dst[s_off[d] + pos[i] - sm.dstart[d]] = it[i];
+        }
       __syncthreads();
       if (threadIdx.x < 256) s_off[threadIdx.x] += sm.dstart[threadIdx.x + 1] - sm.dstart[threadIdx.x];
       __syncthreads();
@@ -227,7 +260,7 @@ constexpr size_t kBucketSmemBytes = sizeof(BucketSmem);
 // One CTA per nonempty top-byte bucket (ticket t -> bucket first + t).
 // words0: the batch partitioned by top byte (stable); words1: scratch of the
 // same size for oversized buckets; top_hist: rows per top byte.
-__global__ void __launch_bounds__(kThreads, 1) admit_bucket_kernel(
+__global__ void __launch_bounds__(kThreads, 2) admit_bucket_kernel(
     unsigned long long *__restrict__ words0, unsigned long long *__restrict__ words1,
     const uint32_t *__restrict__ top_hist, uint32_t n, int tombstone, uint32_t *__restrict__ out_keys,
     uint32_t *__restrict__ out_vals, uint8_t *__restrict__ out_flags, LevelDesc *__restrict__ out_desc,
@@ -272,9 +305,9 @@ __global__ void __launch_bounds__(kThreads, 1) admit_bucket_kernel(
     for (uint32_t bit = 0; bit < 24; bit += 8) {
       if (((vary >> bit) & 0xffu) == 0u) continue;
       unsigned long long it[kItems];
-      uint32_t pos[kItems], dg[kItems];
+      uint32_t pos[kItems];
       load_striped(sm.words, keff, cnt, it);
-      rank_chunk(it, keff, cnt, bit, sm.rank, pos, dg);  // its barriers order the loads before the stores
+      rank_chunk(it, keff, cnt, bit, sm.rank, pos);  // its barriers order the loads before the stores
       const uint32_t wbase = (threadIdx.x >> 5) * 32u * keff;
 #pragma unroll
       for (int i = 0; i < kItems; ++i)

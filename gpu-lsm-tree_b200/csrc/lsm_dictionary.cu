@@ -22,6 +22,7 @@
 
 #include "lsm_admit.cuh"
 #include "lsm_kernels.cuh"
+#include "model_api.h"
 #include "radix_sort.cuh"
 
 namespace gpulsm {
@@ -31,6 +32,12 @@ using lsm::LevelDesc;
 namespace {
 constexpr uint64_t kMaxBatch = uint64_t{1} << 20;  // kMaximumOperationTile, GPULSMOpt.cuh:56
 constexpr size_t kAlign = 256;
+// learned search: levels of at least this many rows get a model, with about
+// kRowsPerSegment rows per segment and kFitIters gradient steps
+constexpr uint64_t kLearnedMinRows = uint64_t(1) << 16;
+constexpr uint64_t kRowsPerSegment = 64;
+constexpr uint32_t kFitIters = 4;
+constexpr uint32_t kMaxSegments = 1u << 22;
 
 size_t align_up(size_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }
 
@@ -72,8 +79,10 @@ struct LsmDictionary::Receipt {
 
 // ----------------------------------------------------------------------------
 RunPool::~RunPool() {
-  for (auto &b : all_)
+  for (auto &b : all_) {
     if (b->block) cudaFree(b->block);
+    if (b->model) cudaFree(b->model);
+  }
 }
 
 RunBuffer *RunPool::acquire(uint64_t min_rows, cudaStream_t stream) {
@@ -88,6 +97,7 @@ RunBuffer *RunPool::acquire(uint64_t min_rows, cudaStream_t stream) {
     }
   if (best && best->cap <= cap * 2) {
     free_.erase(free_.begin() + best_i);
+    best->model_ok = false;
     return best;
   }
   auto b = std::make_unique<RunBuffer>();
@@ -126,7 +136,9 @@ void RunPool::release(RunBuffer *b) {
 void RunPool::release_all_free(cudaStream_t stream) {
   for (RunBuffer *f : free_) {
     cudaFreeAsync(f->block, stream);
-    bytes_ -= f->bytes;
+    if (f->model) cudaFreeAsync(f->model, stream);
+    f->model = nullptr;
+    bytes_ -= f->bytes + f->model_cap;
     for (size_t i = 0; i < all_.size(); ++i)
       if (all_[i].get() == f) {
         all_[i]->block = nullptr;
@@ -147,7 +159,7 @@ LsmDictionary::LsmDictionary(const DictConfig &config)
   if (fan_in_ < 2 || fan_in_ > 16) throw std::invalid_argument("fan_in must be in [2, 16]");
   rows_log2_ = config.rows_per_bucket_log2 ? config.rows_per_bucket_log2 : 3u;
   if (rows_log2_ > 16) throw std::invalid_argument("rows_per_bucket_log2 must be <= 16");
-  if (config.search_mode > 1) throw std::invalid_argument("unknown search_mode");
+  if (config.search_mode > 2) throw std::invalid_argument("unknown search_mode");
   // publication capacity as in initial_storage_capacity (GPULSMOpt.cuh:255-263)
   budget_ = std::max<uint64_t>(config.max_elements, batch_capacity_ * 16u);
   if (budget_ > 0xffffffffull)
@@ -371,11 +383,11 @@ RunBuffer *LsmDictionary::merge(RunBuffer *newer, RunBuffer *older, uint64_t out
   lsm::merge_partition_kernel<<<grid_for(tiles + 1, 256), 256, 0, s>>>(newer->keys, newer->desc, older->keys,
                                                                          older->desc, parts, uint32_t(tiles + 1));
   note_launch();
-  lsm::merge_kernel<<<unsigned(tiles), lsm::kMergeThreads, 0, s>>>(
+  auto kernel = drop_tombstones ? lsm::merge_kernel<true> : lsm::merge_kernel<false>;
+  kernel<<<unsigned(tiles), lsm::kMergeThreads, 0, s>>>(
       newer->keys, newer->vals, newer->flags, newer->desc, older->keys, older->vals, older->flags,
       older->desc, out->keys, out->vals, out->flags, out->desc, out->dir, out->dir_bits, rows_log2_,
-      std::min<uint64_t>(out_upper, out->cap), out->cap, drop_tombstones ? 1 : 0, parts, lb, counter,
-      dev_status_);
+      std::min<uint64_t>(out_upper, out->cap), out->cap, parts, lb, counter, dev_status_);
   note_launch();
   GPULSM_CUDA(cudaGetLastError());
   pool_.release(newer);
@@ -383,6 +395,32 @@ RunBuffer *LsmDictionary::merge(RunBuffer *newer, RunBuffer *older, uint64_t out
   return out;
 }
 
+
+// Search mode 1: fit the learned position model of a freshly written level
+// on the GPU (forward/backward kernels), reading its exact row count from the
+// device descriptor; small levels keep the directory.
+void LsmDictionary::fit_model(RunBuffer *run, uint64_t upper, cudaStream_t s) {
+  if (cfg_.search_mode != 1 || upper < kLearnedMinRows) return;
+  uint32_t segs = 64;
+  while (segs < upper / kRowsPerSegment && segs < kMaxSegments) segs <<= 1;
+  const size_t bytes = learned::bytes_for(segs);
+  if (bytes > run->model_cap) {
+    if (run->model) GPULSM_CUDA(cudaFreeAsync(run->model, s));
+    run->model = nullptr;
+    pool_.account(-int64_t(run->model_cap));
+    run->model_cap = 0;
+    if (cudaMallocAsync(&run->model, bytes, s) != cudaSuccess) {
+      (void)cudaGetLastError();
+      run->model = nullptr;
+      throw std::bad_alloc();
+    }
+    run->model_cap = bytes;
+    pool_.account(int64_t(bytes));
+  }
+  learned::fit<uint32_t>(run->keys, upper, segs, kFitIters, run->model, nullptr, s, &run->desc->n);
+  run->model_segments = segs;
+  run->model_ok = true;
+}
 
 void LsmDictionary::cascade(RunBuffer *carry, uint64_t carry_upper, bool carry_tombs, cudaStream_t s) {
   const size_t L = levels_.size();
@@ -420,6 +458,7 @@ void LsmDictionary::cascade(RunBuffer *carry, uint64_t carry_upper, bool carry_t
   levels_[dest].upper = std::min<uint64_t>(xu, x->cap);
   levels_[dest].gen = next_gen_++;
   levels_[dest].tombs = xt;  // its directory was written by the kernel that wrote its rows
+  fit_model(x, levels_[dest].upper, s);
 }
 
 // Merge every occupied level, newest first, into one tombstone-free run at
@@ -453,6 +492,7 @@ void LsmDictionary::compact_all(cudaStream_t s) {
   levels_[dest].upper = std::min<uint64_t>(xu, x->cap);
   levels_[dest].gen = next_gen_++;
   levels_[dest].tombs = false;
+  fit_model(x, levels_[dest].upper, s);
 }
 
 int LsmDictionary::ranges_on_single_level(const uint32_t *lo, const uint32_t *hi, uint64_t n, cudaStream_t s) {
@@ -561,6 +601,7 @@ void LsmDictionary::bulk_build(const uint32_t *keys, const uint32_t *values, uin
     top.upper = n;
     top.gen = next_gen_++;
     top.tombs = false;
+    fit_model(run, n, s);
     post_receipt(s);
   }
   end_op(s);
@@ -593,21 +634,20 @@ void LsmDictionary::erase(const uint32_t *keys, uint64_t n, cudaStream_t s) {
 
 lsm::LevelView LsmDictionary::view_of(int level) const {
   const RunBuffer *r = levels_[level].run;
-  return lsm::LevelView{r->keys, r->vals, r->flags, r->dir, r->desc};
+  lsm::LevelView v{r->keys, r->vals, r->flags, cfg_.search_mode == 2 ? nullptr : r->dir, r->desc};
+  if (cfg_.search_mode == 1 && r->model_ok) {
+    v.mh = static_cast<const learned::ModelHeader *>(r->model);
+    v.ms = reinterpret_cast<const learned::Segment *>(static_cast<const char *>(r->model) +
+                                                      sizeof(learned::ModelHeader));
+  }
+  return v;
 }
 
 void LsmDictionary::level_set(void *out) const {
   auto *set = static_cast<lsm::LevelSet *>(out);
   set->count = 0;
-  for (const auto &l : levels_) {
-    if (!l.run) continue;
-    lsm::LevelView &v = set->lv[set->count++];
-    v.keys = l.run->keys;
-    v.vals = l.run->vals;
-    v.flags = l.run->flags;
-    v.dir = l.run->dir;
-    v.desc = l.run->desc;
-  }
+  for (size_t i = 0; i < levels_.size(); ++i)
+    if (levels_[i].run) set->lv[set->count++] = view_of(int(i));
 }
 
 void LsmDictionary::lookup(const uint32_t *queries, uint64_t n, uint32_t *out_values,
@@ -642,6 +682,21 @@ void LsmDictionary::range_sum(const uint32_t *lo, const uint32_t *hi, uint64_t n
     lsm::range_kernel<0><<<grid_for(n, 256), 256, 0, s>>>(set, lo, hi, n, out, nullptr, nullptr,
                                                          nullptr); note_launch();
   }
+  GPULSM_CUDA(cudaGetLastError());
+  end_op(s);
+}
+
+void LsmDictionary::range_sum_kway(const uint32_t *lo, const uint32_t *hi, uint64_t n, uint32_t *out,
+                                   cudaStream_t s) {
+  std::lock_guard<std::mutex> g(mu_);
+  if (!n) return;
+  if (!lo || !hi || !out) throw std::invalid_argument("invalid GPU dictionary range");
+  apply_receipt(false);
+  begin_op(s);
+  lsm::LevelSet set;
+  level_set(&set);
+  lsm::range_kernel<0><<<grid_for(n, 256), 256, 0, s>>>(set, lo, hi, n, out, nullptr, nullptr, nullptr);
+  note_launch();
   GPULSM_CUDA(cudaGetLastError());
   end_op(s);
 }

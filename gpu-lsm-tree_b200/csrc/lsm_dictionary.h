@@ -39,6 +39,12 @@ struct RunBuffer {
   lsm::LevelDesc *desc = nullptr;
   void *block = nullptr;   // single device allocation backing all streams
   size_t bytes = 0;
+  // learned position model of the run's keys (search mode 1); valid only
+  // while model_ok (reset when the buffer is reused)
+  void *model = nullptr;
+  size_t model_cap = 0;
+  uint32_t model_segments = 0;
+  bool model_ok = false;
 };
 
 class RunPool {
@@ -49,6 +55,7 @@ class RunPool {
   void release(RunBuffer *b);
   void release_all_free(cudaStream_t stream);
   size_t bytes() const { return bytes_; }
+  void account(int64_t delta) { bytes_ = size_t(int64_t(bytes_) + delta); }
 
  private:
   uint32_t rows_log2_;
@@ -71,6 +78,9 @@ class LsmDictionary {
   void lookup(const uint32_t *queries, uint64_t n, uint32_t *out_values, uint8_t *out_found,
               cudaStream_t s);
   void range_sum(const uint32_t *lo, const uint32_t *hi, uint64_t n, uint32_t *out, cudaStream_t s);
+  // range_sum answered by the per-query merge over the levels, never by a
+  // compaction (no host wait: for a serving loop that must not stall)
+  void range_sum_kway(const uint32_t *lo, const uint32_t *hi, uint64_t n, uint32_t *out, cudaStream_t s);
   void range_count(const uint32_t *lo, const uint32_t *hi, uint64_t n, uint32_t *out,
                    cudaStream_t s);
   void range_offsets(const uint32_t *lo, const uint32_t *hi, uint64_t n, uint64_t *offsets,
@@ -116,6 +126,7 @@ class LsmDictionary {
   void compact_all(cudaStream_t s);
   const unsigned long long *value_prefix(int level, cudaStream_t s);
   void release_levels(cudaStream_t s);
+  void fit_model(RunBuffer *run, uint64_t upper, cudaStream_t s);
   void *scratch(size_t bytes, cudaStream_t s);
   void ensure_sort_space(uint64_t n, cudaStream_t s);
   void level_set(void *out) const;

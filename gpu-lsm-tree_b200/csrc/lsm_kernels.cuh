@@ -13,6 +13,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "learned.cuh"
 
 namespace gpulsm {
 namespace lsm {
@@ -28,12 +29,16 @@ struct LevelDesc {
 };
 static_assert(sizeof(LevelDesc) == 32, "LevelDesc layout");
 
+// How a level is searched: its radix directory (dir), its learned position
+// model (mh/ms, search mode 1) or, with neither, binary search over all rows.
 struct LevelView {
   const uint32_t *keys;
   const uint32_t *vals;
   const uint8_t *flags;
   const uint32_t *dir;
   const LevelDesc *desc;
+  const learned::ModelHeader *mh = nullptr;
+  const learned::Segment *ms = nullptr;
 };
 
 struct LevelSet {
@@ -212,9 +217,17 @@ __global__ void __launch_bounds__(kCompactThreads) dedup_last_kernel(
 // Merge-path tiles of kMergeTile outputs; ties put A first, so a B row whose
 // key was just taken from A is shadowed and dropped (newest level wins).  With
 // drop_tombstones (the output becomes the oldest level) tombstones disappear.
+//
+// Only keys (and, when tombstones drop, flags) are staged in shared memory.
+// Each thread merges kMergeItems consecutive outputs with the two run heads
+// cached in registers and records the tile-local source index of every kept
+// row; a block scan compacts them; the rows are then written in striped
+// order, gathering values and flags from global memory (consecutive outputs
+// come from consecutive source rows, so those loads stay coalesced).  An odd
+// item count keeps the threads' starting diagonals in distinct banks.
 constexpr int kMergeThreads = 256;
-constexpr int kMergeItems = 16;
-constexpr uint32_t kMergeTile = kMergeThreads * kMergeItems;
+constexpr int kMergeItems = 15;
+constexpr uint32_t kMergeTile = kMergeThreads * kMergeItems;  // 3840 outputs per tile
 
 __device__ __forceinline__ uint64_t merge_path(const uint32_t *a, uint64_t na, const uint32_t *b,
                                                uint64_t nb, uint64_t diag) {
@@ -244,18 +257,20 @@ __global__ void __launch_bounds__(256) merge_partition_kernel(const uint32_t *__
   parts[i] = merge_path(ak, na, bk, nb, d);
 }
 
-__global__ void __launch_bounds__(kMergeThreads) merge_kernel(
+template <bool kDropTombstones>
+__global__ void __launch_bounds__(kMergeThreads, 4) merge_kernel(
     const uint32_t *__restrict__ ak, const uint32_t *__restrict__ av, const uint8_t *__restrict__ af,
     const LevelDesc *__restrict__ adesc, const uint32_t *__restrict__ bk,
     const uint32_t *__restrict__ bv, const uint8_t *__restrict__ bf,
     const LevelDesc *__restrict__ bdesc, uint32_t *__restrict__ ok, uint32_t *__restrict__ ov,
     uint8_t *__restrict__ of, LevelDesc *__restrict__ odesc, uint32_t *__restrict__ odir, uint32_t dir_bits,
-    uint32_t rows_log2, unsigned long long out_upper, unsigned long long out_capacity, int drop_tombstones,
+    uint32_t rows_log2, unsigned long long out_upper, unsigned long long out_capacity,
     const unsigned long long *__restrict__ parts, unsigned long long *__restrict__ lb,
     uint32_t *__restrict__ tile_counter, uint32_t *__restrict__ status) {
-  __shared__ uint32_t s_k[kMergeTile];
-  __shared__ uint32_t s_v[kMergeTile];
-  __shared__ uint8_t s_f[kMergeTile];
+  __shared__ uint32_t s_key[kMergeTile];   // A segment, then B segment
+  __shared__ uint32_t s_out[kMergeTile];   // compacted output keys
+  __shared__ uint16_t s_src[kMergeTile];   // tile-local source index of each kept row
+  __shared__ uint8_t s_flag[kDropTombstones ? kMergeTile : 1];
   __shared__ uint32_t s_scan[kMergeThreads / 32];
   __shared__ uint32_t s_total;
   __shared__ uint32_t s_tile;
@@ -276,17 +291,29 @@ __global__ void __launch_bounds__(kMergeThreads) merge_kernel(
   const uint32_t kmax = na == 0 ? bdesc->kmax : nb == 0 ? adesc->kmax : max(adesc->kmax, bdesc->kmax);
   const DirGeom geom = dir_geometry(kmin, kmax, out_upper, dir_bits, rows_log2);
   const uint64_t a0 = parts[tile], a1 = parts[tile + 1], b0 = d0 - a0, b1 = d1 - a1;
-  const uint32_t alen = uint32_t(a1 - a0), blen = uint32_t(b1 - b0);
-  // stage A then B in shared memory
-  for (uint32_t j = threadIdx.x; j < alen; j += kMergeThreads) {
-    s_k[j] = ak[a0 + j];
-    s_v[j] = av[a0 + j];
-    s_f[j] = af[a0 + j];
-  }
-  for (uint32_t j = threadIdx.x; j < blen; j += kMergeThreads) {
-    s_k[alen + j] = bk[b0 + j];
-    s_v[alen + j] = bv[b0 + j];
-    s_f[alen + j] = bf[b0 + j];
+  const uint32_t alen = uint32_t(a1 - a0), blen = uint32_t(b1 - b0), len = alen + blen;
+  const uint32_t *kA = ak + a0, *kB = bk + b0;
+  // stage the tile's keys: every thread issues all its loads before its stores
+  {
+    uint32_t k[kMergeItems];
+#pragma unroll
+    for (int i = 0; i < kMergeItems; ++i) {
+      const uint32_t j = uint32_t(i) * kMergeThreads + threadIdx.x;
+      k[i] = j < len ? *(j < alen ? kA + j : kB + (j - alen)) : 0u;
+    }
+#pragma unroll
+    for (int i = 0; i < kMergeItems; ++i) {
+      const uint32_t j = uint32_t(i) * kMergeThreads + threadIdx.x;
+      if (j < len) s_key[j] = k[i];
+    }
+    if (kDropTombstones) {
+      const uint8_t *fA = af + a0, *fB = bf + b0;
+#pragma unroll
+      for (int i = 0; i < kMergeItems; ++i) {
+        const uint32_t j = uint32_t(i) * kMergeThreads + threadIdx.x;
+        if (j < len) s_flag[j] = *(j < alen ? fA + j : fB + (j - alen));
+      }
+    }
   }
   // key of the A row just before this tile (shadows a leading B row); the
   // largest key consumed before / by this tile bounds its directory buckets
@@ -296,76 +323,102 @@ __global__ void __launch_bounds__(kMergeThreads) merge_kernel(
   const uint32_t prev_key = max(has_prev_a ? prev_a_global : 0u, b0 > 0 ? bk[b0 - 1] : 0u);
   const uint32_t last_key = max(a1 > 0 ? ak[a1 - 1] : 0u, b1 > 0 ? bk[b1 - 1] : 0u);
   __syncthreads();
-  const uint32_t *sa = s_k, *sb = s_k + alen;
-  const uint32_t my_d = min(uint32_t(threadIdx.x) * kMergeItems, alen + blen);
-  const uint32_t my_e = min(my_d + kMergeItems, alen + blen);
-  uint32_t ai = uint32_t(merge_path(sa, alen, sb, blen, my_d));
+  // serial merge of this thread's outputs, branch-free: one shared load per
+  // output (the new head of the side that advanced)
+  const uint32_t my_d = min(uint32_t(threadIdx.x) * kMergeItems, len);
+  const uint32_t my_n = min(uint32_t(kMergeItems), len - my_d);
+  uint32_t ai = uint32_t(merge_path(s_key, alen, s_key + alen, blen, my_d));
   uint32_t bi = my_d - ai;
-  bool have_prev = ai > 0 ? true : has_prev_a;
-  uint32_t prev_a = ai > 0 ? sa[ai - 1] : prev_a_global;
-  uint32_t src[kMergeItems];  // smem index of each item, kept ones flagged in keep_mask
+  bool hp = ai > 0 ? true : has_prev_a;
+  uint32_t prev = ai > 0 ? s_key[ai - 1] : prev_a_global;
+  const uint32_t last = len ? len - 1 : 0;
+  uint32_t ka = s_key[min(ai, last)], kb = s_key[min(alen + bi, last)];
+  uint16_t src[kMergeItems];
   uint32_t keep_mask = 0;
 #pragma unroll
   for (int i = 0; i < kMergeItems; ++i) {
-    src[i] = 0;
-    if (my_d + i < my_e) {
-      const bool take_a = ai < alen && (bi >= blen || sa[ai] <= sb[bi]);
-      uint32_t idx, key;
-      bool keep;
-      if (take_a) {
-        idx = ai++;
-        key = sa[idx];
-        have_prev = true;
-        prev_a = key;
-        keep = true;
-      } else {
-        idx = alen + bi++;
-        key = sb[idx - alen];
-        keep = !(have_prev && prev_a == key);
-      }
-      if (keep && drop_tombstones && s_v[idx] == kTombValue && (s_f[idx] & kFlagTomb)) keep = false;
-      src[i] = idx;
-      if (keep) keep_mask |= 1u << i;
-    }
+    const bool ta = ai < alen && (bi >= blen || ka <= kb);
+    const uint32_t idx = ta ? ai : alen + bi;
+    const bool shadow = !ta && hp && prev == kb;
+    hp = hp || ta;
+    prev = ta ? ka : prev;
+    ai += ta ? 1u : 0u;
+    bi += ta ? 0u : 1u;
+    const uint32_t nxt = s_key[min(ta ? ai : alen + bi, last)];
+    ka = ta ? nxt : ka;
+    kb = ta ? kb : nxt;
+    bool keep = uint32_t(i) < my_n && !shadow;
+    if (kDropTombstones) keep = keep && !(s_flag[min(idx, last)] & kFlagTomb);
+    src[i] = uint16_t(idx);
+    keep_mask |= keep ? (1u << i) : 0u;
   }
-  const uint32_t kept = __popc(keep_mask);
-  const uint32_t local = block_exclusive_scan<kMergeThreads>(kept, s_scan, &s_total);
+  uint32_t o = block_exclusive_scan<kMergeThreads>(uint32_t(__popc(keep_mask)), s_scan, &s_total);
   const uint32_t tile_kept = s_total;
-  if (threadIdx.x < 32) {
-    const unsigned long long lb_excl = warp_lookback(lb, tile, tile_kept, status);
-    if (threadIdx.x == 0) s_base = lb_excl;
-  }
+  if (threadIdx.x == 0) lookback_publish(lb, tile, tile_kept);  // successors may proceed
+#pragma unroll
+  for (int i = 0; i < kMergeItems; ++i)
+    if (keep_mask & (1u << i)) s_src[o++] = src[i];
+  __syncthreads();
+  // striped output: gather values and flags (their latency overlaps the
+  // look-back walk), then store at the tile's global offset
+  const uint32_t *vA = av + a0, *vB = bv + b0;
+  const uint8_t *fA = af + a0, *fB = bf + b0;
   uint32_t rk[kMergeItems], rv[kMergeItems];
   uint8_t rf[kMergeItems];
 #pragma unroll
   for (int i = 0; i < kMergeItems; ++i) {
-    rk[i] = s_k[src[i]];
-    rv[i] = s_v[src[i]];
-    rf[i] = s_f[src[i]];
+    const uint32_t j = uint32_t(i) * kMergeThreads + threadIdx.x;
+    rk[i] = 0;
+    rv[i] = 0;
+    rf[i] = 0;
+    if (j < tile_kept) {
+      const uint32_t sidx = s_src[j];
+      const bool in_a = sidx < alen;
+      const uint32_t off = in_a ? sidx : sidx - alen;
+      rk[i] = s_key[sidx];
+      rv[i] = *((in_a ? vA : vB) + off);
+      rf[i] = *((in_a ? fA : fB) + off);
+      s_out[j] = rk[i];
+    }
+  }
+  if (threadIdx.x < 32) {
+    const unsigned long long e = lookback_walk(lb, tile, tile_kept, status);
+    if (threadIdx.x == 0) s_base = e;
   }
   __syncthreads();
-#pragma unroll
-  for (int i = 0; i < kMergeItems; ++i)
-    if (keep_mask & (1u << i)) {
-      const uint32_t o = local + __popc(keep_mask & ((1u << i) - 1u));
-      s_k[o] = rk[i];
-      s_v[o] = rv[i];
-      s_f[o] = rf[i];
-    }
-  __syncthreads();
   const unsigned long long gbase = s_base;
-  for (uint32_t j = threadIdx.x; j < tile_kept; j += kMergeThreads) {
-    const unsigned long long o = gbase + j;
-    if (o < out_capacity) {
-      ok[o] = s_k[j];
-      ov[o] = s_v[j];
-      of[o] = s_f[j];
+  const unsigned long long space = gbase < out_capacity ? out_capacity - gbase : 0ull;
+  const uint32_t room = space < tile_kept ? uint32_t(space) : tile_kept;
+  uint32_t *okb = ok + gbase, *ovb = ov + gbase;
+  uint8_t *ofb = of + gbase;
+  // rows, and the directory entries they start: row j owns the buckets
+  // (bucket(key j-1), bucket(key j)] (the tile's first row starts after the
+  // bucket of the key consumed before the tile), as in fill_directory
+  const uint32_t gk = geom.kmin, gs = geom.shift;
+  const int32_t bp = has_prev ? int32_t((prev_key - gk) >> gs) : -1;
+  const uint32_t g0 = uint32_t(gbase);
+#pragma unroll
+  for (int i = 0; i < kMergeItems; ++i) {
+    const uint32_t j = uint32_t(i) * kMergeThreads + threadIdx.x;
+    if (j < room) {
+      okb[j] = rk[i];
+      ovb[j] = rv[i];
+      ofb[j] = rf[i];
+    }
+    if (j < tile_kept) {
+      const int32_t bj = int32_t((rk[i] - gk) >> gs);
+      const int32_t bprev = j ? int32_t((s_out[j - 1] - gk) >> gs) : bp;
+      for (int32_t b = bprev + 1; b <= bj; ++b) odir[b] = g0 + j;
     }
   }
   const bool last_tile = d1 == total;
   const unsigned long long n_out = gbase + tile_kept;
-  fill_directory(odir, geom, has_prev, prev_key, last_key, last_tile, gbase, tile_kept,
-                 n_out < out_capacity ? n_out : out_capacity, [&](uint32_t j) { return s_k[j]; });
+  if (threadIdx.x == 0) {
+    const int32_t blast = tile_kept ? int32_t((s_out[tile_kept - 1] - gk) >> gs) : bp;
+    const int32_t bl = last_tile ? int32_t(geom.nbuckets) - 1 : int32_t((last_key - gk) >> gs);
+    for (int32_t b = blast + 1; b <= bl; ++b) odir[b] = g0 + tile_kept;
+    if (last_tile) odir[geom.nbuckets] = uint32_t(n_out < out_capacity ? n_out : out_capacity);
+  }
   if (tile == 0 && threadIdx.x == 0) {
     odesc->kmin = geom.kmin;
     odesc->kmax = geom.kmax;
@@ -396,6 +449,21 @@ __device__ __forceinline__ uint64_t level_lower_bound(const LevelView &L, const 
                                                       uint32_t x) {
   if (d.n == 0 || x <= d.kmin) return 0;
   if (x > d.kmax) return d.n;
+  if (L.ms) {
+    // learned: the model's error window, then a check of the answer; a failed
+    // check (never expected: the window bounds every key's error) falls back
+    // to binary search over the whole level
+    learned::ModelHeader h;
+    h.n = __ldg(&L.mh->n);
+    h.kmin = __ldg(&L.mh->kmin);
+    h.kmax = __ldg(&L.mh->kmax);
+    h.shift = __ldg(&L.mh->shift);
+    h.nseg = __ldg(&L.mh->nseg);
+    const uint64_t p = learned::model_lower_bound<uint32_t>(h, L.ms, L.keys, x);
+    if (h.n == d.n && (p == 0 || L.keys[p - 1] < x) && (p == d.n || L.keys[p] >= x)) return p;
+    return learned::lower_bound_range<uint32_t>(L.keys, 0, d.n, x);
+  }
+  if (!L.dir) return learned::lower_bound_range<uint32_t>(L.keys, 0, d.n, x);
   const uint32_t b = (x - d.kmin) >> d.shift;
   return bucket_lower_bound(L.keys, L.dir[b], L.dir[b + 1], x);
 }
@@ -435,9 +503,15 @@ __global__ void __launch_bounds__(256) lookup_kernel(LevelSet set, const uint32_
     const LevelView &L = set.lv[l];
     const LevelDesc d = load_desc(L.desc);
     if (q < d.kmin || q > d.kmax) continue;
-    const uint32_t b = (q - d.kmin) >> d.shift;
-    const uint32_t s = L.dir[b], e = L.dir[b + 1];
-    const uint32_t p = bucket_lower_bound(L.keys, s, e, q);
+    uint64_t p, e;
+    if (L.dir && !L.ms) {  // radix directory: the bucket's rows only
+      const uint32_t b = (q - d.kmin) >> d.shift;
+      e = L.dir[b + 1];
+      p = bucket_lower_bound(L.keys, L.dir[b], uint32_t(e), q);
+    } else {  // learned model window or binary search
+      p = level_lower_bound(L, d, q);
+      e = d.n;
+    }
     if (p < e && L.keys[p] == q) {
       const uint32_t v = L.vals[p];
       const bool live = !row_is_tomb(L, p, v);

@@ -56,10 +56,10 @@ size_t bytes_for(uint32_t segments) { return model_bytes(pow2_at_least(segments)
 
 template <typename K>
 void fit(const K *keys, uint64_t n, uint32_t segments, uint32_t iters, void *model, float *loss_hist,
-         cudaStream_t s) {
+         cudaStream_t s, const unsigned long long *n_dev) {
   segments = pow2_at_least(std::max<uint32_t>(segments, 1));
   Parts p = parts(model, segments);
-  model_header_kernel<K><<<1, 1, 0, s>>>(keys, n, segments, p.h); note_launch();
+  model_header_kernel<K><<<1, 1, 0, s>>>(keys, n, segments, p.h, n_dev); note_launch();
   model_init_kernel<K><<<grid_for(segments + 1, 256), 256, 0, s>>>(keys, p.h, p.seg); note_launch();
   model_init_params_kernel<K><<<grid_for(segments, 256), 256, 0, s>>>(p.h, p.seg); note_launch();
   GPULSM_CUDA(cudaMemsetAsync(p.acc, 0, size_t(segments) * 16, s));
@@ -116,9 +116,10 @@ void binary_lower_bound(const K *keys, uint64_t n, const K *q, uint64_t count, u
   GPULSM_CUDA(cudaGetLastError());
 }
 
-template void fit<uint32_t>(const uint32_t *, uint64_t, uint32_t, uint32_t, void *, float *, cudaStream_t);
+template void fit<uint32_t>(const uint32_t *, uint64_t, uint32_t, uint32_t, void *, float *, cudaStream_t,
+                            const unsigned long long *);
 template void fit<unsigned long long>(const unsigned long long *, uint64_t, uint32_t, uint32_t, void *, float *,
-                                      cudaStream_t);
+                                      cudaStream_t, const unsigned long long *);
 template void gradients<uint32_t>(const uint32_t *, uint64_t, uint32_t, void *, float *, float *, cudaStream_t);
 template void gradients<unsigned long long>(const unsigned long long *, uint64_t, uint32_t, void *, float *,
                                             float *, cudaStream_t);

@@ -14,9 +14,10 @@ size_t bytes_for(uint32_t segments);
 // (forward/backward kernels), then per-segment maximum error.  loss_hist
 // (device, iters + 1 floats, may be null) receives the mean squared error
 // before each step and after the last one.
+// n_dev (optional): the exact count on the device; n is then an upper bound.
 template <typename K>
 void fit(const K *keys, uint64_t n, uint32_t segments, uint32_t iters, void *model, float *loss_hist,
-         cudaStream_t s);
+         cudaStream_t s, const unsigned long long *n_dev = nullptr);
 // dL/da_s, dL/db_s interleaved per segment (device, 2 * segments floats) and
 // the mean squared error, for the model's current parameters.
 template <typename K>

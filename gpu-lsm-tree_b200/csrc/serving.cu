@@ -1,0 +1,460 @@
+// Serving loop (serving.h): rounds formed in arrival order, a device-memory
+// budget for admission, pipelined slots, per-request latency.
+#include "serving.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <random>
+#include <stdexcept>
+#include <string>
+
+#include "common.cuh"
+
+namespace gpulsm {
+
+namespace {
+// Device bytes an update of one key may add before its receipt is applied:
+// the admitted run (9 B/row plus directory), sort words (16 B) and the
+// transient merge output (9 B/row), rounded up.
+constexpr uint64_t kUpdateBytesPerKey = 48;
+constexpr int kErrCapacity = 2;  // GPULSM_ERR_CAPACITY
+constexpr int kErrCuda = 5;      // GPULSM_ERR_CUDA
+
+int status_of(const std::exception &e) {
+  const std::string m = e.what();
+  return m.find("capacity") != std::string::npos ? -kErrCapacity : -kErrCuda;
+}
+
+bool is_update(uint32_t kind) { return kind == kServeInsert || kind == kServeErase; }
+bool has_aux(uint32_t kind) { return kind == kServeInsert || kind == kServeRangeSum; }
+bool has_out(uint32_t kind) { return kind == kServeLookup || kind == kServeRangeSum; }
+}  // namespace
+
+double Server::now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+Server::Server(const DictConfig &cfg, uint64_t budget_bytes, uint32_t max_round_keys, uint32_t depth)
+    : dict_(cfg), budget_(budget_bytes), max_round_keys_(max_round_keys ? max_round_keys : (1u << 20)) {
+  if (depth == 0) depth = 3;
+  if (depth > 8) throw std::invalid_argument("serving depth must be in [1, 8]");
+  if (max_round_keys_ > (1u << 24)) throw std::invalid_argument("max_round_keys must be <= 2^24");
+  GPULSM_CUDA(cudaGetDevice(&device_));
+  GPULSM_CUDA(cudaStreamCreateWithFlags(&compute_, cudaStreamNonBlocking));
+  GPULSM_CUDA(cudaStreamCreateWithFlags(&upload_, cudaStreamNonBlocking));
+  GPULSM_CUDA(cudaStreamCreateWithFlags(&download_, cudaStreamNonBlocking));
+  const uint64_t m = max_round_keys_;
+  slot_bytes_ = m * 8 + m * 4 + m;  // inputs (two words a key), outputs, found flags
+  slots_.resize(depth);
+  for (uint32_t i = 0; i < depth; ++i) {
+    Slot &s = slots_[i];
+    GPULSM_CUDA(cudaMallocHost(&s.h_in, m * 8));
+    GPULSM_CUDA(cudaMallocHost(&s.h_out, m * 4));
+    GPULSM_CUDA(cudaMallocHost(&s.h_found, m));
+    GPULSM_CUDA(cudaMalloc(&s.d_in, m * 8));
+    GPULSM_CUDA(cudaMalloc(&s.d_out, m * 4));
+    GPULSM_CUDA(cudaMalloc(&s.d_found, m));
+    GPULSM_CUDA(cudaEventCreateWithFlags(&s.uploaded, cudaEventDisableTiming));
+    GPULSM_CUDA(cudaEventCreateWithFlags(&s.computed, cudaEventDisableTiming));
+    GPULSM_CUDA(cudaEventCreateWithFlags(&s.downloaded, cudaEventDisableTiming));
+    free_slots_.push_back(i);
+  }
+  worker_ = std::thread(&Server::worker, this);
+  completer_ = std::thread(&Server::completer, this);
+}
+
+Server::~Server() {
+  try {
+    drain();
+  } catch (...) {
+  }
+  {
+    std::lock_guard<std::mutex> g(mu_);
+    stop_ = true;
+  }
+  cv_work_.notify_all();
+  cv_inflight_.notify_all();
+  if (worker_.joinable()) worker_.join();
+  if (completer_.joinable()) completer_.join();
+  cudaStreamSynchronize(compute_);
+  cudaStreamSynchronize(upload_);
+  cudaStreamSynchronize(download_);
+  for (Slot &s : slots_) {
+    cudaFreeHost(s.h_in);
+    cudaFreeHost(s.h_out);
+    cudaFreeHost(s.h_found);
+    cudaFree(s.d_in);
+    cudaFree(s.d_out);
+    cudaFree(s.d_found);
+    cudaEventDestroy(s.uploaded);
+    cudaEventDestroy(s.computed);
+    cudaEventDestroy(s.downloaded);
+  }
+  cudaStreamDestroy(compute_);
+  cudaStreamDestroy(upload_);
+  cudaStreamDestroy(download_);
+}
+
+uint64_t Server::submit(uint32_t kind, const uint32_t *keys, const uint32_t *aux, uint64_t n, uint32_t *out,
+                        uint8_t *found) {
+  if (kind > kServeRangeSum) throw std::invalid_argument("unknown request kind");
+  if (n > max_round_keys_) throw std::length_error("request larger than max_round_keys");
+  if (n && !keys) throw std::invalid_argument("null request keys");
+  if (n && has_aux(kind) && !aux) throw std::invalid_argument("null request values / upper bounds");
+  if (n && has_out(kind) && !out) throw std::invalid_argument("null request output");
+  const double t = now_s();
+  uint64_t tk;
+  {
+    std::lock_guard<std::mutex> g(mu_);
+    if (stop_) throw std::runtime_error("server is shutting down");
+    tk = next_ticket_++;
+    reqs_[tk] = Req{kind, keys, aux, n, out, found, t, 0};
+    if (st_first_ < 0) st_first_ = t;
+    queue_.push_back(tk);
+  }
+  cv_work_.notify_one();
+  return tk;
+}
+
+int Server::poll(uint64_t ticket) {
+  std::lock_guard<std::mutex> g(mu_);
+  auto it = reqs_.find(ticket);
+  if (it == reqs_.end()) throw std::invalid_argument("unknown or already collected ticket");
+  const int st = it->second.state;
+  if (st != 0) reqs_.erase(it);
+  return st;
+}
+
+int Server::wait(uint64_t ticket) {
+  std::unique_lock<std::mutex> lk(mu_);
+  if (reqs_.find(ticket) == reqs_.end()) throw std::invalid_argument("unknown or already collected ticket");
+  cv_done_.wait(lk, [&] { return reqs_.at(ticket).state != 0; });
+  const int st = reqs_.at(ticket).state;
+  reqs_.erase(ticket);
+  return st;
+}
+
+void Server::drain() {
+  std::unique_lock<std::mutex> lk(mu_);
+  cv_done_.wait(lk, [&] { return queue_.empty() && inflight_.empty() && free_slots_.size() == slots_.size(); });
+}
+
+void Server::reset_stats() {
+  std::lock_guard<std::mutex> g(mu_);
+  lat_us_.clear();
+  st_completed_ = st_rejected_ = st_rounds_ = st_keys_ = st_round_keys_ = 0;
+  st_first_ = -1;
+  st_last_ = 0;
+}
+
+ServeStats Server::stats() {
+  std::vector<float> lat;
+  ServeStats s;
+  {
+    std::lock_guard<std::mutex> g(mu_);
+    lat = lat_us_;
+    s.completed = st_completed_;
+    s.rejected = st_rejected_;
+    s.rounds = st_rounds_;
+    s.keys = st_keys_;
+    s.mean_round_keys = st_rounds_ ? double(st_round_keys_) / double(st_rounds_) : 0.0;
+    s.wall_s = st_first_ >= 0 ? std::max(0.0, st_last_ - st_first_) : 0.0;
+  }
+  if (!lat.empty()) {
+    auto pct = [&](double p) {
+      const size_t k = std::min(lat.size() - 1, size_t(p * double(lat.size() - 1) + 0.5));
+      std::nth_element(lat.begin(), lat.begin() + long(k), lat.end());
+      return double(lat[k]);
+    };
+    double sum = 0;
+    float mx = 0;
+    for (float v : lat) {
+      sum += v;
+      mx = std::max(mx, v);
+    }
+    s.mean_us = sum / double(lat.size());
+    s.max_us = mx;
+    s.p50_us = pct(0.50);
+    s.p99_us = pct(0.99);
+  }
+  return s;
+}
+
+// Called with mu_ held: take requests in arrival order into runs of one kind
+// until the round is full; reject updates the budget cannot hold.
+bool Server::form_round(Slot &slot) {
+  slot.runs.clear();
+  slot.parts.clear();
+  slot.bytes = 0;
+  uint64_t keys = 0;
+  const uint64_t resident = dict_.resident_bytes();
+  const double t = now_s();
+  bool any = false;
+  while (!queue_.empty()) {
+    const uint64_t tk = queue_.front();
+    Req &q = reqs_.at(tk);
+    if (keys > 0 && keys + q.n > max_round_keys_) break;
+    queue_.pop_front();
+    if (q.n == 0) {  // nothing to do: done at once
+      q.state = 1;
+      lat_us_.push_back(float((t - q.t_submit) * 1e6));
+      ++st_completed_;
+      st_last_ = t;
+      continue;
+    }
+    if (is_update(q.kind)) {
+      const uint64_t growth = q.n * kUpdateBytesPerKey;
+      if (resident + device_bytes() + inflight_bytes_ + slot.bytes + growth > budget_) {
+        q.state = -kErrCapacity;  // the device-memory budget cannot hold this update
+        ++st_rejected_;
+        st_last_ = t;
+        continue;
+      }
+      slot.bytes += growth;
+    }
+    if (slot.runs.empty() || slot.runs.back().kind != q.kind) {
+      Run r{};
+      r.kind = q.kind;
+      r.first_part = slot.parts.size();
+      slot.runs.push_back(r);
+    }
+    Run &r = slot.runs.back();
+    slot.parts.push_back(Part{tk, r.n, q.n, q.keys, q.aux, q.out, q.found});
+    ++r.parts;
+    r.n += q.n;
+    keys += q.n;
+    any = true;
+  }
+  // staging layout: each run's keys, then its values / upper bounds
+  uint64_t in = 0, out = 0;
+  for (Run &r : slot.runs) {
+    r.in_off = in;
+    r.out_off = out;
+    r.status = 0;
+    in += r.n * (has_aux(r.kind) ? 2 : 1);
+    if (has_out(r.kind)) out += r.n;
+  }
+  slot.in_words = in;
+  slot.out_words = out;
+  slot.keys = keys;
+  return any;
+}
+
+void Server::launch_round(Slot &slot) {
+  for (const Run &r : slot.runs)
+    for (uint64_t i = 0; i < r.parts; ++i) {
+      const Part &p = slot.parts[r.first_part + i];
+      std::memcpy(slot.h_in + r.in_off + p.off, p.keys, p.n * 4);
+      if (has_aux(r.kind)) std::memcpy(slot.h_in + r.in_off + r.n + p.off, p.aux, p.n * 4);
+    }
+  GPULSM_CUDA(cudaMemcpyAsync(slot.d_in, slot.h_in, slot.in_words * 4, cudaMemcpyHostToDevice, upload_));
+  GPULSM_CUDA(cudaEventRecord(slot.uploaded, upload_));
+  GPULSM_CUDA(cudaStreamWaitEvent(compute_, slot.uploaded, 0));
+  for (Run &r : slot.runs) {
+    const uint32_t *in = slot.d_in + r.in_off;
+    try {
+      switch (r.kind) {
+        case kServeLookup:
+          dict_.lookup(in, r.n, slot.d_out + r.out_off, slot.d_found + r.out_off, compute_);
+          break;
+        case kServeInsert:
+          dict_.insert(in, in + r.n, r.n, compute_);
+          break;
+        case kServeErase:
+          dict_.erase(in, r.n, compute_);
+          break;
+        default:
+          dict_.range_sum_kway(in, in + r.n, r.n, slot.d_out + r.out_off, compute_);
+          break;
+      }
+    } catch (const std::exception &e) {
+      r.status = status_of(e);
+    }
+  }
+  GPULSM_CUDA(cudaEventRecord(slot.computed, compute_));
+  GPULSM_CUDA(cudaStreamWaitEvent(download_, slot.computed, 0));
+  if (slot.out_words) {
+    GPULSM_CUDA(cudaMemcpyAsync(slot.h_out, slot.d_out, slot.out_words * 4, cudaMemcpyDeviceToHost, download_));
+    GPULSM_CUDA(cudaMemcpyAsync(slot.h_found, slot.d_found, slot.out_words, cudaMemcpyDeviceToHost, download_));
+  }
+  GPULSM_CUDA(cudaEventRecord(slot.downloaded, download_));
+}
+
+void Server::worker() {
+  cudaSetDevice(device_);
+  for (;;) {
+    std::unique_lock<std::mutex> lk(mu_);
+    cv_work_.wait(lk, [&] { return stop_ || (!queue_.empty() && !free_slots_.empty()); });
+    if (stop_) return;
+    const uint32_t si = free_slots_.front();
+    free_slots_.pop_front();
+    Slot &slot = slots_[si];
+    const bool any = form_round(slot);
+    lk.unlock();
+    if (!any) {  // only empty or rejected requests: their waiters are notified
+      lk.lock();
+      free_slots_.push_front(si);
+      lk.unlock();
+      cv_done_.notify_all();
+      continue;
+    }
+    bool ok = true;
+    try {
+      launch_round(slot);
+    } catch (const std::exception &e) {
+      ok = false;
+      for (Run &r : slot.runs) r.status = status_of(e);
+    }
+    lk.lock();
+    slot.launched = ok;
+    inflight_.push_back(si);
+    inflight_bytes_ += slot.bytes;
+    lk.unlock();
+    cv_inflight_.notify_one();
+  }
+}
+
+void Server::completer() {
+  cudaSetDevice(device_);
+  for (;;) {
+    std::unique_lock<std::mutex> lk(mu_);
+    cv_inflight_.wait(lk, [&] { return stop_ || !inflight_.empty(); });
+    if (inflight_.empty()) return;  // stopping
+    const uint32_t si = inflight_.front();
+    lk.unlock();
+    Slot &slot = slots_[si];
+    int fail = 0;
+    if (slot.launched && cudaEventSynchronize(slot.downloaded) != cudaSuccess) fail = -kErrCuda;
+    const double t = now_s();
+    if (!fail)
+      for (const Run &r : slot.runs) {
+        if (r.status || !has_out(r.kind)) continue;
+        for (uint64_t i = 0; i < r.parts; ++i) {
+          const Part &p = slot.parts[r.first_part + i];
+          std::memcpy(p.out, slot.h_out + r.out_off + p.off, p.n * 4);
+          if (r.kind == kServeLookup && p.found) std::memcpy(p.found, slot.h_found + r.out_off + p.off, p.n);
+        }
+      }
+    lk.lock();
+    inflight_.pop_front();
+    inflight_bytes_ -= slot.bytes;
+    for (const Run &r : slot.runs)
+      for (uint64_t i = 0; i < r.parts; ++i) {
+        const Part &p = slot.parts[r.first_part + i];
+        Req &q = reqs_.at(p.ticket);
+        q.state = fail ? fail : (r.status ? r.status : 1);
+        lat_us_.push_back(float((t - q.t_submit) * 1e6));
+        ++st_completed_;
+        st_keys_ += p.n;
+      }
+    ++st_rounds_;
+    st_round_keys_ += slot.keys;
+    st_last_ = t;
+    free_slots_.push_back(si);
+    lk.unlock();
+    cv_done_.notify_all();
+    cv_work_.notify_one();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Open-loop load generator.  Keys are drawn by Zipf rank over the caller's
+// universe: rank = floor(x) - 1 with x sampled from the continuous power law
+// x^-s on [1, N + 1) by inverse CDF (a bounded continuous approximation of
+// the discrete Zipf law).  Request sizes are log-uniform in [min, max].
+void Server::run_load(const LoadSpec &sp, ServeStats *out) {
+  if (!sp.universe || sp.universe_n == 0) throw std::invalid_argument("load needs a key universe");
+  if (sp.min_keys == 0 || sp.min_keys > sp.max_keys || sp.max_keys > max_round_keys_)
+    throw std::invalid_argument("load request sizes must satisfy 1 <= min <= max <= max_round_keys");
+  std::mt19937_64 rng(sp.seed);
+  std::uniform_real_distribution<double> U(0.0, 1.0);
+  const double N = double(sp.universe_n);
+  const double one_s = 1.0 - sp.zipf_s;
+  const double hi_pow = std::pow(N + 1.0, one_s);
+  auto zipf_key = [&]() {
+    const double u = U(rng);
+    double x = std::fabs(one_s) < 1e-9 ? std::exp(u * std::log(N + 1.0)) : std::pow(1.0 + u * (hi_pow - 1.0), 1.0 / one_s);
+    uint64_t r = uint64_t(x) - 1;
+    if (r >= sp.universe_n) r = sp.universe_n - 1;
+    return sp.universe[r];
+  };
+  auto log_uniform = [&](double lo, double hi) { return std::exp(std::log(lo) + U(rng) * (std::log(hi + 1.0) - std::log(lo))); };
+  // a pool of prepared requests, reused round-robin
+  struct Payload {
+    uint32_t kind;
+    std::vector<uint32_t> keys, aux, out;
+    std::vector<uint8_t> found;
+    uint64_t ticket = 0;
+  };
+  const size_t P = 512;
+  std::vector<Payload> pool(P);
+  double csum[4];
+  double acc = 0;
+  for (int k = 0; k < 4; ++k) csum[k] = (acc += sp.mix[k]);
+  for (Payload &p : pool) {
+    const double r = U(rng) * acc;
+    p.kind = r < csum[0] ? kServeLookup : r < csum[1] ? kServeInsert : r < csum[2] ? kServeErase : kServeRangeSum;
+    const uint64_t n = std::min<uint64_t>(sp.max_keys, std::max<uint64_t>(sp.min_keys, uint64_t(log_uniform(sp.min_keys, sp.max_keys))));
+    p.keys.resize(n);
+    for (auto &k : p.keys) k = zipf_key();
+    if (p.kind == kServeInsert) {
+      p.aux.resize(n);
+      for (auto &v : p.aux) v = uint32_t(rng());
+    } else if (p.kind == kServeRangeSum) {
+      p.aux.resize(n);
+      for (uint64_t i = 0; i < n; ++i) {
+        const uint64_t w = uint64_t(log_uniform(1.0, double(sp.range_width_max)));
+        p.aux[i] = uint32_t(std::min<uint64_t>(0xffffffffull, uint64_t(p.keys[i]) + std::max<uint64_t>(w, 1) - 1));
+      }
+    }
+    if (has_out(p.kind)) p.out.resize(n);
+    if (p.kind == kServeLookup) p.found.resize(n);
+  }
+  drain();
+  reset_stats();
+  std::exponential_distribution<double> gap(sp.rate_per_s > 0 ? sp.rate_per_s : 1.0);
+  std::deque<size_t> outstanding;
+  const double t0 = now_s();
+  double next = t0;
+  size_t i = 0;
+  auto issue = [&](size_t pi) {
+    Payload &p = pool[pi];
+    if (p.ticket) {  // the payload's previous request must have returned its buffers
+      wait(p.ticket);
+      p.ticket = 0;
+    }
+    p.ticket = submit(p.kind, p.keys.data(), p.aux.empty() ? nullptr : p.aux.data(), p.keys.size(),
+                      p.out.empty() ? nullptr : p.out.data(), p.found.empty() ? nullptr : p.found.data());
+    if (sp.rate_per_s <= 0) outstanding.push_back(pi);
+  };
+  while (now_s() - t0 < sp.seconds) {
+    if (sp.rate_per_s > 0) {
+      next += gap(rng);
+      double now = now_s();
+      while (now < next) {
+        if (next - now > 200e-6) std::this_thread::sleep_for(std::chrono::microseconds(50));
+        now = now_s();
+      }
+    } else {
+      while (outstanding.size() >= sp.max_outstanding) {
+        Payload &p = pool[outstanding.front()];
+        outstanding.pop_front();
+        if (p.ticket) {
+          wait(p.ticket);
+          p.ticket = 0;
+        }
+      }
+    }
+    issue(i++ % P);
+  }
+  for (Payload &p : pool)
+    if (p.ticket) {
+      wait(p.ticket);
+      p.ticket = 0;
+    }
+  *out = stats();
+}
+
+}  // namespace gpulsm

@@ -1,0 +1,158 @@
+// Serving loop over one LSM dictionary: continuous batching of mixed
+// lookup / insert / erase / range-sum requests of uneven sizes.
+//
+// The reference has no serving facility: GPULSMOpt serialises every call
+// behind a mutex and an operation event (GPULSMOpt.cuh:6852-6858), so a
+// caller batches by hand.  Here requests are submitted from any host thread
+// with host buffers; a worker thread forms rounds in arrival order,
+// coalescing each run of same-kind requests into one dictionary call, and
+// admits a request only while the dictionary's resident bytes plus the
+// rounds in flight stay inside a device-memory budget.  Rounds occupy one of
+// `depth` pipeline slots (pinned staging + device buffers): the upload of
+// round r+1 and the host staging of round r+2 overlap the kernels of round r,
+// and a completion thread returns results and records each request's latency
+// (submit to results in the caller's buffers).
+//
+// Semantics: the outcome equals applying the requests one at a time in
+// submission order (a lookup sees every earlier update and no later one):
+// rounds run in order on one compute stream, runs inside a round in order,
+// and a run of inserts or erases is one batch with keep-last semantics.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <condition_variable>
+#include <cstdint>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "lsm_dictionary.h"
+
+namespace gpulsm {
+
+enum ServeKind : uint32_t { kServeLookup = 0, kServeInsert = 1, kServeErase = 2, kServeRangeSum = 3 };
+
+struct ServeStats {
+  uint64_t completed = 0;
+  uint64_t rejected = 0;
+  uint64_t rounds = 0;
+  uint64_t keys = 0;          // keys (or range queries) of completed requests
+  double p50_us = 0, p99_us = 0, max_us = 0, mean_us = 0;
+  double mean_round_keys = 0;
+  double wall_s = 0;          // first submit to last completion since the last reset
+};
+
+// Open-loop load: Poisson arrivals, kind mix, log-uniform sizes, Zipf keys.
+struct LoadSpec {
+  double rate_per_s = 0;       // request arrivals per second; 0 = closed loop
+  double seconds = 1.0;
+  uint32_t max_outstanding = 64;  // closed loop: requests kept in flight
+  double mix[4] = {0.6, 0.2, 0.1, 0.1};  // lookup, insert, erase, range-sum
+  uint32_t min_keys = 1, max_keys = 1u << 16;
+  double zipf_s = 1.1;
+  uint32_t range_width_max = 1u << 16;
+  uint64_t seed = 1;
+  const uint32_t *universe = nullptr;  // host keys the requests draw from (by Zipf rank)
+  uint64_t universe_n = 0;
+};
+
+class Server {
+ public:
+  Server(const DictConfig &cfg, uint64_t budget_bytes, uint32_t max_round_keys, uint32_t depth);
+  ~Server();
+  Server(const Server &) = delete;
+  Server &operator=(const Server &) = delete;
+
+  // Host buffers, owned by the caller until the request completes.  keys: the
+  // request keys (range: lower bounds); aux: insert values / range upper
+  // bounds; out: lookup values / range sums; found: optional lookup flags.
+  uint64_t submit(uint32_t kind, const uint32_t *keys, const uint32_t *aux, uint64_t n, uint32_t *out,
+                  uint8_t *found);
+  int poll(uint64_t ticket);  // 0 pending, 1 done, < 0 failed (negated gpulsm status)
+  int wait(uint64_t ticket);  // 1 done, < 0 failed
+  void drain();
+  ServeStats stats();
+  void reset_stats();
+  void run_load(const LoadSpec &spec, ServeStats *out);
+  LsmDictionary &dict() { return dict_; }
+  uint64_t device_bytes() const { return slot_bytes_ * slots_.size(); }
+
+ private:
+  struct Req {
+    uint32_t kind;
+    const uint32_t *keys;
+    const uint32_t *aux;
+    uint64_t n;
+    uint32_t *out;
+    uint8_t *found;
+    double t_submit;
+    int state;  // 0 queued, 1 done, < 0 failed
+  };
+  struct Part {  // one request's share of a run
+    uint64_t ticket;
+    uint64_t off;  // first key of this request inside its run
+    uint64_t n;
+    const uint32_t *keys;
+    const uint32_t *aux;
+    uint32_t *out;
+    uint8_t *found;
+  };
+  struct Run {
+    uint32_t kind = 0;
+    uint64_t in_off = 0;   // words into the staging input: keys, then values / upper bounds
+    uint64_t out_off = 0;  // words into the staging output
+    uint64_t n = 0;
+    size_t first_part = 0, parts = 0;
+    int status = 0;        // 0, or the negated gpulsm status of a failed call
+  };
+  struct Slot {
+    uint32_t *h_in = nullptr, *h_out = nullptr;
+    uint8_t *h_found = nullptr;
+    uint32_t *d_in = nullptr, *d_out = nullptr;
+    uint8_t *d_found = nullptr;
+    cudaEvent_t uploaded = nullptr, computed = nullptr, downloaded = nullptr;
+    std::vector<Run> runs;
+    std::vector<Part> parts;
+    uint64_t in_words = 0, out_words = 0, keys = 0;
+    uint64_t bytes = 0;  // device bytes the round's updates may add (admission budget)
+    bool launched = false;
+  };
+
+  void worker();
+  void completer();
+  bool form_round(Slot &slot);
+  void launch_round(Slot &slot);
+  static double now_s();
+
+  LsmDictionary dict_;
+  int device_ = 0;
+  uint64_t budget_;
+  uint32_t max_round_keys_;
+  uint64_t slot_bytes_ = 0;
+  std::vector<Slot> slots_;
+  std::deque<uint32_t> free_slots_;
+  std::deque<uint32_t> inflight_;
+  cudaStream_t compute_ = nullptr, upload_ = nullptr, download_ = nullptr;
+
+  std::mutex mu_;
+  std::condition_variable cv_work_, cv_done_, cv_inflight_;
+  std::deque<uint64_t> queue_;
+  std::unordered_map<uint64_t, Req> reqs_;
+  uint64_t next_ticket_ = 1;
+  uint64_t inflight_bytes_ = 0;
+  bool stop_ = false;
+
+  // statistics since the last reset
+  std::vector<float> lat_us_;
+  uint64_t st_completed_ = 0, st_rejected_ = 0, st_rounds_ = 0, st_keys_ = 0, st_round_keys_ = 0;
+  double st_first_ = -1, st_last_ = 0;
+
+  std::thread worker_, completer_;
+};
+
+}  // namespace gpulsm

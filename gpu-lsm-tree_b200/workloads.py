@@ -183,3 +183,58 @@ def flix(scale: int = 0, rounds: int = 32, key_bits: int = 64) -> FlixWorkload:
         probes = rng.integers(lo_span, hi_span + 2, n_succ, dtype=np.uint64)
         w.rounds.append((ins, ins_vals, dels, probes))
     return w
+
+
+def flix_fast(scale: int = 0, rounds: int = 4, key_bits: int = 64) -> FlixWorkload:
+    """The FliX configuration's shapes without re-sorting the whole live set
+    every round (for timing at full size): 2^28 sorted keys with geometric
+    gaps (mean 16), then per round 2^22 unique absent keys (half uniform over
+    the span, half in 1024 hot ranges), a 2^21-key delete batch drawn from the
+    initial keys not yet deleted (all live), and 2^24 uniform successor
+    probes (sizes / 2^scale)."""
+    rng = rng_for(3)
+    n = 1 << (28 - scale)
+    keys = np.cumsum(rng.geometric(1.0 / 16.0, n).astype(np.uint64), dtype=np.uint64) + np.uint64(1)
+    if key_bits == 32:
+        keys = keys[keys < 0xFFFFFFFE]
+    keys = keys[keys != 0xFFFFFFFF]
+    n = keys.size
+    lo_span, hi_span = int(keys[0]), int(keys[-1])
+    w = FlixWorkload("flix: bulk build of 2^28 sorted u64 keys, rounds of 2^22 inserts, 2^21 deletes, "
+                     "2^24 successor probes", keys, [], (lo_span, hi_span))
+    n_ins, n_del, n_succ = 1 << (22 - scale), 1 << (21 - scale), 1 << (24 - scale)
+    hot_starts = rng.integers(lo_span, hi_span - (1 << 17), 1024, dtype=np.uint64)
+    inserted = np.empty(0, np.uint64)
+    deleted = np.zeros(n, bool)
+    for _ in range(rounds):
+        cand_u = rng.integers(lo_span, hi_span, n_ins, dtype=np.uint64)
+        hr = rng.integers(0, 1024, n_ins)
+        cand_h = hot_starts[hr] + rng.integers(0, 1 << 17, n_ins, dtype=np.uint64)
+        cand = np.concatenate([cand_u, cand_h])
+        cand.sort()
+        keep = np.empty(cand.size, bool)
+        keep[0] = True
+        np.not_equal(cand[1:], cand[:-1], out=keep[1:])
+        cand = cand[keep & (cand >= 2) & (cand != 0xFFFFFFFF)]
+        p = np.searchsorted(keys, cand)
+        present = (p < n) & (keys[np.minimum(p, n - 1)] == cand)
+        if inserted.size:
+            q = np.searchsorted(inserted, cand)
+            present |= (q < inserted.size) & (inserted[np.minimum(q, inserted.size - 1)] == cand)
+        ins = cand[~present]
+        rng.shuffle(ins)
+        ins = ins[:n_ins]
+        inserted = np.sort(np.concatenate([inserted, ins]))
+        ins_vals = rng.integers(0, 1 << 32, ins.size, dtype=np.uint64).astype(np.uint32)
+        pick = rng.integers(0, n, 2 * n_del)
+        pick.sort()
+        first = np.empty(pick.size, bool)
+        first[0] = True
+        np.not_equal(pick[1:], pick[:-1], out=first[1:])
+        pick = pick[first & ~deleted[pick]]
+        pick = pick[rng.permutation(pick.size)[:n_del]]
+        deleted[pick] = True
+        dels = keys[pick]
+        probes = rng.integers(lo_span, hi_span + 2, n_succ, dtype=np.uint64)
+        w.rounds.append((ins, ins_vals, dels, probes))
+    return w

@@ -48,6 +48,7 @@ typedef enum gpulsm_status {
 /* Search structure used inside each sorted level. */
 #define GPULSM_SEARCH_DIRECTORY 0u /* radix directory over the level's key range */
 #define GPULSM_SEARCH_LEARNED 1u   /* piecewise-linear position model + checked window */
+#define GPULSM_SEARCH_BINARY 2u    /* plain binary search over each level (no auxiliary structure) */
 
 /* Message of the last failed call on this thread. */
 const char *gpulsm_last_error(void);
@@ -190,6 +191,66 @@ int gpulsm_tenants_lookup(gpulsm_tenants *pool, const uint32_t *tenant_ids, cons
 int gpulsm_tenants_sizes(gpulsm_tenants *pool, uint64_t *out_rows);
 int gpulsm_tenants_status(gpulsm_tenants *pool, uint32_t *out_status);
 int gpulsm_tenants_resident_bytes(gpulsm_tenants *pool, uint64_t *out_bytes);
+
+/* ===================== serving loop ======================================== */
+/* No reference counterpart: GPULSMOpt serialises every call behind a mutex and
+ * an operation event (GPULSMOpt.cuh:6852-6858) and leaves batching to the
+ * caller.  A server owns one LSM dictionary and serves lookup / insert / erase
+ * / range-sum requests submitted from any host thread with HOST buffers
+ * (unlike the dict calls): a worker thread coalesces the queue, in arrival
+ * order, into rounds (each run of same-kind requests becomes one dictionary
+ * call), admits updates while the dictionary's resident bytes plus the
+ * rounds in flight fit the device budget (an update that cannot fit fails
+ * with GPULSM_ERR_CAPACITY), and pipelines rounds through `depth` staging
+ * slots.  Results equal applying the requests one at a time in submission
+ * order.  Request buffers stay owned by the caller until the request is done. */
+typedef struct gpulsm_server gpulsm_server;
+
+#define GPULSM_SERVE_LOOKUP 0u    /* keys -> out values (miss 0xffffffff), found flags optional */
+#define GPULSM_SERVE_INSERT 1u    /* keys, aux = values */
+#define GPULSM_SERVE_ERASE 2u     /* keys */
+#define GPULSM_SERVE_RANGE_SUM 3u /* keys = lower bounds, aux = upper bounds -> out u32 sums */
+
+typedef struct gpulsm_serve_stats {
+  uint64_t completed, rejected, rounds, keys;
+  double p50_us, p99_us, max_us, mean_us; /* submit -> results in the caller's buffers */
+  double mean_round_keys, wall_s;
+} gpulsm_serve_stats;
+
+/* Open-loop load: Poisson arrivals at rate_per_s (0 = closed loop with
+ * max_outstanding requests in flight) for `seconds`; kind mix (lookup, insert,
+ * erase, range-sum); sizes log-uniform in [min_keys, max_keys]; keys drawn by
+ * Zipf(zipf_s) rank over `universe` (host array); range widths log-uniform in
+ * [1, range_width_max]. */
+typedef struct gpulsm_load_spec {
+  double rate_per_s, seconds;
+  double mix[4];
+  double zipf_s;
+  uint32_t max_outstanding, min_keys, max_keys, range_width_max;
+  uint64_t seed;
+  const uint32_t *universe;
+  uint64_t universe_n;
+} gpulsm_load_spec;
+
+/* budget_bytes: device bytes the dictionary and in-flight rounds may hold;
+ * max_round_keys: keys per round (also the largest request), 0 -> 2^20;
+ * depth: pipeline slots, 0 -> 3. */
+int gpulsm_server_create(const gpulsm_dict_config *config, uint64_t budget_bytes, uint32_t max_round_keys,
+                         uint32_t depth, gpulsm_server **out);
+int gpulsm_server_destroy(gpulsm_server *server);
+/* Preload (device buffers, as gpulsm_dict_bulk_build). */
+int gpulsm_server_bulk_build(gpulsm_server *server, const uint32_t *keys, const uint32_t *values, uint64_t count,
+                             void *stream);
+int gpulsm_server_submit(gpulsm_server *server, uint32_t kind, const uint32_t *keys, const uint32_t *aux,
+                         uint64_t count, uint32_t *out, uint8_t *out_found, uint64_t *out_ticket);
+/* *out_state: 0 pending, 1 done, -status failed; a finished ticket is collected by this call. */
+int gpulsm_server_poll(gpulsm_server *server, uint64_t ticket, int32_t *out_state);
+int gpulsm_server_wait(gpulsm_server *server, uint64_t ticket, int32_t *out_state);
+int gpulsm_server_drain(gpulsm_server *server);
+int gpulsm_server_stats(gpulsm_server *server, gpulsm_serve_stats *out);
+int gpulsm_server_reset_stats(gpulsm_server *server);
+int gpulsm_server_run_load(gpulsm_server *server, const gpulsm_load_spec *spec, gpulsm_serve_stats *out);
+int gpulsm_server_resident_bytes(gpulsm_server *server, uint64_t *out_bytes);
 
 /* ===================== learned position model ============================ */
 /* A piecewise-linear CDF over one sorted key array (no reference counterpart:

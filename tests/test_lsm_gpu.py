@@ -346,3 +346,32 @@ def test_lsm_scale_full_size_properties(gl, cuda, workloads):
     o_off, o_k, o_v = t.o.range_pairs(lo[sample], hi[sample])
     got_k = np.concatenate([to_host(k[int(off[i]):int(off[i + 1])]) for i in sample])
     assert np.array_equal(got_k, o_k)
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+def test_search_modes_match_oracle(gl, cuda, mode):
+    """Radix directory (0), learned position model per level (1) and plain
+    binary search (2) must give identical, exact answers; the levels here are
+    large enough (>= 2^16 rows) for the learned mode to fit its models."""
+    rng = np.random.default_rng(40 + mode)
+    t = Twin(gl, max_elements=1 << 21, batch_capacity=1 << 16, search_mode=mode)
+    base = rng.integers(0, 1 << 32, 1 << 19, dtype=np.uint64).astype(np.uint32)
+    base[:3] = [0, 1, 0xFFFFFFFF]
+    t.d.bulk_build(to_dev(base), to_dev(np.arange(base.size, dtype=np.uint32)))
+    t.o.bulk_build(base, np.arange(base.size, dtype=np.uint32))
+    for i in range(12):
+        k = np.concatenate([base[rng.integers(0, base.size, 1 << 14)],
+                            rng.integers(0, 1 << 32, 1 << 15, dtype=np.uint64).astype(np.uint32)])
+        if i % 4 == 3:
+            t.apply(("erase", k))
+        else:
+            t.apply(("insert", k, rng.integers(0, 1 << 32, k.size, dtype=np.uint64).astype(np.uint32)))
+    q = np.concatenate([base[rng.integers(0, base.size, 50_000)],
+                        rng.integers(0, 1 << 32, 50_000, dtype=np.uint64).astype(np.uint32),
+                        np.array([0, 1, 2, 0xFFFFFFFE, 0xFFFFFFFF], np.uint32)])
+    t.lookup(q, with_found=True)
+    t.successor(q[:20_000])
+    lo = q[:3000]
+    hi = (lo.astype(np.uint64) + rng.integers(0, 1 << 24, lo.size, dtype=np.uint64)).clip(0, 0xFFFFFFFF)
+    t.ranges(lo, hi.astype(np.uint32))
+    assert t.d.canonical_carry_status() == 0

@@ -1,0 +1,148 @@
+"""GPU tests of the serving loop (gpulsm_server_*): continuous batching must
+give every request the result it gets alone, equal to the oracle applied in
+submission order; the device-memory budget must refuse updates it cannot
+hold; the native load generator must report consistent statistics."""
+import threading
+
+import numpy as np
+import pytest
+
+from conftest import to_dev
+from oracle import OracleLSM
+
+pytestmark = pytest.mark.gpu
+
+KINDS = ("lookup", "insert", "erase", "range")
+
+
+def make_requests(rng, universe, count, max_keys=4096):
+    reqs = []
+    for _ in range(count):
+        kind = KINDS[rng.choice(4, p=[0.5, 0.2, 0.15, 0.15])]
+        n = int(np.exp(rng.uniform(0, np.log(max_keys + 1))))
+        n = max(1, min(max_keys, n))
+        # skewed choice of keys: half from a hot prefix of the universe
+        hot = rng.integers(0, 64, n)
+        cold = rng.integers(0, universe.size, n)
+        keys = universe[np.where(rng.random(n) < 0.5, hot, cold)]
+        if kind == "insert":
+            reqs.append((kind, keys, rng.integers(0, 1 << 32, n, dtype=np.uint64).astype(np.uint32)))
+        elif kind == "range":
+            width = np.exp(rng.uniform(0, np.log(1 << 20), n)).astype(np.uint64)
+            hi = np.minimum(keys.astype(np.uint64) + width, 0xFFFFFFFF).astype(np.uint32)
+            reqs.append((kind, keys, hi))
+        else:
+            reqs.append((kind, keys, None))
+    return reqs
+
+
+def submit(srv, req):
+    kind, keys, aux = req
+    if kind == "lookup":
+        return srv.submit_lookup(keys, with_found=True)
+    if kind == "insert":
+        return srv.submit_insert(keys, aux)
+    if kind == "erase":
+        return srv.submit_erase(keys)
+    return srv.submit_range_sum(keys, aux)
+
+
+def fresh_server(gl, base_k, base_v):
+    srv = gl.Server(gl.DictionaryConfig(max_elements=1 << 20, batch_capacity=1 << 16), budget_bytes=4 << 30,
+                    max_round_keys=1 << 16, depth=3)
+    srv.bulk_build(to_dev(base_k), to_dev(base_v))
+    return srv
+
+
+def oracle_answers(base_k, base_v, ordered):
+    o = OracleLSM()
+    o.bulk_build(base_k, base_v)
+    out = []
+    for kind, keys, aux in ordered:
+        if kind == "lookup":
+            out.append(o.lookup(keys, with_found=True))
+        elif kind == "insert":
+            o.insert(keys, aux)
+            out.append(None)
+        elif kind == "erase":
+            o.erase(keys)
+            out.append(None)
+        else:
+            out.append(o.range_sum(keys, aux))
+    return out
+
+
+def same(a, b):
+    if a is None or b is None:
+        return a is None and b is None
+    if isinstance(a, tuple):
+        return all(np.array_equal(x, y) for x, y in zip(a, b))
+    return np.array_equal(a, b)
+
+
+def test_results_same_alone_and_in_mix(gl, cuda):
+    rng = np.random.default_rng(11)
+    base_k = rng.integers(0, 1 << 32, 1 << 16, dtype=np.uint64).astype(np.uint32)
+    base_v = np.arange(base_k.size, dtype=np.uint32)
+    universe = np.concatenate([base_k, rng.integers(0, 1 << 32, 1 << 14, dtype=np.uint64).astype(np.uint32)])
+    per_thread = [make_requests(np.random.default_rng(100 + t), universe, 60) for t in range(4)]
+
+    # in the mix: four threads submit at once, nothing waits until all are in
+    srv = fresh_server(gl, base_k, base_v)
+    submitted = [[] for _ in range(4)]
+
+    def client(t):
+        for req in per_thread[t]:
+            submitted[t].append((submit(srv, req), req))
+
+    threads = [threading.Thread(target=client, args=(t,)) for t in range(4)]
+    for th in threads:
+        th.start()
+    for th in threads:
+        th.join()
+    flat = sorted((tk.id, tk, req) for lst in submitted for tk, req in lst)
+    mix = [srv.wait(tk) for _, tk, _ in flat]
+    st = srv.stats()
+    assert st["completed"] == len(flat) and st["rejected"] == 0
+    assert st["rounds"] < len(flat), "requests that arrived together were not coalesced"
+    srv.close()
+
+    # alone: one request at a time, in the order the server assigned
+    ordered = [req for _, _, req in flat]
+    srv = fresh_server(gl, base_k, base_v)
+    alone = [srv.wait(submit(srv, req)) for req in ordered]
+    srv.close()
+
+    want = oracle_answers(base_k, base_v, ordered)
+    for i, (m, a, w) in enumerate(zip(mix, alone, want)):
+        assert same(m, a), f"request {i} ({ordered[i][0]}): result differs between the mix and alone"
+        assert same(a, w), f"request {i} ({ordered[i][0]}): result differs from the oracle"
+
+
+def test_budget_refuses_updates_it_cannot_hold(gl, cuda):
+    rng = np.random.default_rng(5)
+    base_k = rng.integers(0, 1 << 32, 1 << 14, dtype=np.uint64).astype(np.uint32)
+    base_v = np.arange(base_k.size, dtype=np.uint32)
+    srv = gl.Server(gl.DictionaryConfig(max_elements=1 << 20), budget_bytes=1, max_round_keys=1 << 16, depth=2)
+    srv.bulk_build(to_dev(base_k), to_dev(base_v))
+    t_ins = srv.submit_insert(base_k[:100], base_v[:100])
+    t_look = srv.submit_lookup(base_k[:1000])
+    with pytest.raises(gl.CapacityError):
+        srv.wait(t_ins)
+    assert np.array_equal(srv.wait(t_look), base_v[:1000])  # reads are still served
+    assert srv.stats()["rejected"] == 1
+    srv.close()
+
+
+def test_load_generator_reports_consistent_stats(gl, cuda):
+    rng = np.random.default_rng(7)
+    base_k = rng.integers(0, 1 << 32, 1 << 18, dtype=np.uint64).astype(np.uint32)
+    srv = gl.Server(gl.DictionaryConfig(max_elements=1 << 21), budget_bytes=8 << 30, max_round_keys=1 << 18)
+    srv.bulk_build(to_dev(base_k), to_dev(np.arange(base_k.size, dtype=np.uint32)))
+    closed = srv.run_load(base_k, rate_per_s=0, seconds=0.3, max_keys=1 << 12, max_outstanding=32)
+    assert closed["completed"] > 10 and closed["rejected"] == 0
+    assert 0 < closed["p50_us"] <= closed["p99_us"] <= closed["max_us"]
+    rate = 0.3 * closed["completed"] / max(closed["wall_s"], 1e-6)
+    opened = srv.run_load(base_k, rate_per_s=rate, seconds=0.3, max_keys=1 << 12, seed=2)
+    assert opened["completed"] > 5 and opened["p50_us"] <= opened["p99_us"]
+    srv.close()
