@@ -54,6 +54,8 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-serving", action="store_true")
     p.add_argument("--no-tenants", action="store_true")
+    p.add_argument("--no-flix", action="store_true")
+    p.add_argument("--flix-rounds", type=int, default=3)
     p.add_argument("--tenant-rounds", type=int, default=4)
     p.add_argument("--serving-seconds", type=float, default=2.0)
     return p.parse_args()
@@ -292,6 +294,8 @@ def run_ours(args):
         result["e2e"] = e2e_ours(args, gl, w, dev, total_pairs, max_el)
     if not args.no_tenants:
         result["tenants"] = tenants_leg(args, gl, dev)
+    if not args.no_flix:
+        result["flix"] = flix_leg(args, gl, W, dev)
     if not args.no_serving:
         del d, ops_dev, q, lo, hi, out_v, out_f, offsets, pairs
         torch.cuda.empty_cache()
@@ -305,6 +309,82 @@ def run_ours(args):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(result), flush=True)
+
+
+def flix_leg(args, gl, W, dev):
+    """FliX-style updatable sorted index: bulk build of 2^28 sorted u64 keys
+    (geometric gaps, mean 16), then rounds of 2^22 inserts (half uniform, half
+    in 1024 hot ranges), 2^21 deletes and 2^24 uniform successor probes; bucket
+    routing by binary search over the bucket maxima (plain) against the learned
+    piecewise-linear model with 4096 segments (learned).  The first round of
+    each run warms up; the others are timed with CUDA events."""
+    import torch
+
+    w = W.flix_fast(0, rounds=args.flix_rounds + 1)
+    u64 = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.int64)).to(dev)  # noqa: E731
+    u32 = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.int32)).to(dev)  # noqa: E731
+    keys = u64(w.build_keys)
+    # the reference's interface takes sorted batches (its driver sorts before
+    # the timed calls); probes are timed both pre-sorted (ordered lookups, as
+    # the published numbers) and unsorted (sort inside the call)
+    rounds = []
+    for i, v, d, p in w.rounds:
+        o = np.argsort(i, kind="stable")
+        rounds.append((u64(i[o]), u32(v[o]), u64(np.sort(d)), u64(np.sort(p)), u64(p)))
+    n_build = w.build_keys.size
+    cap = n_build + len(w.rounds) * rounds[0][0].numel()
+    out = torch.empty(rounds[0][3].numel(), dtype=torch.int64, device=dev)
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    res = {}
+    warm = gl.FlixIndex(key_bits=64, max_elements=1 << 20)
+    warm.build(keys[: 1 << 20])
+    torch.cuda.synchronize()
+    warm.close()
+    for name, mode in (("plain", 0), ("learned", 1)):
+        idx = gl.FlixIndex(key_bits=64, search_mode=mode, max_elements=cap)
+        idx.build(keys, max_size=cap)  # first build maps the index's device memory; time a rebuild from keys
+        torch.cuda.synchronize()
+        e0, e1 = ev(), ev()
+        e0.record()
+        idx.build(keys, max_size=cap)
+        e1.record()
+        torch.cuda.synchronize()
+        build_ms = e0.elapsed_time(e1)
+        t_ins = t_del = t_ord = t_suc = 0.0
+        n_ins = n_del = n_suc = 0
+        for r, (ins, vals, dels, sprobes, probes) in enumerate(rounds):
+            a, b, c, d, e = ev(), ev(), ev(), ev(), ev()
+            a.record()
+            idx.insert(ins, vals)
+            b.record()
+            idx.remove(dels)
+            c.record()
+            idx.lookups_successor(sprobes, out)
+            d.record()
+            idx.successor(probes, out)
+            e.record()
+            torch.cuda.synchronize()
+            if r == 0:
+                continue
+            t_ins += a.elapsed_time(b)
+            t_del += b.elapsed_time(c)
+            t_ord += c.elapsed_time(d)
+            t_suc += d.elapsed_time(e)
+            n_ins += ins.numel()
+            n_del += dels.numel()
+            n_suc += probes.numel()
+        res[name] = {"build_ms": round(build_ms, 2), "build_mkeys_s": round(n_build / build_ms / 1e3, 1),
+                     "insert_mkeys_s": round(n_ins / t_ins / 1e3, 1), "delete_mkeys_s": round(n_del / t_del / 1e3, 1),
+                     "ordered_successor_mops_s": round(n_suc / t_ord / 1e3, 1),
+                     "unsorted_successor_mops_s": round(n_suc / t_suc / 1e3, 1), "status": idx.status(),
+                     "resident_gb": round(idx.gpu_resident_bytes() / 1e9, 2)}
+        idx.close()
+        torch.cuda.synchronize()
+    res["rounds_timed"] = args.flix_rounds
+    res["learned_successor_speedup"] = round(res["learned"]["ordered_successor_mops_s"] /
+                                             res["plain"]["ordered_successor_mops_s"], 3)
+    res["learned_insert_speedup"] = round(res["learned"]["insert_mkeys_s"] / res["plain"]["insert_mkeys_s"], 3)
+    return res
 
 
 def tenant_round(rng, sizes, lo=6, hi=16):
@@ -422,34 +502,43 @@ def serving_leg(args, gl, w, dev):
     (60% lookup, 20% insert, 10% erase, 10% range sum; Zipf s=1.1 keys).
     Peak = closed loop with 64 requests in flight; latency = open-loop Poisson
     arrivals at half the peak request rate (host submit to results in host
-    buffers)."""
+    buffers).  Run once with each level search: the radix directory (plain)
+    and the learned position model (learned)."""
     import torch
 
     keys = np.concatenate([o[1] for o in w.ops if o[0] == "insert"])
-    srv = gl.Server(gl.DictionaryConfig(max_elements=keys.size + w.erased_keys + (1 << 24)),
-                    budget_bytes=16 << 30, max_round_keys=1 << 20, depth=3)
-    kd = torch.from_numpy(keys.view(np.int32)).to(dev)
-    vd = torch.arange(keys.size, dtype=torch.int32, device=dev)
-    srv.bulk_build(kd, vd)
-    del kd, vd
     secs = args.serving_seconds
-    srv.run_load(keys, rate_per_s=0, seconds=0.3, max_outstanding=64, seed=3)  # warm-up
-    peak = srv.run_load(keys, rate_per_s=0, seconds=secs, max_outstanding=64, seed=4)
-    peak_rate = peak["completed"] / max(peak["wall_s"], 1e-9)
-    half = srv.run_load(keys, rate_per_s=0.5 * peak_rate, seconds=secs, seed=5)
-    srv.close()
-    return {
-        "dictionary_keys": int(keys.size), "budget_gb": 16,
-        "peak_mkeys_s": round(peak["keys"] / max(peak["wall_s"], 1e-9) / 1e6, 1),
-        "peak_requests_s": round(peak_rate, 1),
-        "load_requests_s": round(0.5 * peak_rate, 1),
-        "mkeys_s": round(half["keys"] / max(half["wall_s"], 1e-9) / 1e6, 1),
-        "p50_ms": round(half["p50_us"] / 1e3, 4), "p99_ms": round(half["p99_us"] / 1e3, 4),
-        "max_ms": round(half["max_us"] / 1e3, 4),
-        "peak_p50_ms": round(peak["p50_us"] / 1e3, 4), "peak_p99_ms": round(peak["p99_us"] / 1e3, 4),
-        "mean_round_keys": round(half["mean_round_keys"], 1), "requests": int(half["completed"]),
-        "rejected": int(half["rejected"] + peak["rejected"]),
-    }
+    out = {"dictionary_keys": int(keys.size), "budget_gb": 16}
+    for name, mode in (("plain", 0), ("learned", 1)):
+        # serving requests are small: a small level 0 (2^17 rows, fan-in 4) keeps
+        # a run's merge proportional to the run instead of to a 4M-row level
+        srv = gl.Server(gl.DictionaryConfig(max_elements=keys.size + w.erased_keys + (1 << 24), search_mode=mode,
+                                            level_zero_capacity=1 << 17),
+                        budget_bytes=16 << 30, max_round_keys=1 << 20, depth=3)
+        kd = torch.from_numpy(keys.view(np.int32)).to(dev)
+        vd = torch.arange(keys.size, dtype=torch.int32, device=dev)
+        srv.bulk_build(kd, vd)
+        del kd, vd
+        srv.run_load(keys, rate_per_s=0, seconds=0.3, max_outstanding=64, seed=3)  # warm-up
+        peak = srv.run_load(keys, rate_per_s=0, seconds=secs, max_outstanding=64, seed=4)
+        peak_rate = peak["completed"] / max(peak["wall_s"], 1e-9)
+        half = srv.run_load(keys, rate_per_s=0.5 * peak_rate, seconds=secs, seed=5)
+        srv.close()
+        out[name] = {
+            "peak_mkeys_s": round(peak["keys"] / max(peak["wall_s"], 1e-9) / 1e6, 1),
+            "peak_requests_s": round(peak_rate, 1),
+            "load_requests_s": round(0.5 * peak_rate, 1),
+            "mkeys_s": round(half["keys"] / max(half["wall_s"], 1e-9) / 1e6, 1),
+            "p50_ms": round(half["p50_us"] / 1e3, 4), "p99_ms": round(half["p99_us"] / 1e3, 4),
+            "max_ms": round(half["max_us"] / 1e3, 4),
+            "peak_p50_ms": round(peak["p50_us"] / 1e3, 4), "peak_p99_ms": round(peak["p99_us"] / 1e3, 4),
+            "mean_round_keys": round(half["mean_round_keys"], 1),
+            "peak_mean_round_keys": round(peak["mean_round_keys"], 1),
+            "peak_gpu_busy_frac": round(peak["gpu_busy_s"] / max(peak["wall_s"], 1e-9), 3),
+            "peak_host_launch_frac": round(peak["host_launch_s"] / max(peak["wall_s"], 1e-9), 3),
+            "requests": int(half["completed"]), "rejected": int(half["rejected"] + peak["rejected"]),
+        }
+    return out
 
 
 def e2e_ours(args, gl, w, dev, total_pairs, max_el):

@@ -114,6 +114,8 @@ class ServeStats(C.Structure):
         ("mean_us", C.c_double),
         ("mean_round_keys", C.c_double),
         ("wall_s", C.c_double),
+        ("gpu_busy_s", C.c_double),
+        ("host_launch_s", C.c_double),
     ]
 
 

@@ -121,6 +121,8 @@ void copy_stats(const gpulsm::ServeStats &s, gpulsm_serve_stats *o) {
   o->mean_us = s.mean_us;
   o->mean_round_keys = s.mean_round_keys;
   o->wall_s = s.wall_s;
+  o->gpu_busy_s = s.gpu_busy_s;
+  o->host_launch_s = s.host_launch_s;
 }
 }  // namespace
 

@@ -57,9 +57,12 @@ inline unsigned grid_for(uint64_t n, unsigned threads) {
 }
 
 __host__ __device__ inline uint32_t ceil_log2_u64(uint64_t x) {
-  uint32_t b = 0;
-  while ((uint64_t{1} << b) < x) ++b;
-  return b;
+  if (x <= 1) return 0;
+#ifdef __CUDA_ARCH__
+  return 64u - uint32_t(__clzll((long long)(x - 1)));
+#else
+  return 64u - uint32_t(__builtin_clzll(x - 1));
+#endif
 }
 
 #ifdef __CUDACC__
@@ -104,6 +107,20 @@ __device__ __forceinline__ bool gpulsm_check(bool ok, uint32_t site, unsigned lo
 #else
 #define GPULSM_OK(cond, site, v) true
 #endif
+
+// Lanes of the warp holding the same BITS-bit value as this lane (all 32
+// lanes take part).  BITS ballots replace match.any, which issues on a slow
+// pipe and limited the ranking loops of the sorts.
+template <int BITS>
+__device__ __forceinline__ uint32_t match_any_bits(uint32_t v) {
+  uint32_t peers = 0xffffffffu;
+#pragma unroll
+  for (int b = 0; b < BITS; ++b) {
+    const uint32_t m = __ballot_sync(0xffffffffu, (v >> b) & 1u);
+    peers &= ((v >> b) & 1u) ? m : ~m;
+  }
+  return peers;
+}
 
 // Exclusive scan across a block of BLOCK threads (one value per thread).
 // `warp_sums` must hold BLOCK/32 entries.  Returns the exclusive prefix and

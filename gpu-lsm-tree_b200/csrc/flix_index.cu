@@ -340,7 +340,7 @@ class FlixImpl final : public FlixIndex::Impl {
 
   // copy, sort (with values or a permutation), optional first-wins dedup, route to runs
   Sorted prepare(const K *keys, const uint32_t *vals, uint64_t n, bool with_vals, bool perm, bool dedup,
-                 cudaStream_t s) {
+                 cudaStream_t s, bool route = true) {
     if (n > radix::kMaxKeys) throw std::length_error("FliX batch limited to 2^30-1 keys per call");
     const uint32_t nn = uint32_t(n);
     const bool carry = with_vals || perm;
@@ -369,17 +369,27 @@ class FlixImpl final : public FlixIndex::Impl {
     unsigned long long *dlb = b.take<unsigned long long>(dtiles + 1);
     unsigned long long *rlb = b.take<unsigned long long>(rtiles + 1);
     GPULSM_CUDA(cudaMemsetAsync(zero_from, 0, (b.p + b.off) - zero_from, s));
-    GPULSM_CUDA(cudaMemcpyAsync(k0, keys, n * sizeof(K), cudaMemcpyDeviceToDevice, s));
-    if (with_vals) GPULSM_CUDA(cudaMemcpyAsync(v0, vals, n * 4, cudaMemcpyDeviceToDevice, s));
-    if (perm) {
-      flix::iota_kernel<K><<<grid_for(n, 256), 256, 0, s>>>(v0, nn); note_launch();
-    }
+    // a batch that is already sorted (the reference's interface requires it)
+    // is used in place: no copy, no sort, identity permutation
+    const bool sorted_in = (ctr_host_->flags & 1u) == 0;
+    const bool unique_in = (ctr_host_->flags & 2u) == 0;
     K *kk[2] = {k0, k1};
     uint32_t *vv[2] = {v0, v1};
-    const int cur = carry ? radix::sort<K, true>(kk, vv, nn, 0, bits, w, &ctr_->status, num_sms_, s)
-                          : radix::sort<K, false>(kk, vv, nn, 0, bits, w, &ctr_->status, num_sms_, s);
-    Sorted out{kk[cur], carry ? vv[cur] : nullptr, n_dev, runs, run_count};
-    if (dedup) {
+    int cur = 0;
+    if (sorted_in) {
+      kk[0] = const_cast<K *>(keys);  // read only below
+      vv[0] = with_vals ? const_cast<uint32_t *>(vals) : nullptr;
+    } else {
+      GPULSM_CUDA(cudaMemcpyAsync(k0, keys, n * sizeof(K), cudaMemcpyDeviceToDevice, s));
+      if (with_vals) GPULSM_CUDA(cudaMemcpyAsync(v0, vals, n * 4, cudaMemcpyDeviceToDevice, s));
+      if (perm) {
+        flix::iota_kernel<K><<<grid_for(n, 256), 256, 0, s>>>(v0, nn); note_launch();
+      }
+      cur = carry ? radix::sort<K, true>(kk, vv, nn, 0, bits, w, &ctr_->status, num_sms_, s)
+                  : radix::sort<K, false>(kk, vv, nn, 0, bits, w, &ctr_->status, num_sms_, s);
+    }
+    Sorted out{kk[cur], (sorted_in && !with_vals) ? nullptr : (carry ? vv[cur] : nullptr), n_dev, runs, run_count};
+    if (dedup && !unique_in) {
       flix::dedup_first_kernel<K><<<unsigned(std::max<uint64_t>(dtiles, 1)), flix::kDedupThreads, 0, s>>>(
           kk[cur], carry ? vv[cur] : nullptr, nn, ko, carry ? vo : nullptr, n_dev, dlb, dctr,
           &ctr_->status); note_launch();
@@ -388,9 +398,11 @@ class FlixImpl final : public FlixIndex::Impl {
     } else {
       flix::set_u32_kernel<K><<<1, 1, 0, s>>>(n_dev, nn); note_launch();
     }
-    flix::route_runs_kernel<K><<<unsigned(std::max<uint64_t>(rtiles, 1)), flix::kRouteThreads, 0, s>>>(
-        out.keys, n_dev, bmax_, buckets_, runs, run_count, rlb, rctr, &ctr_->status, model_header(),
-        model_segments()); note_launch();
+    if (route) {
+      flix::route_runs_kernel<K><<<unsigned(std::max<uint64_t>(rtiles, 1)), flix::kRouteThreads, 0, s>>>(
+          out.keys, n_dev, bmax_, buckets_, runs, run_count, rlb, rctr, &ctr_->status, model_header(),
+          model_segments()); note_launch();
+    }
     return out;
   }
 
@@ -453,22 +465,10 @@ class FlixImpl final : public FlixIndex::Impl {
     require_built();
     if (n > radix::kMaxKeys) throw std::length_error("FliX query limited to 2^30-1 probes per call");
     begin(s);
-    const uint64_t rtiles = (n + flix::kRouteTile - 1) / flix::kRouteTile;
-    const size_t total = align_up((n + 1) * sizeof(flix::Run)) + 3 * align_up(8) + align_up((rtiles + 1) * 8);
-    Bump b{static_cast<char *>(scratch(total, s))};
-    flix::Run *runs = b.take<flix::Run>(n + 1);
-    char *zero_from = b.p + b.off;
+    Bump b{static_cast<char *>(scratch(align_up(8), s))};
     uint32_t *n_dev = b.take<uint32_t>(2);
-    uint32_t *run_count = b.take<uint32_t>(2);
-    uint32_t *rctr = b.take<uint32_t>(2);
-    unsigned long long *rlb = b.take<unsigned long long>(rtiles + 1);
-    GPULSM_CUDA(cudaMemsetAsync(zero_from, 0, (b.p + b.off) - zero_from, s));
-    const uint32_t nn = uint32_t(n);
-    flix::set_u32_kernel<K><<<1, 1, 0, s>>>(n_dev, nn); note_launch();
-    flix::route_runs_kernel<K><<<unsigned(std::max<uint64_t>(rtiles, 1)), flix::kRouteThreads, 0, s>>>(
-        probes, n_dev, bmax_, buckets_, runs, run_count, rlb, rctr, &ctr_->status, model_header(),
-        model_segments()); note_launch();
-    run_queries(probes, n_dev, runs, run_count, n, perm, out_v, out_k, s);
+    flix::set_u32_kernel<K><<<1, 1, 0, s>>>(n_dev, uint32_t(n)); note_launch();
+    direct_queries(probes, n_dev, n, perm, out_v, out_k, s);
     end(s);
   }
 
@@ -484,12 +484,27 @@ class FlixImpl final : public FlixIndex::Impl {
     GPULSM_CUDA(cudaGetLastError());
   }
 
+  // sorted probes, one thread each (routing by the model in search mode 1)
+  void direct_queries(const K *probes, const uint32_t *n_dev, uint64_t n, const uint32_t *perm, uint32_t *out_v,
+                      K *out_k, cudaStream_t s) {
+    const unsigned grid = grid_for(std::max<uint64_t>(n, 1), 256);
+    if (out_v) {
+      flix::lookup_direct_kernel<K><<<grid, 256, 0, s>>>(probes, n_dev, bmax_, buckets_, model_header(),
+                                                         model_segments(), nodes_, perm, out_v);
+    } else {
+      flix::successor_direct_kernel<K><<<grid, 256, 0, s>>>(probes, n_dev, bmax_, buckets_, model_header(),
+                                                            model_segments(), nodes_, perm, out_k);
+    }
+    note_launch();
+    GPULSM_CUDA(cudaGetLastError());
+  }
+
   // unsorted probes: sort with a permutation, walk, write results in input order
   void sorted_query(const K *probes, uint64_t n, uint32_t *out_v, K *out_k, cudaStream_t s) {
     require_built();
     begin(s);
-    Sorted st = prepare(probes, nullptr, n, false, true, false, s);
-    run_queries(st.keys, st.n_dev, st.runs, st.run_count, n, st.vals, out_v, out_k, s);
+    Sorted st = prepare(probes, nullptr, n, false, true, false, s, false);
+    direct_queries(st.keys, st.n_dev, n, st.vals, out_v, out_k, s);
     end(s);
   }
 

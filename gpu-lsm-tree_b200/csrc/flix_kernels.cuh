@@ -474,6 +474,116 @@ __global__ void __launch_bounds__(256) successor_runs_kernel(
 }
 
 // ---------------------------------------------------------------------------
+// Thread-per-probe queries over SORTED probes (ordered lookup / successor).
+// A warp-per-bucket walk reads a whole node (keys, values, header) for each
+// probe when probes are spread over many buckets; here every thread routes its
+// own probe and reads only the node header and the keys its binary search
+// touches.  Plain routing narrows each lane's binary search over the bucket
+// maxima to the bucket range spanned by its warp's (sorted) probes; learned
+// routing uses the model's error window.
+template <typename K>
+__device__ __forceinline__ uint32_t bucket_in(const K *__restrict__ bmax, uint32_t lo, uint32_t hi, K key) {
+  while (lo < hi) {  // first bucket in [lo, hi] whose maximum is >= key
+    const uint32_t mid = (lo + hi) >> 1;
+    if (bmax[mid] < key) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+template <typename K>
+__device__ __forceinline__ uint32_t route_sorted(const K *__restrict__ bmax, uint32_t buckets,
+                                                 const learned::ModelHeader *model, const learned::Segment *segs,
+                                                 K k, bool valid) {
+  if (model) {
+    const learned::ModelHeader h = *model;
+    return valid ? bucket_of_model<K>(h, segs, bmax, k) : 0u;
+  }
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t vmask = __ballot_sync(0xffffffffu, valid);
+  if (!vmask) return 0u;
+  const uint32_t first = __ffs(vmask) - 1, lastl = 31u - __clz(vmask);
+  const K kf = __shfl_sync(0xffffffffu, k, first), kl = __shfl_sync(0xffffffffu, k, lastl);
+  uint32_t bb = 0;
+  if (lane == first) bb = bucket_in(bmax, 0u, buckets - 1, kf);
+  if (lane == lastl) bb = bucket_in(bmax, 0u, buckets - 1, kl);
+  const uint32_t blo = __shfl_sync(0xffffffffu, bb, first), bhi = __shfl_sync(0xffffffffu, bb, lastl);
+  if (!valid) return 0u;
+  // a key outside the warp's first..last range (unsorted input) searches everything
+  return (kf <= k && k <= kl) ? bucket_in(bmax, blo, bhi, k) : bucket_in(bmax, 0u, buckets - 1, k);
+}
+
+// first position in node p whose key is >= k (count when none)
+template <typename K>
+__device__ __forceinline__ uint32_t node_lower_bound(const Node<K> *p, uint32_t count, K k) {
+  uint32_t lo = 0, hi = count;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (p->keys[mid] < k) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+template <typename K>
+__global__ void __launch_bounds__(256) lookup_direct_kernel(
+    const K *__restrict__ probes, const uint32_t *__restrict__ n_ptr, const K *__restrict__ bmax, uint32_t buckets,
+    const learned::ModelHeader *__restrict__ model, const learned::Segment *__restrict__ segs,
+    const Node<K> *__restrict__ nodes, const uint32_t *__restrict__ perm, uint32_t *__restrict__ out) {
+  const uint32_t n = *n_ptr;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if ((i & ~31u) >= n) return;  // whole warps leave together (routing uses warp votes)
+  const bool valid = i < n;
+  const K k = valid ? probes[i] : K(0);
+  uint32_t id = route_sorted<K>(bmax, buckets, model, segs, k, valid);
+  if (!valid) return;
+  uint32_t result = kNotFound;
+  for (uint32_t hops = 0; id != kNone && hops < (1u << 20); ++hops) {
+    const Node<K> *p = nodes + id;
+    const uint32_t count = p->count;
+    if (count && k <= p->max) {
+      const uint32_t pos = node_lower_bound(p, count, k);
+      if (pos < count && p->keys[pos] == k) result = p->vals[pos];
+      if (pos < count) break;
+    }
+    id = p->next;
+  }
+  out[perm ? perm[i] : i] = result;
+}
+
+template <typename K>
+__global__ void __launch_bounds__(256) successor_direct_kernel(
+    const K *__restrict__ probes, const uint32_t *__restrict__ n_ptr, const K *__restrict__ bmax, uint32_t buckets,
+    const learned::ModelHeader *__restrict__ model, const learned::Segment *__restrict__ segs,
+    const Node<K> *__restrict__ nodes, const uint32_t *__restrict__ perm, K *__restrict__ out) {
+  const uint32_t n = *n_ptr;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if ((i & ~31u) >= n) return;
+  const bool valid = i < n;
+  const K k = valid ? probes[i] : K(0);
+  const uint32_t b = route_sorted<K>(bmax, buckets, model, segs, k, valid);
+  if (!valid) return;
+  uint32_t id = b;
+  bool found = false;
+  K result = successor_miss<K>();
+  for (uint32_t hops = 0; id != kNone && hops < (1u << 20); ++hops) {
+    const Node<K> *p = nodes + id;
+    const uint32_t count = p->count;
+    if (count && k <= p->max) {
+      const uint32_t pos = node_lower_bound(p, count, k);
+      if (pos < count) {
+        result = p->keys[pos];
+        found = true;
+        break;
+      }
+    }
+    id = p->next;
+  }
+  if (!found) result = first_key_from_bucket(nodes, b + 1, buckets);
+  out[perm ? perm[i] : i] = result;
+}
+
+// ---------------------------------------------------------------------------
 // helpers for sorting / dedup of batches
 template <typename K>
 __global__ void set_u32_kernel(uint32_t *__restrict__ p, uint32_t v) {

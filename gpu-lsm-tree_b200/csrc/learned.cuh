@@ -134,6 +134,36 @@ __global__ void model_init_kernel(const K *__restrict__ keys, const ModelHeader 
   seg[s].err = 0;
 }
 
+// step 1 (linear): first index of every segment from one pass over the keys:
+// key i starts the segments (seg(key i-1), seg(key i)]; the last key closes
+// the array (first[nseg] = n).  Same result as a lower_bound per segment.
+template <typename K>
+__global__ void __launch_bounds__(256) model_init_scan_kernel(const K *__restrict__ keys,
+                                                              const ModelHeader *__restrict__ hp,
+                                                              Segment *__restrict__ seg) {
+  const ModelHeader h = *hp;
+  const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (h.n == 0) {
+    if (i <= h.nseg) {
+      seg[i].first = 0;
+      seg[i].err = 0;
+    }
+    return;
+  }
+  if (i >= h.n) return;
+  const int64_t si = seg_of<K>(keys[i], K(h.kmin), h.shift, h.nseg);
+  const int64_t sp = i ? int64_t(seg_of<K>(keys[i - 1], K(h.kmin), h.shift, h.nseg)) : -1;
+  for (int64_t s = sp + 1; s <= si; ++s) {
+    seg[s].first = uint32_t(i);
+    seg[s].err = 0;
+  }
+  if (i + 1 == h.n)
+    for (int64_t s = si + 1; s <= int64_t(h.nseg); ++s) {
+      seg[s].first = uint32_t(h.n);
+      seg[s].err = 0;
+    }
+}
+
 template <typename K>
 __global__ void model_init_params_kernel(const ModelHeader *__restrict__ hp, Segment *__restrict__ seg) {
   const ModelHeader h = *hp;

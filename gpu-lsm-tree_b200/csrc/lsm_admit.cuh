@@ -47,16 +47,9 @@ struct RankSmem {
   uint32_t total;
 };
 
-// Lanes of the warp whose 8-bit digit equals this lane's, among the lanes in
-// `valid` (eight ballots instead of match.any, which issues on a slow pipe).
+// Lanes of the warp whose 8-bit digit equals this lane's, among the lanes in `valid`.
 __device__ __forceinline__ uint32_t digit_peers(uint32_t d, uint32_t valid) {
-  uint32_t peers = valid;
-#pragma unroll
-  for (int b = 0; b < 8; ++b) {
-    const uint32_t m = __ballot_sync(0xffffffffu, (d >> b) & 1u);
-    peers &= ((d >> b) & 1u) ? m : ~m;
-  }
-  return peers;
+  return match_any_bits<8>(d) & valid;
 }
 
 __device__ __forceinline__ uint32_t digit_of(unsigned long long w, uint32_t bit) {
@@ -120,26 +113,30 @@ __device__ __forceinline__ void load_striped(const unsigned long long *src, uint
   }
 }
 
-__device__ __forceinline__ bool run_end(const unsigned long long *src, uint32_t j, uint32_t cnt) {
-  return j + 1 == cnt || word_key(src[j]) != word_key(src[j + 1]);
+// at(j): the j-th word of a sorted sequence (an array, or an index into one)
+template <typename At>
+__device__ __forceinline__ bool run_end(const At &at, uint32_t j, uint32_t cnt) {
+  return j + 1 == cnt || word_key(at(j)) != word_key(at(j + 1));
 }
 
 // Distinct keys of a sorted sequence.
-__device__ __forceinline__ uint32_t count_distinct(const unsigned long long *src, uint32_t cnt, RankSmem &sm) {
+template <typename At>
+__device__ __forceinline__ uint32_t count_distinct(const At &at, uint32_t cnt, RankSmem &sm) {
   uint32_t c = 0;
-  for (uint32_t j = threadIdx.x; j < cnt; j += kThreads) c += run_end(src, j, cnt) ? 1u : 0u;
+  for (uint32_t j = threadIdx.x; j < cnt; j += kThreads) c += run_end(at, j, cnt) ? 1u : 0u;
   (void)block_exclusive_scan<kThreads>(c, sm.scan, &sm.total);
   return sm.total;
 }
 
 // Write the last row of every equal-key run of the sorted sequence
-// src[0, cnt) to out[g0 ...], in chunks of kCap read striped (element
+// at(0 .. cnt) to out[g0 ...], in chunks of kCap read striped (element
 // c0 + i*kThreads + t): per item a warp ballot counts the kept rows, one block
 // scan over the (item, warp) counts gives every warp its output offset, and
 // consecutive lanes store consecutive rows.
-__device__ __forceinline__ void write_rows(const unsigned long long *src, uint32_t cnt, int tombstone,
-                                           uint32_t *out_keys, uint32_t *out_vals, uint8_t *out_flags,
-                                           unsigned long long g0, RankSmem &rs) {
+template <typename At>
+__device__ __forceinline__ void write_rows(const At &at, uint32_t cnt, int tombstone, uint32_t *out_keys,
+                                           uint32_t *out_vals, uint8_t *out_flags, unsigned long long g0,
+                                           RankSmem &rs) {
   static_assert(kItems * kWarps <= 256, "one scan slot per (item, warp)");
   const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
   const uint32_t lt = lanemask_lt();
@@ -151,7 +148,7 @@ __device__ __forceinline__ void write_rows(const unsigned long long *src, uint32
 #pragma unroll
     for (int i = 0; i < kItems; ++i) {
       const uint32_t e = c0 + uint32_t(i) * kThreads + threadIdx.x;
-      ends[i] = __ballot_sync(0xffffffffu, e < c0 + cc && run_end(src, e, cnt));
+      ends[i] = __ballot_sync(0xffffffffu, e < c0 + cc && run_end(at, e, cnt));
       if (lane == 0) slot[i * kWarps + w] = __popc(ends[i]);
     }
     __syncthreads();
@@ -164,7 +161,7 @@ __device__ __forceinline__ void write_rows(const unsigned long long *src, uint32
     for (int i = 0; i < kItems; ++i)
       if ((ends[i] >> lane) & 1u) {
         const uint32_t e = c0 + uint32_t(i) * kThreads + threadIdx.x;
-        const unsigned long long w64 = src[e];
+        const unsigned long long w64 = at(e);
         const unsigned long long r = g0 + written + slot[i * kWarps + w] + __popc(ends[i] & lt);
         out_keys[r] = word_key(w64);
         out_vals[r] = uint32_t(w64);  // the tombstone value was packed for erase batches
@@ -247,14 +244,190 @@ __device__ __noinline__ unsigned long long *sort_global(unsigned long long *a, u
   return src;
 }
 
+// ---------------------------------------------------------------------------
+// Stable partition of a batch by the key's top byte without a look-back chain
+// (reduce, then scan, then scatter), reading keys and values directly:
+//   part_hist_kernel    per tile of kPartTile keys: its 256 top-byte counts,
+//                       stored byte-major (cnt[byte * tiles + tile])
+//   part_scan_kernel    per byte: exclusive scan over the tiles, and the
+//                       byte's total
+//   part_scatter_kernel per tile: byte bases from the totals, a stable rank
+//                       inside the tile (ballot peer groups), then the words
+//                       (key << 32 | value) staged by byte and written in runs
+constexpr int kPartThreads = 256;
+constexpr int kPartItems = 16;
+constexpr uint32_t kPartTile = uint32_t(kPartThreads) * kPartItems;  // 4096 keys
+constexpr int kPartWarps = kPartThreads / 32;
+
+inline uint32_t part_tiles(uint64_t n) { return uint32_t((n + kPartTile - 1) / kPartTile); }
+
+__global__ void __launch_bounds__(kPartThreads) part_hist_kernel(const uint32_t *__restrict__ keys, uint32_t n,
+                                                                 uint32_t tiles, uint32_t *__restrict__ cnt) {
+  __shared__ uint32_t h[256];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  const uint32_t base = blockIdx.x * kPartTile;
+#pragma unroll
+  for (int i = 0; i < kPartItems; ++i) {
+    const uint32_t e = base + uint32_t(i) * kPartThreads + threadIdx.x;
+    if (e < n) atomicAdd(&h[keys[e] >> 24], 1u);
+  }
+  __syncthreads();
+  cnt[threadIdx.x * tiles + blockIdx.x] = h[threadIdx.x];
+}
+
+// one block per top byte; prefix[byte * tiles + tile] = rows of that byte in
+// earlier tiles, total[byte] = the byte's rows
+__global__ void __launch_bounds__(kPartThreads) part_scan_kernel(const uint32_t *__restrict__ cnt, uint32_t tiles,
+                                                                 uint32_t *__restrict__ prefix,
+                                                                 uint32_t *__restrict__ total) {
+  __shared__ uint32_t s_scan[kPartWarps];
+  __shared__ uint32_t s_total;
+  const uint32_t b = blockIdx.x;
+  uint32_t carry = 0;
+  for (uint32_t t0 = 0; t0 < tiles; t0 += kPartThreads) {
+    const uint32_t t = t0 + threadIdx.x;
+    const uint32_t c = t < tiles ? cnt[b * tiles + t] : 0u;
+    const uint32_t ex = block_exclusive_scan<kPartThreads>(c, s_scan, &s_total);
+    if (t < tiles) prefix[b * tiles + t] = carry + ex;
+    carry += s_total;
+  }
+  if (threadIdx.x == 0) total[b] = carry;
+}
+
+__global__ void __launch_bounds__(kPartThreads) part_scatter_kernel(
+    const uint32_t *__restrict__ keys, const uint32_t *__restrict__ vals, uint32_t n, uint32_t tiles,
+    const uint32_t *__restrict__ prefix, const uint32_t *__restrict__ total, unsigned long long *__restrict__ out) {
+  __shared__ unsigned long long s_words[kPartTile];
+  __shared__ uint32_t warp_hist[kPartWarps][256];
+  __shared__ uint32_t s_start[256];   // first staged position of each byte in the tile
+  __shared__ uint32_t s_dst[256];     // global position of the tile's first row of each byte
+  __shared__ uint32_t s_scan[kPartWarps];
+  __shared__ uint32_t s_total;
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, tile = blockIdx.x;
+  for (uint32_t i = lane; i < 256; i += 32) warp_hist[warp][i] = 0;
+  // byte bases: exclusive scan of the totals (every tile repeats this 256-entry scan)
+  const uint32_t tot = total[threadIdx.x];
+  const uint32_t base = block_exclusive_scan<kPartThreads>(tot, s_scan, &s_total);
+  s_dst[threadIdx.x] = base + prefix[threadIdx.x * tiles + tile];
+  const uint32_t wbase = tile * kPartTile + warp * 32u * kPartItems;
+  unsigned long long w[kPartItems];
+  uint32_t d[kPartItems], rank[kPartItems];
+  const uint32_t lt = lanemask_lt();
+#pragma unroll
+  for (int i = 0; i < kPartItems; ++i) {
+    const uint32_t e = wbase + uint32_t(i) * 32u + lane;
+    const bool valid = e < n;
+    const uint32_t k = valid ? keys[e] : 0u;
+    w[i] = (static_cast<unsigned long long>(k) << 32) | (vals ? (valid ? vals[e] : 0u) : kTombValue);
+    d[i] = valid ? (k >> 24) : 256u;
+  }
+  __syncwarp();
+#pragma unroll
+  for (int i = 0; i < kPartItems; ++i) {  // stable rank per warp, items in element order
+    const uint32_t peers = match_any_bits<9>(d[i]);
+    const uint32_t leader = 31u - __clz(peers);
+    uint32_t r = 0;
+    if (lane == leader && d[i] < 256u) {
+      r = warp_hist[warp][d[i]];
+      warp_hist[warp][d[i]] = r + __popc(peers);
+    }
+    rank[i] = __shfl_sync(0xffffffffu, r, leader) + __popc(peers & lt);
+    __syncwarp();
+  }
+  __syncthreads();
+  // thread b: exclusive offsets of each warp for byte b, then byte starts in the tile
+  uint32_t run = 0;
+#pragma unroll
+  for (int ww = 0; ww < kPartWarps; ++ww) {
+    const uint32_t c = warp_hist[ww][threadIdx.x];
+    warp_hist[ww][threadIdx.x] = run;
+    run += c;
+  }
+  const uint32_t st = block_exclusive_scan<kPartThreads>(run, s_scan, &s_total);
+  s_start[threadIdx.x] = st;
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < kPartItems; ++i)
+    if (d[i] < 256u) s_words[s_start[d[i]] + warp_hist[warp][d[i]] + rank[i]] = w[i];
+  __syncthreads();
+  const uint32_t count = min(kPartTile, n - tile * kPartTile);
+  for (uint32_t j = threadIdx.x; j < count; j += kPartThreads) {
+    const unsigned long long x = s_words[j];
+    const uint32_t b = uint32_t(x >> 56);
+    out[s_dst[b] + (j - s_start[b])] = x;
+  }
+}
+
+constexpr uint32_t kBins = 4096;   // counting-sort bins of the fast path (12 key bits)
+constexpr uint32_t kMaxBin = 32;   // larger bins (skew) take the LSD passes instead
+
 struct BucketSmem {
-  unsigned long long words[kCap];
+  unsigned long long words[kCap];  // the bucket's words in input order
+  uint16_t idx[kCap];              // input position of each element, in sorted order
+  uint32_t bins[kBins];            // bin counts, then bin ends
   RankSmem rank;
   uint32_t start[kBuckets + 1];
   uint32_t off[256];
-  uint32_t first, last, tile;
+  uint32_t first, last, tile, maxbin;
   unsigned long long g0;
 };
+
+// Fast in-bucket sort: one counting pass on the 12 highest varying key bits
+// (shared atomics: order inside a bin is arbitrary), then every bin - about
+// one element on uniform keys - is insertion-sorted by (key, input position),
+// which restores input order among equal keys.  Leaves the sorted order in
+// sm.idx; returns false (nothing changed) when a bin exceeds kMaxBin.
+__device__ __forceinline__ bool bin_sort(BucketSmem &sm, uint32_t cnt, uint32_t vary) {
+  const uint32_t hb = 31u - __clz(vary);
+  const uint32_t ds = hb >= 11u ? hb - 11u : 0u;
+  for (uint32_t d = threadIdx.x; d < kBins; d += kThreads) sm.bins[d] = 0;
+  if (threadIdx.x == 0) sm.maxbin = 0;
+  __syncthreads();
+  for (uint32_t e = threadIdx.x; e < cnt; e += kThreads) atomicAdd(&sm.bins[(word_key(sm.words[e]) >> ds) & (kBins - 1)], 1u);
+  __syncthreads();
+  // exclusive scan of the bins: thread t owns kBins / kThreads consecutive bins
+  constexpr uint32_t per = kBins / kThreads;
+  uint32_t c[per], sum = 0, mx = 0;
+#pragma unroll
+  for (uint32_t j = 0; j < per; ++j) {
+    c[j] = sm.bins[threadIdx.x * per + j];
+    sum += c[j];
+    mx = max(mx, c[j]);
+  }
+  uint32_t run = block_exclusive_scan<kThreads>(sum, sm.rank.scan, &sm.rank.total);
+  if (mx) atomicMax(&sm.maxbin, mx);
+#pragma unroll
+  for (uint32_t j = 0; j < per; ++j) {
+    sm.bins[threadIdx.x * per + j] = run;
+    run += c[j];
+  }
+  __syncthreads();
+  if (sm.maxbin > kMaxBin) return false;  // uniform across the block
+  for (uint32_t e = threadIdx.x; e < cnt; e += kThreads) {
+    const uint32_t p = atomicAdd(&sm.bins[(word_key(sm.words[e]) >> ds) & (kBins - 1)], 1u);
+    sm.idx[p] = uint16_t(e);
+  }
+  __syncthreads();  // bins[d] now holds the end of bin d
+  for (uint32_t d = threadIdx.x; d < kBins; d += kThreads) {
+    const uint32_t b = d ? sm.bins[d - 1] : 0u, e = sm.bins[d];
+    for (uint32_t i = b + 1; i < e; ++i) {  // insertion sort by (key, input position)
+      const uint16_t x = sm.idx[i];
+      const uint32_t kx = word_key(sm.words[x]);
+      uint32_t j = i;
+      while (j > b) {
+        const uint16_t y = sm.idx[j - 1];
+        const uint32_t ky = word_key(sm.words[y]);
+        if (ky < kx || (ky == kx && y < x)) break;
+        sm.idx[j] = y;
+        --j;
+      }
+      sm.idx[j] = x;
+    }
+  }
+  __syncthreads();
+  return true;
+}
 constexpr size_t kBucketSmemBytes = sizeof(BucketSmem);
 
 // One CTA per nonempty top-byte bucket (ticket t -> bucket first + t).
@@ -296,31 +469,37 @@ __global__ void __launch_bounds__(kThreads, 2) admit_bucket_kernel(
     atomicOr(status, kDevBadInput);
     return;
   }
-  const unsigned long long *sorted;
+  const unsigned long long *sorted = nullptr;  // sorted words, or null when sm.idx holds the order
   if (cnt <= kCap) {
     for (uint32_t j = threadIdx.x; j < cnt; j += kThreads) sm.words[j] = words0[s0 + j];
     __syncthreads();
-    const uint32_t vary = cnt > 1 ? varying_bits(sm.words, cnt, sm.rank) : 0u;
-    const uint32_t keff = (cnt + kThreads - 1) / kThreads;
-    for (uint32_t bit = 0; bit < 24; bit += 8) {
-      if (((vary >> bit) & 0xffu) == 0u) continue;
-      unsigned long long it[kItems];
-      uint32_t pos[kItems];
-      load_striped(sm.words, keff, cnt, it);
-      rank_chunk(it, keff, cnt, bit, sm.rank, pos);  // its barriers order the loads before the stores
-      const uint32_t wbase = (threadIdx.x >> 5) * 32u * keff;
+    const uint32_t vary = cnt > 1 ? varying_bits(sm.words, cnt, sm.rank) & 0x00ffffffu : 0u;
+    if (!(vary && bin_sort(sm, cnt, vary))) {
+      // no varying bits (one key, input order kept) or a skewed bucket: LSD passes
+      const uint32_t keff = (cnt + kThreads - 1) / kThreads;
+      for (uint32_t bit = 0; bit < 24; bit += 8) {
+        if (((vary >> bit) & 0xffu) == 0u) continue;
+        unsigned long long it[kItems];
+        uint32_t pos[kItems];
+        load_striped(sm.words, keff, cnt, it);
+        rank_chunk(it, keff, cnt, bit, sm.rank, pos);  // its barriers order the loads before the stores
+        const uint32_t wbase = (threadIdx.x >> 5) * 32u * keff;
 #pragma unroll
-      for (int i = 0; i < kItems; ++i)
-        if (uint32_t(i) < keff && wbase + uint32_t(i) * 32u + (threadIdx.x & 31u) < cnt) sm.words[pos[i]] = it[i];
-      __syncthreads();
+        for (int i = 0; i < kItems; ++i)
+          if (uint32_t(i) < keff && wbase + uint32_t(i) * 32u + (threadIdx.x & 31u) < cnt)
+            sm.words[pos[i]] = it[i];
+        __syncthreads();
+      }
+      sorted = sm.words;
     }
-    sorted = sm.words;
   } else {
     const uint32_t vary = varying_bits(words0 + s0, cnt, sm.rank) & 0x00ffffffu;
     sorted = sort_global(words0 + s0, words1 + s0, cnt, vary, sm.rank, sm.off);
     __syncthreads();
   }
-  const uint32_t kept = count_distinct(sorted, cnt, sm.rank);
+  const auto by_array = [sorted](uint32_t j) { return sorted[j]; };
+  const auto by_index = [&sm](uint32_t j) { return sm.words[sm.idx[j]]; };
+  const uint32_t kept = sorted ? count_distinct(by_array, cnt, sm.rank) : count_distinct(by_index, cnt, sm.rank);
   if (threadIdx.x < 32) {
     const unsigned long long e = warp_lookback(lb, tile, kept, status);
     if (threadIdx.x == 0) sm.g0 = e;
@@ -331,7 +510,8 @@ __global__ void __launch_bounds__(kThreads, 2) admit_bucket_kernel(
     atomicOr(status, kDevWaitTimeout);
     return;
   }
-  write_rows(sorted, cnt, tombstone, out_keys, out_vals, out_flags, g0, sm.rank);
+  if (sorted) write_rows(by_array, cnt, tombstone, out_keys, out_vals, out_flags, g0, sm.rank);
+  else write_rows(by_index, cnt, tombstone, out_keys, out_vals, out_flags, g0, sm.rank);
   __syncthreads();
   // directory share: the bucket consumed the keys [b << 24, b << 24 | 0xffffff]
   const uint32_t kmin = first << 24, kmax = (last << 24) | 0x00ffffffu;

@@ -34,9 +34,9 @@ constexpr uint64_t kMaxBatch = uint64_t{1} << 20;  // kMaximumOperationTile, GPU
 constexpr size_t kAlign = 256;
 // learned search: levels of at least this many rows get a model, with about
 // kRowsPerSegment rows per segment and kFitIters gradient steps
-constexpr uint64_t kLearnedMinRows = uint64_t(1) << 16;
+constexpr uint64_t kLearnedMinRows = uint64_t(1) << 22;
 constexpr uint64_t kRowsPerSegment = 64;
-constexpr uint32_t kFitIters = 4;
+constexpr uint32_t kFitIters = 2;
 constexpr uint32_t kMaxSegments = 1u << 22;
 
 size_t align_up(size_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }
@@ -203,6 +203,8 @@ LsmDictionary::~LsmDictionary() {
   if (receipt_dev_) cudaFree(receipt_dev_);
   if (receipt_host_) cudaFreeHost(receipt_host_);
   if (prefix_) cudaFree(prefix_);
+  for (auto &lp : live_)
+    if (lp.p) cudaFree(lp.p);
   if (width_) cudaFree(width_);
   if (width_host_) cudaFreeHost(width_host_);
   if (op_done_) cudaEventDestroy(op_done_);
@@ -325,7 +327,7 @@ RunBuffer *LsmDictionary::sort_dedup(const uint32_t *keys, const uint32_t *value
   uint32_t *counter = bump.take<uint32_t>(2);
   unsigned long long *lb = bump.take<unsigned long long>(dtiles + 1);
   const unsigned hist_blocks = std::min<unsigned>(grid_for(n, 4096), unsigned(num_sms_) * 4u);
-  lsm::pack_histogram_kernel<<<hist_blocks, 256, 0, s>>>(keys, tombstone ? nullptr : values, nn,
+  lsm::pack_histogram_kernel<false><<<hist_blocks, 256, 0, s>>>(keys, tombstone ? nullptr : values, nn,
                                                           words_[0], ws); note_launch();
   unsigned long long *bufs[2] = {words_[0], words_[1]};
   const int cur = radix::run_passes<unsigned long long, false>(bufs, nullptr, nn, 32, 64, ws,
@@ -338,31 +340,32 @@ RunBuffer *LsmDictionary::sort_dedup(const uint32_t *keys, const uint32_t *value
   return carry;
 }
 
-// Batches up to 2^20 rows: pack, one stable pass on the key's top byte, then
-// one CTA per top-byte bucket sorts, deduplicates and writes the level rows
-// (lsm_admit.cuh).
+// Batches up to 2^20 rows: a stable partition by the key's top byte
+// (histogram, scan, scatter - no look-back chain), then one CTA per top-byte
+// bucket sorts, deduplicates and writes the level rows (lsm_admit.cuh).
 RunBuffer *LsmDictionary::bucket_admit(const uint32_t *keys, const uint32_t *values, uint64_t n,
                                        bool tombstone, cudaStream_t s) {
   namespace ad = lsm::admit;
   const uint32_t nn = uint32_t(n);
-  // [key-byte histograms 0..2][top-byte histogram | onesweep counters | onesweep look-back]
-  const size_t hist_words = 3 * 256 + radix::workspace_words(n, 1);
-  const size_t total = align_up(hist_words * 4) + align_up(8) + align_up((ad::kBuckets + 1) * 8);
+  const uint32_t tiles = ad::part_tiles(n);
+  const size_t zero_bytes = align_up(8) + align_up((ad::kBuckets + 1) * 8);
+  const size_t total = zero_bytes + 2 * align_up(size_t(tiles) * 256 * 4) + align_up(256 * 4);
   Bump bump{static_cast<char *>(scratch(total, s))};
-  GPULSM_CUDA(cudaMemsetAsync(bump.p, 0, total, s));
-  uint32_t *hist = bump.take<uint32_t>(hist_words);
+  GPULSM_CUDA(cudaMemsetAsync(bump.p, 0, zero_bytes, s));
   uint32_t *counter = bump.take<uint32_t>(2);
   unsigned long long *lb = bump.take<unsigned long long>(ad::kBuckets + 1);
-  const unsigned hist_blocks = std::min<unsigned>(grid_for(n, 4096), unsigned(num_sms_) * 4u);
-  lsm::pack_histogram_kernel<<<hist_blocks, 256, 0, s>>>(keys, tombstone ? nullptr : values, nn, words_[0], hist);
+  uint32_t *cnt = bump.take<uint32_t>(size_t(tiles) * 256);
+  uint32_t *prefix = bump.take<uint32_t>(size_t(tiles) * 256);
+  uint32_t *top = bump.take<uint32_t>(256);
+  ad::part_hist_kernel<<<tiles, ad::kPartThreads, 0, s>>>(keys, nn, tiles, cnt); note_launch();
+  ad::part_scan_kernel<<<256, ad::kPartThreads, 0, s>>>(cnt, tiles, prefix, top); note_launch();
+  ad::part_scatter_kernel<<<tiles, ad::kPartThreads, 0, s>>>(keys, tombstone ? nullptr : values, nn, tiles, prefix,
+                                                             top, words_[1]);
   note_launch();
-  unsigned long long *bufs[2] = {words_[0], words_[1]};
-  const int cur = radix::run_passes<unsigned long long, false>(bufs, nullptr, nn, 56, 64, hist + 3 * 256,
-                                                               dev_status_, s);
   RunBuffer *carry = pool_.acquire(n, s);
   ad::admit_bucket_kernel<<<ad::kBuckets, ad::kThreads, ad::kBucketSmemBytes, s>>>(
-      bufs[cur], bufs[cur ^ 1], hist + 3 * 256, nn, tombstone ? 1 : 0, carry->keys, carry->vals, carry->flags,
-      carry->desc, carry->dir, carry->dir_bits, rows_log2_, lb, counter, dev_status_);
+      words_[1], words_[0], top, nn, tombstone ? 1 : 0, carry->keys, carry->vals, carry->flags, carry->desc,
+      carry->dir, carry->dir_bits, rows_log2_, lb, counter, dev_status_);
   note_launch();
   GPULSM_CUDA(cudaGetLastError());
   return carry;
@@ -380,7 +383,7 @@ RunBuffer *LsmDictionary::merge(RunBuffer *newer, RunBuffer *older, uint64_t out
   unsigned long long *lb = bump.take<unsigned long long>(tiles + 1);
   bump.off = zero_bytes;
   unsigned long long *parts = bump.take<unsigned long long>(tiles + 2);
-  lsm::merge_partition_kernel<<<grid_for(tiles + 1, 256), 256, 0, s>>>(newer->keys, newer->desc, older->keys,
+  lsm::merge_partition_kernel<<<grid_for((tiles + 1) * 32, 256), 256, 0, s>>>(newer->keys, newer->desc, older->keys,
                                                                          older->desc, parts, uint32_t(tiles + 1));
   note_launch();
   auto kernel = drop_tombstones ? lsm::merge_kernel<true> : lsm::merge_kernel<false>;
@@ -546,10 +549,55 @@ const unsigned long long *LsmDictionary::value_prefix(int level, cudaStream_t s)
   GPULSM_CUDA(cudaMemsetAsync(bump.p, 0, bytes, s));
   uint32_t *counter = bump.take<uint32_t>(2);
   unsigned long long *lb = bump.take<unsigned long long>(tiles + 1);
-  lsm::scan_counts_kernel<<<tiles, lsm::kScanThreads, 0, s>>>(l.run->vals, n, prefix_, lb, counter, dev_status_);
+  lsm::scan_kernel<unsigned long long, false><<<tiles, lsm::kScanThreads, 0, s>>>(l.run->vals, nullptr, n, prefix_, lb,
+                                                                              counter, dev_status_);
   note_launch();
   prefix_gen_ = l.gen;
   return prefix_;
+}
+
+// The level set of a range sum over several levels: every view carries its
+// level's live-value prefix, scanned here (over the host upper bound of the
+// rows) when the level changed since its last scan.
+void LsmDictionary::live_level_set(void *out, cudaStream_t s) {
+  auto *set = static_cast<lsm::LevelSet *>(out);
+  set->count = 0;
+  if (live_.size() < levels_.size()) live_.resize(levels_.size());
+  for (size_t i = 0; i < levels_.size(); ++i) {
+    const Level &l = levels_[i];
+    if (!l.run) continue;
+    LivePrefix &lp = live_[i];
+    if (lp.gen != l.gen || !lp.p) {
+      const uint64_t n = l.upper;
+      if (n + 1 > lp.cap) {
+        if (lp.p) GPULSM_CUDA(cudaFreeAsync(lp.p, s));
+        live_bytes_ -= lp.cap * 4;
+        lp.p = nullptr;
+        lp.cap = 0;
+        const uint64_t cap = std::max<uint64_t>(n + 1, 1024);
+        if (cudaMallocAsync(reinterpret_cast<void **>(&lp.p), cap * 4, s) != cudaSuccess) {
+          (void)cudaGetLastError();
+          lp.p = nullptr;
+          throw std::bad_alloc();
+        }
+        lp.cap = cap;
+        live_bytes_ += cap * 4;
+      }
+      const uint32_t tiles = lsm::scan_tiles(n);
+      const size_t bytes = align_up(8) + align_up(size_t(tiles + 1) * 8);
+      Bump bump{static_cast<char *>(scratch(bytes, s))};
+      GPULSM_CUDA(cudaMemsetAsync(bump.p, 0, bytes, s));
+      uint32_t *counter = bump.take<uint32_t>(2);
+      unsigned long long *lb = bump.take<unsigned long long>(tiles + 1);
+      lsm::scan_kernel<uint32_t, true><<<tiles, lsm::kScanThreads, 0, s>>>(l.run->vals, l.run->flags, n, lp.p, lb,
+                                                                           counter, dev_status_);
+      note_launch();
+      lp.gen = l.gen;
+    }
+    lsm::LevelView v = view_of(int(i));
+    v.live = lp.p;
+    set->lv[set->count++] = v;
+  }
 }
 
 void LsmDictionary::admit(const uint32_t *keys, const uint32_t *values, uint64_t n, bool tombstone,
@@ -678,9 +726,9 @@ void LsmDictionary::range_sum(const uint32_t *lo, const uint32_t *hi, uint64_t n
     note_launch();
   } else {
     lsm::LevelSet set;
-    level_set(&set);
-    lsm::range_kernel<0><<<grid_for(n, 256), 256, 0, s>>>(set, lo, hi, n, out, nullptr, nullptr,
-                                                         nullptr); note_launch();
+    live_level_set(&set, s);
+    lsm::range_sum_levels_kernel<<<grid_for(n, 256), 256, 0, s>>>(set, lo, hi, n, out);
+    note_launch();
   }
   GPULSM_CUDA(cudaGetLastError());
   end_op(s);
@@ -694,8 +742,8 @@ void LsmDictionary::range_sum_kway(const uint32_t *lo, const uint32_t *hi, uint6
   apply_receipt(false);
   begin_op(s);
   lsm::LevelSet set;
-  level_set(&set);
-  lsm::range_kernel<0><<<grid_for(n, 256), 256, 0, s>>>(set, lo, hi, n, out, nullptr, nullptr, nullptr);
+  live_level_set(&set, s);
+  lsm::range_sum_levels_kernel<<<grid_for(n, 256), 256, 0, s>>>(set, lo, hi, n, out);
   note_launch();
   GPULSM_CUDA(cudaGetLastError());
   end_op(s);
@@ -750,8 +798,8 @@ void LsmDictionary::range_offsets(const uint32_t *lo, const uint32_t *hi, uint64
                                                            nullptr); note_launch();
     }
   }
-  lsm::scan_counts_kernel<<<tiles, lsm::kScanThreads, 0, s>>>(
-      counts, n, reinterpret_cast<unsigned long long *>(offsets), lb, counter, dev_status_); note_launch();
+  lsm::scan_kernel<unsigned long long, false><<<tiles, lsm::kScanThreads, 0, s>>>(
+      counts, nullptr, n, reinterpret_cast<unsigned long long *>(offsets), lb, counter, dev_status_); note_launch();
   GPULSM_CUDA(cudaGetLastError());
   end_op(s);
 }
@@ -808,7 +856,7 @@ uint32_t LsmDictionary::status() {
 
 uint64_t LsmDictionary::resident_bytes() {
   std::lock_guard<std::mutex> g(mu_);
-  return pool_.bytes() + words_cap_ * 16 + scratch_bytes_ + sizeof(Receipt) + 256;
+  return pool_.bytes() + words_cap_ * 16 + scratch_bytes_ + live_bytes_ + sizeof(Receipt) + 256;
 }
 
 void LsmDictionary::size(uint64_t *rows, uint32_t *levels) {

@@ -125,6 +125,7 @@ class LsmDictionary {
   int ranges_on_single_level(const uint32_t *lo, const uint32_t *hi, uint64_t n, cudaStream_t s);
   void compact_all(cudaStream_t s);
   const unsigned long long *value_prefix(int level, cudaStream_t s);
+  void live_level_set(void *out, cudaStream_t s);
   void release_levels(cudaStream_t s);
   void fit_model(RunBuffer *run, uint64_t upper, cudaStream_t s);
   void *scratch(size_t bytes, cudaStream_t s);
@@ -161,6 +162,15 @@ class LsmDictionary {
   unsigned long long *prefix_ = nullptr;
   uint64_t prefix_cap_ = 0;
   uint64_t prefix_gen_ = 0;
+  // u32 live-value prefix of every level (range sums over several levels),
+  // rebuilt for a level only when its generation changed
+  struct LivePrefix {
+    uint32_t *p = nullptr;
+    uint64_t cap = 0;
+    uint64_t gen = ~0ull;
+  };
+  std::vector<LivePrefix> live_;
+  uint64_t live_bytes_ = 0;
   unsigned long long *width_ = nullptr;  // device word for the range-width estimate
   unsigned long long *width_host_ = nullptr;
 

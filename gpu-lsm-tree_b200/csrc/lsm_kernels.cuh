@@ -39,6 +39,7 @@ struct LevelView {
   const LevelDesc *desc;
   const learned::ModelHeader *mh = nullptr;
   const learned::Segment *ms = nullptr;
+  const uint32_t *live = nullptr;  // live-value prefix (range sums over levels), u32 modulo 2^32
 };
 
 struct LevelSet {
@@ -50,6 +51,9 @@ struct LevelSet {
 // Admission: pack (key, value) into one u64 word (key in the high half so an
 // LSD sort on bits 32..63 orders by key and keeps input order among equal
 // keys) and count the key bytes of the four sort passes.
+// kTopOnly: count only the top key byte (hist[3 * 256 ...]), for admission
+// by top-byte buckets.
+template <bool kTopOnly>
 __global__ void __launch_bounds__(256) pack_histogram_kernel(const uint32_t *__restrict__ keys,
                                                              const uint32_t *__restrict__ vals,
                                                              uint32_t n,
@@ -62,13 +66,15 @@ __global__ void __launch_bounds__(256) pack_histogram_kernel(const uint32_t *__r
     const uint32_t k = keys[i];
     const uint32_t v = vals ? vals[i] : kTombValue;
     words[i] = (static_cast<unsigned long long>(k) << 32) | v;
-    atomicAdd(&s[0][k & 0xffu], 1u);
-    atomicAdd(&s[1][(k >> 8) & 0xffu], 1u);
-    atomicAdd(&s[2][(k >> 16) & 0xffu], 1u);
+    if (!kTopOnly) {
+      atomicAdd(&s[0][k & 0xffu], 1u);
+      atomicAdd(&s[1][(k >> 8) & 0xffu], 1u);
+      atomicAdd(&s[2][(k >> 16) & 0xffu], 1u);
+    }
     atomicAdd(&s[3][k >> 24], 1u);
   }
   __syncthreads();
-  for (int p = 0; p < 4; ++p) {
+  for (int p = kTopOnly ? 3 : 0; p < 4; ++p) {
     const uint32_t c = s[p][threadIdx.x];
     if (c) atomicAdd(&hist[p * 256 + threadIdx.x], c);
   }
@@ -240,21 +246,47 @@ __device__ __forceinline__ uint64_t merge_path(const uint32_t *a, uint64_t na, c
   return lo;
 }
 
-// Split points of every merge tile, one thread per tile boundary: the
-// dependent binary searches run in parallel here instead of serialising each
-// merge tile behind one searching thread.  parts[i] = A rows before diagonal
-// min(i * kMergeTile, na + nb).
+// merge_path on tile-local (32-bit) lengths, for shared-memory segments
+__device__ __forceinline__ uint32_t merge_path32(const uint32_t *a, uint32_t na, const uint32_t *b, uint32_t nb,
+                                                 uint32_t diag) {
+  uint32_t lo = diag > nb ? diag - nb : 0, hi = diag < na ? diag : na;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (a[mid] <= b[diag - 1 - mid]) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Split points of every merge tile: parts[i] = A rows before diagonal
+// min(i * kMergeTile, na + nb), one warp per split.  The merge-path predicate
+// P(k) = A[k] <= B[d-1-k] is true then false along k; each step probes 32
+// evenly spaced k at once (one round trip) and keeps the interval where P
+// turns false, so a split costs about log32(na) dependent loads instead of
+// log2(na).
 __global__ void __launch_bounds__(256) merge_partition_kernel(const uint32_t *__restrict__ ak,
                                                               const LevelDesc *__restrict__ adesc,
                                                               const uint32_t *__restrict__ bk,
                                                               const LevelDesc *__restrict__ bdesc,
                                                               unsigned long long *__restrict__ parts,
                                                               uint32_t max_parts) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= max_parts) return;
+  const uint32_t split = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t lane = threadIdx.x & 31u;
+  if (split >= max_parts) return;  // whole warps leave together
   const uint64_t na = adesc->n, nb = bdesc->n, total = na + nb;
-  const uint64_t d = min(uint64_t(i) * kMergeTile, total);
-  parts[i] = merge_path(ak, na, bk, nb, d);
+  const uint64_t d = min(uint64_t(split) * kMergeTile, total);
+  uint64_t lo = d > nb ? d - nb : 0, hi = d < na ? d : na;  // the answer lies in [lo, hi]
+  while (hi > lo) {
+    const uint64_t span = hi - lo;
+    const uint64_t step = span <= 32 ? 1 : (span + 31) / 32;
+    const uint64_t k = lo + (uint64_t(lane) + 1) * step - 1;  // probe P(k)
+    const bool t = k < hi && ak[k] <= bk[d - 1 - k];
+    const uint32_t trues = __popc(__ballot_sync(0xffffffffu, t));  // a prefix of the lanes
+    const uint64_t nlo = lo + uint64_t(trues) * step;  // P holds below nlo
+    hi = min(hi, nlo + step - 1);                      // and fails at the first false probe
+    lo = nlo;
+  }
+  if (lane == 0) parts[split] = lo;
 }
 
 template <bool kDropTombstones>
@@ -327,7 +359,7 @@ __global__ void __launch_bounds__(kMergeThreads, 4) merge_kernel(
   // output (the new head of the side that advanced)
   const uint32_t my_d = min(uint32_t(threadIdx.x) * kMergeItems, len);
   const uint32_t my_n = min(uint32_t(kMergeItems), len - my_d);
-  uint32_t ai = uint32_t(merge_path(s_key, alen, s_key + alen, blen, my_d));
+  uint32_t ai = merge_path32(s_key, alen, s_key + alen, blen, my_d);
   uint32_t bi = my_d - ai;
   bool hp = ai > 0 ? true : has_prev_a;
   uint32_t prev = ai > 0 ? s_key[ai - 1] : prev_a_global;
@@ -580,6 +612,82 @@ __global__ void __launch_bounds__(256) range_kernel(LevelSet set, const uint32_t
 }
 
 // ---------------------------------------------------------------------------
+// Range sums over every level without merging them (same answers as
+// range_kernel<0>).  Each level's live-value prefix gives the sum of its
+// live rows in [lo, hi] in O(1); what it over-counts is every row SHADOWED
+// by a newer version of its key.  Each level holds a key at most once, so
+// the versions of a key form a chain newest -> oldest over the levels, and
+// walking the rows of every level but the oldest, each row subtracts the
+// next older version of its key (when that version is live).  The row count
+// walked is that of the newer (small) levels only; the search for a row's
+// key in an older level gallops forward from the previous row's position.
+
+// First index in [pos, end) whose key is >= k (keys ascending).
+__device__ __forceinline__ uint64_t gallop_lower_bound(const uint32_t *__restrict__ keys, uint64_t pos,
+                                                       uint64_t end, uint32_t k) {
+  if (pos >= end || keys[pos] >= k) return pos;
+  uint64_t lo = pos, hi = end, step = 1;  // keys[lo] < k; answer in (lo, hi]
+  while (true) {
+    const uint64_t probe = lo + step;
+    if (probe >= end) break;
+    if (keys[probe] >= k) {
+      hi = probe;
+      break;
+    }
+    lo = probe;
+    step <<= 1;
+  }
+  while (hi - lo > 1) {
+    const uint64_t mid = lo + ((hi - lo) >> 1);
+    if (keys[mid] < k) lo = mid;
+    else hi = mid;
+  }
+  return hi;
+}
+
+__global__ void __launch_bounds__(256) range_sum_levels_kernel(LevelSet set, const uint32_t *__restrict__ lo,
+                                                               const uint32_t *__restrict__ hi, uint64_t n,
+                                                               uint32_t *__restrict__ out) {
+  const uint64_t q = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const uint32_t a = lo[q], z = hi[q];
+  uint32_t acc = 0;
+  if (a <= z) {
+    uint64_t cur[kMaxLevels], end[kMaxLevels], pos[kMaxLevels];
+    uint32_t lv[kMaxLevels];  // levels with rows in [a, z], newest first
+    uint32_t m = 0;
+    for (uint32_t l = 0; l < set.count; ++l) {
+      const LevelDesc d = load_desc(set.lv[l].desc);
+      const uint64_t b = level_lower_bound(set.lv[l], d, a), e = level_upper_bound(set.lv[l], d, z);
+      if (e > b) {
+        acc += set.lv[l].live[e] - set.lv[l].live[b];
+        cur[m] = b;
+        end[m] = e;
+        lv[m++] = l;
+      }
+    }
+    for (uint32_t i = 0; i + 1 < m; ++i) {
+      const LevelView &N = set.lv[lv[i]];
+      for (uint32_t j = i + 1; j < m; ++j) pos[j] = cur[j];
+      for (uint64_t r = cur[i]; r < end[i]; ++r) {
+        const uint32_t k = N.keys[r];
+        for (uint32_t j = i + 1; j < m; ++j) {
+          const LevelView &O = set.lv[lv[j]];
+          const uint64_t p = gallop_lower_bound(O.keys, pos[j], end[j], k);
+          pos[j] = p;
+          if (p < end[j] && O.keys[p] == k) {
+            const uint32_t v = O.vals[p];
+            if (!row_is_tomb(O, p, v)) acc -= v;
+            break;
+          }
+        }
+      }
+    }
+  }
+  out[q] = acc;
+}
+
+// ---------------------------------------------------------------------------
 // Ranges over ONE tombstone-free level (after a compaction): the answer of a
 // query is the contiguous row slice [lower_bound(lo), upper_bound(hi)).
 
@@ -690,15 +798,19 @@ __global__ void __launch_bounds__(256) successor_kernel(LevelSet set, const uint
 }
 
 // ---------------------------------------------------------------------------
-// Exclusive scan of u32 counts into u64 offsets (offsets[n] = total), single
-// pass with decoupled look-back.
+// Exclusive scan of u32 inputs into offsets (offsets[n] = total), single
+// pass with decoupled look-back.  kLive: the inputs are a level's values and
+// a tombstone row (value kTombValue with the flag bit) counts as 0, which
+// gives the level's live-value prefix; OutT = u32 keeps it modulo 2^32, the
+// width of a range sum.
 constexpr int kScanThreads = 256;
 constexpr int kScanItems = 8;
 constexpr uint32_t kScanTile = kScanThreads * kScanItems;
 
-__global__ void __launch_bounds__(kScanThreads) scan_counts_kernel(
-    const uint32_t *__restrict__ counts, uint64_t n, unsigned long long *__restrict__ offsets,
-    unsigned long long *__restrict__ lb, uint32_t *__restrict__ tile_counter,
+template <typename OutT, bool kLive>
+__global__ void __launch_bounds__(kScanThreads) scan_kernel(
+    const uint32_t *__restrict__ in, const uint8_t *__restrict__ flags, uint64_t n,
+    OutT *__restrict__ offsets, unsigned long long *__restrict__ lb, uint32_t *__restrict__ tile_counter,
     uint32_t *__restrict__ status) {
   __shared__ unsigned long long s_scan[kScanThreads / 32];
   __shared__ unsigned long long s_total;
@@ -712,7 +824,8 @@ __global__ void __launch_bounds__(kScanThreads) scan_counts_kernel(
   unsigned long long sum = 0;
 #pragma unroll
   for (int i = 0; i < kScanItems; ++i) {
-    c[i] = base + i < n ? counts[base + i] : 0u;
+    c[i] = base + i < n ? in[base + i] : 0u;
+    if (kLive && c[i] == kTombValue && base + i < n && (flags[base + i] & kFlagTomb)) c[i] = 0u;
     sum += c[i];
   }
   const unsigned long long local = block_exclusive_scan<kScanThreads>(sum, s_scan, &s_total);
@@ -724,7 +837,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_counts_kernel(
   unsigned long long o = s_base + local;
 #pragma unroll
   for (int i = 0; i < kScanItems; ++i) {
-    if (base + i <= n) offsets[base + i] = o;  // index n receives the total
+    if (base + i <= n) offsets[base + i] = OutT(o);  // index n receives the total
     o += c[i];
   }
 }

@@ -1,5 +1,6 @@
 // Host side of the learned position model (learned.cuh): fit, gradient
 // export for checking against the CPU, and exact lower-bound queries.
+#include <algorithm>
 #include <stdexcept>
 
 #include "learned.cuh"
@@ -60,7 +61,8 @@ void fit(const K *keys, uint64_t n, uint32_t segments, uint32_t iters, void *mod
   segments = pow2_at_least(std::max<uint32_t>(segments, 1));
   Parts p = parts(model, segments);
   model_header_kernel<K><<<1, 1, 0, s>>>(keys, n, segments, p.h, n_dev); note_launch();
-  model_init_kernel<K><<<grid_for(segments + 1, 256), 256, 0, s>>>(keys, p.h, p.seg); note_launch();
+  model_init_scan_kernel<K><<<grid_for(std::max<uint64_t>(n, segments + 1), 256), 256, 0, s>>>(keys, p.h, p.seg);
+  note_launch();
   model_init_params_kernel<K><<<grid_for(segments, 256), 256, 0, s>>>(p.h, p.seg); note_launch();
   GPULSM_CUDA(cudaMemsetAsync(p.acc, 0, size_t(segments) * 16, s));
   if (loss_hist) GPULSM_CUDA(cudaMemsetAsync(loss_hist, 0, size_t(iters + 1) * 4, s));

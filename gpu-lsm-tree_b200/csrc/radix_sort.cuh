@@ -1,7 +1,7 @@
 // Onesweep-style LSD radix sort (8-bit digits) for 32/64-bit keys with an
 // optional u32 payload.  One upfront histogram pass computes the digit counts
 // of every pass; each pass then ranks a 4096-key tile in registers with
-// __match_any_sync peer groups, publishes its digit counts through a
+// ballot-built peer groups (match_any_bits), publishes its digit counts through a
 // decoupled look-back (bounded spin, never a hang), stages the tile in shared
 // memory in digit order and writes it out in coalesced runs.  Stable, so a
 // later "keep the last of each equal-key run" pass sees input order.
@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(kThreads) onesweep_kernel(
 #pragma unroll
   for (int i = 0; i < kItems; ++i) {
     const uint32_t d = digits[i];
-    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    const uint32_t peers = match_any_bits<9>(d);  // digits 0..255, 256 = no key
     const uint32_t leader = 31u - __clz(peers);
     uint32_t base = 0;
     if (lane == leader && d < kDigits) {

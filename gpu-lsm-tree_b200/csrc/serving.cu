@@ -19,6 +19,7 @@ namespace {
 // the admitted run (9 B/row plus directory), sort words (16 B) and the
 // transient merge output (9 B/row), rounded up.
 constexpr uint64_t kUpdateBytesPerKey = 48;
+constexpr size_t kMaxInflight = 2;
 constexpr int kErrCapacity = 2;  // GPULSM_ERR_CAPACITY
 constexpr int kErrCuda = 5;      // GPULSM_ERR_CUDA
 
@@ -56,8 +57,8 @@ Server::Server(const DictConfig &cfg, uint64_t budget_bytes, uint32_t max_round_
     GPULSM_CUDA(cudaMalloc(&s.d_in, m * 8));
     GPULSM_CUDA(cudaMalloc(&s.d_out, m * 4));
     GPULSM_CUDA(cudaMalloc(&s.d_found, m));
-    GPULSM_CUDA(cudaEventCreateWithFlags(&s.uploaded, cudaEventDisableTiming));
-    GPULSM_CUDA(cudaEventCreateWithFlags(&s.computed, cudaEventDisableTiming));
+    GPULSM_CUDA(cudaEventCreate(&s.uploaded));  // timed: device busy time per round
+    GPULSM_CUDA(cudaEventCreate(&s.computed));
     GPULSM_CUDA(cudaEventCreateWithFlags(&s.downloaded, cudaEventDisableTiming));
     free_slots_.push_back(i);
   }
@@ -146,7 +147,7 @@ void Server::reset_stats() {
   lat_us_.clear();
   st_completed_ = st_rejected_ = st_rounds_ = st_keys_ = st_round_keys_ = 0;
   st_first_ = -1;
-  st_last_ = 0;
+  st_last_ = st_gpu_s_ = st_launch_s_ = 0;
 }
 
 ServeStats Server::stats() {
@@ -161,6 +162,8 @@ ServeStats Server::stats() {
     s.keys = st_keys_;
     s.mean_round_keys = st_rounds_ ? double(st_round_keys_) / double(st_rounds_) : 0.0;
     s.wall_s = st_first_ >= 0 ? std::max(0.0, st_last_ - st_first_) : 0.0;
+    s.gpu_busy_s = st_gpu_s_;
+    s.host_launch_s = st_launch_s_;
   }
   if (!lat.empty()) {
     auto pct = [&](double p) {
@@ -286,7 +289,11 @@ void Server::worker() {
   cudaSetDevice(device_);
   for (;;) {
     std::unique_lock<std::mutex> lk(mu_);
-    cv_work_.wait(lk, [&] { return stop_ || (!queue_.empty() && !free_slots_.empty()); });
+    // at most kMaxInflight rounds launched and not yet returned: while the
+    // GPU works on them, arrivals accumulate into the next round
+    cv_work_.wait(lk, [&] {
+      return stop_ || (!queue_.empty() && !free_slots_.empty() && inflight_.size() < kMaxInflight);
+    });
     if (stop_) return;
     const uint32_t si = free_slots_.front();
     free_slots_.pop_front();
@@ -301,13 +308,16 @@ void Server::worker() {
       continue;
     }
     bool ok = true;
+    const double t0 = now_s();
     try {
       launch_round(slot);
     } catch (const std::exception &e) {
       ok = false;
       for (Run &r : slot.runs) r.status = status_of(e);
     }
+    const double t1 = now_s();
     lk.lock();
+    st_launch_s_ += t1 - t0;
     slot.launched = ok;
     inflight_.push_back(si);
     inflight_bytes_ += slot.bytes;
@@ -328,6 +338,11 @@ void Server::completer() {
     int fail = 0;
     if (slot.launched && cudaEventSynchronize(slot.downloaded) != cudaSuccess) fail = -kErrCuda;
     const double t = now_s();
+    float gpu_ms = 0.f;
+    if (slot.launched && !fail && cudaEventElapsedTime(&gpu_ms, slot.uploaded, slot.computed) != cudaSuccess) {
+      (void)cudaGetLastError();
+      gpu_ms = 0.f;
+    }
     if (!fail)
       for (const Run &r : slot.runs) {
         if (r.status || !has_out(r.kind)) continue;
@@ -351,6 +366,7 @@ void Server::completer() {
       }
     ++st_rounds_;
     st_round_keys_ += slot.keys;
+    st_gpu_s_ += double(gpu_ms) * 1e-3;
     st_last_ = t;
     free_slots_.push_back(si);
     lk.unlock();

@@ -45,6 +45,8 @@ struct ServeStats {
   double p50_us = 0, p99_us = 0, max_us = 0, mean_us = 0;
   double mean_round_keys = 0;
   double wall_s = 0;          // first submit to last completion since the last reset
+  double gpu_busy_s = 0;      // device time of the rounds (upload done -> kernels done)
+  double host_launch_s = 0;   // worker time staging and launching rounds
 };
 
 // Open-loop load: Poisson arrivals, kind mix, log-uniform sizes, Zipf keys.
@@ -150,7 +152,7 @@ class Server {
   // statistics since the last reset
   std::vector<float> lat_us_;
   uint64_t st_completed_ = 0, st_rejected_ = 0, st_rounds_ = 0, st_keys_ = 0, st_round_keys_ = 0;
-  double st_first_ = -1, st_last_ = 0;
+  double st_first_ = -1, st_last_ = 0, st_gpu_s_ = 0, st_launch_s_ = 0;
 
   std::thread worker_, completer_;
 };

@@ -352,10 +352,10 @@ def test_lsm_scale_full_size_properties(gl, cuda, workloads):
 def test_search_modes_match_oracle(gl, cuda, mode):
     """Radix directory (0), learned position model per level (1) and plain
     binary search (2) must give identical, exact answers; the levels here are
-    large enough (>= 2^16 rows) for the learned mode to fit its models."""
+    large enough (>= 2^22 rows) for the learned mode to fit its models."""
     rng = np.random.default_rng(40 + mode)
-    t = Twin(gl, max_elements=1 << 21, batch_capacity=1 << 16, search_mode=mode)
-    base = rng.integers(0, 1 << 32, 1 << 19, dtype=np.uint64).astype(np.uint32)
+    t = Twin(gl, max_elements=1 << 23, batch_capacity=1 << 16, search_mode=mode)
+    base = rng.integers(0, 1 << 32, 1 << 22, dtype=np.uint64).astype(np.uint32)
     base[:3] = [0, 1, 0xFFFFFFFF]
     t.d.bulk_build(to_dev(base), to_dev(np.arange(base.size, dtype=np.uint32)))
     t.o.bulk_build(base, np.arange(base.size, dtype=np.uint32))
