@@ -1,24 +1,23 @@
 // Batch admission by top-byte buckets: the sorted, deduplicated level run of
 // one update batch (GPULSMOpt.cuh:2578-2633 sorts the batch, ages the
-// duplicates and keeps the newest) in three launches instead of a four-pass
+// duplicates and keeps the newest) in four launches instead of a four-pass
 // LSD sort plus a dedup pass:
 //
-//   1. pack_histogram_kernel   words (key << 32 | value) in input order and
-//                              the key-byte histograms (lsm_kernels.cuh)
-//   2. one onesweep pass       stable partition of the words by the key's top
-//                              byte (radix_sort.cuh)
-//   3. admit_bucket_kernel     one CTA per top-byte bucket, in bucket order:
-//                              sorts the bucket's varying low key bits in
-//                              shared memory (a stable 8-bit LSD pass per
-//                              varying byte), keeps the last row of every
-//                              equal-key run (input order survives both
-//                              stable sorts, so the last row is the newest),
-//                              chains its row count to the earlier buckets by
-//                              decoupled look-back and writes the level rows
-//                              plus its share of the radix directory.  A
-//                              bucket larger than shared memory is sorted
-//                              through global memory by the same CTA in
-//                              chunks (correct for any skew, slower).
+//   1. part_hist_kernel     per 4096-key tile, the counts of the key's top byte
+//   2. part_scan_kernel     per top byte, the exclusive scan over the tiles
+//   3. part_scatter_kernel  words (key << 32 | value) written to their top-byte
+//                           bucket in input order (a stable partition)
+//   4. admit_bucket_kernel  one CTA per top-byte bucket, in bucket order:
+//                           sorts the bucket by (key, input position) in
+//                           shared memory (a 12-bit counting sort plus an
+//                           insertion sort of every bin, or stable 8-bit LSD
+//                           passes when a bin is large), keeps the last row of
+//                           every equal-key run (the newest), chains its row
+//                           count to the earlier buckets by decoupled look-back
+//                           and writes the level rows plus its share of the
+//                           radix directory.  A bucket larger than shared
+//                           memory is sorted through global memory by the
+//                           same CTA in chunks (correct for any skew, slower).
 //
 // The level's key bounds are the top-byte span of the batch
 // [first << 24, last << 24 | 0xffffff]: every search uses kmin/kmax only as
@@ -132,11 +131,14 @@ __device__ __forceinline__ uint32_t count_distinct(const At &at, uint32_t cnt, R
 // at(0 .. cnt) to out[g0 ...], in chunks of kCap read striped (element
 // c0 + i*kThreads + t): per item a warp ballot counts the kept rows, one block
 // scan over the (item, warp) counts gives every warp its output offset, and
-// consecutive lanes store consecutive rows.
+// consecutive lanes store consecutive rows.  Each kept row also writes the
+// radix-directory entries it starts: the buckets after the bucket of the
+// previous distinct key (bp before the first row) up to its own.
 template <typename At>
 __device__ __forceinline__ void write_rows(const At &at, uint32_t cnt, int tombstone, uint32_t *out_keys,
                                            uint32_t *out_vals, uint8_t *out_flags, unsigned long long g0,
-                                           RankSmem &rs) {
+                                           RankSmem &rs, uint32_t *__restrict__ dir, const DirGeom &g,
+                                           int64_t bp) {
   static_assert(kItems * kWarps <= 256, "one scan slot per (item, warp)");
   const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
   const uint32_t lt = lanemask_lt();
@@ -163,9 +165,16 @@ __device__ __forceinline__ void write_rows(const At &at, uint32_t cnt, int tombs
         const uint32_t e = c0 + uint32_t(i) * kThreads + threadIdx.x;
         const unsigned long long w64 = at(e);
         const unsigned long long r = g0 + written + slot[i * kWarps + w] + __popc(ends[i] & lt);
-        out_keys[r] = word_key(w64);
+        const uint32_t k = word_key(w64);
+        out_keys[r] = k;
         out_vals[r] = uint32_t(w64);  // the tombstone value was packed for erase batches
         out_flags[r] = tombstone ? kFlagTomb : uint8_t(0);
+        uint32_t p = e;  // first element of this key's run
+        while (p > 0 && word_key(at(p - 1)) == k) --p;
+        const int64_t bprev = p > 0 ? int64_t((word_key(at(p - 1)) - g.kmin) >> g.shift) : bp;
+        const int64_t bj = int64_t((k - g.kmin) >> g.shift);
+        for (int64_t b = bprev + 1; b <= bj; ++b)
+          if (GPULSM_OK(b >= 0 && b < int64_t(g.nbuckets), 10, b)) dir[b] = uint32_t(r);
       }
     __syncthreads();
     written += chunk_kept;
@@ -262,16 +271,26 @@ constexpr int kPartWarps = kPartThreads / 32;
 inline uint32_t part_tiles(uint64_t n) { return uint32_t((n + kPartTile - 1) / kPartTile); }
 
 __global__ void __launch_bounds__(kPartThreads) part_hist_kernel(const uint32_t *__restrict__ keys, uint32_t n,
-                                                                 uint32_t tiles, uint32_t *__restrict__ cnt) {
+                                                                 uint32_t tiles, uint32_t *__restrict__ cnt,
+                                                                 unsigned long long *__restrict__ zero,
+                                                                 uint32_t zero_words) {
   __shared__ uint32_t h[256];
+  chain_wait();
+  // the bucket kernel's ticket counter and look-back slots start at zero
+  for (uint32_t i = blockIdx.x * kPartThreads + threadIdx.x; i < zero_words; i += gridDim.x * kPartThreads)
+    zero[i] = 0ull;
+  const uint32_t base = blockIdx.x * kPartTile;
+  uint32_t k[kPartItems];
+#pragma unroll
+  for (int i = 0; i < kPartItems; ++i) {  // all loads in flight before the first atomic
+    const uint32_t e = base + uint32_t(i) * kPartThreads + threadIdx.x;
+    k[i] = e < n ? keys[e] : 0u;
+  }
   h[threadIdx.x] = 0;
   __syncthreads();
-  const uint32_t base = blockIdx.x * kPartTile;
 #pragma unroll
-  for (int i = 0; i < kPartItems; ++i) {
-    const uint32_t e = base + uint32_t(i) * kPartThreads + threadIdx.x;
-    if (e < n) atomicAdd(&h[keys[e] >> 24], 1u);
-  }
+  for (int i = 0; i < kPartItems; ++i)
+    if (base + uint32_t(i) * kPartThreads + threadIdx.x < n) atomicAdd(&h[k[i] >> 24], 1u);
   __syncthreads();
   cnt[threadIdx.x * tiles + blockIdx.x] = h[threadIdx.x];
 }
@@ -283,6 +302,7 @@ __global__ void __launch_bounds__(kPartThreads) part_scan_kernel(const uint32_t 
                                                                  uint32_t *__restrict__ total) {
   __shared__ uint32_t s_scan[kPartWarps];
   __shared__ uint32_t s_total;
+  chain_wait();
   const uint32_t b = blockIdx.x;
   uint32_t carry = 0;
   for (uint32_t t0 = 0; t0 < tiles; t0 += kPartThreads) {
@@ -304,12 +324,10 @@ __global__ void __launch_bounds__(kPartThreads) part_scatter_kernel(
   __shared__ uint32_t s_dst[256];     // global position of the tile's first row of each byte
   __shared__ uint32_t s_scan[kPartWarps];
   __shared__ uint32_t s_total;
+  chain_wait();
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, tile = blockIdx.x;
-  for (uint32_t i = lane; i < 256; i += 32) warp_hist[warp][i] = 0;
-  // byte bases: exclusive scan of the totals (every tile repeats this 256-entry scan)
-  const uint32_t tot = total[threadIdx.x];
-  const uint32_t base = block_exclusive_scan<kPartThreads>(tot, s_scan, &s_total);
-  s_dst[threadIdx.x] = base + prefix[threadIdx.x * tiles + tile];
+  // the tile's keys and values, then the byte bases: all loads are in flight
+  // before the first shared-memory step waits on any of them
   const uint32_t wbase = tile * kPartTile + warp * 32u * kPartItems;
   unsigned long long w[kPartItems];
   uint32_t d[kPartItems], rank[kPartItems];
@@ -322,6 +340,12 @@ __global__ void __launch_bounds__(kPartThreads) part_scatter_kernel(
     w[i] = (static_cast<unsigned long long>(k) << 32) | (vals ? (valid ? vals[e] : 0u) : kTombValue);
     d[i] = valid ? (k >> 24) : 256u;
   }
+  const uint32_t tot = total[threadIdx.x];
+  const uint32_t pre = prefix[threadIdx.x * tiles + tile];
+  for (uint32_t i = lane; i < 256; i += 32) warp_hist[warp][i] = 0;
+  // byte bases: exclusive scan of the totals (every tile repeats this 256-entry scan)
+  const uint32_t base = block_exclusive_scan<kPartThreads>(tot, s_scan, &s_total);
+  s_dst[threadIdx.x] = base + pre;
   __syncwarp();
 #pragma unroll
   for (int i = 0; i < kPartItems; ++i) {  // stable rank per warp, items in element order
@@ -441,6 +465,7 @@ __global__ void __launch_bounds__(kThreads, 2) admit_bucket_kernel(
     uint32_t *__restrict__ tile_counter, uint32_t *__restrict__ status) {
   extern __shared__ __align__(16) unsigned char dyn[];
   BucketSmem &sm = *reinterpret_cast<BucketSmem *>(dyn);
+  chain_wait();
   if (threadIdx.x == 0) {
     sm.tile = atomicAdd(tile_counter, 1u);
     sm.first = kBuckets;
@@ -471,7 +496,19 @@ __global__ void __launch_bounds__(kThreads, 2) admit_bucket_kernel(
   }
   const unsigned long long *sorted = nullptr;  // sorted words, or null when sm.idx holds the order
   if (cnt <= kCap) {
-    for (uint32_t j = threadIdx.x; j < cnt; j += kThreads) sm.words[j] = words0[s0 + j];
+    {  // every thread issues all its loads before its shared stores
+      unsigned long long t[kItems];
+#pragma unroll
+      for (int i = 0; i < kItems; ++i) {
+        const uint32_t j = uint32_t(i) * kThreads + threadIdx.x;
+        t[i] = j < cnt ? words0[s0 + j] : 0ull;
+      }
+#pragma unroll
+      for (int i = 0; i < kItems; ++i) {
+        const uint32_t j = uint32_t(i) * kThreads + threadIdx.x;
+        if (j < cnt) sm.words[j] = t[i];
+      }
+    }
     __syncthreads();
     const uint32_t vary = cnt > 1 ? varying_bits(sm.words, cnt, sm.rank) & 0x00ffffffu : 0u;
     if (!(vary && bin_sort(sm, cnt, vary))) {
@@ -510,15 +547,27 @@ __global__ void __launch_bounds__(kThreads, 2) admit_bucket_kernel(
     atomicOr(status, kDevWaitTimeout);
     return;
   }
-  if (sorted) write_rows(by_array, cnt, tombstone, out_keys, out_vals, out_flags, g0, sm.rank);
-  else write_rows(by_index, cnt, tombstone, out_keys, out_vals, out_flags, g0, sm.rank);
-  __syncthreads();
-  // directory share: the bucket consumed the keys [b << 24, b << 24 | 0xffffff]
+  // directory share: the bucket consumed the keys [b << 24, b << 24 | 0xffffff];
+  // its rows start the buckets after bucket((b << 24) - 1) (the previous
+  // bucket's last key) and it closes the range up to bucket(b << 24 | 0xffffff)
   const uint32_t kmin = first << 24, kmax = (last << 24) | 0x00ffffffu;
   const DirGeom g = dir_geometry(kmin, kmax, n, dir_bits, rows_log2);
-  const uint32_t *rows = out_keys + g0;
-  fill_directory(out_dir, g, b > first, (b << 24) - 1u, (b << 24) | 0x00ffffffu, b == last, g0, kept, g0 + kept,
-                 [&](uint32_t j) { return rows[j]; });
+  const int64_t bp = b > first ? int64_t((((b << 24) - 1u) - g.kmin) >> g.shift) : -1;
+  const int64_t bl = b == last ? int64_t(g.nbuckets) - 1 : int64_t((((b << 24) | 0x00ffffffu) - g.kmin) >> g.shift);
+  // an empty bucket between the first and the last one only closes its range
+  int64_t blast = bp;
+  if (sorted) {
+    write_rows(by_array, cnt, tombstone, out_keys, out_vals, out_flags, g0, sm.rank, out_dir, g, bp);
+    if (cnt) blast = int64_t((word_key(by_array(cnt - 1)) - g.kmin) >> g.shift);
+  } else {
+    write_rows(by_index, cnt, tombstone, out_keys, out_vals, out_flags, g0, sm.rank, out_dir, g, bp);
+    if (cnt) blast = int64_t((word_key(by_index(cnt - 1)) - g.kmin) >> g.shift);
+  }
+  if (threadIdx.x == 0) {
+    for (int64_t bb = blast + 1; bb <= bl; ++bb)
+      if (GPULSM_OK(bb >= 0 && bb < int64_t(g.nbuckets), 13, bb)) out_dir[bb] = uint32_t(g0 + kept);
+    if (b == last) out_dir[g.nbuckets] = uint32_t(g0 + kept);
+  }
   if (b == first && threadIdx.x == 0) {
     out_desc->kmin = g.kmin;
     out_desc->kmax = g.kmax;
