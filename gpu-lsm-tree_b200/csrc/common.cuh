@@ -56,6 +56,32 @@ inline unsigned grid_for(uint64_t n, unsigned threads) {
   return static_cast<unsigned>(g ? g : 1);
 }
 
+#ifdef __CUDACC__
+// Programmatic dependent launch.  A kernel started by launch_chained may have
+// its CTAs made resident while the previous kernel in the stream drains; its
+// first statement is chain_wait(), which blocks until that kernel has
+// completed with its writes visible, then lets the next chained kernel
+// launch.  Because every chained kernel waits before it touches global memory
+// (and before any early return), completion stays transitive along the
+// stream; what the chain saves is the launch gap between dependent kernels.
+template <typename... KArgs, typename... Args>
+inline void launch_chained(void (*kernel)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t s,
+                           Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  GPULSM_CUDA(cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...));
+  note_launch();
+}
+#endif
+
 __host__ __device__ inline uint32_t ceil_log2_u64(uint64_t x) {
   if (x <= 1) return 0;
 #ifdef __CUDA_ARCH__
@@ -66,6 +92,13 @@ __host__ __device__ inline uint32_t ceil_log2_u64(uint64_t x) {
 }
 
 #ifdef __CUDACC__
+// First statement of every kernel started by launch_chained (a no-op for a
+// kernel launched without the attribute).
+__device__ __forceinline__ void chain_wait() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 __device__ __forceinline__ uint32_t lanemask_lt() {
   uint32_t m;
   asm volatile("mov.u32 %0, %%lanemask_lt;" : "=r"(m));

@@ -49,6 +49,7 @@ struct ReceiptSrc {
 };
 
 __global__ void receipt_kernel(ReceiptSrc src) {
+  chain_wait();
   const uint32_t i = threadIdx.x;
   if (i < lsm::kMaxLevels)
     src.out[i] = (i < src.count && src.desc[i]) ? src.desc[i]->n : 0ull;
@@ -183,9 +184,10 @@ LsmDictionary::LsmDictionary(const DictConfig &config)
                                    int(lsm::admit::kBucketSmemBytes)));
   GPULSM_CUDA(cudaMalloc(&dev_status_, 256));
   GPULSM_CUDA(cudaMemset(dev_status_, 0, 256));
-  GPULSM_CUDA(cudaMalloc(&receipt_dev_, sizeof(Receipt)));
-  GPULSM_CUDA(cudaMallocHost(&receipt_host_, sizeof(Receipt)));
+  // the receipt kernel writes the pinned host copy directly (no copy in the stream)
+  GPULSM_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&receipt_host_), sizeof(Receipt), cudaHostAllocMapped));
   std::memset(receipt_host_, 0, sizeof(Receipt));
+  GPULSM_CUDA(cudaHostGetDevicePointer(&receipt_dev_, receipt_host_, 0));
   GPULSM_CUDA(cudaMalloc(&width_, 8));
   GPULSM_CUDA(cudaMallocHost(&width_host_, 8));
   GPULSM_CUDA(cudaEventCreateWithFlags(&op_done_, cudaEventDisableTiming));
@@ -200,7 +202,6 @@ LsmDictionary::~LsmDictionary() {
     if (w) cudaFree(w);
   if (scratch_) cudaFree(scratch_);
   if (dev_status_) cudaFree(dev_status_);
-  if (receipt_dev_) cudaFree(receipt_dev_);
   if (receipt_host_) cudaFreeHost(receipt_host_);
   if (prefix_) cudaFree(prefix_);
   for (auto &lp : live_)
@@ -255,10 +256,8 @@ void LsmDictionary::post_receipt(cudaStream_t s) {
     receipt_gens_[i] = levels_[i].gen;
   }
   src.status = dev_status_;
-  src.out = static_cast<unsigned long long *>(receipt_dev_);
-  receipt_kernel<<<1, 32, 0, s>>>(src); note_launch();
-  GPULSM_CUDA(cudaGetLastError());
-  GPULSM_CUDA(cudaMemcpyAsync(receipt_host_, receipt_dev_, sizeof(Receipt), cudaMemcpyDeviceToHost, s));
+  src.out = static_cast<unsigned long long *>(receipt_dev_);  // the mapped pinned host copy
+  launch_chained(receipt_kernel, 1, 32, 0, s, src);
   GPULSM_CUDA(cudaEventRecord(receipt_event_, s));
   receipt_pending_ = true;
 }
@@ -351,23 +350,21 @@ RunBuffer *LsmDictionary::bucket_admit(const uint32_t *keys, const uint32_t *val
   const size_t zero_bytes = align_up(8) + align_up((ad::kBuckets + 1) * 8);
   const size_t total = zero_bytes + 2 * align_up(size_t(tiles) * 256 * 4) + align_up(256 * 4);
   Bump bump{static_cast<char *>(scratch(total, s))};
-  GPULSM_CUDA(cudaMemsetAsync(bump.p, 0, zero_bytes, s));
+  RunBuffer *carry = pool_.acquire(n, s);  // before the chain: a fresh buffer is a stream-ordered allocation
+  unsigned long long *zero = reinterpret_cast<unsigned long long *>(bump.p);  // zeroed by part_hist_kernel
   uint32_t *counter = bump.take<uint32_t>(2);
   unsigned long long *lb = bump.take<unsigned long long>(ad::kBuckets + 1);
   uint32_t *cnt = bump.take<uint32_t>(size_t(tiles) * 256);
   uint32_t *prefix = bump.take<uint32_t>(size_t(tiles) * 256);
   uint32_t *top = bump.take<uint32_t>(256);
-  ad::part_hist_kernel<<<tiles, ad::kPartThreads, 0, s>>>(keys, nn, tiles, cnt); note_launch();
-  ad::part_scan_kernel<<<256, ad::kPartThreads, 0, s>>>(cnt, tiles, prefix, top); note_launch();
-  ad::part_scatter_kernel<<<tiles, ad::kPartThreads, 0, s>>>(keys, tombstone ? nullptr : values, nn, tiles, prefix,
-                                                             top, words_[1]);
-  note_launch();
-  RunBuffer *carry = pool_.acquire(n, s);
-  ad::admit_bucket_kernel<<<ad::kBuckets, ad::kThreads, ad::kBucketSmemBytes, s>>>(
-      words_[1], words_[0], top, nn, tombstone ? 1 : 0, carry->keys, carry->vals, carry->flags, carry->desc,
-      carry->dir, carry->dir_bits, rows_log2_, lb, counter, dev_status_);
-  note_launch();
-  GPULSM_CUDA(cudaGetLastError());
+  launch_chained(ad::part_hist_kernel, tiles, ad::kPartThreads, 0, s, keys, nn, tiles, cnt, zero,
+                 uint32_t(zero_bytes / 8));
+  launch_chained(ad::part_scan_kernel, 256, ad::kPartThreads, 0, s, cnt, tiles, prefix, top);
+  launch_chained(ad::part_scatter_kernel, tiles, ad::kPartThreads, 0, s, keys, tombstone ? nullptr : values, nn,
+                 tiles, static_cast<const uint32_t *>(prefix), static_cast<const uint32_t *>(top), words_[1]);
+  launch_chained(ad::admit_bucket_kernel, ad::kBuckets, ad::kThreads, ad::kBucketSmemBytes, s, words_[1], words_[0],
+                 static_cast<const uint32_t *>(top), nn, tombstone ? 1 : 0, carry->keys, carry->vals, carry->flags,
+                 carry->desc, carry->dir, carry->dir_bits, rows_log2_, lb, counter, dev_status_);
   return carry;
 }
 
@@ -378,21 +375,21 @@ RunBuffer *LsmDictionary::merge(RunBuffer *newer, RunBuffer *older, uint64_t out
   const size_t zero_bytes = merge_scratch_bytes(out_upper);
   const size_t bytes = zero_bytes + align_up((tiles + 2) * 8);
   Bump bump{static_cast<char *>(scratch(bytes, s))};
-  GPULSM_CUDA(cudaMemsetAsync(bump.p, 0, zero_bytes, s));
+  unsigned long long *zero = reinterpret_cast<unsigned long long *>(bump.p);  // zeroed by the partition kernel
   uint32_t *counter = bump.take<uint32_t>(2);
   unsigned long long *lb = bump.take<unsigned long long>(tiles + 1);
   bump.off = zero_bytes;
   unsigned long long *parts = bump.take<unsigned long long>(tiles + 2);
-  lsm::merge_partition_kernel<<<grid_for((tiles + 1) * 32, 256), 256, 0, s>>>(newer->keys, newer->desc, older->keys,
-                                                                         older->desc, parts, uint32_t(tiles + 1));
-  note_launch();
+  launch_chained(lsm::merge_partition_kernel, grid_for((tiles + 1) * 32, 256), 256, 0, s,
+                 static_cast<const uint32_t *>(newer->keys), static_cast<const lsm::LevelDesc *>(newer->desc),
+                 static_cast<const uint32_t *>(older->keys), static_cast<const lsm::LevelDesc *>(older->desc), parts,
+                 uint32_t(tiles + 1), zero, uint32_t(zero_bytes / 8));
   auto kernel = drop_tombstones ? lsm::merge_kernel<true> : lsm::merge_kernel<false>;
-  kernel<<<unsigned(tiles), lsm::kMergeThreads, 0, s>>>(
-      newer->keys, newer->vals, newer->flags, newer->desc, older->keys, older->vals, older->flags,
-      older->desc, out->keys, out->vals, out->flags, out->desc, out->dir, out->dir_bits, rows_log2_,
-      std::min<uint64_t>(out_upper, out->cap), out->cap, parts, lb, counter, dev_status_);
-  note_launch();
-  GPULSM_CUDA(cudaGetLastError());
+  launch_chained(kernel, unsigned(tiles), lsm::kMergeThreads, 0, s, newer->keys, newer->vals, newer->flags,
+                 newer->desc, older->keys, older->vals, older->flags, older->desc, out->keys, out->vals, out->flags,
+                 out->desc, out->dir, out->dir_bits, rows_log2_,
+                 static_cast<unsigned long long>(std::min<uint64_t>(out_upper, out->cap)),
+                 static_cast<unsigned long long>(out->cap), parts, lb, counter, dev_status_);
   pool_.release(newer);
   pool_.release(older);
   return out;

@@ -269,7 +269,12 @@ __global__ void __launch_bounds__(256) merge_partition_kernel(const uint32_t *__
                                                               const uint32_t *__restrict__ bk,
                                                               const LevelDesc *__restrict__ bdesc,
                                                               unsigned long long *__restrict__ parts,
-                                                              uint32_t max_parts) {
+                                                              uint32_t max_parts,
+                                                              unsigned long long *__restrict__ zero,
+                                                              uint32_t zero_words) {
+  chain_wait();
+  // the merge's ticket counter and look-back slots start at zero
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < zero_words; i += gridDim.x * blockDim.x) zero[i] = 0ull;
   const uint32_t split = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t lane = threadIdx.x & 31u;
   if (split >= max_parts) return;  // whole warps leave together
@@ -307,6 +312,7 @@ __global__ void __launch_bounds__(kMergeThreads, 4) merge_kernel(
   __shared__ uint32_t s_total;
   __shared__ uint32_t s_tile;
   __shared__ unsigned long long s_base;
+  chain_wait();
   if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
   __syncthreads();
   const uint64_t na = adesc->n, nb = bdesc->n, total = na + nb;
