@@ -36,6 +36,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "M lookups/s & M inserted keys/s at 2^26 keys vs plain form; p50/p99 request latency"
+# DRAM bytes (read + write) of merge_kernel per algorithmic byte, from an ncu
+# capture of a 21M-row merge whose output exceeds L2; None until captured
+MERGE_TRAFFIC_RATIO = None
 LOOKUP_BYTES = 41  # algorithmic bytes per u32 point lookup (query + value + found + one row sector)
 INSERT_BYTES = 16  # per inserted (key, value): read 8 + write 8 into the structure
 DELETE_BYTES = 12
@@ -58,6 +61,8 @@ def parse():
     p.add_argument("--flix-rounds", type=int, default=3)
     p.add_argument("--tenant-rounds", type=int, default=4)
     p.add_argument("--serving-seconds", type=float, default=2.0)
+    p.add_argument("--case", default=None, choices=["merge", "admit", "serving-mix"],
+                   help="run one small profiling case instead of the benchmark (see profile_case)")
     return p.parse_args()
 
 
@@ -228,6 +233,15 @@ def run_ours(args):
         t1.record(stream)
         torch.cuda.synchronize(dev)
     launches = lib.gpulsm_launch_count() - launches0
+    # the dominant kernel (merge_kernel): one more step of the same workload
+    # with every merge launch bracketed by CUDA events on the dictionary's
+    # launching stream (events between chained launches would slow the timed
+    # steps, so they stay out of them)
+    d.kernel_timing(True)
+    d.kernel_timing_read()
+    step()
+    merge_timing = d.kernel_timing_read()
+    d.kernel_timing(False)
     total_ms = t0.elapsed_time(t1)
     if world > 1:
         import torch.distributed as dist
@@ -261,10 +275,17 @@ def run_ours(args):
     range_gbs = (nr * RANGE_BYTES + total_pairs * 16) / (rng_ms * 1e-3) / 1e9
     update_gbs = (w.inserted_keys * INSERT_BYTES + w.erased_keys * DELETE_BYTES) / (upd * 1e-3) / 1e9
     phases = {"update": (upd, update_gbs), "lookup": (look, lookup_gbs), "range": (rng_ms, range_gbs)}
-    dom = max(phases, key=lambda k: phases[k][0])
-    roofline = {"bound": "hbm", "kernel_phase": dom, "achieved": round(phases[dom][1], 1), "peak": peak,
-                "unit": "GB/s", "frac": round(phases[dom][1] / peak, 4), "peak_source": peak_kind,
-                "traffic": None,
+    ml = max(merge_timing["launches"], 1)
+    merge_gbs = merge_timing["bytes"] / max(merge_timing["ms"], 1e-9) / 1e6
+    roofline = {"bound": "hbm", "kernel": "lsm::merge_kernel", "measured": "one extra step, CUDA events per launch",
+                "achieved": round(merge_gbs, 1), "peak": peak,
+                "unit": "GB/s", "frac": round(merge_gbs / peak, 4), "peak_source": peak_kind,
+                "traffic": None if MERGE_TRAFFIC_RATIO is None else
+                round(MERGE_TRAFFIC_RATIO * merge_timing["bytes"] / ml),
+                "launches": merge_timing["launches"],
+                "ms_per_launch": round(merge_timing["ms"] / ml, 4),
+                "algorithmic_bytes_per_launch": round(merge_timing["bytes"] / ml),
+                "share_of_update_ms": round(merge_timing["ms"] / upd, 3),
                 "phases_gbs": {k: round(v[1], 1) for k, v in phases.items()}}
 
     result = {
@@ -671,9 +692,66 @@ def run_reference(args):
     }), flush=True)
 
 
+def profile_case(args):
+    """Small, self-contained cases for ncu captures (a few GB on the device):
+    merge       a 2^24-key level plus one 2^20-key batch, then full-width
+                range counts that compact both into one: a single 17M-row merge
+                whose inputs and output exceed L2;
+    admit       64 x (clear + insert of a 2^20-key batch): the admission
+                kernels alone, no merges;
+    serving-mix the serving loop over 2^26 keys, closed loop for 0.3 s with
+                the default request mix."""
+    import torch
+
+    gl = importlib.import_module("gpu-lsm-tree_b200")
+    rng = np.random.default_rng(1)
+
+    def dev(a):
+        return torch.from_numpy(np.ascontiguousarray(a).view(np.int32)).cuda()
+
+    def keys(n):
+        return rng.integers(0, 1 << 32, n, dtype=np.uint64).astype(np.uint32)
+
+    if args.case == "merge":
+        d = gl.GPULSMOpt(gl.DictionaryConfig(max_elements=1 << 25, batch_capacity=1 << 20))
+        base = keys(1 << 24)
+        d.bulk_build(dev(base), dev(np.arange(base.size, dtype=np.uint32)))
+        k = keys(1 << 20)
+        d.insert(dev(k), dev(np.arange(k.size, dtype=np.uint32)))
+        # 1024 full-width ranges: the covered rows outweigh a compaction
+        out = torch.empty(1024, dtype=torch.int32, device="cuda")
+        d.range_count(dev(np.zeros(1024, np.uint32)), dev(np.full(1024, 0xFFFFFFFF, np.uint32)), out)
+        torch.cuda.synchronize()
+        print(json.dumps({"case": "merge", "rows": d.size()[0], "status": d.canonical_carry_status()}))
+    elif args.case == "admit":
+        d = gl.GPULSMOpt(gl.DictionaryConfig(max_elements=1 << 22, batch_capacity=1 << 20))
+        batches = [dev(keys(1 << 20)) for _ in range(8)]
+        vals = dev(np.arange(1 << 20, dtype=np.uint32))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for i in range(64):
+            d.clear()
+            d.insert(batches[i % 8], vals)
+        e1.record()
+        torch.cuda.synchronize()
+        print(json.dumps({"case": "admit", "ms_per_batch": round(e0.elapsed_time(e1) / 64, 4),
+                          "status": d.canonical_carry_status()}))
+    else:
+        base = keys(1 << 26)
+        srv = gl.Server(gl.DictionaryConfig(max_elements=(1 << 26) + (1 << 25), level_zero_capacity=1 << 17),
+                        budget_bytes=16 << 30)
+        srv.bulk_build(dev(base), torch.arange(base.size, dtype=torch.int32, device="cuda"))
+        srv.run_load(base, rate_per_s=0, seconds=0.2, seed=2)
+        st = srv.run_load(base, rate_per_s=0, seconds=0.3, seed=3)
+        srv.close()
+        print(json.dumps({"case": "serving-mix", "completed": st["completed"], "p99_us": round(st["p99_us"], 1)}))
+
+
 if __name__ == "__main__":
     a = parse()
-    if a.impl == "reference":
+    if a.case:
+        profile_case(a)
+    elif a.impl == "reference":
         run_reference(a)
     else:
         run_ours(a)

@@ -176,6 +176,8 @@ def load() -> C.CDLL:
         "gpulsm_dict_successor": (i32, [vp, vp, u64, vp, vp]),
         "gpulsm_dict_status": (i32, [vp, C.POINTER(u32)]),
         "gpulsm_dict_resident_bytes": (i32, [vp, C.POINTER(u64)]),
+        "gpulsm_dict_kernel_timing": (i32, [vp, i32]),
+        "gpulsm_dict_kernel_timing_read": (i32, [vp, C.POINTER(u64), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
         "gpulsm_dict_size": (i32, [vp, C.POINTER(u64), C.POINTER(u32)]),
         "gpulsm_flix_create": (i32, [C.POINTER(FlixConfig), pvp]),
         "gpulsm_flix_destroy": (i32, [vp]),

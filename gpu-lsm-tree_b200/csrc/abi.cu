@@ -249,6 +249,20 @@ int gpulsm_dict_resident_bytes(gpulsm_dict *d, uint64_t *out_bytes) {
   });
 }
 
+int gpulsm_dict_kernel_timing(gpulsm_dict *d, int enable) {
+  return guarded([&] {
+    need(d, "dict");
+    d->impl.set_kernel_timing(enable != 0);
+  });
+}
+
+int gpulsm_dict_kernel_timing_read(gpulsm_dict *d, uint64_t *out_launches, double *out_ms, double *out_bytes) {
+  return guarded([&] {
+    need(d, "dict");
+    d->impl.kernel_timing(out_launches, out_ms, out_bytes);
+  });
+}
+
 int gpulsm_dict_size(gpulsm_dict *d, uint64_t *out_rows, uint32_t *out_levels) {
   return guarded([&] {
     need(d, "dict");

@@ -383,6 +383,34 @@ __global__ void __launch_bounds__(kPartThreads) part_scatter_kernel(
   }
 }
 
+// Exclusive prefix of a bucket's row count over the earlier buckets.  Every
+// bucket publishes its own count (never an inclusive prefix) and reads all the
+// earlier counts at once, one thread per bucket, so once they are published
+// the wait is one round trip instead of a walk of distance / 32 round trips.
+// Waits are bounded: a count that never appears sets the timeout bit and
+// reads as 0 (the host then fails the dictionary).
+static_assert(kBuckets <= kThreads, "one thread per earlier bucket");
+__device__ __forceinline__ uint32_t bucket_prefix(unsigned long long *lb, uint32_t tile, uint32_t kept,
+                                                  uint32_t *status, RankSmem &rs) {
+  if (threadIdx.x == 0) st_relaxed_u64(lb + tile, kLbAgg | kept);
+  uint32_t v = 0;
+  if (threadIdx.x < tile) {
+    uint32_t spins = 0;
+    unsigned long long x;
+    while (((x = ld_relaxed_u64(lb + threadIdx.x)) & ~kLbMask) == 0ull) {
+      if (++spins > kMaxSpins) {
+        atomicOr(status, kDevWaitTimeout);
+        x = kLbAgg;
+        break;
+      }
+      __nanosleep(32);
+    }
+    v = uint32_t(x & kLbMask);
+  }
+  (void)block_exclusive_scan<kThreads>(v, rs.scan, &rs.total);
+  return rs.total;
+}
+
 constexpr uint32_t kBins = 4096;   // counting-sort bins of the fast path (12 key bits)
 constexpr uint32_t kMaxBin = 32;   // larger bins (skew) take the LSD passes instead
 
@@ -400,8 +428,9 @@ struct BucketSmem {
 // Fast in-bucket sort: one counting pass on the 12 highest varying key bits
 // (shared atomics: order inside a bin is arbitrary), then every bin - about
 // one element on uniform keys - is insertion-sorted by (key, input position),
-// which restores input order among equal keys.  Leaves the sorted order in
-// sm.idx; returns false (nothing changed) when a bin exceeds kMaxBin.
+// which restores input order among equal keys, and the words are permuted
+// into that order in place (through registers).  Returns false (nothing
+// changed) when a bin exceeds kMaxBin.
 __device__ __forceinline__ bool bin_sort(BucketSmem &sm, uint32_t cnt, uint32_t vary) {
   const uint32_t hb = 31u - __clz(vary);
   const uint32_t ds = hb >= 11u ? hb - 11u : 0u;
@@ -450,6 +479,20 @@ __device__ __forceinline__ bool bin_sort(BucketSmem &sm, uint32_t cnt, uint32_t 
     }
   }
   __syncthreads();
+  const uint32_t keff = (cnt + kThreads - 1) / kThreads;
+  unsigned long long t[kItems];
+#pragma unroll
+  for (int i = 0; i < kItems; ++i) {
+    const uint32_t j = uint32_t(i) * kThreads + threadIdx.x;
+    t[i] = uint32_t(i) < keff && j < cnt ? sm.words[sm.idx[j]] : 0ull;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < kItems; ++i) {
+    const uint32_t j = uint32_t(i) * kThreads + threadIdx.x;
+    if (uint32_t(i) < keff && j < cnt) sm.words[j] = t[i];
+  }
+  __syncthreads();
   return true;
 }
 constexpr size_t kBucketSmemBytes = sizeof(BucketSmem);
@@ -491,10 +534,13 @@ __global__ void __launch_bounds__(kThreads, 2) admit_bucket_kernel(
   const uint32_t s0 = sm.start[b];
   const uint32_t cnt = sm.start[b + 1] - s0;
   if (s0 > n || cnt > n - s0) {  // histogram inconsistent with the batch: refuse
-    atomicOr(status, kDevBadInput);
+    if (threadIdx.x == 0) {
+      atomicOr(status, kDevBadInput);
+      st_relaxed_u64(lb + tile, kLbAgg);  // later buckets need not wait for it
+    }
     return;
   }
-  const unsigned long long *sorted = nullptr;  // sorted words, or null when sm.idx holds the order
+  const unsigned long long *sorted;  // the bucket's words sorted by (key, input position)
   if (cnt <= kCap) {
     {  // every thread issues all its loads before its shared stores
       unsigned long long t[kItems];
@@ -527,45 +573,83 @@ __global__ void __launch_bounds__(kThreads, 2) admit_bucket_kernel(
             sm.words[pos[i]] = it[i];
         __syncthreads();
       }
-      sorted = sm.words;
     }
+    sorted = sm.words;
   } else {
     const uint32_t vary = varying_bits(words0 + s0, cnt, sm.rank) & 0x00ffffffu;
     sorted = sort_global(words0 + s0, words1 + s0, cnt, vary, sm.rank, sm.off);
     __syncthreads();
-  }
-  const auto by_array = [sorted](uint32_t j) { return sorted[j]; };
-  const auto by_index = [&sm](uint32_t j) { return sm.words[sm.idx[j]]; };
-  const uint32_t kept = sorted ? count_distinct(by_array, cnt, sm.rank) : count_distinct(by_index, cnt, sm.rank);
-  if (threadIdx.x < 32) {
-    const unsigned long long e = warp_lookback(lb, tile, kept, status);
-    if (threadIdx.x == 0) sm.g0 = e;
-  }
-  __syncthreads();
-  const unsigned long long g0 = sm.g0;
-  if (g0 + kept > n) {  // only after a timed-out look-back (status bit set)
-    atomicOr(status, kDevWaitTimeout);
-    return;
   }
   // directory share: the bucket consumed the keys [b << 24, b << 24 | 0xffffff];
   // its rows start the buckets after bucket((b << 24) - 1) (the previous
   // bucket's last key) and it closes the range up to bucket(b << 24 | 0xffffff)
   const uint32_t kmin = first << 24, kmax = (last << 24) | 0x00ffffffu;
   const DirGeom g = dir_geometry(kmin, kmax, n, dir_bits, rows_log2);
-  const int64_t bp = b > first ? int64_t((((b << 24) - 1u) - g.kmin) >> g.shift) : -1;
-  const int64_t bl = b == last ? int64_t(g.nbuckets) - 1 : int64_t((((b << 24) | 0x00ffffffu) - g.kmin) >> g.shift);
-  // an empty bucket between the first and the last one only closes its range
-  int64_t blast = bp;
-  if (sorted) {
-    write_rows(by_array, cnt, tombstone, out_keys, out_vals, out_flags, g0, sm.rank, out_dir, g, bp);
-    if (cnt) blast = int64_t((word_key(by_array(cnt - 1)) - g.kmin) >> g.shift);
+  const int32_t bp = b > first ? int32_t((((b << 24) - 1u) - g.kmin) >> g.shift) : -1;
+  const int32_t bl = b == last ? int32_t(g.nbuckets) - 1 : int32_t((((b << 24) | 0x00ffffffu) - g.kmin) >> g.shift);
+  uint32_t kept;
+  unsigned long long g0;
+  if (cnt <= kCap) {
+    // one ballot pass marks the last row of every equal-key run; a block scan
+    // gives every kept row its offset and the bucket its row count, which is
+    // published before the bucket reads the earlier buckets' counts
+    const unsigned long long *w = sm.words;
+    const uint32_t keff = (cnt + kThreads - 1) / kThreads;
+    const uint32_t lane = threadIdx.x & 31u, wi = threadIdx.x >> 5, lt = lanemask_lt();
+    uint32_t *slot = sm.rank.dstart;  // kItems * kWarps counts, then their offsets
+    static_assert(kItems * kWarps <= kBuckets, "one scan slot per (item, warp)");
+    uint32_t ends[kItems];
+#pragma unroll
+    for (int i = 0; i < kItems; ++i) {
+      ends[i] = 0u;
+      if (uint32_t(i) < keff) {
+        const uint32_t e = uint32_t(i) * kThreads + threadIdx.x;
+        ends[i] = __ballot_sync(0xffffffffu, e < cnt && (e + 1 == cnt || word_key(w[e]) != word_key(w[e + 1])));
+      }
+      if (lane == 0) slot[i * kWarps + wi] = __popc(ends[i]);
+    }
+    __syncthreads();
+    const uint32_t v = threadIdx.x < uint32_t(kItems * kWarps) ? slot[threadIdx.x] : 0u;
+    const uint32_t ex = block_exclusive_scan<kThreads>(v, sm.rank.scan, &sm.rank.total);
+    kept = sm.rank.total;
+    if (threadIdx.x < uint32_t(kItems * kWarps)) slot[threadIdx.x] = ex;
+    g0 = bucket_prefix(lb, tile, kept, status, sm.rank);  // its block scan orders the slot stores
+    if (g0 + kept > n) {  // only after a timed-out wait (status bit set)
+      atomicOr(status, kDevWaitTimeout);
+      return;
+    }
+#pragma unroll
+    for (int i = 0; i < kItems; ++i)
+      if (uint32_t(i) < keff && ((ends[i] >> lane) & 1u)) {
+        const uint32_t e = uint32_t(i) * kThreads + threadIdx.x;
+        const unsigned long long w64 = w[e];
+        const unsigned long long r = g0 + slot[i * kWarps + wi] + __popc(ends[i] & lt);
+        const uint32_t k = word_key(w64);
+        out_keys[r] = k;
+        out_vals[r] = uint32_t(w64);  // the tombstone value was packed for erase batches
+        out_flags[r] = tombstone ? kFlagTomb : uint8_t(0);
+        uint32_t p = e;  // first element of this key's run
+        while (p > 0 && word_key(w[p - 1]) == k) --p;
+        const int32_t bprev = p > 0 ? int32_t((word_key(w[p - 1]) - g.kmin) >> g.shift) : bp;
+        const int32_t bj = int32_t((k - g.kmin) >> g.shift);
+        for (int32_t bb = bprev + 1; bb <= bj; ++bb)
+          if (GPULSM_OK(bb >= 0 && bb < int32_t(g.nbuckets), 10, bb)) out_dir[bb] = uint32_t(r);
+      }
   } else {
-    write_rows(by_index, cnt, tombstone, out_keys, out_vals, out_flags, g0, sm.rank, out_dir, g, bp);
-    if (cnt) blast = int64_t((word_key(by_index(cnt - 1)) - g.kmin) >> g.shift);
+    const auto by_array = [sorted](uint32_t j) { return sorted[j]; };
+    kept = count_distinct(by_array, cnt, sm.rank);
+    g0 = bucket_prefix(lb, tile, kept, status, sm.rank);
+    if (g0 + kept > n) {  // only after a timed-out wait (status bit set)
+      atomicOr(status, kDevWaitTimeout);
+      return;
+    }
+    write_rows(by_array, cnt, tombstone, out_keys, out_vals, out_flags, g0, sm.rank, out_dir, g, int64_t(bp));
   }
   if (threadIdx.x == 0) {
-    for (int64_t bb = blast + 1; bb <= bl; ++bb)
-      if (GPULSM_OK(bb >= 0 && bb < int64_t(g.nbuckets), 13, bb)) out_dir[bb] = uint32_t(g0 + kept);
+    // an empty bucket between the first and the last one only closes its range
+    const int32_t blast = cnt ? int32_t((word_key(sorted[cnt - 1]) - g.kmin) >> g.shift) : bp;
+    for (int32_t bb = blast + 1; bb <= bl; ++bb)
+      if (GPULSM_OK(bb >= 0 && bb < int32_t(g.nbuckets), 13, bb)) out_dir[bb] = uint32_t(g0 + kept);
     if (b == last) out_dir[g.nbuckets] = uint32_t(g0 + kept);
   }
   if (b == first && threadIdx.x == 0) {

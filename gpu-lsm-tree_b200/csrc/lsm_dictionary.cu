@@ -204,6 +204,12 @@ LsmDictionary::~LsmDictionary() {
   if (dev_status_) cudaFree(dev_status_);
   if (receipt_host_) cudaFreeHost(receipt_host_);
   if (prefix_) cudaFree(prefix_);
+  if (trace_dev_) cudaFree(trace_dev_);
+  for (auto &t : traces_) {
+    cudaEventDestroy(t.start);
+    cudaEventDestroy(t.stop);
+  }
+  for (cudaEvent_t e : spare_events_) cudaEventDestroy(e);
   for (auto &lp : live_)
     if (lp.p) cudaFree(lp.p);
   if (width_) cudaFree(width_);
@@ -212,9 +218,19 @@ LsmDictionary::~LsmDictionary() {
   if (receipt_event_) cudaEventDestroy(receipt_event_);
 }
 
-void LsmDictionary::begin_op(cudaStream_t s) { GPULSM_CUDA(cudaStreamWaitEvent(s, op_done_, 0)); }
+// Operations are ordered by op_done_ across streams; on the stream of the
+// previous operation the stream order already holds (not for the per-thread
+// default stream, whose handle names a different stream in every thread).
+void LsmDictionary::begin_op(cudaStream_t s) {
+  if (last_stream_known_ && s == last_stream_ && s != cudaStreamPerThread) return;
+  GPULSM_CUDA(cudaStreamWaitEvent(s, op_done_, 0));
+}
 
-void LsmDictionary::end_op(cudaStream_t s) { GPULSM_CUDA(cudaEventRecord(op_done_, s)); }
+void LsmDictionary::end_op(cudaStream_t s) {
+  GPULSM_CUDA(cudaEventRecord(op_done_, s));
+  last_stream_ = s;
+  last_stream_known_ = true;
+}
 
 void *LsmDictionary::scratch(size_t bytes, cudaStream_t s) {
   bytes = align_up(std::max<size_t>(bytes, kAlign));
@@ -248,7 +264,13 @@ void LsmDictionary::ensure_sort_space(uint64_t n, cudaStream_t s) {
   words_cap_ = cap;
 }
 
+// A receipt still in flight is enough while no level's row bound exceeds the
+// capacity (only then can a receipt reveal an overflow): the host keeps
+// planning with upper bounds and applies the pending receipt when it lands.
 void LsmDictionary::post_receipt(cudaStream_t s) {
+  uint64_t largest = 0;
+  for (const auto &l : levels_) largest = std::max<uint64_t>(largest, l.upper);
+  if (receipt_pending_ && largest <= budget_) return;
   ReceiptSrc src{};
   src.count = uint32_t(levels_.size());
   for (size_t i = 0; i < levels_.size(); ++i) {
@@ -385,11 +407,29 @@ RunBuffer *LsmDictionary::merge(RunBuffer *newer, RunBuffer *older, uint64_t out
                  static_cast<const uint32_t *>(older->keys), static_cast<const lsm::LevelDesc *>(older->desc), parts,
                  uint32_t(tiles + 1), zero, uint32_t(zero_bytes / 8));
   auto kernel = drop_tombstones ? lsm::merge_kernel<true> : lsm::merge_kernel<false>;
+  unsigned long long *trace = nullptr;
+  MergeTrace tr{};
+  if (timing_ && traces_.size() < kMaxTraces) {
+    trace = trace_dev_ + 4 * traces_.size();
+    for (cudaEvent_t *e : {&tr.start, &tr.stop}) {
+      if (!spare_events_.empty()) {
+        *e = spare_events_.back();
+        spare_events_.pop_back();
+      } else {
+        GPULSM_CUDA(cudaEventCreate(e));
+      }
+    }
+    GPULSM_CUDA(cudaEventRecord(tr.start, s));
+  }
   launch_chained(kernel, unsigned(tiles), lsm::kMergeThreads, 0, s, newer->keys, newer->vals, newer->flags,
                  newer->desc, older->keys, older->vals, older->flags, older->desc, out->keys, out->vals, out->flags,
                  out->desc, out->dir, out->dir_bits, rows_log2_,
                  static_cast<unsigned long long>(std::min<uint64_t>(out_upper, out->cap)),
-                 static_cast<unsigned long long>(out->cap), parts, lb, counter, dev_status_);
+                 static_cast<unsigned long long>(out->cap), parts, lb, counter, dev_status_, trace);
+  if (trace) {
+    GPULSM_CUDA(cudaEventRecord(tr.stop, s));
+    traces_.push_back(tr);
+  }
   pool_.release(newer);
   pool_.release(older);
   return out;
@@ -849,6 +889,38 @@ uint32_t LsmDictionary::status() {
   GPULSM_CUDA(cudaMemcpy(&bits, dev_status_, 4, cudaMemcpyDeviceToHost));
   status_bits_ |= bits;
   return status_bits_;
+}
+
+void LsmDictionary::set_kernel_timing(bool on) {
+  std::lock_guard<std::mutex> g(mu_);
+  if (on && !trace_dev_) GPULSM_CUDA(cudaMalloc(&trace_dev_, kMaxTraces * 4 * sizeof(unsigned long long)));
+  timing_ = on;
+}
+
+// Sum over the merges timed since the last read: launches, device time and
+// algorithmic bytes (9 B per row read from either input - key, value, flag -
+// 9 B per row written, 4 B per directory entry written).  Synchronises.
+void LsmDictionary::kernel_timing(uint64_t *launches, double *total_ms, double *bytes) {
+  std::lock_guard<std::mutex> g(mu_);
+  const size_t m = traces_.size();
+  double ms = 0, b = 0;
+  if (m) {
+    GPULSM_CUDA(cudaEventSynchronize(traces_.back().stop));
+    std::vector<unsigned long long> t(4 * m);
+    GPULSM_CUDA(cudaMemcpy(t.data(), trace_dev_, t.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < m; ++i) {
+      float e = 0;
+      GPULSM_CUDA(cudaEventElapsedTime(&e, traces_[i].start, traces_[i].stop));
+      ms += e;
+      b += 9.0 * double(t[4 * i] + t[4 * i + 1]) + 9.0 * double(t[4 * i + 2]) + 4.0 * double(t[4 * i + 3] + 1);
+      spare_events_.push_back(traces_[i].start);
+      spare_events_.push_back(traces_[i].stop);
+    }
+    traces_.clear();
+  }
+  if (launches) *launches = m;
+  if (total_ms) *total_ms = ms;
+  if (bytes) *bytes = b;
 }
 
 uint64_t LsmDictionary::resident_bytes() {

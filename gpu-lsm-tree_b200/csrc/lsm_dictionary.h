@@ -90,6 +90,10 @@ class LsmDictionary {
   void successor(const uint32_t *queries, uint64_t n, uint32_t *out_keys, cudaStream_t s);
   uint32_t status();
   uint64_t resident_bytes();
+  // Kernel timing of the merge launches (CUDA events on the launching stream
+  // around each merge kernel, plus the rows it read and wrote).
+  void set_kernel_timing(bool on);
+  void kernel_timing(uint64_t *launches, double *total_ms, double *bytes);
   void size(uint64_t *rows, uint32_t *levels);
 
   // Introspection for tests and benchmarks.
@@ -177,7 +181,17 @@ class LsmDictionary {
   uint32_t status_bits_ = 0;
   bool failed_ = false;
   std::string failure_;
+  struct MergeTrace {
+    cudaEvent_t start, stop;
+  };
+  bool timing_ = false;
+  std::vector<MergeTrace> traces_;           // events of the merges timed so far
+  std::vector<cudaEvent_t> spare_events_;
+  unsigned long long *trace_dev_ = nullptr;  // 4 words per timed merge
+  static constexpr size_t kMaxTraces = 8192;
   cudaEvent_t op_done_ = nullptr;
+  cudaStream_t last_stream_ = nullptr;  // stream of the last operation (op_done_ was recorded there)
+  bool last_stream_known_ = false;
   mutable std::mutex mu_;
 };
 

@@ -303,7 +303,7 @@ __global__ void __launch_bounds__(kMergeThreads, 4) merge_kernel(
     uint8_t *__restrict__ of, LevelDesc *__restrict__ odesc, uint32_t *__restrict__ odir, uint32_t dir_bits,
     uint32_t rows_log2, unsigned long long out_upper, unsigned long long out_capacity,
     const unsigned long long *__restrict__ parts, unsigned long long *__restrict__ lb,
-    uint32_t *__restrict__ tile_counter, uint32_t *__restrict__ status) {
+    uint32_t *__restrict__ tile_counter, uint32_t *__restrict__ status, unsigned long long *__restrict__ trace) {
   __shared__ uint32_t s_key[kMergeTile];   // A segment, then B segment
   __shared__ uint32_t s_out[kMergeTile];   // compacted output keys
   __shared__ uint16_t s_src[kMergeTile];   // tile-local source index of each kept row
@@ -466,6 +466,12 @@ __global__ void __launch_bounds__(kMergeThreads, 4) merge_kernel(
   if (last_tile && threadIdx.x == 0) {
     if (n_out > out_capacity) atomicOr(status, kDevOutputOverflow);
     odesc->n = n_out < out_capacity ? n_out : out_capacity;
+    if (trace) {  // kernel timing: the rows this launch read and wrote
+      trace[0] = na;
+      trace[1] = nb;
+      trace[2] = n_out < out_capacity ? n_out : out_capacity;
+      trace[3] = geom.nbuckets;
+    }
   }
 }
 

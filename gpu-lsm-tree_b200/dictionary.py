@@ -153,6 +153,16 @@ class GPULSMOpt:
         N.check(self._lib.gpulsm_dict_resident_bytes(self._h, C.byref(v)))
         return int(v.value)
 
+    def kernel_timing(self, enable: bool) -> None:
+        """Bracket every merge kernel launch with CUDA events (measurement hook)."""
+        N.check(self._lib.gpulsm_dict_kernel_timing(self._h, 1 if enable else 0))
+
+    def kernel_timing_read(self) -> dict:
+        """Merges timed since the last read: launches, summed device ms, algorithmic bytes."""
+        n, ms, b = C.c_uint64(), C.c_double(), C.c_double()
+        N.check(self._lib.gpulsm_dict_kernel_timing_read(self._h, C.byref(n), C.byref(ms), C.byref(b)))
+        return {"launches": int(n.value), "ms": float(ms.value), "bytes": float(b.value)}
+
     def size(self) -> tuple[int, int]:
         rows, levels = C.c_uint64(), C.c_uint32()
         N.check(self._lib.gpulsm_dict_size(self._h, C.byref(rows), C.byref(levels)))

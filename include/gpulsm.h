@@ -117,6 +117,15 @@ int gpulsm_dict_status(gpulsm_dict *dict, uint32_t *out_status);
 int gpulsm_dict_resident_bytes(gpulsm_dict *dict, uint64_t *out_bytes);
 /* Number of live rows (synchronises; diagnostics). */
 int gpulsm_dict_size(gpulsm_dict *dict, uint64_t *out_rows, uint32_t *out_levels);
+/* Measurement hook (no reference counterpart): while enabled, every merge
+ * kernel launch is bracketed by CUDA events on its stream and records the
+ * rows it read and wrote.  _read (synchronises) returns, over the merges
+ * timed since the previous read, the launch count, the summed device time in
+ * ms and the algorithmic bytes (9 B per row read, 9 B per row written, 4 B
+ * per directory entry). */
+int gpulsm_dict_kernel_timing(gpulsm_dict *dict, int enable);
+int gpulsm_dict_kernel_timing_read(gpulsm_dict *dict, uint64_t *out_launches, double *out_ms,
+                                   double *out_bytes);
 
 /* ===================== FliX bucket layer ================================== */
 typedef struct gpulsm_flix gpulsm_flix;
