@@ -421,7 +421,8 @@ RunBuffer *LsmDictionary::merge(RunBuffer *newer, RunBuffer *older, uint64_t out
     }
     GPULSM_CUDA(cudaEventRecord(tr.start, s));
   }
-  launch_chained(kernel, unsigned(tiles), lsm::kMergeThreads, 0, s, newer->keys, newer->vals, newer->flags,
+  launch_chained(kernel, unsigned(tiles), lsm::kMergeThreads, lsm::kMergeSmemBytes, s, newer->keys, newer->vals,
+                 newer->flags,
                  newer->desc, older->keys, older->vals, older->flags, older->desc, out->keys, out->vals, out->flags,
                  out->desc, out->dir, out->dir_bits, rows_log2_,
                  static_cast<unsigned long long>(std::min<uint64_t>(out_upper, out->cap)),

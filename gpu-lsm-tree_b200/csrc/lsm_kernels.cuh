@@ -224,12 +224,12 @@ __global__ void __launch_bounds__(kCompactThreads) dedup_last_kernel(
 // key was just taken from A is shadowed and dropped (newest level wins).  With
 // drop_tombstones (the output becomes the oldest level) tombstones disappear.
 //
-// Only keys (and, when tombstones drop, flags) are staged in shared memory.
-// Each thread merges kMergeItems consecutive outputs with the two run heads
-// cached in registers and records the tile-local source index of every kept
-// row; a block scan compacts them; the rows are then written in striped
-// order, gathering values and flags from global memory (consecutive outputs
-// come from consecutive source rows, so those loads stay coalesced).  An odd
+// The tile's input slices (keys, values, flags) arrive in shared memory by
+// bulk copies.  Each thread merges kMergeItems consecutive outputs with the
+// two run heads cached in registers and records the tile-local source index
+// of every kept row; a block scan compacts them; the kept rows are gathered
+// in striped order, staged at the alignment of their output position and
+// written by bulk stores (plus a few unaligned head and tail rows).  An odd
 // item count keeps the threads' starting diagonals in distinct banks.
 constexpr int kMergeThreads = 256;
 constexpr int kMergeItems = 15;
@@ -294,6 +294,58 @@ __global__ void __launch_bounds__(256) merge_partition_kernel(const uint32_t *__
   if (lane == 0) parts[split] = lo;
 }
 
+// Shared memory of one merge tile.  The two input slices arrive by bulk
+// copies (16-byte aligned chunks, so a slice starts 0-3 keys / 0-15 flags into
+// its chunk); after the gather the same arrays stage the output rows at the
+// alignment of their global position, for bulk stores of the aligned middle.
+struct MergeSmem {
+  uint32_t key[kMergeTile + 16];  // A chunk, then B chunk (each at most slice + 6 keys)
+  uint32_t val[kMergeTile + 16];
+  uint8_t flag[kMergeTile + 64];  // A chunk, then B chunk (each at most slice + 30 flags)
+  uint16_t src[kMergeTile];       // tile-local source index of each kept row
+  uint32_t scan[kMergeThreads / 32];
+  uint32_t total;
+  uint32_t tile;
+  unsigned long long base;
+  unsigned long long bar;         // mbarrier of the input copies
+};
+constexpr size_t kMergeSmemBytes = sizeof(MergeSmem);
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_store(void *dst, const void *src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_addr(src)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait for the input copies; false (and the status bit) on timeout.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t *status) {
+  for (uint32_t spins = 0; !mbar_test(bar, 0); ++spins) {
+    if (spins > kMaxSpins) {
+      atomicOr(status, kDevWaitTimeout);
+      return false;
+    }
+    __nanosleep(20);
+  }
+  return true;
+}
+
 template <bool kDropTombstones>
 __global__ void __launch_bounds__(kMergeThreads, 4) merge_kernel(
     const uint32_t *__restrict__ ak, const uint32_t *__restrict__ av, const uint8_t *__restrict__ af,
@@ -304,19 +356,13 @@ __global__ void __launch_bounds__(kMergeThreads, 4) merge_kernel(
     uint32_t rows_log2, unsigned long long out_upper, unsigned long long out_capacity,
     const unsigned long long *__restrict__ parts, unsigned long long *__restrict__ lb,
     uint32_t *__restrict__ tile_counter, uint32_t *__restrict__ status, unsigned long long *__restrict__ trace) {
-  __shared__ uint32_t s_key[kMergeTile];   // A segment, then B segment
-  __shared__ uint32_t s_out[kMergeTile];   // compacted output keys
-  __shared__ uint16_t s_src[kMergeTile];   // tile-local source index of each kept row
-  __shared__ uint8_t s_flag[kDropTombstones ? kMergeTile : 1];
-  __shared__ uint32_t s_scan[kMergeThreads / 32];
-  __shared__ uint32_t s_total;
-  __shared__ uint32_t s_tile;
-  __shared__ unsigned long long s_base;
+  extern __shared__ __align__(128) unsigned char merge_dyn[];
+  MergeSmem &sm = *reinterpret_cast<MergeSmem *>(merge_dyn);
   chain_wait();
-  if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
+  if (threadIdx.x == 0) sm.tile = atomicAdd(tile_counter, 1u);
   __syncthreads();
   const uint64_t na = adesc->n, nb = bdesc->n, total = na + nb;
-  const uint32_t tile = s_tile;
+  const uint32_t tile = sm.tile;
   const uint64_t d0 = uint64_t(tile) * kMergeTile;
   if (total == 0) {
     if (tile == 0 && threadIdx.x == 0) write_empty_desc(odesc, odir);
@@ -324,35 +370,38 @@ __global__ void __launch_bounds__(kMergeThreads, 4) merge_kernel(
   }
   if (d0 >= total) return;  // beyond the merged length (grid sized for an upper bound)
   const uint64_t d1 = min(d0 + kMergeTile, total);
+  const uint64_t a0 = parts[tile], a1 = parts[tile + 1], b0 = d0 - a0, b1 = d1 - a1;
+  const uint32_t alen = uint32_t(a1 - a0), blen = uint32_t(b1 - b0), len = alen + blen;
+  // input chunks: [x0 & ~3, (x1 + 3) & ~3) keys/values and [x0 & ~15, (x1 + 15) & ~15)
+  // flags; every run buffer's capacity is a multiple of 16 rows, so the
+  // rounded-up ends stay inside the allocations
+  const uint32_t oa = uint32_t(a0) & 3u, ob = uint32_t(b0) & 3u, fa = uint32_t(a0) & 15u, fb = uint32_t(b0) & 15u;
+  const uint32_t la = alen ? uint32_t(((a1 + 3) & ~3ull) - (a0 & ~3ull)) : 0u;
+  const uint32_t lbn = blen ? uint32_t(((b1 + 3) & ~3ull) - (b0 & ~3ull)) : 0u;
+  const uint32_t fla = alen ? uint32_t(((a1 + 15) & ~15ull) - (a0 & ~15ull)) : 0u;
+  const uint32_t flb = blen ? uint32_t(((b1 + 15) & ~15ull) - (b0 & ~15ull)) : 0u;
+  const uint32_t bar = smem_addr(&sm.bar);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    const uint32_t bytes = 8u * (la + lbn) + fla + flb;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+    if (alen) {
+      bulk_load(sm.key, ak + (a0 & ~3ull), 4u * la, bar);
+      bulk_load(sm.val, av + (a0 & ~3ull), 4u * la, bar);
+      bulk_load(sm.flag, af + (a0 & ~15ull), fla, bar);
+    }
+    if (blen) {
+      bulk_load(sm.key + la, bk + (b0 & ~3ull), 4u * lbn, bar);
+      bulk_load(sm.val + la, bv + (b0 & ~3ull), 4u * lbn, bar);
+      bulk_load(sm.flag + fla, bf + (b0 & ~15ull), flb, bar);
+    }
+  }
+  // while the copies fly: the keys around the tile, the output geometry
   // every output key lies in the union of the inputs' key ranges
   const uint32_t kmin = na == 0 ? bdesc->kmin : nb == 0 ? adesc->kmin : min(adesc->kmin, bdesc->kmin);
   const uint32_t kmax = na == 0 ? bdesc->kmax : nb == 0 ? adesc->kmax : max(adesc->kmax, bdesc->kmax);
   const DirGeom geom = dir_geometry(kmin, kmax, out_upper, dir_bits, rows_log2);
-  const uint64_t a0 = parts[tile], a1 = parts[tile + 1], b0 = d0 - a0, b1 = d1 - a1;
-  const uint32_t alen = uint32_t(a1 - a0), blen = uint32_t(b1 - b0), len = alen + blen;
-  const uint32_t *kA = ak + a0, *kB = bk + b0;
-  // stage the tile's keys: every thread issues all its loads before its stores
-  {
-    uint32_t k[kMergeItems];
-#pragma unroll
-    for (int i = 0; i < kMergeItems; ++i) {
-      const uint32_t j = uint32_t(i) * kMergeThreads + threadIdx.x;
-      k[i] = j < len ? *(j < alen ? kA + j : kB + (j - alen)) : 0u;
-    }
-#pragma unroll
-    for (int i = 0; i < kMergeItems; ++i) {
-      const uint32_t j = uint32_t(i) * kMergeThreads + threadIdx.x;
-      if (j < len) s_key[j] = k[i];
-    }
-    if (kDropTombstones) {
-      const uint8_t *fA = af + a0, *fB = bf + b0;
-#pragma unroll
-      for (int i = 0; i < kMergeItems; ++i) {
-        const uint32_t j = uint32_t(i) * kMergeThreads + threadIdx.x;
-        if (j < len) s_flag[j] = *(j < alen ? fA + j : fB + (j - alen));
-      }
-    }
-  }
   // key of the A row just before this tile (shadows a leading B row); the
   // largest key consumed before / by this tile bounds its directory buckets
   const bool has_prev_a = a0 > 0;
@@ -360,17 +409,24 @@ __global__ void __launch_bounds__(kMergeThreads, 4) merge_kernel(
   const bool has_prev = a0 > 0 || b0 > 0;
   const uint32_t prev_key = max(has_prev_a ? prev_a_global : 0u, b0 > 0 ? bk[b0 - 1] : 0u);
   const uint32_t last_key = max(a1 > 0 ? ak[a1 - 1] : 0u, b1 > 0 ? bk[b1 - 1] : 0u);
-  __syncthreads();
+  __syncthreads();  // the barrier is initialised before anyone waits on it
+  if (!mbar_wait(bar, status)) {
+    (void)mbar_wait(bar, status);  // a second bounded wait for copies still in flight
+    return;
+  }
+  const uint32_t *sA = sm.key + oa, *sB = sm.key + la + ob;
+  const uint32_t *vA = sm.val + oa, *vB = sm.val + la + ob;
+  const uint8_t *gA = sm.flag + fa, *gB = sm.flag + fla + fb;
   // serial merge of this thread's outputs, branch-free: one shared load per
   // output (the new head of the side that advanced)
   const uint32_t my_d = min(uint32_t(threadIdx.x) * kMergeItems, len);
   const uint32_t my_n = min(uint32_t(kMergeItems), len - my_d);
-  uint32_t ai = merge_path32(s_key, alen, s_key + alen, blen, my_d);
+  const uint32_t amax = alen ? alen - 1 : 0u, bmax = blen ? blen - 1 : 0u;
+  uint32_t ai = merge_path32(sA, alen, sB, blen, my_d);
   uint32_t bi = my_d - ai;
   bool hp = ai > 0 ? true : has_prev_a;
-  uint32_t prev = ai > 0 ? s_key[ai - 1] : prev_a_global;
-  const uint32_t last = len ? len - 1 : 0;
-  uint32_t ka = s_key[min(ai, last)], kb = s_key[min(alen + bi, last)];
+  uint32_t prev = ai > 0 ? sA[ai - 1] : prev_a_global;
+  uint32_t ka = sA[min(ai, amax)], kb = sB[min(bi, bmax)];
   uint16_t src[kMergeItems];
   uint32_t keep_mask = 0;
 #pragma unroll
@@ -378,29 +434,27 @@ __global__ void __launch_bounds__(kMergeThreads, 4) merge_kernel(
     const bool ta = ai < alen && (bi >= blen || ka <= kb);
     const uint32_t idx = ta ? ai : alen + bi;
     const bool shadow = !ta && hp && prev == kb;
+    bool keep = uint32_t(i) < my_n && !shadow;
+    if (kDropTombstones) keep = keep && !(*(ta ? gA + min(ai, amax) : gB + min(bi, bmax)) & kFlagTomb);
     hp = hp || ta;
     prev = ta ? ka : prev;
     ai += ta ? 1u : 0u;
     bi += ta ? 0u : 1u;
-    const uint32_t nxt = s_key[min(ta ? ai : alen + bi, last)];
+    const uint32_t nxt = *(ta ? sA + min(ai, amax) : sB + min(bi, bmax));
     ka = ta ? nxt : ka;
     kb = ta ? kb : nxt;
-    bool keep = uint32_t(i) < my_n && !shadow;
-    if (kDropTombstones) keep = keep && !(s_flag[min(idx, last)] & kFlagTomb);
     src[i] = uint16_t(idx);
     keep_mask |= keep ? (1u << i) : 0u;
   }
-  uint32_t o = block_exclusive_scan<kMergeThreads>(uint32_t(__popc(keep_mask)), s_scan, &s_total);
-  const uint32_t tile_kept = s_total;
+  uint32_t o = block_exclusive_scan<kMergeThreads>(uint32_t(__popc(keep_mask)), sm.scan, &sm.total);
+  const uint32_t tile_kept = sm.total;
   if (threadIdx.x == 0) lookback_publish(lb, tile, tile_kept);  // successors may proceed
 #pragma unroll
   for (int i = 0; i < kMergeItems; ++i)
-    if (keep_mask & (1u << i)) s_src[o++] = src[i];
+    if (keep_mask & (1u << i)) sm.src[o++] = src[i];
   __syncthreads();
-  // striped output: gather values and flags (their latency overlaps the
-  // look-back walk), then store at the tile's global offset
-  const uint32_t *vA = av + a0, *vB = bv + b0;
-  const uint8_t *fA = af + a0, *fB = bf + b0;
+  // gather the kept rows (striped) from the staged inputs; the look-back walk
+  // runs after the gathers are issued
   uint32_t rk[kMergeItems], rv[kMergeItems];
   uint8_t rf[kMergeItems];
 #pragma unroll
@@ -410,68 +464,99 @@ __global__ void __launch_bounds__(kMergeThreads, 4) merge_kernel(
     rv[i] = 0;
     rf[i] = 0;
     if (j < tile_kept) {
-      const uint32_t sidx = s_src[j];
+      const uint32_t sidx = sm.src[j];
       const bool in_a = sidx < alen;
       const uint32_t off = in_a ? sidx : sidx - alen;
-      rk[i] = s_key[sidx];
-      rv[i] = *((in_a ? vA : vB) + off);
-      rf[i] = *((in_a ? fA : fB) + off);
-      s_out[j] = rk[i];
+      rk[i] = (in_a ? sA : sB)[off];
+      rv[i] = (in_a ? vA : vB)[off];
+      rf[i] = (in_a ? gA : gB)[off];
     }
   }
   if (threadIdx.x < 32) {
     const unsigned long long e = lookback_walk(lb, tile, tile_kept, status);
-    if (threadIdx.x == 0) s_base = e;
+    if (threadIdx.x == 0) sm.base = e;
   }
-  __syncthreads();
-  const unsigned long long gbase = s_base;
-  const unsigned long long space = gbase < out_capacity ? out_capacity - gbase : 0ull;
-  const uint32_t room = space < tile_kept ? uint32_t(space) : tile_kept;
-  uint32_t *okb = ok + gbase, *ovb = ov + gbase;
-  uint8_t *ofb = of + gbase;
-  // rows, and the directory entries they start: row j owns the buckets
-  // (bucket(key j-1), bucket(key j)] (the tile's first row starts after the
-  // bucket of the key consumed before the tile), as in fill_directory
-  const uint32_t gk = geom.kmin, gs = geom.shift;
-  const int32_t bp = has_prev ? int32_t((prev_key - gk) >> gs) : -1;
-  const uint32_t g0 = uint32_t(gbase);
+  __syncthreads();  // every gather is done: the arrays now stage the output
+  const unsigned long long gbase = sm.base;
+  const uint32_t o4 = uint32_t(gbase) & 3u, o16 = uint32_t(gbase) & 15u;
 #pragma unroll
   for (int i = 0; i < kMergeItems; ++i) {
     const uint32_t j = uint32_t(i) * kMergeThreads + threadIdx.x;
-    if (j < room) {
-      okb[j] = rk[i];
-      ovb[j] = rv[i];
-      ofb[j] = rf[i];
+    if (j < tile_kept) {
+      sm.key[o4 + j] = rk[i];
+      sm.val[o4 + j] = rv[i];
+      sm.flag[o16 + j] = rf[i];
     }
+  }
+  __syncthreads();
+  const unsigned long long space = gbase < out_capacity ? out_capacity - gbase : 0ull;
+  const uint32_t room = space < tile_kept ? uint32_t(space) : tile_kept;
+  // rows [h, h + m) start and end on 16-byte boundaries of the output arrays
+  const uint32_t h4 = (4u - o4) & 3u, m4 = room > h4 ? ((room - h4) & ~3u) : 0u;
+  const uint32_t h16 = (16u - o16) & 15u, m16 = room > h16 ? ((room - h16) & ~15u) : 0u;
+  if (threadIdx.x == 0) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (m4) {
+      bulk_store(ok + gbase + h4, sm.key + o4 + h4, 4u * m4);
+      bulk_store(ov + gbase + h4, sm.val + o4 + h4, 4u * m4);
+    }
+    if (m16) bulk_store(of + gbase + h16, sm.flag + o16 + h16, m16);
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+  }
+  {  // the unaligned head and tail rows
+    const uint32_t t = threadIdx.x;
+    if (t < 8) {
+      const uint32_t j = t < 4 ? t : h4 + m4 + (t - 4);
+      if (j < room && (t < 4 ? j < h4 : true)) {
+        ok[gbase + j] = sm.key[o4 + j];
+        ov[gbase + j] = sm.val[o4 + j];
+      }
+    } else if (t >= 32 && t < 64) {
+      const uint32_t u = t - 32;
+      const uint32_t j = u < 16 ? u : h16 + m16 + (u - 16);
+      if (j < room && (u < 16 ? j < h16 : true)) of[gbase + j] = sm.flag[o16 + j];
+    }
+  }
+  // directory entries: row j owns the buckets (bucket(key j-1), bucket(key j)]
+  // (the tile's first row starts after the bucket of the key consumed before
+  // the tile), as in fill_directory
+  const uint32_t gk = geom.kmin, gs = geom.shift;
+  const int32_t bp = has_prev ? int32_t((prev_key - gk) >> gs) : -1;
+  const uint32_t g0 = uint32_t(gbase);
+  const uint32_t *sout = sm.key + o4;
+#pragma unroll
+  for (int i = 0; i < kMergeItems; ++i) {
+    const uint32_t j = uint32_t(i) * kMergeThreads + threadIdx.x;
     if (j < tile_kept) {
       const int32_t bj = int32_t((rk[i] - gk) >> gs);
-      const int32_t bprev = j ? int32_t((s_out[j - 1] - gk) >> gs) : bp;
-      for (int32_t b = bprev + 1; b <= bj; ++b) odir[b] = g0 + j;
+      const int32_t bprev = j ? int32_t((sout[j - 1] - gk) >> gs) : bp;
+      for (int32_t bb = bprev + 1; bb <= bj; ++bb) odir[bb] = g0 + j;
     }
   }
   const bool last_tile = d1 == total;
   const unsigned long long n_out = gbase + tile_kept;
   if (threadIdx.x == 0) {
-    const int32_t blast = tile_kept ? int32_t((s_out[tile_kept - 1] - gk) >> gs) : bp;
+    const int32_t blast = tile_kept ? int32_t((sout[tile_kept - 1] - gk) >> gs) : bp;
     const int32_t bl = last_tile ? int32_t(geom.nbuckets) - 1 : int32_t((last_key - gk) >> gs);
-    for (int32_t b = blast + 1; b <= bl; ++b) odir[b] = g0 + tile_kept;
+    for (int32_t bb = blast + 1; bb <= bl; ++bb) odir[bb] = g0 + tile_kept;
     if (last_tile) odir[geom.nbuckets] = uint32_t(n_out < out_capacity ? n_out : out_capacity);
-  }
-  if (tile == 0 && threadIdx.x == 0) {
-    odesc->kmin = geom.kmin;
-    odesc->kmax = geom.kmax;
-    odesc->shift = geom.shift;
-    odesc->nbuckets = geom.nbuckets;
-  }
-  if (last_tile && threadIdx.x == 0) {
-    if (n_out > out_capacity) atomicOr(status, kDevOutputOverflow);
-    odesc->n = n_out < out_capacity ? n_out : out_capacity;
-    if (trace) {  // kernel timing: the rows this launch read and wrote
-      trace[0] = na;
-      trace[1] = nb;
-      trace[2] = n_out < out_capacity ? n_out : out_capacity;
-      trace[3] = geom.nbuckets;
+    if (tile == 0) {
+      odesc->kmin = geom.kmin;
+      odesc->kmax = geom.kmax;
+      odesc->shift = geom.shift;
+      odesc->nbuckets = geom.nbuckets;
     }
+    if (last_tile) {
+      if (n_out > out_capacity) atomicOr(status, kDevOutputOverflow);
+      odesc->n = n_out < out_capacity ? n_out : out_capacity;
+      if (trace) {  // kernel timing: the rows this launch read and wrote
+        trace[0] = na;
+        trace[1] = nb;
+        trace[2] = n_out < out_capacity ? n_out : out_capacity;
+        trace[3] = geom.nbuckets;
+      }
+    }
+    asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");  // stores done before the CTA retires
   }
 }
 
