@@ -37,8 +37,10 @@ sys.path.insert(0, ROOT)
 
 METRIC = "M lookups/s & M inserted keys/s at 2^26 keys vs plain form; p50/p99 request latency"
 # DRAM bytes (read + write) of merge_kernel per algorithmic byte, from an ncu
-# capture of a 21M-row merge whose output exceeds L2; None until captured
-MERGE_TRAFFIC_RATIO = None
+# capture of `bench.py --case merge` (one 17.8M-row merge: 160.3 MB read,
+# 126.8 MB written against 328.6 MB algorithmic; the rest of the writes were
+# still in L2 when the kernel ended)
+MERGE_TRAFFIC_RATIO = 0.874
 LOOKUP_BYTES = 41  # algorithmic bytes per u32 point lookup (query + value + found + one row sector)
 INSERT_BYTES = 16  # per inserted (key, value): read 8 + write 8 into the structure
 DELETE_BYTES = 12
@@ -697,7 +699,7 @@ def profile_case(args):
     merge       a 2^24-key level plus one 2^20-key batch, then full-width
                 range counts that compact both into one: a single 17M-row merge
                 whose inputs and output exceed L2;
-    admit       64 x (clear + insert of a 2^20-key batch): the admission
+    admit       8 + 64 x (clear + insert of a 2^20-key batch): the admission
                 kernels alone, no merges;
     serving-mix the serving loop over 2^26 keys, closed loop for 0.3 s with
                 the default request mix."""
@@ -727,6 +729,9 @@ def profile_case(args):
         d = gl.GPULSMOpt(gl.DictionaryConfig(max_elements=1 << 22, batch_capacity=1 << 20))
         batches = [dev(keys(1 << 20)) for _ in range(8)]
         vals = dev(np.arange(1 << 20, dtype=np.uint32))
+        for i in range(8):  # buffers allocated, kernels loaded
+            d.clear()
+            d.insert(batches[i], vals)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         for i in range(64):
