@@ -99,6 +99,7 @@ RunBuffer *RunPool::acquire(uint64_t min_rows, cudaStream_t stream) {
   if (best && best->cap <= cap * 2) {
     free_.erase(free_.begin() + best_i);
     best->model_ok = false;
+    best->model_rows = 0;
     return best;
   }
   auto b = std::make_unique<RunBuffer>();
@@ -437,11 +438,24 @@ RunBuffer *LsmDictionary::merge(RunBuffer *newer, RunBuffer *older, uint64_t out
 }
 
 
-// Search mode 1: fit the learned position model of a freshly written level
-// on the GPU (forward/backward kernels), reading its exact row count from the
-// device descriptor; small levels keep the directory.
-void LsmDictionary::fit_model(RunBuffer *run, uint64_t upper, cudaStream_t s) {
-  if (cfg_.search_mode != 1 || upper < kLearnedMinRows) return;
+// Search mode 1: a freshly written level of at least kLearnedMinRows rows
+// gets its learned position model before the next read that searches it
+// (fitting when the level is written would refit levels that the next update
+// replaces unread); smaller levels keep the directory.
+void LsmDictionary::fit_model(RunBuffer *run, uint64_t upper, cudaStream_t) {
+  run->model_ok = false;
+  run->model_rows = (cfg_.search_mode == 1 && upper >= kLearnedMinRows) ? upper : 0;
+}
+
+void LsmDictionary::ensure_models(cudaStream_t s) {
+  if (cfg_.search_mode != 1) return;
+  for (auto &l : levels_)
+    if (l.run && l.run->model_rows && !l.run->model_ok) fit_now(l.run, l.run->model_rows, s);
+}
+
+// Fit the model on the GPU (forward/backward kernels), reading the level's
+// exact row count from its device descriptor.
+void LsmDictionary::fit_now(RunBuffer *run, uint64_t upper, cudaStream_t s) {
   uint32_t segs = 64;
   while (segs < upper / kRowsPerSegment && segs < kMaxSegments) segs <<= 1;
   const size_t bytes = learned::bytes_for(segs);
@@ -743,6 +757,7 @@ void LsmDictionary::lookup(const uint32_t *queries, uint64_t n, uint32_t *out_va
   if (!queries || !out_values) throw std::invalid_argument("invalid GPU dictionary lookup");
   apply_receipt(false);
   begin_op(s);
+  ensure_models(s);
   lsm::LevelSet set;
   level_set(&set);
   lsm::lookup_kernel<<<grid_for(n, 256), 256, 0, s>>>(set, queries, n, out_values, out_found); note_launch();
@@ -757,7 +772,9 @@ void LsmDictionary::range_sum(const uint32_t *lo, const uint32_t *hi, uint64_t n
   if (!lo || !hi || !out) throw std::invalid_argument("invalid GPU dictionary range");
   apply_receipt(false);
   begin_op(s);
+  ensure_models(s);
   const int single = ranges_on_single_level(lo, hi, n, s);
+  ensure_models(s);  // a compaction wrote a new level
   if (single >= 0) {
     const unsigned long long *prefix = value_prefix(single, s);
     lsm::single_level_range_kernel<0><<<grid_for(n, 256), 256, 0, s>>>(view_of(single), lo, hi, n, prefix, out);
@@ -779,6 +796,7 @@ void LsmDictionary::range_sum_kway(const uint32_t *lo, const uint32_t *hi, uint6
   if (!lo || !hi || !out) throw std::invalid_argument("invalid GPU dictionary range");
   apply_receipt(false);
   begin_op(s);
+  ensure_models(s);
   lsm::LevelSet set;
   live_level_set(&set, s);
   lsm::range_sum_levels_kernel<<<grid_for(n, 256), 256, 0, s>>>(set, lo, hi, n, out);
@@ -794,7 +812,9 @@ void LsmDictionary::range_count(const uint32_t *lo, const uint32_t *hi, uint64_t
   if (!lo || !hi || !out) throw std::invalid_argument("invalid GPU dictionary range");
   apply_receipt(false);
   begin_op(s);
+  ensure_models(s);
   const int single = ranges_on_single_level(lo, hi, n, s);
+  ensure_models(s);  // a compaction wrote a new level
   if (single >= 0) {
     lsm::single_level_range_kernel<1><<<grid_for(n, 256), 256, 0, s>>>(view_of(single), lo, hi, n, nullptr, out);
     note_launch();
@@ -815,6 +835,7 @@ void LsmDictionary::range_offsets(const uint32_t *lo, const uint32_t *hi, uint64
   if (n && (!lo || !hi)) throw std::invalid_argument("invalid GPU dictionary range");
   apply_receipt(false);
   begin_op(s);
+  ensure_models(s);
   const uint32_t tiles = lsm::scan_tiles(n);
   const size_t count_bytes = align_up(std::max<uint64_t>(n, 1) * 4);
   const size_t bytes = count_bytes + align_up(8) + align_up(size_t(tiles + 1) * 8);
@@ -825,6 +846,7 @@ void LsmDictionary::range_offsets(const uint32_t *lo, const uint32_t *hi, uint64
   unsigned long long *lb = bump.take<unsigned long long>(tiles + 1);
   if (n) {
     const int single = ranges_on_single_level(lo, hi, n, s);
+    ensure_models(s);  // a compaction wrote a new level
     if (single >= 0) {
       lsm::single_level_range_kernel<1><<<grid_for(n, 256), 256, 0, s>>>(view_of(single), lo, hi, n, nullptr,
                                                                           counts);
@@ -851,7 +873,9 @@ void LsmDictionary::range_pairs(const uint32_t *lo, const uint32_t *hi, uint64_t
     throw std::invalid_argument("invalid GPU dictionary range");
   apply_receipt(false);
   begin_op(s);
+  ensure_models(s);
   const int single = ranges_on_single_level(lo, hi, n, s);
+  ensure_models(s);  // a compaction wrote a new level
   if (single >= 0) {
     const unsigned grid = std::min<unsigned>(grid_for(n * 32, 256), unsigned(num_sms_) * 64u);
     lsm::single_level_pairs_kernel<<<grid, 256, 0, s>>>(
@@ -875,6 +899,7 @@ void LsmDictionary::successor(const uint32_t *queries, uint64_t n, uint32_t *out
   if (!queries || !out_keys) throw std::invalid_argument("invalid GPU dictionary successor");
   apply_receipt(false);
   begin_op(s);
+  ensure_models(s);
   lsm::LevelSet set;
   level_set(&set);
   lsm::successor_kernel<<<grid_for(n, 256), 256, 0, s>>>(set, queries, n, out_keys); note_launch();

@@ -44,6 +44,7 @@ struct RunBuffer {
   void *model = nullptr;
   size_t model_cap = 0;
   uint32_t model_segments = 0;
+  uint64_t model_rows = 0;  // rows bound of a level that wants a model before its next read (0: none)
   bool model_ok = false;
 };
 
@@ -132,6 +133,8 @@ class LsmDictionary {
   void live_level_set(void *out, cudaStream_t s);
   void release_levels(cudaStream_t s);
   void fit_model(RunBuffer *run, uint64_t upper, cudaStream_t s);
+  void fit_now(RunBuffer *run, uint64_t upper, cudaStream_t s);
+  void ensure_models(cudaStream_t s);
   void *scratch(size_t bytes, cudaStream_t s);
   void ensure_sort_space(uint64_t n, cudaStream_t s);
   void level_set(void *out) const;
