@@ -63,7 +63,7 @@ def parse():
     p.add_argument("--flix-rounds", type=int, default=3)
     p.add_argument("--tenant-rounds", type=int, default=4)
     p.add_argument("--serving-seconds", type=float, default=2.0)
-    p.add_argument("--case", default=None, choices=["merge", "admit", "serving-mix"],
+    p.add_argument("--case", default=None, choices=["merge", "admit", "serving-mix", "flix"],
                    help="run one small profiling case instead of the benchmark (see profile_case)")
     return p.parse_args()
 
@@ -702,7 +702,10 @@ def profile_case(args):
     admit       8 + 64 x (clear + insert of a 2^20-key batch): the admission
                 kernels alone, no merges;
     serving-mix the serving loop over 2^26 keys, closed loop for 0.3 s with
-                the default request mix."""
+                the default request mix;
+    flix        FliX at 1/4 of its sizes: 2^26 sorted u64 keys built, then 2
+                rounds of 2^20 sorted inserts, 2^19 sorted deletes and 2^22
+                sorted successor probes (plain bucket routing)."""
     import torch
 
     gl = importlib.import_module("gpu-lsm-tree_b200")
@@ -741,6 +744,22 @@ def profile_case(args):
         torch.cuda.synchronize()
         print(json.dumps({"case": "admit", "ms_per_batch": round(e0.elapsed_time(e1) / 64, 4),
                           "status": d.canonical_carry_status()}))
+    elif args.case == "flix":
+        W = importlib.import_module("gpu-lsm-tree_b200.workloads")
+        w = W.flix_fast(2, rounds=2)
+        u64 = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.int64)).cuda()  # noqa: E731
+        cap = w.build_keys.size + 2 * (1 << 20)
+        idx = gl.FlixIndex(key_bits=64, max_elements=cap)
+        idx.build(u64(w.build_keys), max_size=cap)
+        out = torch.empty(1 << 22, dtype=torch.int64, device="cuda")
+        for ins, vals, dels, probes in w.rounds:
+            o = np.argsort(ins, kind="stable")
+            idx.insert(u64(ins[o]), torch.from_numpy(vals[o].view(np.int32)).cuda())
+            idx.remove(u64(np.sort(dels)))
+            idx.lookups_successor(u64(np.sort(probes)), out)
+        torch.cuda.synchronize()
+        print(json.dumps({"case": "flix", "status": idx.status()}))
+        idx.close()
     else:
         base = keys(1 << 26)
         srv = gl.Server(gl.DictionaryConfig(max_elements=(1 << 26) + (1 << 25), level_zero_capacity=1 << 17),

@@ -430,14 +430,23 @@ class FlixImpl final : public FlixIndex::Impl {
       }
       begin(s);
       Sorted st = prepare(keys, vals, n, is_insert, false, true, s);
-      const unsigned grid = grid_for(n * 32, 256);
+      // persistent warps: the CTAs every SM holds at once, never more than one warp per key
+      int per_sm = 1;
+      GPULSM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &per_sm, is_insert ? reinterpret_cast<const void *>(flix::insert_runs_kernel<K>)
+                             : reinterpret_cast<const void *>(flix::delete_runs_kernel<K>),
+          flix::kUpdateThreads, 0));
+      const unsigned grid = std::min<unsigned>(grid_for(n * 32, flix::kUpdateThreads),
+                                               unsigned(num_sms_) * unsigned(std::max(per_sm, 1)));
       flix::PoolView pool{&ctr_->alloc_top, capacity_, &ctr_->status};
       if (is_insert) {
-        flix::insert_runs_kernel<K><<<grid, 256, 0, s>>>(st.keys, st.vals, st.n_dev, st.runs, st.run_count,
-                                                         nodes_, pool, &ctr_->inserted); note_launch();
+        flix::insert_runs_kernel<K><<<grid, flix::kUpdateThreads, 0, s>>>(
+            st.keys, st.vals, st.n_dev, st.runs, st.run_count, nodes_, pool, &ctr_->inserted);
+        note_launch();
       } else {
-        flix::delete_runs_kernel<K><<<grid, 256, 0, s>>>(st.keys, st.n_dev, st.runs, st.run_count, nodes_,
-                                                         &ctr_->removed); note_launch();
+        flix::delete_runs_kernel<K><<<grid, flix::kUpdateThreads, 0, s>>>(st.keys, st.n_dev, st.runs,
+                                                                           st.run_count, nodes_, &ctr_->removed);
+        note_launch();
       }
       GPULSM_CUDA(cudaGetLastError());
       if (!is_insert) {

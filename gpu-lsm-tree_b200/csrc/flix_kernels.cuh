@@ -229,6 +229,14 @@ __device__ __forceinline__ uint32_t run_end(const Run *runs, uint32_t r, uint32_
   return r + 1 < run_count ? runs[r + 1].start : n;
 }
 
+// Update kernels run persistent warps: warp w takes runs w, w + W, ... (W =
+// warps in the grid), so the launch size does not depend on the run count
+// (known only on the device) and each warp adds its count to the global
+// counter once.  A run's first 32 keys (and values) are loaded by the lanes
+// together with the head node, and consumed by shuffles, so a multi-key run
+// does not wait on one global load per key.
+constexpr uint32_t kUpdateThreads = 256;
+
 // Insert if absent (FliX/coarse_granular_inserts_tiles_bulk.cuh:1307-1602):
 // the run's keys are sorted and unique; an existing key keeps its value.  A
 // full node splits: the lower half keeps 16 entries, the upper half moves to
@@ -236,79 +244,91 @@ __device__ __forceinline__ uint32_t run_end(const Run *runs, uint32_t r, uint32_
 // allocation region sets kDevOutputOverflow and the key is reported, not
 // silently dropped.
 template <typename K>
-__global__ void __launch_bounds__(256) insert_runs_kernel(
+__global__ void __launch_bounds__(kUpdateThreads) insert_runs_kernel(
     const K *__restrict__ keys, const uint32_t *__restrict__ vals, const uint32_t *__restrict__ n_ptr,
     const Run *__restrict__ runs, const uint32_t *__restrict__ run_count_ptr, Node<K> *nodes,
     PoolView pool, unsigned long long *__restrict__ inserted) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t n = *n_ptr;
-  const uint32_t r = (uint32_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   const uint32_t run_count = *run_count_ptr;
-  if (r >= run_count) return;
-  const Run run = runs[r];
-  const uint32_t end = run_end(runs, r, run_count, n);
-  WarpNode<K> w;
-  load_node(nodes, run.bucket, lane, w);
-  bool dirty = false;
+  const uint32_t stride = gridDim.x * (kUpdateThreads / 32);
   uint32_t added = 0;
-  for (uint32_t i = run.start; i < end; ++i) {
-    const K k = keys[i];
-    const uint32_t v = vals[i];
-    while (k > w.max && w.next != kNone) {
-      if (dirty) store_node(nodes, lane, w);
-      dirty = false;
-      load_node(nodes, w.next, lane, w);
+  for (uint32_t r = (blockIdx.x * kUpdateThreads + threadIdx.x) >> 5; r < run_count; r += stride) {
+    const Run run = runs[r];
+    const uint32_t end = run_end(runs, r, run_count, n);
+    K kreg = 0;
+    uint32_t vreg = 0;
+    if (run.start + lane < end) {
+      kreg = keys[run.start + lane];
+      vreg = vals[run.start + lane];
     }
-    if (k > w.max) {  // chain ends below the key: broken invariant, report and skip
-      if (lane == 0) atomicOr(pool.status, kDevBadInput);
-      continue;
-    }
-    if (__ballot_sync(0xffffffffu, lane < w.count && w.key == k)) continue;  // present: keep
-    if (w.count == kNodeSize) {
-      uint32_t fresh = 0;
-      if (lane == 0) fresh = atomicAdd(pool.alloc_top, 1u);
-      fresh = __shfl_sync(0xffffffffu, fresh, 0);
-      if (fresh >= pool.capacity) {
-        if (lane == 0) atomicOr(pool.status, kDevOutputOverflow);
+    WarpNode<K> w;
+    load_node(nodes, run.bucket, lane, w);
+    bool dirty = false;
+    for (uint32_t i = run.start; i < end; ++i) {
+      const uint32_t slot = (i - run.start) & 31u;
+      if (slot == 0 && i != run.start) {  // next 32 keys of a long run
+        kreg = i + lane < end ? keys[i + lane] : K(0);
+        vreg = i + lane < end ? vals[i + lane] : 0u;
+      }
+      const K k = __shfl_sync(0xffffffffu, kreg, slot);
+      const uint32_t v = __shfl_sync(0xffffffffu, vreg, slot);
+      while (k > w.max && w.next != kNone) {
+        if (dirty) store_node(nodes, lane, w);
+        dirty = false;
+        load_node(nodes, w.next, lane, w);
+      }
+      if (k > w.max) {  // chain ends below the key: broken invariant, report and skip
+        if (lane == 0) atomicOr(pool.status, kDevBadInput);
         continue;
       }
-      constexpr uint32_t half = kNodeSize / 2;
-      const K lower_max = __shfl_sync(0xffffffffu, w.key, half - 1);
-      // upper half -> fresh node (slots 0..15)
-      WarpNode<K> up;
-      up.id = fresh;
-      up.key = __shfl_down_sync(0xffffffffu, w.key, half);
-      up.val = __shfl_down_sync(0xffffffffu, w.val, half);
-      up.max = w.max;
-      up.count = kNodeSize - half;
-      up.next = w.next;
-      w.max = lower_max;
-      w.count = half;
-      w.next = fresh;
-      if (k > lower_max) {
-        store_node(nodes, lane, w);
-        w = up;
-      } else {
-        store_node(nodes, lane, up);
+      if (__ballot_sync(0xffffffffu, lane < w.count && w.key == k)) continue;  // present: keep
+      if (w.count == kNodeSize) {
+        uint32_t fresh = 0;
+        if (lane == 0) fresh = atomicAdd(pool.alloc_top, 1u);
+        fresh = __shfl_sync(0xffffffffu, fresh, 0);
+        if (fresh >= pool.capacity) {
+          if (lane == 0) atomicOr(pool.status, kDevOutputOverflow);
+          continue;
+        }
+        constexpr uint32_t half = kNodeSize / 2;
+        const K lower_max = __shfl_sync(0xffffffffu, w.key, half - 1);
+        // upper half -> fresh node (slots 0..15)
+        WarpNode<K> up;
+        up.id = fresh;
+        up.key = __shfl_down_sync(0xffffffffu, w.key, half);
+        up.val = __shfl_down_sync(0xffffffffu, w.val, half);
+        up.max = w.max;
+        up.count = kNodeSize - half;
+        up.next = w.next;
+        w.max = lower_max;
+        w.count = half;
+        w.next = fresh;
+        if (k > lower_max) {
+          store_node(nodes, lane, w);
+          w = up;
+        } else {
+          store_node(nodes, lane, up);
+        }
+        dirty = true;
       }
+      const uint32_t pos = __popc(__ballot_sync(0xffffffffu, lane < w.count && w.key < k));
+      const K sk = __shfl_up_sync(0xffffffffu, w.key, 1);
+      const uint32_t sv = __shfl_up_sync(0xffffffffu, w.val, 1);
+      if (lane > pos && lane <= w.count) {
+        w.key = sk;
+        w.val = sv;
+      }
+      if (lane == pos) {
+        w.key = k;
+        w.val = v;
+      }
+      ++w.count;
+      ++added;
       dirty = true;
     }
-    const uint32_t pos = __popc(__ballot_sync(0xffffffffu, lane < w.count && w.key < k));
-    const K sk = __shfl_up_sync(0xffffffffu, w.key, 1);
-    const uint32_t sv = __shfl_up_sync(0xffffffffu, w.val, 1);
-    if (lane > pos && lane <= w.count) {
-      w.key = sk;
-      w.val = sv;
-    }
-    if (lane == pos) {
-      w.key = k;
-      w.val = v;
-    }
-    ++w.count;
-    ++added;
-    dirty = true;
+    if (dirty) store_node(nodes, lane, w);
   }
-  if (dirty) store_node(nodes, lane, w);
   if (lane == 0 && added) atomicAdd(inserted, (unsigned long long)added);
 }
 
@@ -316,57 +336,61 @@ __global__ void __launch_bounds__(256) insert_runs_kernel(
 // are removed and survivors compacted left; an emptied non-head node is
 // unlinked from its chain (its range passes to its neighbour).
 template <typename K>
-__global__ void __launch_bounds__(256) delete_runs_kernel(
+__global__ void __launch_bounds__(kUpdateThreads) delete_runs_kernel(
     const K *__restrict__ keys, const uint32_t *__restrict__ n_ptr, const Run *__restrict__ runs,
     const uint32_t *__restrict__ run_count_ptr, Node<K> *nodes,
     unsigned long long *__restrict__ removed) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t n = *n_ptr;
-  const uint32_t r = (uint32_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   const uint32_t run_count = *run_count_ptr;
-  if (r >= run_count) return;
-  const Run run = runs[r];
-  const uint32_t end = run_end(runs, r, run_count, n);
-  WarpNode<K> w;
-  load_node(nodes, run.bucket, lane, w);
-  uint32_t prev = kNone;
-  bool dirty = false;
+  const uint32_t stride = gridDim.x * (kUpdateThreads / 32);
   uint32_t gone = 0;
-  auto flush = [&]() {
-    if (!dirty) return;
-    if (w.count == 0 && prev != kNone) {
-      // unlink the emptied node; the predecessor inherits its key range
-      if (lane == 0) {
-        nodes[prev].next = w.next;
-        if (w.next == kNone) nodes[prev].max = w.max;
+  for (uint32_t r = (blockIdx.x * kUpdateThreads + threadIdx.x) >> 5; r < run_count; r += stride) {
+    const Run run = runs[r];
+    const uint32_t end = run_end(runs, r, run_count, n);
+    K kreg = run.start + lane < end ? keys[run.start + lane] : K(0);
+    WarpNode<K> w;
+    load_node(nodes, run.bucket, lane, w);
+    uint32_t prev = kNone;
+    bool dirty = false;
+    auto flush = [&]() {
+      if (!dirty) return;
+      if (w.count == 0 && prev != kNone) {
+        // unlink the emptied node; the predecessor inherits its key range
+        if (lane == 0) {
+          nodes[prev].next = w.next;
+          if (w.next == kNone) nodes[prev].max = w.max;
+        }
+      } else {
+        store_node(nodes, lane, w);
       }
-    } else {
-      store_node(nodes, lane, w);
+      dirty = false;
+    };
+    for (uint32_t i = run.start; i < end; ++i) {
+      const uint32_t slot = (i - run.start) & 31u;
+      if (slot == 0 && i != run.start) kreg = i + lane < end ? keys[i + lane] : K(0);
+      const K k = __shfl_sync(0xffffffffu, kreg, slot);
+      while (k > w.max && w.next != kNone) {
+        const bool unlinked = dirty && w.count == 0 && prev != kNone;
+        flush();
+        if (!unlinked) prev = w.id;
+        load_node(nodes, w.next, lane, w);
+      }
+      const uint32_t match = __ballot_sync(0xffffffffu, lane < w.count && w.key == k);
+      if (!match) continue;
+      const uint32_t p = __ffs(match) - 1;
+      const K sk = __shfl_down_sync(0xffffffffu, w.key, 1);
+      const uint32_t sv = __shfl_down_sync(0xffffffffu, w.val, 1);
+      if (lane >= p && lane + 1 < w.count) {
+        w.key = sk;
+        w.val = sv;
+      }
+      --w.count;
+      ++gone;
+      dirty = true;
     }
-    dirty = false;
-  };
-  for (uint32_t i = run.start; i < end; ++i) {
-    const K k = keys[i];
-    while (k > w.max && w.next != kNone) {
-      const bool unlinked = dirty && w.count == 0 && prev != kNone;
-      flush();
-      if (!unlinked) prev = w.id;
-      load_node(nodes, w.next, lane, w);
-    }
-    const uint32_t match = __ballot_sync(0xffffffffu, lane < w.count && w.key == k);
-    if (!match) continue;
-    const uint32_t p = __ffs(match) - 1;
-    const K sk = __shfl_down_sync(0xffffffffu, w.key, 1);
-    const uint32_t sv = __shfl_down_sync(0xffffffffu, w.val, 1);
-    if (lane >= p && lane + 1 < w.count) {
-      w.key = sk;
-      w.val = sv;
-    }
-    --w.count;
-    ++gone;
-    dirty = true;
+    flush();
   }
-  flush();
   if (lane == 0 && gone) atomicAdd(removed, (unsigned long long)gone);
 }
 
