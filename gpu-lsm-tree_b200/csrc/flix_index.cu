@@ -285,7 +285,7 @@ class FlixImpl final : public FlixIndex::Impl {
   }
 
   void inspect(const K *keys, uint64_t n, cudaStream_t s) {
-    const unsigned blocks = std::min<unsigned>(grid_for(n, 256), unsigned(num_sms_) * 8u);
+    const unsigned blocks = std::min<unsigned>(grid_for(n, 256), unsigned(num_sms_) * 4u);
     flix::inspect_keys_kernel<K><<<blocks, 256, 0, s>>>(keys, n, &ctr_->flags, &ctr_->max_key); note_launch();
   }
 

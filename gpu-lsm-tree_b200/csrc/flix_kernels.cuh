@@ -105,6 +105,16 @@ __device__ __forceinline__ uint32_t bucket_of(const K *__restrict__ bmax, uint32
   return lo;
 }
 
+template <typename K>
+__device__ __forceinline__ uint32_t bucket_in(const K *__restrict__ bmax, uint32_t lo, uint32_t hi, K key) {
+  while (lo < hi) {  // first bucket in [lo, hi] whose maximum is >= key
+    const uint32_t mid = (lo + hi) >> 1;
+    if (bmax[mid] < key) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
 // Same answer through the learned model fitted on bmax[0, buckets-1): the
 // model narrows the search to its error window (learned.cuh); keys above
 // bmax[buckets-2] fall into the last bucket.
@@ -150,10 +160,43 @@ __global__ void __launch_bounds__(kRouteThreads) route_runs_kernel(
   const uint64_t mine = base + uint64_t(threadIdx.x) * kRouteItems;
   uint32_t bk[kRouteItems];
   uint32_t starts = 0, cnt = 0;
+  K kk[kRouteItems];
 #pragma unroll
-  for (int i = 0; i < kRouteItems; ++i) {
-    const uint64_t g = mine + i;
-    bk[i] = g < n ? route(keys[g]) : kNone;
+  for (int i = 0; i < kRouteItems; ++i) kk[i] = mine + i < n ? keys[mine + i] : K(0);
+  if (model) {
+#pragma unroll
+    for (int i = 0; i < kRouteItems; ++i) bk[i] = mine + i < n ? route(kk[i]) : kNone;
+  } else {
+    // the keys are sorted: the warp's first and last key take a full search,
+    // every other key searches only the buckets between theirs (a key outside
+    // that interval - unsorted input - searches everything)
+    const uint32_t lane = threadIdx.x & 31u;
+    const bool any = mine < n;
+    const uint64_t left = any ? uint64_t(n) - mine : 0ull;
+    const uint32_t nv = left < uint64_t(kRouteItems) ? uint32_t(left) : uint32_t(kRouteItems);
+    const uint32_t vmask = __ballot_sync(0xffffffffu, any);
+    uint32_t blo = 0, bhi = buckets - 1;
+    K kf = 0, kl = 0;
+    if (vmask) {
+      const uint32_t fl = __ffs(vmask) - 1, ll = 31u - __clz(vmask);
+      kf = __shfl_sync(0xffffffffu, kk[0], fl);
+      K mylast = kk[0];
+#pragma unroll
+      for (int i = 1; i < kRouteItems; ++i)
+        if (uint32_t(i) < nv) mylast = kk[i];
+      kl = __shfl_sync(0xffffffffu, mylast, ll);
+      // (one lane may hold both the first and the last key)
+      const uint32_t bf = lane == fl ? bucket_in(bmax, 0u, buckets - 1, kf) : 0u;
+      const uint32_t bl = lane == ll ? bucket_in(bmax, 0u, buckets - 1, kl) : 0u;
+      blo = __shfl_sync(0xffffffffu, bf, fl);
+      bhi = __shfl_sync(0xffffffffu, bl, ll);
+    }
+#pragma unroll
+    for (int i = 0; i < kRouteItems; ++i) {
+      const K k = kk[i];
+      bk[i] = uint32_t(i) < nv ? ((kf <= k && k <= kl) ? bucket_in(bmax, blo, bhi, k) : bucket_in(bmax, 0u, buckets - 1, k))
+                               : kNone;
+    }
   }
   // previous key's bucket for item 0 of this thread
   uint32_t prev = __shfl_up_sync(0xffffffffu, bk[kRouteItems - 1], 1);
@@ -253,9 +296,16 @@ __global__ void __launch_bounds__(kUpdateThreads) insert_runs_kernel(
   const uint32_t run_count = *run_count_ptr;
   const uint32_t stride = gridDim.x * (kUpdateThreads / 32);
   uint32_t added = 0;
-  for (uint32_t r = (blockIdx.x * kUpdateThreads + threadIdx.x) >> 5; r < run_count; r += stride) {
-    const Run run = runs[r];
-    const uint32_t end = run_end(runs, r, run_count, n);
+  uint32_t r = (blockIdx.x * kUpdateThreads + threadIdx.x) >> 5;
+  Run next_run = r < run_count ? runs[r] : Run{};
+  uint32_t next_end = r < run_count ? run_end(runs, r, run_count, n) : 0u;
+  for (; r < run_count; r += stride) {
+    const Run run = next_run;
+    const uint32_t end = next_end;
+    if (r + stride < run_count) {  // the next run's bounds load while this one is processed
+      next_run = runs[r + stride];
+      next_end = run_end(runs, r + stride, run_count, n);
+    }
     K kreg = 0;
     uint32_t vreg = 0;
     if (run.start + lane < end) {
@@ -345,9 +395,16 @@ __global__ void __launch_bounds__(kUpdateThreads) delete_runs_kernel(
   const uint32_t run_count = *run_count_ptr;
   const uint32_t stride = gridDim.x * (kUpdateThreads / 32);
   uint32_t gone = 0;
-  for (uint32_t r = (blockIdx.x * kUpdateThreads + threadIdx.x) >> 5; r < run_count; r += stride) {
-    const Run run = runs[r];
-    const uint32_t end = run_end(runs, r, run_count, n);
+  uint32_t r = (blockIdx.x * kUpdateThreads + threadIdx.x) >> 5;
+  Run next_run = r < run_count ? runs[r] : Run{};
+  uint32_t next_end = r < run_count ? run_end(runs, r, run_count, n) : 0u;
+  for (; r < run_count; r += stride) {
+    const Run run = next_run;
+    const uint32_t end = next_end;
+    if (r + stride < run_count) {  // the next run's bounds load while this one is processed
+      next_run = runs[r + stride];
+      next_end = run_end(runs, r + stride, run_count, n);
+    }
     K kreg = run.start + lane < end ? keys[run.start + lane] : K(0);
     WarpNode<K> w;
     load_node(nodes, run.bucket, lane, w);
@@ -505,15 +562,6 @@ __global__ void __launch_bounds__(256) successor_runs_kernel(
 // touches.  Plain routing narrows each lane's binary search over the bucket
 // maxima to the bucket range spanned by its warp's (sorted) probes; learned
 // routing uses the model's error window.
-template <typename K>
-__device__ __forceinline__ uint32_t bucket_in(const K *__restrict__ bmax, uint32_t lo, uint32_t hi, K key) {
-  while (lo < hi) {  // first bucket in [lo, hi] whose maximum is >= key
-    const uint32_t mid = (lo + hi) >> 1;
-    if (bmax[mid] < key) lo = mid + 1;
-    else hi = mid;
-  }
-  return lo;
-}
 
 template <typename K>
 __device__ __forceinline__ uint32_t route_sorted(const K *__restrict__ bmax, uint32_t buckets,
@@ -672,25 +720,51 @@ __global__ void __launch_bounds__(kDedupThreads) dedup_first_kernel(
 // sortedness / max probe of a key array: flags bit0 = not sorted ascending,
 // bit1 = has equal neighbours; max key via atomicMax
 template <typename K>
-__global__ void inspect_keys_kernel(const K *__restrict__ keys, uint64_t n, uint32_t *__restrict__ flags,
-                                    unsigned long long *__restrict__ max_key) {
+__global__ void __launch_bounds__(256) inspect_keys_kernel(const K *__restrict__ keys, uint64_t n,
+                                                           uint32_t *__restrict__ flags,
+                                                           unsigned long long *__restrict__ max_key) {
+  // four independent loads in flight per thread and step; one atomic pair per block
+  __shared__ unsigned long long s_max[8];
+  __shared__ uint32_t s_flags[8];
   unsigned long long local_max = 0;
   uint32_t f = 0;
-  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-       i += uint64_t(gridDim.x) * blockDim.x) {
-    const K k = keys[i];
-    local_max = max(local_max, (unsigned long long)k);
-    if (i + 1 < n) {
-      const K nx = keys[i + 1];
-      if (nx < k) f |= 1u;
-      if (nx == k) f |= 2u;
+  const uint64_t step = uint64_t(gridDim.x) * blockDim.x;
+  for (uint64_t i0 = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i0 < n; i0 += 4 * step) {
+    K k[4], nx[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const uint64_t i = i0 + u * step;
+      k[u] = i < n ? keys[i] : K(0);
+      nx[u] = i + 1 < n ? keys[i + 1] : K(0);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const uint64_t i = i0 + u * step;
+      if (i < n) {
+        local_max = max(local_max, (unsigned long long)k[u]);
+        if (i + 1 < n) {
+          if (nx[u] < k[u]) f |= 1u;
+          if (nx[u] == k[u]) f |= 2u;
+        }
+      }
     }
   }
   f = __reduce_or_sync(0xffffffffu, f);
   for (int o = 16; o; o >>= 1) local_max = max(local_max, __shfl_down_sync(0xffffffffu, local_max, o));
   if ((threadIdx.x & 31) == 0) {
-    if (f) atomicOr(flags, f);
-    atomicMax(max_key, local_max);
+    s_max[threadIdx.x >> 5] = local_max;
+    s_flags[threadIdx.x >> 5] = f;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long m = 0;
+    uint32_t ff = 0;
+    for (uint32_t w = 0; w < blockDim.x / 32; ++w) {
+      m = max(m, s_max[w]);
+      ff |= s_flags[w];
+    }
+    if (ff) atomicOr(flags, ff);
+    atomicMax(max_key, m);
   }
 }
 

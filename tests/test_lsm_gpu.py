@@ -375,3 +375,24 @@ def test_search_modes_match_oracle(gl, cuda, mode):
     hi = (lo.astype(np.uint64) + rng.integers(0, 1 << 24, lo.size, dtype=np.uint64)).clip(0, 0xFFFFFFFF)
     t.ranges(lo, hi.astype(np.uint32))
     assert t.d.canonical_carry_status() == 0
+
+
+def test_merge_timing_hook_counts_rows(gl, cuda):
+    """The measurement hook brackets every merge launch: launch count, positive
+    device time, and algorithmic bytes equal to 9 B per row read and written
+    plus 4 B per directory entry (so at least 18 B per merged output row)."""
+    rng = np.random.default_rng(21)
+    t = Twin(gl, max_elements=1 << 16, batch_capacity=1 << 10)
+    t.d.kernel_timing(True)
+    t.d.kernel_timing_read()
+    for _ in range(12):
+        k = rng.integers(0, 1 << 32, 1 << 10, dtype=np.uint64).astype(np.uint32)
+        t.apply(("insert", k, np.arange(k.size, dtype=np.uint32)))
+    got = t.d.kernel_timing_read()
+    t.d.kernel_timing(False)
+    assert got["launches"] > 0 and got["ms"] > 0
+    rows_out_min = 2 * (1 << 10) * got["launches"] / 2  # every merge reads and writes at least one batch
+    assert got["bytes"] >= 18 * rows_out_min
+    assert t.d.kernel_timing_read()["launches"] == 0  # a read resets the record
+    q = rng.integers(0, 1 << 32, 4096, dtype=np.uint64).astype(np.uint32)
+    t.lookup(q)
