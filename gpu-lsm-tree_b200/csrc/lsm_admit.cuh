@@ -3,7 +3,7 @@
 // duplicates and keeps the newest) in four launches instead of a four-pass
 // LSD sort plus a dedup pass:
 //
-//   1. part_hist_kernel     per 4096-key tile, the counts of the key's top byte
+//   1. part_hist_kernel     per 2048-key tile, the counts of the key's top byte
 //   2. part_scan_kernel     per top byte, the exclusive scan over the tiles
 //   3. part_scatter_kernel  words (key << 32 | value) written to their top-byte
 //                           bucket in input order (a stable partition)
@@ -264,8 +264,8 @@ __device__ __noinline__ unsigned long long *sort_global(unsigned long long *a, u
 //                       inside the tile (ballot peer groups), then the words
 //                       (key << 32 | value) staged by byte and written in runs
 constexpr int kPartThreads = 256;
-constexpr int kPartItems = 16;
-constexpr uint32_t kPartTile = uint32_t(kPartThreads) * kPartItems;  // 4096 keys
+constexpr int kPartItems = 8;
+constexpr uint32_t kPartTile = uint32_t(kPartThreads) * kPartItems;  // 2048 keys
 constexpr int kPartWarps = kPartThreads / 32;
 
 inline uint32_t part_tiles(uint64_t n) { return uint32_t((n + kPartTile - 1) / kPartTile); }
