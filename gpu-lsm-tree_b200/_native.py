@@ -116,6 +116,7 @@ class ServeStats(C.Structure):
         ("wall_s", C.c_double),
         ("gpu_busy_s", C.c_double),
         ("host_launch_s", C.c_double),
+        ("graph_rounds", C.c_uint64),
     ]
 
 

@@ -123,6 +123,7 @@ void copy_stats(const gpulsm::ServeStats &s, gpulsm_serve_stats *o) {
   o->wall_s = s.wall_s;
   o->gpu_busy_s = s.gpu_busy_s;
   o->host_launch_s = s.host_launch_s;
+  o->graph_rounds = s.graph_rounds;
 }
 }  // namespace
 

@@ -131,9 +131,10 @@ __device__ __forceinline__ uint32_t count_distinct(const At &at, uint32_t cnt, R
 // at(0 .. cnt) to out[g0 ...], in chunks of kCap read striped (element
 // c0 + i*kThreads + t): per item a warp ballot counts the kept rows, one block
 // scan over the (item, warp) counts gives every warp its output offset, and
-// consecutive lanes store consecutive rows.  Each kept row also writes the
-// radix-directory entries it starts: the buckets after the bucket of the
-// previous distinct key (bp before the first row) up to its own.
+// consecutive lanes store consecutive rows.  The first element of every
+// equal-key run writes the radix-directory entries its run's row starts: the
+// buckets after the bucket of the previous distinct key (bp before the first
+// row) up to its own, pointing at the row (= run ends before the element).
 template <typename At>
 __device__ __forceinline__ void write_rows(const At &at, uint32_t cnt, int tombstone, uint32_t *out_keys,
                                            uint32_t *out_vals, uint8_t *out_flags, unsigned long long g0,
@@ -160,22 +161,27 @@ __device__ __forceinline__ void write_rows(const At &at, uint32_t cnt, int tombs
     if (threadIdx.x < uint32_t(kItems * kWarps)) slot[threadIdx.x] = ex;
     __syncthreads();
 #pragma unroll
-    for (int i = 0; i < kItems; ++i)
+    for (int i = 0; i < kItems; ++i) {
+      const uint32_t e = c0 + uint32_t(i) * kThreads + threadIdx.x;
+      if (e >= c0 + cc) continue;
+      // run ends before e = the output row of e's run (its last element is kept)
+      const unsigned long long r = g0 + written + slot[i * kWarps + w] + __popc(ends[i] & lt);
+      const unsigned long long w64 = at(e);
+      const uint32_t k = word_key(w64);
       if ((ends[i] >> lane) & 1u) {
-        const uint32_t e = c0 + uint32_t(i) * kThreads + threadIdx.x;
-        const unsigned long long w64 = at(e);
-        const unsigned long long r = g0 + written + slot[i * kWarps + w] + __popc(ends[i] & lt);
-        const uint32_t k = word_key(w64);
         out_keys[r] = k;
         out_vals[r] = uint32_t(w64);  // the tombstone value was packed for erase batches
         out_flags[r] = tombstone ? kFlagTomb : uint8_t(0);
-        uint32_t p = e;  // first element of this key's run
-        while (p > 0 && word_key(at(p - 1)) == k) --p;
-        const int64_t bprev = p > 0 ? int64_t((word_key(at(p - 1)) - g.kmin) >> g.shift) : bp;
+      }
+      // the first element of a run writes the directory entries its row starts
+      const uint32_t kp = e > 0 ? word_key(at(e - 1)) : 0u;
+      if (e == 0 || kp != k) {
+        const int64_t bprev = e > 0 ? int64_t((kp - g.kmin) >> g.shift) : bp;
         const int64_t bj = int64_t((k - g.kmin) >> g.shift);
         for (int64_t b = bprev + 1; b <= bj; ++b)
           if (GPULSM_OK(b >= 0 && b < int64_t(g.nbuckets), 10, b)) dir[b] = uint32_t(r);
       }
+    }
     __syncthreads();
     written += chunk_kept;
   }
@@ -619,22 +625,27 @@ __global__ void __launch_bounds__(kThreads, 2) admit_bucket_kernel(
       return;
     }
 #pragma unroll
-    for (int i = 0; i < kItems; ++i)
-      if (uint32_t(i) < keff && ((ends[i] >> lane) & 1u)) {
-        const uint32_t e = uint32_t(i) * kThreads + threadIdx.x;
-        const unsigned long long w64 = w[e];
-        const unsigned long long r = g0 + slot[i * kWarps + wi] + __popc(ends[i] & lt);
-        const uint32_t k = word_key(w64);
+    for (int i = 0; i < kItems; ++i) {
+      const uint32_t e = uint32_t(i) * kThreads + threadIdx.x;
+      if (uint32_t(i) >= keff || e >= cnt) continue;
+      // run ends before e = the output row of e's run (its last element is kept)
+      const unsigned long long r = g0 + slot[i * kWarps + wi] + __popc(ends[i] & lt);
+      const unsigned long long w64 = w[e];
+      const uint32_t k = word_key(w64);
+      if ((ends[i] >> lane) & 1u) {
         out_keys[r] = k;
         out_vals[r] = uint32_t(w64);  // the tombstone value was packed for erase batches
         out_flags[r] = tombstone ? kFlagTomb : uint8_t(0);
-        uint32_t p = e;  // first element of this key's run
-        while (p > 0 && word_key(w[p - 1]) == k) --p;
-        const int32_t bprev = p > 0 ? int32_t((word_key(w[p - 1]) - g.kmin) >> g.shift) : bp;
+      }
+      // the first element of a run writes the directory entries its row starts
+      const uint32_t kp = e > 0 ? word_key(w[e - 1]) : 0u;
+      if (e == 0 || kp != k) {
+        const int32_t bprev = e > 0 ? int32_t((kp - g.kmin) >> g.shift) : bp;
         const int32_t bj = int32_t((k - g.kmin) >> g.shift);
         for (int32_t bb = bprev + 1; bb <= bj; ++bb)
           if (GPULSM_OK(bb >= 0 && bb < int32_t(g.nbuckets), 10, bb)) out_dir[bb] = uint32_t(r);
       }
+    }
   } else {
     const auto by_array = [sorted](uint32_t j) { return sorted[j]; };
     kept = count_distinct(by_array, cnt, sm.rank);

@@ -16,6 +16,7 @@
 #include "lsm_dictionary.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <new>
 #include <stdexcept>
@@ -45,15 +46,25 @@ struct ReceiptSrc {
   const LevelDesc *desc[lsm::kMaxLevels];
   uint32_t count;
   const uint32_t *status;
-  unsigned long long *out;  // [kMaxLevels] counts then status
+  unsigned long long *out;  // [kMaxLevels] counts, status, then the sequence number
+  unsigned long long seq;
 };
 
+// Writes the receipt into mapped pinned host memory; the sequence number goes
+// last, after a system-scope fence, so a host that reads the expected number
+// reads a complete receipt (no event in the stream, which would end the
+// chain of dependent launches).
 __global__ void receipt_kernel(ReceiptSrc src) {
   chain_wait();
   const uint32_t i = threadIdx.x;
   if (i < lsm::kMaxLevels)
     src.out[i] = (i < src.count && src.desc[i]) ? src.desc[i]->n : 0ull;
   if (i == lsm::kMaxLevels) src.out[i] = *src.status;
+  __syncwarp();
+  if (i == 0) {
+    __threadfence_system();
+    *reinterpret_cast<volatile unsigned long long *>(src.out + lsm::kMaxLevels + 1) = src.seq;
+  }
 }
 
 // Bump allocator over one zeroed scratch region.
@@ -76,6 +87,7 @@ size_t merge_scratch_bytes(uint64_t rows) {
 struct LsmDictionary::Receipt {
   unsigned long long n[lsm::kMaxLevels];
   unsigned long long status;
+  unsigned long long seq;  // written last by the receipt kernel
 };
 
 // ----------------------------------------------------------------------------
@@ -184,6 +196,7 @@ LsmDictionary::LsmDictionary(const DictConfig &config)
   GPULSM_CUDA(cudaFuncSetAttribute(lsm::admit::admit_bucket_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    int(lsm::admit::kBucketSmemBytes)));
   GPULSM_CUDA(cudaMalloc(&dev_status_, 256));
+  GPULSM_CUDA(cudaMalloc(&table_dev_, sizeof(lsm::LevelSet)));
   GPULSM_CUDA(cudaMemset(dev_status_, 0, 256));
   // the receipt kernel writes the pinned host copy directly (no copy in the stream)
   GPULSM_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&receipt_host_), sizeof(Receipt), cudaHostAllocMapped));
@@ -192,7 +205,6 @@ LsmDictionary::LsmDictionary(const DictConfig &config)
   GPULSM_CUDA(cudaMalloc(&width_, 8));
   GPULSM_CUDA(cudaMallocHost(&width_host_, 8));
   GPULSM_CUDA(cudaEventCreateWithFlags(&op_done_, cudaEventDisableTiming));
-  GPULSM_CUDA(cudaEventCreateWithFlags(&receipt_event_, cudaEventDisableTiming));
   GPULSM_CUDA(cudaEventRecord(op_done_, 0));
 }
 
@@ -206,6 +218,7 @@ LsmDictionary::~LsmDictionary() {
   if (receipt_host_) cudaFreeHost(receipt_host_);
   if (prefix_) cudaFree(prefix_);
   if (trace_dev_) cudaFree(trace_dev_);
+  if (table_dev_) cudaFree(table_dev_);
   for (auto &t : traces_) {
     cudaEventDestroy(t.start);
     cudaEventDestroy(t.stop);
@@ -216,7 +229,6 @@ LsmDictionary::~LsmDictionary() {
   if (width_) cudaFree(width_);
   if (width_host_) cudaFreeHost(width_host_);
   if (op_done_) cudaEventDestroy(op_done_);
-  if (receipt_event_) cudaEventDestroy(receipt_event_);
 }
 
 // Operations are ordered by op_done_ across streams; on the stream of the
@@ -265,13 +277,7 @@ void LsmDictionary::ensure_sort_space(uint64_t n, cudaStream_t s) {
   words_cap_ = cap;
 }
 
-// A receipt still in flight is enough while no level's row bound exceeds the
-// capacity (only then can a receipt reveal an overflow): the host keeps
-// planning with upper bounds and applies the pending receipt when it lands.
 void LsmDictionary::post_receipt(cudaStream_t s) {
-  uint64_t largest = 0;
-  for (const auto &l : levels_) largest = std::max<uint64_t>(largest, l.upper);
-  if (receipt_pending_ && largest <= budget_) return;
   ReceiptSrc src{};
   src.count = uint32_t(levels_.size());
   for (size_t i = 0; i < levels_.size(); ++i) {
@@ -280,20 +286,21 @@ void LsmDictionary::post_receipt(cudaStream_t s) {
   }
   src.status = dev_status_;
   src.out = static_cast<unsigned long long *>(receipt_dev_);  // the mapped pinned host copy
+  src.seq = ++receipt_seq_;
   launch_chained(receipt_kernel, 1, 32, 0, s, src);
-  GPULSM_CUDA(cudaEventRecord(receipt_event_, s));
   receipt_pending_ = true;
 }
 
+// Applies the newest posted receipt once it has landed (wait: after the last
+// operation, which posted it, has completed).  An older receipt that landed
+// while a newer one is in flight is never read: the newer one may be half
+// written over it.
 void LsmDictionary::apply_receipt(bool wait) {
   if (!receipt_pending_) return;
-  if (wait) {
-    GPULSM_CUDA(cudaEventSynchronize(receipt_event_));
-  } else {
-    const cudaError_t q = cudaEventQuery(receipt_event_);
-    if (q == cudaErrorNotReady) return;
-    GPULSM_CUDA(q);
-  }
+  const volatile unsigned long long *seq = &receipt_host_->seq;
+  if (wait) GPULSM_CUDA(cudaEventSynchronize(op_done_));
+  if (*seq != receipt_seq_) return;
+  std::atomic_thread_fence(std::memory_order_acquire);
   receipt_pending_ = false;
   const Receipt r = *receipt_host_;
   status_bits_ |= uint32_t(r.status);
@@ -475,6 +482,7 @@ void LsmDictionary::fit_now(RunBuffer *run, uint64_t upper, cudaStream_t s) {
   learned::fit<uint32_t>(run->keys, upper, segs, kFitIters, run->model, nullptr, s, &run->desc->n);
   run->model_segments = segs;
   run->model_ok = true;
+  ++next_gen_;  // the level table must pick up the model
 }
 
 void LsmDictionary::cascade(RunBuffer *carry, uint64_t carry_upper, bool carry_tombs, cudaStream_t s) {
@@ -915,6 +923,32 @@ uint32_t LsmDictionary::status() {
   GPULSM_CUDA(cudaMemcpy(&bits, dev_status_, 4, cudaMemcpyDeviceToHost));
   status_bits_ |= bits;
   return status_bits_;
+}
+
+void LsmDictionary::enqueue_table_lookup(const uint32_t *queries, uint64_t n, uint32_t *out_values,
+                                         uint8_t *out_found, cudaStream_t capturing) {
+  std::lock_guard<std::mutex> g(mu_);
+  lsm::lookup_table_kernel<<<grid_for(n, 256), 256, 0, capturing>>>(static_cast<const lsm::LevelSet *>(table_dev_),
+                                                                     queries, n, out_values, out_found);
+  GPULSM_CUDA(cudaGetLastError());
+}
+
+void LsmDictionary::launch_read_graph(cudaGraphExec_t exec, cudaStream_t s) {
+  std::lock_guard<std::mutex> g(mu_);
+  apply_receipt(false);
+  begin_op(s);
+  ensure_models(s);
+  if (table_gen_ != next_gen_) {  // the levels changed since the table was written
+    lsm::LevelSet set;
+    level_set(&set);
+    lsm::write_table_kernel<<<1, 64, 0, s>>>(set, static_cast<lsm::LevelSet *>(table_dev_));
+    note_launch();
+    GPULSM_CUDA(cudaGetLastError());
+    table_gen_ = next_gen_;
+  }
+  GPULSM_CUDA(cudaGraphLaunch(exec, s));
+  note_launch();
+  end_op(s);
 }
 
 void LsmDictionary::set_kernel_timing(bool on) {

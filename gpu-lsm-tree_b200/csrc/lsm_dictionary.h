@@ -91,6 +91,13 @@ class LsmDictionary {
   void successor(const uint32_t *queries, uint64_t n, uint32_t *out_keys, cudaStream_t s);
   uint32_t status();
   uint64_t resident_bytes();
+  // Lookups replayable from a CUDA graph: enqueue_table_lookup records (into
+  // a capturing stream) a lookup that reads the level table from device
+  // memory; launch_read_graph orders a captured graph like any operation and
+  // brings the table up to date before it runs.
+  void enqueue_table_lookup(const uint32_t *queries, uint64_t n, uint32_t *out_values, uint8_t *out_found,
+                            cudaStream_t capturing);
+  void launch_read_graph(cudaGraphExec_t exec, cudaStream_t s);
   // Kernel timing of the merge launches (CUDA events on the launching stream
   // around each merge kernel, plus the rows it read and wrote).
   void set_kernel_timing(bool on);
@@ -161,7 +168,7 @@ class LsmDictionary {
   // receipts (pinned host copy of the level row counts and status)
   Receipt *receipt_host_ = nullptr;
   void *receipt_dev_ = nullptr;
-  cudaEvent_t receipt_event_ = nullptr;
+  unsigned long long receipt_seq_ = 0;  // sequence number of the newest posted receipt
   bool receipt_pending_ = false;
   std::vector<uint64_t> receipt_gens_;
 
@@ -192,6 +199,8 @@ class LsmDictionary {
   std::vector<cudaEvent_t> spare_events_;
   unsigned long long *trace_dev_ = nullptr;  // 4 words per timed merge
   static constexpr size_t kMaxTraces = 8192;
+  void *table_dev_ = nullptr;  // device copy of the level set (graph-replayed lookups)
+  uint64_t table_gen_ = ~0ull;            // next_gen_ when the table was last written
   cudaEvent_t op_done_ = nullptr;
   cudaStream_t last_stream_ = nullptr;  // stream of the last operation (op_done_ was recorded there)
   bool last_stream_known_ = false;

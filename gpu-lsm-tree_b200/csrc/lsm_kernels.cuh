@@ -621,11 +621,8 @@ __device__ __forceinline__ bool row_is_tomb(const LevelView &L, uint64_t p, uint
 
 // ---------------------------------------------------------------------------
 // Point lookup: newest level first; miss value follows GPULSMOpt.cuh:4742-4749.
-__global__ void __launch_bounds__(256) lookup_kernel(LevelSet set, const uint32_t *__restrict__ queries,
-                                                     uint64_t n, uint32_t *__restrict__ out_values,
-                                                     uint8_t *__restrict__ out_found) {
-  const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+__device__ __forceinline__ void lookup_one(const LevelSet &set, uint64_t i, const uint32_t *__restrict__ queries,
+                                           uint32_t *__restrict__ out_values, uint8_t *__restrict__ out_found) {
   const uint32_t q = queries[i];
   const uint32_t miss = out_found ? 0u : kNotFound;
   for (uint32_t l = 0; l < set.count; ++l) {
@@ -651,6 +648,37 @@ __global__ void __launch_bounds__(256) lookup_kernel(LevelSet set, const uint32_
   }
   out_values[i] = miss;
   if (out_found) out_found[i] = 0u;
+}
+
+__global__ void __launch_bounds__(256) lookup_kernel(LevelSet set, const uint32_t *__restrict__ queries,
+                                                     uint64_t n, uint32_t *__restrict__ out_values,
+                                                     uint8_t *__restrict__ out_found) {
+  const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n) lookup_one(set, i, queries, out_values, out_found);
+}
+
+// The same lookup with the level set read from device memory (a level table
+// the dictionary rewrites when its levels change), so that a captured CUDA
+// graph stays valid across updates; every block copies the table to shared
+// memory first.
+__global__ void __launch_bounds__(256) lookup_table_kernel(const LevelSet *__restrict__ table,
+                                                           const uint32_t *__restrict__ queries, uint64_t n,
+                                                           uint32_t *__restrict__ out_values,
+                                                           uint8_t *__restrict__ out_found) {
+  __shared__ LevelSet s_set;
+  static_assert(sizeof(LevelSet) % 4 == 0, "table copied in words");
+  const uint32_t *src = reinterpret_cast<const uint32_t *>(table);
+  uint32_t *dst = reinterpret_cast<uint32_t *>(&s_set);
+  for (uint32_t w = threadIdx.x; w < sizeof(LevelSet) / 4; w += blockDim.x) dst[w] = src[w];
+  __syncthreads();
+  const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n) lookup_one(s_set, i, queries, out_values, out_found);
+}
+
+__global__ void write_table_kernel(LevelSet set, LevelSet *__restrict__ table) {
+  const uint32_t *src = reinterpret_cast<const uint32_t *>(&set);
+  uint32_t *dst = reinterpret_cast<uint32_t *>(table);
+  for (uint32_t w = threadIdx.x; w < sizeof(LevelSet) / 4; w += blockDim.x) dst[w] = src[w];
 }
 
 // ---------------------------------------------------------------------------

@@ -46,6 +46,7 @@ Server::Server(const DictConfig &cfg, uint64_t budget_bytes, uint32_t max_round_
   GPULSM_CUDA(cudaStreamCreateWithFlags(&compute_, cudaStreamNonBlocking));
   GPULSM_CUDA(cudaStreamCreateWithFlags(&upload_, cudaStreamNonBlocking));
   GPULSM_CUDA(cudaStreamCreateWithFlags(&download_, cudaStreamNonBlocking));
+  GPULSM_CUDA(cudaStreamCreateWithFlags(&capture_, cudaStreamNonBlocking));
   const uint64_t m = max_round_keys_;
   slot_bytes_ = m * 8 + m * 4 + m;  // inputs (two words a key), outputs, found flags
   slots_.resize(depth);
@@ -92,7 +93,9 @@ Server::~Server() {
     cudaEventDestroy(s.uploaded);
     cudaEventDestroy(s.computed);
     cudaEventDestroy(s.downloaded);
+    for (auto &g : s.graphs) cudaGraphExecDestroy(g.second);
   }
+  cudaStreamDestroy(capture_);
   cudaStreamDestroy(compute_);
   cudaStreamDestroy(upload_);
   cudaStreamDestroy(download_);
@@ -145,7 +148,7 @@ void Server::drain() {
 void Server::reset_stats() {
   std::lock_guard<std::mutex> g(mu_);
   lat_us_.clear();
-  st_completed_ = st_rejected_ = st_rounds_ = st_keys_ = st_round_keys_ = 0;
+  st_completed_ = st_rejected_ = st_rounds_ = st_keys_ = st_round_keys_ = st_graph_rounds_ = 0;
   st_first_ = -1;
   st_last_ = st_gpu_s_ = st_launch_s_ = 0;
 }
@@ -164,6 +167,7 @@ ServeStats Server::stats() {
     s.wall_s = st_first_ >= 0 ? std::max(0.0, st_last_ - st_first_) : 0.0;
     s.gpu_busy_s = st_gpu_s_;
     s.host_launch_s = st_launch_s_;
+    s.graph_rounds = st_graph_rounds_;
   }
   if (!lat.empty()) {
     auto pct = [&](double p) {
@@ -245,6 +249,36 @@ bool Server::form_round(Slot &slot) {
   return any;
 }
 
+// The graph of a lookup-only round of up to `size_class` keys in this slot:
+// copy the keys in, look them up against the dictionary's device level
+// table, copy values and flags out.  Keys past the round's own are stale
+// staging contents; their answers land past the round's results and are
+// never read.
+cudaGraphExec_t Server::lookup_graph(Slot &slot, uint32_t size_class) {
+  for (const auto &g : slot.graphs)
+    if (g.first == size_class) return g.second;
+  const uint64_t c = size_class;
+  cudaGraph_t graph = nullptr;
+  GPULSM_CUDA(cudaStreamBeginCapture(capture_, cudaStreamCaptureModeThreadLocal));
+  try {
+    GPULSM_CUDA(cudaMemcpyAsync(slot.d_in, slot.h_in, c * 4, cudaMemcpyHostToDevice, capture_));
+    dict_.enqueue_table_lookup(slot.d_in, c, slot.d_out, slot.d_found, capture_);
+    GPULSM_CUDA(cudaMemcpyAsync(slot.h_out, slot.d_out, c * 4, cudaMemcpyDeviceToHost, capture_));
+    GPULSM_CUDA(cudaMemcpyAsync(slot.h_found, slot.d_found, c, cudaMemcpyDeviceToHost, capture_));
+  } catch (...) {
+    cudaStreamEndCapture(capture_, &graph);
+    if (graph) cudaGraphDestroy(graph);
+    throw;
+  }
+  GPULSM_CUDA(cudaStreamEndCapture(capture_, &graph));
+  cudaGraphExec_t exec = nullptr;
+  const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  GPULSM_CUDA(e);
+  slot.graphs.emplace_back(size_class, exec);
+  return exec;
+}
+
 void Server::launch_round(Slot &slot) {
   for (const Run &r : slot.runs)
     for (uint64_t i = 0; i < r.parts; ++i) {
@@ -252,6 +286,25 @@ void Server::launch_round(Slot &slot) {
       std::memcpy(slot.h_in + r.in_off + p.off, p.keys, p.n * 4);
       if (has_aux(r.kind)) std::memcpy(slot.h_in + r.in_off + r.n + p.off, p.aux, p.n * 4);
     }
+  if (slot.runs.size() == 1 && slot.runs[0].kind == kServeLookup) {
+    // lookup-only round: one graph launch (size classes are powers of two
+    // from 1024 keys, the last one the round limit)
+    Run &r = slot.runs[0];
+    uint64_t c = 1024;
+    while (c < r.n) c <<= 1;
+    if (c > max_round_keys_) c = max_round_keys_;
+    GPULSM_CUDA(cudaEventRecord(slot.uploaded, compute_));
+    try {
+      dict_.launch_read_graph(lookup_graph(slot, uint32_t(c)), compute_);
+    } catch (const std::exception &e) {
+      r.status = status_of(e);
+    }
+    GPULSM_CUDA(cudaEventRecord(slot.computed, compute_));
+    GPULSM_CUDA(cudaEventRecord(slot.downloaded, compute_));
+    std::lock_guard<std::mutex> g(mu_);
+    ++st_graph_rounds_;
+    return;
+  }
   GPULSM_CUDA(cudaMemcpyAsync(slot.d_in, slot.h_in, slot.in_words * 4, cudaMemcpyHostToDevice, upload_));
   GPULSM_CUDA(cudaEventRecord(slot.uploaded, upload_));
   GPULSM_CUDA(cudaStreamWaitEvent(compute_, slot.uploaded, 0));

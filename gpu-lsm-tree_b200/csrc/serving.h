@@ -47,6 +47,7 @@ struct ServeStats {
   double wall_s = 0;          // first submit to last completion since the last reset
   double gpu_busy_s = 0;      // device time of the rounds (upload done -> kernels done)
   double host_launch_s = 0;   // worker time staging and launching rounds
+  uint64_t graph_rounds = 0;  // lookup-only rounds replayed from a captured CUDA graph
 };
 
 // Open-loop load: Poisson arrivals, kind mix, log-uniform sizes, Zipf keys.
@@ -123,12 +124,16 @@ class Server {
     uint64_t in_words = 0, out_words = 0, keys = 0;
     uint64_t bytes = 0;  // device bytes the round's updates may add (admission budget)
     bool launched = false;
+    // lookup-only rounds replay a CUDA graph per size class (copy in, lookup
+    // against the device level table, copy out) captured on first use
+    std::vector<std::pair<uint32_t, cudaGraphExec_t>> graphs;
   };
 
   void worker();
   void completer();
   bool form_round(Slot &slot);
   void launch_round(Slot &slot);
+  cudaGraphExec_t lookup_graph(Slot &slot, uint32_t size_class);
   static double now_s();
 
   LsmDictionary dict_;
@@ -140,6 +145,8 @@ class Server {
   std::deque<uint32_t> free_slots_;
   std::deque<uint32_t> inflight_;
   cudaStream_t compute_ = nullptr, upload_ = nullptr, download_ = nullptr;
+  cudaStream_t capture_ = nullptr;  // graphs are captured here (thread-local mode)
+  uint64_t st_graph_rounds_ = 0;
 
   std::mutex mu_;
   std::condition_variable cv_work_, cv_done_, cv_inflight_;

@@ -225,6 +225,7 @@ typedef struct gpulsm_serve_stats {
   double p50_us, p99_us, max_us, mean_us; /* submit -> results in the caller's buffers */
   double mean_round_keys, wall_s;
   double gpu_busy_s, host_launch_s; /* device time of the rounds; worker time staging + launching */
+  uint64_t graph_rounds;            /* lookup-only rounds replayed from a captured CUDA graph */
 } gpulsm_serve_stats;
 
 /* Open-loop load: Poisson arrivals at rate_per_s (0 = closed loop with

@@ -111,6 +111,8 @@ def test_results_same_alone_and_in_mix(gl, cuda):
     ordered = [req for _, _, req in flat]
     srv = fresh_server(gl, base_k, base_v)
     alone = [srv.wait(submit(srv, req)) for req in ordered]
+    # a lookup submitted alone is a lookup-only round: replayed from a CUDA graph
+    assert srv.stats()["graph_rounds"] == sum(1 for r in ordered if r[0] == "lookup")
     srv.close()
 
     want = oracle_answers(base_k, base_v, ordered)
