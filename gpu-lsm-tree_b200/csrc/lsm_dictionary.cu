@@ -17,6 +17,8 @@
 
 #include <algorithm>
 #include <atomic>
+#include <thread>
+#include <chrono>
 #include <cstring>
 #include <new>
 #include <stdexcept>
@@ -42,29 +44,10 @@ constexpr uint32_t kMaxSegments = 1u << 22;
 
 size_t align_up(size_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }
 
-struct ReceiptSrc {
-  const LevelDesc *desc[lsm::kMaxLevels];
-  uint32_t count;
-  const uint32_t *status;
-  unsigned long long *out;  // [kMaxLevels] counts, status, then the sequence number
-  unsigned long long seq;
-};
-
-// Writes the receipt into mapped pinned host memory; the sequence number goes
-// last, after a system-scope fence, so a host that reads the expected number
-// reads a complete receipt (no event in the stream, which would end the
-// chain of dependent launches).
-__global__ void receipt_kernel(ReceiptSrc src) {
+// Standalone receipt (updates embed theirs in their finishing kernel).
+__global__ void receipt_kernel(lsm::ReceiptSrc src) {
   chain_wait();
-  const uint32_t i = threadIdx.x;
-  if (i < lsm::kMaxLevels)
-    src.out[i] = (i < src.count && src.desc[i]) ? src.desc[i]->n : 0ull;
-  if (i == lsm::kMaxLevels) src.out[i] = *src.status;
-  __syncwarp();
-  if (i == 0) {
-    __threadfence_system();
-    *reinterpret_cast<volatile unsigned long long *>(src.out + lsm::kMaxLevels + 1) = src.seq;
-  }
+  lsm::write_receipt(src, 0ull);
 }
 
 // Bump allocator over one zeroed scratch region.
@@ -85,9 +68,7 @@ size_t merge_scratch_bytes(uint64_t rows) {
 }  // namespace
 
 struct LsmDictionary::Receipt {
-  unsigned long long n[lsm::kMaxLevels];
-  unsigned long long status;
-  unsigned long long seq;  // written last by the receipt kernel
+  unsigned long long w[lsm::kReceiptWords];  // tagged counts, then the tagged status
 };
 
 // ----------------------------------------------------------------------------
@@ -277,32 +258,66 @@ void LsmDictionary::ensure_sort_space(uint64_t n, cudaStream_t s) {
   words_cap_ = cap;
 }
 
-void LsmDictionary::post_receipt(cudaStream_t s) {
-  ReceiptSrc src{};
-  src.count = uint32_t(levels_.size());
-  for (size_t i = 0; i < levels_.size(); ++i) {
-    src.desc[i] = levels_[i].run ? levels_[i].run->desc : nullptr;
-    receipt_gens_[i] = levels_[i].gen;
-  }
-  src.status = dev_status_;
-  src.out = static_cast<unsigned long long *>(receipt_dev_);  // the mapped pinned host copy
-  src.seq = ++receipt_seq_;
-  launch_chained(receipt_kernel, 1, 32, 0, s, src);
+// A receipt for the level layout as it is on the host now (self = -1), or as
+// it will be after a cascade into `dest` whose own output is `self` (levels
+// above dest emptied).  Takes the next sequence number.
+lsm::ReceiptSrc LsmDictionary::next_receipt(int dest) {
+  lsm::ReceiptSrc r{};
+  r.count = uint32_t(levels_.size());
+  for (size_t i = 0; i < levels_.size(); ++i)
+    r.desc[i] = (int(i) < dest || !levels_[i].run) ? nullptr : levels_[i].run->desc;
+  r.self = dest;
+  r.out = static_cast<unsigned long long *>(receipt_dev_);  // the mapped pinned host copy
+  r.status = dev_status_;
+  r.seq = ++receipt_seq_;
+  return r;
+}
+
+// After an operation that posted a receipt: the gens it describes.
+void LsmDictionary::receipt_posted() {
+  for (size_t i = 0; i < levels_.size(); ++i) receipt_gens_[i] = levels_[i].gen;
   receipt_pending_ = true;
 }
 
-// Applies the newest posted receipt once it has landed (wait: after the last
-// operation, which posted it, has completed).  An older receipt that landed
-// while a newer one is in flight is never read: the newer one may be half
-// written over it.
+void LsmDictionary::post_receipt(cudaStream_t s) {
+  lsm::ReceiptSrc src = next_receipt(-1);
+  launch_chained(receipt_kernel, 1, 32, 0, s, src);
+  receipt_posted();
+}
+
+// Applies the newest posted receipt once every word of it carries its
+// sequence number (wait: after the last operation, which posted it, has
+// completed).  An older receipt that landed while a newer one is in flight is
+// never read: the newer one may be half written over it.
 void LsmDictionary::apply_receipt(bool wait) {
   if (!receipt_pending_) return;
-  const volatile unsigned long long *seq = &receipt_host_->seq;
-  if (wait) GPULSM_CUDA(cudaEventSynchronize(op_done_));
-  if (*seq != receipt_seq_) return;
-  std::atomic_thread_fence(std::memory_order_acquire);
+  const volatile unsigned long long *w = receipt_host_->w;
+  unsigned long long v[lsm::kReceiptWords];
+  auto landed = [&]() {
+    for (int i = 0; i < lsm::kReceiptWords; ++i) v[i] = w[i];
+    for (int i = 0; i < lsm::kMaxLevels; ++i)
+      if ((v[i] >> 33) != (receipt_seq_ & 0x7fffffffu)) return false;
+    return (v[lsm::kMaxLevels] >> 32) == receipt_seq_;
+  };
+  if (!landed()) {
+    if (!wait) return;
+    // the receipt may belong to an earlier batch of the operation in progress:
+    // wait for the operations before it, then for the receipt itself
+    GPULSM_CUDA(cudaEventSynchronize(op_done_));
+    const auto t0 = std::chrono::steady_clock::now();
+    while (!landed()) {
+      if (std::chrono::steady_clock::now() - t0 > std::chrono::seconds(60))
+        throw std::runtime_error("GPU dictionary receipt did not arrive");
+      std::this_thread::yield();
+    }
+  }
   receipt_pending_ = false;
-  const Receipt r = *receipt_host_;
+  struct {
+    unsigned long long n[lsm::kMaxLevels];
+    unsigned long long status;
+  } r;
+  for (int i = 0; i < lsm::kMaxLevels; ++i) r.n[i] = v[i] & lsm::kReceiptCountMask;
+  r.status = v[lsm::kMaxLevels] & 0xffffffffull;
   status_bits_ |= uint32_t(r.status);
   // A level holds each key once, so one level with more rows than the
   // capacity means more live keys (tombstones included) than the capacity;
@@ -343,9 +358,9 @@ void LsmDictionary::release_levels(cudaStream_t) {
 
 // ----------------------------------------------------------------------------
 RunBuffer *LsmDictionary::sort_dedup(const uint32_t *keys, const uint32_t *values, uint64_t n,
-                                     bool tombstone, cudaStream_t s) {
+                                     bool tombstone, cudaStream_t s, const lsm::ReceiptSrc *rcpt) {
   ensure_sort_space(n, s);
-  if (n <= lsm::admit::kMaxKeys) return bucket_admit(keys, values, n, tombstone, s);
+  if (n <= lsm::admit::kMaxKeys) return bucket_admit(keys, values, n, tombstone, s, rcpt);
   const uint32_t nn = uint32_t(n);
   const size_t radix_bytes = align_up(radix::workspace_bytes(n, 4));
   const uint64_t dtiles = (n + lsm::kCompactTile - 1) / lsm::kCompactTile;
@@ -373,7 +388,7 @@ RunBuffer *LsmDictionary::sort_dedup(const uint32_t *keys, const uint32_t *value
 // (histogram, scan, scatter - no look-back chain), then one CTA per top-byte
 // bucket sorts, deduplicates and writes the level rows (lsm_admit.cuh).
 RunBuffer *LsmDictionary::bucket_admit(const uint32_t *keys, const uint32_t *values, uint64_t n,
-                                       bool tombstone, cudaStream_t s) {
+                                       bool tombstone, cudaStream_t s, const lsm::ReceiptSrc *rcpt) {
   namespace ad = lsm::admit;
   const uint32_t nn = uint32_t(n);
   const uint32_t tiles = ad::part_tiles(n);
@@ -394,12 +409,13 @@ RunBuffer *LsmDictionary::bucket_admit(const uint32_t *keys, const uint32_t *val
                  tiles, static_cast<const uint32_t *>(prefix), static_cast<const uint32_t *>(top), words_[1]);
   launch_chained(ad::admit_bucket_kernel, ad::kBuckets, ad::kThreads, ad::kBucketSmemBytes, s, words_[1], words_[0],
                  static_cast<const uint32_t *>(top), nn, tombstone ? 1 : 0, carry->keys, carry->vals, carry->flags,
-                 carry->desc, carry->dir, carry->dir_bits, rows_log2_, lb, counter, dev_status_);
+                 carry->desc, carry->dir, carry->dir_bits, rows_log2_, lb, counter, dev_status_,
+                 rcpt ? *rcpt : lsm::ReceiptSrc{});
   return carry;
 }
 
 RunBuffer *LsmDictionary::merge(RunBuffer *newer, RunBuffer *older, uint64_t out_upper,
-                                bool drop_tombstones, cudaStream_t s) {
+                                bool drop_tombstones, cudaStream_t s, const lsm::ReceiptSrc *rcpt) {
   RunBuffer *out = pool_.acquire(out_upper, s);
   const uint64_t tiles = std::max<uint64_t>(1, (out_upper + lsm::kMergeTile - 1) / lsm::kMergeTile);
   const size_t zero_bytes = merge_scratch_bytes(out_upper);
@@ -434,7 +450,8 @@ RunBuffer *LsmDictionary::merge(RunBuffer *newer, RunBuffer *older, uint64_t out
                  newer->desc, older->keys, older->vals, older->flags, older->desc, out->keys, out->vals, out->flags,
                  out->desc, out->dir, out->dir_bits, rows_log2_,
                  static_cast<unsigned long long>(std::min<uint64_t>(out_upper, out->cap)),
-                 static_cast<unsigned long long>(out->cap), parts, lb, counter, dev_status_, trace);
+                 static_cast<unsigned long long>(out->cap), parts, lb, counter, dev_status_, trace,
+                 rcpt ? *rcpt : lsm::ReceiptSrc{});
   if (trace) {
     GPULSM_CUDA(cudaEventRecord(tr.stop, s));
     traces_.push_back(tr);
@@ -485,7 +502,11 @@ void LsmDictionary::fit_now(RunBuffer *run, uint64_t upper, cudaStream_t s) {
   ++next_gen_;  // the level table must pick up the model
 }
 
-void LsmDictionary::cascade(RunBuffer *carry, uint64_t carry_upper, bool carry_tombs, cudaStream_t s) {
+// Lands a sorted, deduplicated batch (leveling).  With want_receipt the
+// update's receipt goes into its final merge kernel (or, without a merge, a
+// standalone receipt kernel).
+void LsmDictionary::cascade(RunBuffer *carry, uint64_t carry_upper, bool carry_tombs, cudaStream_t s,
+                            bool want_receipt) {
   const size_t L = levels_.size();
   size_t dest = 0;
   uint64_t acc = carry_upper;
@@ -501,11 +522,14 @@ void LsmDictionary::cascade(RunBuffer *carry, uint64_t carry_upper, bool carry_t
   RunBuffer *x = carry;
   uint64_t xu = carry_upper;
   bool xt = carry_tombs;
+  const size_t merges = dest + (dest_occupied ? 1 : 0);
+  lsm::ReceiptSrc rcpt{};
+  if (want_receipt && merges) rcpt = next_receipt(int(dest));  // the layout after this cascade
   for (size_t i = 0; i < dest; ++i) {
     const bool last = (i + 1 == dest) && !dest_occupied;
     const uint64_t ou = xu + levels_[i].upper;
     const bool drop = last && !deeper;
-    x = merge(x, levels_[i].run, ou, drop, s);
+    x = merge(x, levels_[i].run, ou, drop, s, (want_receipt && i + 1 == merges) ? &rcpt : nullptr);
     xu = ou;
     xt = !drop && (xt || levels_[i].tombs);
     levels_[i] = Level{};
@@ -513,7 +537,7 @@ void LsmDictionary::cascade(RunBuffer *carry, uint64_t carry_upper, bool carry_t
   }
   if (dest_occupied) {
     const uint64_t ou = xu + levels_[dest].upper;
-    x = merge(x, levels_[dest].run, ou, !deeper, s);
+    x = merge(x, levels_[dest].run, ou, !deeper, s, want_receipt ? &rcpt : nullptr);
     xu = ou;
     xt = deeper && (xt || levels_[dest].tombs);
   }
@@ -522,6 +546,7 @@ void LsmDictionary::cascade(RunBuffer *carry, uint64_t carry_upper, bool carry_t
   levels_[dest].gen = next_gen_++;
   levels_[dest].tombs = xt;  // its directory was written by the kernel that wrote its rows
   fit_model(x, levels_[dest].upper, s);
+  if (want_receipt && !merges) post_receipt(s);
 }
 
 // Merge every occupied level, newest first, into one tombstone-free run at
@@ -671,8 +696,16 @@ void LsmDictionary::admit(const uint32_t *keys, const uint32_t *values, uint64_t
       apply_receipt(true);
       reject_if_failed();
     }
-    RunBuffer *carry = sort_dedup(keys + off, values ? values + off : nullptr, m, tombstone, s);
-    cascade(carry, m, tombstone, s);
+    // a batch that lands in the empty level 0 without a merge has its
+    // receipt written by the admission kernel; otherwise the cascade's
+    // final merge writes it
+    const bool embed = levels_[0].run == nullptr && m <= lsm::admit::kMaxKeys;
+    lsm::ReceiptSrc rcpt{};
+    if (embed) rcpt = next_receipt(0);
+    RunBuffer *carry = sort_dedup(keys + off, values ? values + off : nullptr, m, tombstone, s,
+                                  embed ? &rcpt : nullptr);
+    cascade(carry, m, tombstone, s, !embed);
+    receipt_posted();
   }
 }
 
@@ -703,7 +736,7 @@ void LsmDictionary::bulk_build(const uint32_t *keys, const uint32_t *values, uin
   failure_.clear();
   receipt_pending_ = false;
   if (n) {
-    RunBuffer *run = sort_dedup(keys, values, n, false, s);
+    RunBuffer *run = sort_dedup(keys, values, n, false, s, nullptr);
     Level &top = levels_.back();
     top.run = run;
     top.upper = n;
@@ -723,8 +756,7 @@ void LsmDictionary::insert(const uint32_t *keys, const uint32_t *values, uint64_
   apply_receipt(false);
   reject_if_failed();
   begin_op(s);
-  admit(keys, values, n, false, s);
-  post_receipt(s);
+  admit(keys, values, n, false, s);  // every batch's finishing kernel writes the receipt
   end_op(s);
 }
 
@@ -735,8 +767,7 @@ void LsmDictionary::erase(const uint32_t *keys, uint64_t n, cudaStream_t s) {
   apply_receipt(false);
   reject_if_failed();
   begin_op(s);
-  admit(keys, nullptr, n, true, s);
-  post_receipt(s);
+  admit(keys, nullptr, n, true, s);  // every batch's finishing kernel writes the receipt
   end_op(s);
 }
 

@@ -16,6 +16,7 @@ namespace gpulsm {
 
 namespace lsm {
 struct LevelDesc;
+struct ReceiptSrc;
 struct LevelView;
 }
 
@@ -121,16 +122,18 @@ class LsmDictionary {
   void end_op(cudaStream_t s);
   void apply_receipt(bool wait);
   void post_receipt(cudaStream_t s);
+  lsm::ReceiptSrc next_receipt(int dest);
+  void receipt_posted();
   void reject_if_failed() const;
   void admit(const uint32_t *keys, const uint32_t *values, uint64_t n, bool tombstone,
              cudaStream_t s);
   RunBuffer *sort_dedup(const uint32_t *keys, const uint32_t *values, uint64_t n, bool tombstone,
-                        cudaStream_t s);
+                        cudaStream_t s, const lsm::ReceiptSrc *rcpt);
   RunBuffer *bucket_admit(const uint32_t *keys, const uint32_t *values, uint64_t n, bool tombstone,
-                          cudaStream_t s);
-  void cascade(RunBuffer *carry, uint64_t carry_upper, bool carry_tombs, cudaStream_t s);
+                          cudaStream_t s, const lsm::ReceiptSrc *rcpt);
+  void cascade(RunBuffer *carry, uint64_t carry_upper, bool carry_tombs, cudaStream_t s, bool want_receipt);
   RunBuffer *merge(RunBuffer *newer, RunBuffer *older, uint64_t out_upper, bool drop_tombstones,
-                   cudaStream_t s);
+                   cudaStream_t s, const lsm::ReceiptSrc *rcpt = nullptr);
   // Range batches: merge every level into one tombstone-free run when the
   // rows the batch covers outweigh the merge; returns the single level to
   // answer from, or -1 to use the per-query k-way merge.
@@ -168,7 +171,7 @@ class LsmDictionary {
   // receipts (pinned host copy of the level row counts and status)
   Receipt *receipt_host_ = nullptr;
   void *receipt_dev_ = nullptr;
-  unsigned long long receipt_seq_ = 0;  // sequence number of the newest posted receipt
+  uint32_t receipt_seq_ = 0;  // sequence number of the newest posted receipt
   bool receipt_pending_ = false;
   std::vector<uint64_t> receipt_gens_;
 

@@ -47,6 +47,35 @@ struct LevelSet {
   uint32_t count;
 };
 
+// Receipt of an update, written into mapped pinned host memory by the kernel
+// that finishes it: the row count of every level afterwards and the status
+// word, each one 8-byte word tagged with the update's sequence number
+// (count | seq << 33, status | seq << 32), so the host validates every word
+// on its own and neither a fence nor an event is needed.
+struct ReceiptSrc {
+  const LevelDesc *desc[kMaxLevels];
+  unsigned long long *out;  // kMaxLevels counts, then the status
+  const uint32_t *status;
+  uint32_t count;
+  int32_t self;             // level whose count is the writing kernel's own output
+  uint32_t seq;
+};
+constexpr int kReceiptWords = kMaxLevels + 1;
+constexpr unsigned long long kReceiptCountMask = (1ull << 33) - 1ull;
+
+// Run by the first warp of the finishing CTA.
+__device__ __forceinline__ void write_receipt(const ReceiptSrc &r, unsigned long long self_n) {
+  const uint32_t i = threadIdx.x & 31u;
+  if (i < uint32_t(kMaxLevels)) {
+    unsigned long long n = 0;
+    if (int32_t(i) == r.self) n = self_n;
+    else if (i < r.count && r.desc[i]) n = r.desc[i]->n;
+    r.out[i] = (n & kReceiptCountMask) | (static_cast<unsigned long long>(r.seq & 0x7fffffffu) << 33);
+  } else if (i == uint32_t(kMaxLevels)) {
+    r.out[i] = static_cast<unsigned long long>(*r.status) | (static_cast<unsigned long long>(r.seq) << 32);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Admission: pack (key, value) into one u64 word (key in the high half so an
 // LSD sort on bits 32..63 orders by key and keeps input order among equal
@@ -355,7 +384,8 @@ __global__ void __launch_bounds__(kMergeThreads, 4) merge_kernel(
     uint8_t *__restrict__ of, LevelDesc *__restrict__ odesc, uint32_t *__restrict__ odir, uint32_t dir_bits,
     uint32_t rows_log2, unsigned long long out_upper, unsigned long long out_capacity,
     const unsigned long long *__restrict__ parts, unsigned long long *__restrict__ lb,
-    uint32_t *__restrict__ tile_counter, uint32_t *__restrict__ status, unsigned long long *__restrict__ trace) {
+    uint32_t *__restrict__ tile_counter, uint32_t *__restrict__ status, unsigned long long *__restrict__ trace,
+    ReceiptSrc rcpt) {
   extern __shared__ __align__(128) unsigned char merge_dyn[];
   MergeSmem &sm = *reinterpret_cast<MergeSmem *>(merge_dyn);
   chain_wait();
@@ -558,6 +588,7 @@ __global__ void __launch_bounds__(kMergeThreads, 4) merge_kernel(
     }
     asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");  // stores done before the CTA retires
   }
+  if (last_tile && rcpt.out && threadIdx.x < 32) write_receipt(rcpt, n_out < out_capacity ? n_out : out_capacity);
 }
 
 // ---------------------------------------------------------------------------
