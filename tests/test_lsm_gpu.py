@@ -396,3 +396,31 @@ def test_merge_timing_hook_counts_rows(gl, cuda):
     assert t.d.kernel_timing_read()["launches"] == 0  # a read resets the record
     q = rng.integers(0, 1 << 32, 4096, dtype=np.uint64).astype(np.uint32)
     t.lookup(q)
+
+
+def test_paper_sweep_runner_writes_reference_csvs(gl, cuda, tmp_path):
+    """The sweep runner (gpu-lsm-tree_b200/sweep.py) on a reduced protocol:
+    the reference's three CSV files with its columns, every lookup validated,
+    range sums equal to range counts (all values are 1) and digests equal to
+    the oracle's."""
+    import csv
+    import importlib
+
+    sw = importlib.import_module("gpu-lsm-tree_b200.sweep")
+    rc = sw.main(["--out", str(tmp_path), "--batch-logs", "16", "--insert-limit-log", "19",
+                  "--query-limit-log", "18", "--range-chunk-log", "16", "--include-count"])
+    assert rc == 0
+    ins = list(csv.DictReader(open(tmp_path / "insertion_b16.csv")))
+    look = list(csv.DictReader(open(tmp_path / "lookup_b16.csv")))
+    rng = list(csv.DictReader(open(tmp_path / "count_range_b16.csv")))
+    assert len(ins) == 8 and [int(r["resident_elements"]) for r in ins] == [(i + 1) << 16 for i in range(8)]
+    assert {r["scenario"] for r in look} == {"all_existing", "none_existing"} and len(look) == 2 * 4
+    assert len(rng) == 4 * 2 * 2  # 4 steps under the query limit, 8 and 1024 hits, count + range
+    # digests against the oracle for the first step
+    o = OracleLSM()
+    o.insert(key_for_index(np.arange(1 << 16)), np.ones(1 << 16, np.uint32))
+    for expected in (8, 1024):
+        lo, hi = sw.range_queries(1 << 16, 1 << 16, expected, 0x30000 + 1 + expected)
+        want = range_digest(o.range_sum(lo, hi))
+        row = [r for r in rng if r["r"] == "1" and r["operation"] == "range" and r["expected_hits"] == str(expected)]
+        assert (int(row[0]["checksum_sum"]), int(row[0]["checksum_xor"])) == want

@@ -149,3 +149,23 @@ def test_paper_sweep_protocol():
         assert abs(float(sums.mean()) - expected_hits) < 0.2 * expected_hits
         s, x = range_digest(sums)
         assert s == int(sums.sum())
+
+
+def test_sweep_runner_inputs_match_the_sweep_protocol():
+    """The paper-sweep runner generates the same keys, queries and digests as
+    the sweep protocol restated in scenarios.py (FliX/paper_lsmu_sweep.cu)."""
+    import importlib
+
+    import scenarios as sc
+
+    sw = importlib.import_module("gpu-lsm-tree_b200.sweep")
+    i = np.arange(0, 1 << 16, 7, dtype=np.uint64)
+    assert np.array_equal(sw.key_for_index(i), sc.key_for_index(i))
+    for hits in (True, False):
+        assert np.array_equal(sw.lookup_queries(4096, 1 << 20, hits, 0x10003),
+                              sc.sweep_lookup_queries(4096, 1 << 20, hits, 0x10003))
+    lo, hi = sw.range_queries(4096, 1 << 20, 1024, 0x30401)
+    lo2, hi2 = sc.sweep_range_queries(4096, 1 << 20, 1024, 0x30401)
+    assert np.array_equal(lo, lo2) and np.array_equal(hi, hi2)
+    r = np.random.default_rng(3).integers(0, 1 << 32, 5000, dtype=np.uint64).astype(np.uint32)
+    assert sw.range_digest(r, 77) == sc.range_digest(r, 77)
