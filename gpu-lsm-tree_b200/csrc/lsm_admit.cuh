@@ -423,6 +423,7 @@ constexpr uint32_t kMaxBin = 32;   // larger bins (skew) take the LSD passes ins
 struct BucketSmem {
   unsigned long long words[kCap];  // the bucket's words in input order
   uint16_t idx[kCap];              // input position of each element, in sorted order
+  uint32_t sk[kCap];               // counting-sort output: in-bin key bits << 13 | input position
   uint32_t bins[kBins];            // bin counts, then bin ends
   RankSmem rank;
   uint32_t start[kBuckets + 1];
@@ -432,60 +433,67 @@ struct BucketSmem {
 };
 
 // Fast in-bucket sort: one counting pass on the 12 highest varying key bits
-// (shared atomics: order inside a bin is arbitrary), then every bin - about
-// one element on uniform keys - is insertion-sorted by (key, input position),
-// which restores input order among equal keys, and the words are permuted
-// into that order in place (through registers).  Returns false (nothing
-// changed) when a bin exceeds kMaxBin.
+// (shared atomics: order inside a bin is arbitrary), then every element
+// finds its place inside its bin - about one other element on uniform keys -
+// by counting the bin's elements that order before it by (key, input
+// position), which restores input order among equal keys; the words are then
+// permuted into that order in place (through registers).  Inside a bin the
+// keys differ only in the bits below the bin bits (ds <= 12 of them), so
+// (those bits << 13 | input position) orders a bin in one 32-bit compare.
+// Returns false (nothing changed) when a bin exceeds kMaxBin.
+static_assert(kCap <= (1u << 13), "input positions fit 13 bits");
 __device__ __forceinline__ bool bin_sort(BucketSmem &sm, uint32_t cnt, uint32_t vary) {
   const uint32_t hb = 31u - __clz(vary);
   const uint32_t ds = hb >= 11u ? hb - 11u : 0u;
+  const uint32_t low = (1u << ds) - 1u;
   for (uint32_t d = threadIdx.x; d < kBins; d += kThreads) sm.bins[d] = 0;
   if (threadIdx.x == 0) sm.maxbin = 0;
   __syncthreads();
   for (uint32_t e = threadIdx.x; e < cnt; e += kThreads) atomicAdd(&sm.bins[(word_key(sm.words[e]) >> ds) & (kBins - 1)], 1u);
   __syncthreads();
-  // exclusive scan of the bins: thread t owns kBins / kThreads consecutive bins
-  constexpr uint32_t per = kBins / kThreads;
-  uint32_t c[per], sum = 0, mx = 0;
+  // exclusive scan of the bins: thread t owns the 8 consecutive bins [8t, 8t + 8),
+  // read and written as two 16-byte vectors
+  static_assert(kBins == 8u * kThreads, "8 bins per thread");
+  uint4 *bv = reinterpret_cast<uint4 *>(sm.bins);
+  const uint4 lo4 = bv[2 * threadIdx.x], hi4 = bv[2 * threadIdx.x + 1];
+  uint32_t c[8] = {lo4.x, lo4.y, lo4.z, lo4.w, hi4.x, hi4.y, hi4.z, hi4.w};
+  uint32_t sum = 0, mx = 0;
 #pragma unroll
-  for (uint32_t j = 0; j < per; ++j) {
-    c[j] = sm.bins[threadIdx.x * per + j];
+  for (int j = 0; j < 8; ++j) {
     sum += c[j];
     mx = max(mx, c[j]);
   }
   uint32_t run = block_exclusive_scan<kThreads>(sum, sm.rank.scan, &sm.rank.total);
   if (mx) atomicMax(&sm.maxbin, mx);
 #pragma unroll
-  for (uint32_t j = 0; j < per; ++j) {
-    sm.bins[threadIdx.x * per + j] = run;
-    run += c[j];
+  for (int j = 0; j < 8; ++j) {
+    const uint32_t x = c[j];
+    c[j] = run;
+    run += x;
   }
+  bv[2 * threadIdx.x] = make_uint4(c[0], c[1], c[2], c[3]);
+  bv[2 * threadIdx.x + 1] = make_uint4(c[4], c[5], c[6], c[7]);
   __syncthreads();
   if (sm.maxbin > kMaxBin) return false;  // uniform across the block
   for (uint32_t e = threadIdx.x; e < cnt; e += kThreads) {
-    const uint32_t p = atomicAdd(&sm.bins[(word_key(sm.words[e]) >> ds) & (kBins - 1)], 1u);
-    sm.idx[p] = uint16_t(e);
+    const uint32_t k = word_key(sm.words[e]);
+    const uint32_t p = atomicAdd(&sm.bins[(k >> ds) & (kBins - 1)], 1u);
+    sm.sk[p] = ((k & low) << 13) | e;
   }
   __syncthreads();  // bins[d] now holds the end of bin d
-  for (uint32_t d = threadIdx.x; d < kBins; d += kThreads) {
-    const uint32_t b = d ? sm.bins[d - 1] : 0u, e = sm.bins[d];
-    for (uint32_t i = b + 1; i < e; ++i) {  // insertion sort by (key, input position)
-      const uint16_t x = sm.idx[i];
-      const uint32_t kx = word_key(sm.words[x]);
-      uint32_t j = i;
-      while (j > b) {
-        const uint16_t y = sm.idx[j - 1];
-        const uint32_t ky = word_key(sm.words[y]);
-        if (ky < kx || (ky == kx && y < x)) break;
-        sm.idx[j] = y;
-        --j;
-      }
-      sm.idx[j] = x;
-    }
+  const uint32_t keff = (cnt + kThreads - 1) / kThreads;
+#pragma unroll
+  for (int i = 0; i < kItems; ++i) {
+    const uint32_t p = uint32_t(i) * kThreads + threadIdx.x;
+    if (uint32_t(i) >= keff || p >= cnt) continue;
+    const uint32_t x = sm.sk[p], e = x & 0x1fffu;
+    const uint32_t bin = (word_key(sm.words[e]) >> ds) & (kBins - 1);
+    const uint32_t b0 = bin ? sm.bins[bin - 1] : 0u, b1 = sm.bins[bin];
+    uint32_t r = 0;
+    for (uint32_t q = b0; q < b1; ++q) r += sm.sk[q] < x ? 1u : 0u;  // at most kMaxBin
+    sm.idx[b0 + r] = uint16_t(e);
   }
   __syncthreads();
-  const uint32_t keff = (cnt + kThreads - 1) / kThreads;
   unsigned long long t[kItems];
 #pragma unroll
   for (int i = 0; i < kItems; ++i) {

@@ -176,6 +176,9 @@ LsmDictionary::LsmDictionary(const DictConfig &config)
   GPULSM_CUDA(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, dev));
   GPULSM_CUDA(cudaFuncSetAttribute(lsm::admit::admit_bucket_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    int(lsm::admit::kBucketSmemBytes)));
+  // two bucket CTAs per SM need nearly all of its shared memory
+  GPULSM_CUDA(cudaFuncSetAttribute(lsm::admit::admit_bucket_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                   int(cudaSharedmemCarveoutMaxShared)));
   GPULSM_CUDA(cudaMalloc(&dev_status_, 256));
   GPULSM_CUDA(cudaMalloc(&table_dev_, sizeof(lsm::LevelSet)));
   GPULSM_CUDA(cudaMemset(dev_status_, 0, 256));
