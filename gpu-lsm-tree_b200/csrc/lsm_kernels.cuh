@@ -31,6 +31,16 @@ static_assert(sizeof(LevelDesc) == 32, "LevelDesc layout");
 
 // How a level is searched: its radix directory (dir), its learned position
 // model (mh/ms, search mode 1) or, with neither, binary search over all rows.
+__device__ __forceinline__ LevelDesc load_desc(const LevelDesc *p) {
+  LevelDesc d;
+  d.n = __ldg(&p->n);
+  d.kmin = __ldg(&p->kmin);
+  d.kmax = __ldg(&p->kmax);
+  d.shift = __ldg(&p->shift);
+  d.nbuckets = __ldg(&p->nbuckets);
+  return d;
+}
+
 struct LevelView {
   const uint32_t *keys;
   const uint32_t *vals;
@@ -390,8 +400,16 @@ __global__ void __launch_bounds__(kMergeThreads, 4) merge_kernel(
   MergeSmem &sm = *reinterpret_cast<MergeSmem *>(merge_dyn);
   chain_wait();
   if (threadIdx.x == 0) sm.tile = atomicAdd(tile_counter, 1u);
+  // the inputs' descriptors load while the ticket is taken
+  LevelDesc da, db;
+  da.n = adesc->n;
+  da.kmin = adesc->kmin;
+  da.kmax = adesc->kmax;
+  db.n = bdesc->n;
+  db.kmin = bdesc->kmin;
+  db.kmax = bdesc->kmax;
   __syncthreads();
-  const uint64_t na = adesc->n, nb = bdesc->n, total = na + nb;
+  const uint64_t na = da.n, nb = db.n, total = na + nb;
   const uint32_t tile = sm.tile;
   const uint64_t d0 = uint64_t(tile) * kMergeTile;
   if (total == 0) {
@@ -429,8 +447,8 @@ __global__ void __launch_bounds__(kMergeThreads, 4) merge_kernel(
   }
   // while the copies fly: the keys around the tile, the output geometry
   // every output key lies in the union of the inputs' key ranges
-  const uint32_t kmin = na == 0 ? bdesc->kmin : nb == 0 ? adesc->kmin : min(adesc->kmin, bdesc->kmin);
-  const uint32_t kmax = na == 0 ? bdesc->kmax : nb == 0 ? adesc->kmax : max(adesc->kmax, bdesc->kmax);
+  const uint32_t kmin = na == 0 ? db.kmin : nb == 0 ? da.kmin : min(da.kmin, db.kmin);
+  const uint32_t kmax = na == 0 ? db.kmax : nb == 0 ? da.kmax : max(da.kmax, db.kmax);
   const DirGeom geom = dir_geometry(kmin, kmax, out_upper, dir_bits, rows_log2);
   // key of the A row just before this tile (shadows a leading B row); the
   // largest key consumed before / by this tile bounds its directory buckets
@@ -557,9 +575,12 @@ __global__ void __launch_bounds__(kMergeThreads, 4) merge_kernel(
 #pragma unroll
   for (int i = 0; i < kMergeItems; ++i) {
     const uint32_t j = uint32_t(i) * kMergeThreads + threadIdx.x;
+    // row j - 1 is the previous lane's row of the same item (lane 0: shared memory)
+    uint32_t pk = __shfl_up_sync(0xffffffffu, rk[i], 1);
+    if ((threadIdx.x & 31u) == 0 && j) pk = sout[j - 1];
     if (j < tile_kept) {
       const int32_t bj = int32_t((rk[i] - gk) >> gs);
-      const int32_t bprev = j ? int32_t((sout[j - 1] - gk) >> gs) : bp;
+      const int32_t bprev = j ? int32_t((pk - gk) >> gs) : bp;
       for (int32_t bb = bprev + 1; bb <= bj; ++bb) odir[bb] = g0 + j;
     }
   }
@@ -586,7 +607,9 @@ __global__ void __launch_bounds__(kMergeThreads, 4) merge_kernel(
         trace[3] = geom.nbuckets;
       }
     }
-    asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");  // stores done before the CTA retires
+    // the staged rows have been read out of shared memory before the CTA
+    // retires; the global writes complete with the grid
+    asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
   }
   if (last_tile && rcpt.out && threadIdx.x < 32) write_receipt(rcpt, n_out < out_capacity ? n_out : out_capacity);
 }
@@ -636,15 +659,6 @@ __device__ __forceinline__ uint64_t level_upper_bound(const LevelView &L, const 
   return level_lower_bound(L, d, x + 1u);
 }
 
-__device__ __forceinline__ LevelDesc load_desc(const LevelDesc *p) {
-  LevelDesc d;
-  d.n = __ldg(&p->n);
-  d.kmin = __ldg(&p->kmin);
-  d.kmax = __ldg(&p->kmax);
-  d.shift = __ldg(&p->shift);
-  d.nbuckets = __ldg(&p->nbuckets);
-  return d;
-}
 
 __device__ __forceinline__ bool row_is_tomb(const LevelView &L, uint64_t p, uint32_t v) {
   return v == kTombValue && (L.flags[p] & kFlagTomb);
