@@ -184,17 +184,25 @@ def run_ours(args):
     stream = torch.cuda.current_stream(dev)
     pairs = [None, None]
 
-    def step(ev=None):
+    def step(ev=None, batch_ev=None):
         d.clear()
         if ev is not None:
             ev["start"].record(stream)
+        if batch_ev is not None:
+            batch_ev[0].record(stream)
         for i, (kind, k, v) in enumerate(ops_dev):
             if kind == "insert":
                 d.insert(k, v)
             else:
                 d.erase(k)
-            if ev is not None:
-                ev["batch"][i].record(stream)
+            if batch_ev is not None:  # latency of one batch alone: admission and merges
+                d.join()
+                batch_ev[i + 1].record(stream)
+        # updates return once admitted (their merges overlap the next batch's
+        # admission); the update phase ends when every merge has completed
+        d.join()
+        if ev is not None:
+            ev["update"].record(stream)
         d.lookup(q, out_v, out_f)
         if ev is not None:
             ev["lookup"].record(stream)
@@ -218,7 +226,7 @@ def run_ours(args):
 
     def new_events():
         mk = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
-        return {"start": mk(), "batch": [mk() for _ in ops_dev], "lookup": mk(), "range": mk()}
+        return {"start": mk(), "update": mk(), "lookup": mk(), "range": mk()}
 
     events = [new_events() for _ in range(args.steps)]
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -235,15 +243,18 @@ def run_ours(args):
         t1.record(stream)
         torch.cuda.synchronize(dev)
     launches = lib.gpulsm_launch_count() - launches0
-    # the dominant kernel (merge_kernel): one more step of the same workload
-    # with every merge launch bracketed by CUDA events on the dictionary's
-    # launching stream (events between chained launches would slow the timed
-    # steps, so they stay out of them)
+    # One more step of the same workload with every batch joined before the
+    # next (no overlap of its merges with the next admission): per-batch
+    # latency, and the dominant kernel (merge_kernel) timed alone, every merge
+    # launch bracketed by CUDA events on the dictionary's merge stream (events
+    # between chained launches would slow the timed steps, so they stay out)
+    batch_ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(ops_dev) + 1)]
     d.kernel_timing(True)
     d.kernel_timing_read()
-    step()
+    step(batch_ev=batch_ev)
     merge_timing = d.kernel_timing_read()
     d.kernel_timing(False)
+    torch.cuda.synchronize(dev)
     total_ms = t0.elapsed_time(t1)
     if world > 1:
         import torch.distributed as dist
@@ -254,16 +265,12 @@ def run_ours(args):
         dist.barrier()
 
     # per-phase times (device events on the launching stream)
-    upd_ms, look_ms, range_ms, batch_ms = [], [], [], []
-    n_ops = len(ops_dev)
+    upd_ms, look_ms, range_ms = [], [], []
     for ev in events:
-        prev = ev["start"]
-        for i in range(n_ops):
-            batch_ms.append((ops_dev[i][0], prev.elapsed_time(ev["batch"][i])))
-            prev = ev["batch"][i]
-        upd_ms.append(ev["start"].elapsed_time(ev["batch"][-1]))
-        look_ms.append(ev["batch"][-1].elapsed_time(ev["lookup"]))
+        upd_ms.append(ev["start"].elapsed_time(ev["update"]))
+        look_ms.append(ev["update"].elapsed_time(ev["lookup"]))
         range_ms.append(ev["lookup"].elapsed_time(ev["range"]))
+    batch_ms = [(ops_dev[i][0], batch_ev[i].elapsed_time(batch_ev[i + 1])) for i in range(len(ops_dev))]
     ms_per_step = total_ms / args.steps
     upd_keys = w.inserted_keys + w.erased_keys
     ops_per_step = upd_keys + nq + nr
@@ -279,7 +286,8 @@ def run_ours(args):
     phases = {"update": (upd, update_gbs), "lookup": (look, lookup_gbs), "range": (rng_ms, range_gbs)}
     ml = max(merge_timing["launches"], 1)
     merge_gbs = merge_timing["bytes"] / max(merge_timing["ms"], 1e-9) / 1e6
-    roofline = {"bound": "hbm", "kernel": "lsm::merge_kernel", "measured": "one extra step, CUDA events per launch",
+    roofline = {"bound": "hbm", "kernel": "lsm::merge_kernel",
+                "measured": "one extra step with every batch joined, CUDA events per launch",
                 "achieved": round(merge_gbs, 1), "peak": peak,
                 "unit": "GB/s", "frac": round(merge_gbs / peak, 4), "peak_source": peak_kind,
                 "traffic": None if MERGE_TRAFFIC_RATIO is None else
@@ -740,6 +748,7 @@ def profile_case(args):
         for i in range(64):
             d.clear()
             d.insert(batches[i % 8], vals)
+        d.join()
         e1.record()
         torch.cuda.synchronize()
         print(json.dumps({"case": "admit", "ms_per_batch": round(e0.elapsed_time(e1) / 64, 4),

@@ -166,6 +166,7 @@ def load() -> C.CDLL:
         "gpulsm_dict_create": (i32, [C.POINTER(DictConfig), pvp]),
         "gpulsm_dict_destroy": (i32, [vp]),
         "gpulsm_dict_clear": (i32, [vp, vp]),
+        "gpulsm_dict_join": (i32, [vp, vp]),
         "gpulsm_dict_bulk_build": (i32, [vp, vp, vp, u64, vp]),
         "gpulsm_dict_insert": (i32, [vp, vp, vp, u64, vp]),
         "gpulsm_dict_erase": (i32, [vp, vp, u64, vp]),

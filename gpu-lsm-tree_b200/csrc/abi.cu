@@ -153,6 +153,13 @@ int gpulsm_dict_clear(gpulsm_dict *d, void *stream) {
   });
 }
 
+int gpulsm_dict_join(gpulsm_dict *d, void *stream) {
+  return guarded([&] {
+    need(d, "dict");
+    d->impl.join(S(stream));
+  });
+}
+
 int gpulsm_dict_bulk_build(gpulsm_dict *d, const uint32_t *keys, const uint32_t *values,
                            uint64_t count, void *stream) {
   return guarded([&] {

@@ -519,7 +519,7 @@ __global__ void __launch_bounds__(kThreads, 2) admit_bucket_kernel(
     const uint32_t *__restrict__ top_hist, uint32_t n, int tombstone, uint32_t *__restrict__ out_keys,
     uint32_t *__restrict__ out_vals, uint8_t *__restrict__ out_flags, LevelDesc *__restrict__ out_desc,
     uint32_t *__restrict__ out_dir, uint32_t dir_bits, uint32_t rows_log2, unsigned long long *__restrict__ lb,
-    uint32_t *__restrict__ tile_counter, uint32_t *__restrict__ status, ReceiptSrc rcpt) {
+    uint32_t *__restrict__ tile_counter, uint32_t *__restrict__ status) {
   extern __shared__ __align__(16) unsigned char dyn[];
   BucketSmem &sm = *reinterpret_cast<BucketSmem *>(dyn);
   chain_wait();
@@ -678,7 +678,6 @@ __global__ void __launch_bounds__(kThreads, 2) admit_bucket_kernel(
     out_desc->nbuckets = g.nbuckets;
   }
   if (b == last && threadIdx.x == 0) out_desc->n = g0 + kept;
-  if (b == last && rcpt.out && threadIdx.x < 32) write_receipt(rcpt, g0 + kept);
 }
 
 }  // namespace admit

@@ -13,6 +13,14 @@
 // device-side LevelDesc.  Exact counts come back through an asynchronous
 // receipt that the next call applies if it has arrived - the same lazy
 // receipt idea as GPULSMOpt's publication receipt (GPULSMOpt.cuh:6750-6811).
+//
+// Streams.  An update admits its batch on the caller's stream (which orders
+// the reads of the caller's input) and enqueues the batch's merges on the
+// dictionary's own merge stream, behind an event on that admission; the call
+// returns and the next batch's admission overlaps these merges.  Every other
+// operation first makes its stream wait for the merge stream.  Admission and
+// merges therefore use separate scratch, and a run buffer released on one
+// stream is reused on the other only behind the event of its release.
 #include "lsm_dictionary.h"
 
 #include <algorithm>
@@ -44,7 +52,8 @@ constexpr uint32_t kMaxSegments = 1u << 22;
 
 size_t align_up(size_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }
 
-// Standalone receipt (updates embed theirs in their finishing kernel).
+// Standalone receipt, for an update that merges nothing and for a bulk build
+// (an update that merges has its final merge kernel write the receipt).
 __global__ void receipt_kernel(lsm::ReceiptSrc src) {
   chain_wait();
   lsm::write_receipt(src, 0ull);
@@ -76,25 +85,35 @@ RunPool::~RunPool() {
   for (auto &b : all_) {
     if (b->block) cudaFree(b->block);
     if (b->model) cudaFree(b->model);
+    if (b->freed) cudaEventDestroy(b->freed);
   }
 }
 
-RunBuffer *RunPool::acquire(uint64_t min_rows, cudaStream_t stream) {
+RunBuffer *RunPool::acquire(uint64_t min_rows, cudaStream_t stream, bool settled_only) {
   uint64_t cap = 1024;
   while (cap < min_rows) cap <<= 1;
-  RunBuffer *best = nullptr;
-  size_t best_i = 0;
-  for (size_t i = 0; i < free_.size(); ++i)
-    if (free_[i]->cap >= cap && (!best || free_[i]->cap < best->cap)) {
-      best = free_[i];
-      best_i = i;
+  const auto settled = [&](const RunBuffer *f) {
+    return !f->released || f->freed_on == stream || f->freed_epoch + 2 <= epoch_;
+  };
+  RunBuffer *best = nullptr, *young = nullptr;
+  size_t best_i = 0, young_i = 0;
+  for (size_t i = 0; i < free_.size(); ++i) {
+    RunBuffer *f = free_[i];
+    if (f->cap < cap || f->cap > cap * 2) continue;
+    if (!settled_only || settled(f)) {
+      if (!best || f->cap < best->cap) best = f, best_i = i;
+    } else if (!young || f->cap < young->cap) {
+      young = f, young_i = i;
     }
-  if (best && best->cap <= cap * 2) {
-    free_.erase(free_.begin() + best_i);
-    best->model_ok = false;
-    best->model_rows = 0;
-    return best;
   }
+  auto take = [&](RunBuffer *f, size_t i) {
+    free_.erase(free_.begin() + i);
+    if (f->released && f->freed_on != stream) GPULSM_CUDA(cudaStreamWaitEvent(stream, f->freed, 0));
+    f->model_ok = false;
+    f->model_rows = 0;
+    return f;
+  };
+  if (best) return take(best, best_i);
   auto b = std::make_unique<RunBuffer>();
   b->cap = cap;
   const uint32_t cl2 = ceil_log2_u64(cap);
@@ -103,6 +122,10 @@ RunBuffer *RunPool::acquire(uint64_t min_rows, cudaStream_t stream) {
                db = align_up(((size_t(1) << b->dir_bits) + 1) * 4), sb = align_up(sizeof(LevelDesc));
   b->bytes = kb + vb + fb + db + sb;
   cudaError_t e = cudaMallocAsync(&b->block, b->bytes, stream);
+  if (e != cudaSuccess && young) {
+    (void)cudaGetLastError();
+    return take(young, young_i);  // out of memory: wait for the young buffer instead
+  }
   if (e != cudaSuccess) {
     // give cached free buffers back and retry once
     (void)cudaGetLastError();
@@ -124,15 +147,24 @@ RunBuffer *RunPool::acquire(uint64_t min_rows, cudaStream_t stream) {
   return all_.back().get();
 }
 
-void RunPool::release(RunBuffer *b) {
-  if (b) free_.push_back(b);
+void RunPool::release(RunBuffer *b, cudaStream_t stream) {
+  if (!b) return;
+  if (!b->freed) GPULSM_CUDA(cudaEventCreateWithFlags(&b->freed, cudaEventDisableTiming));
+  GPULSM_CUDA(cudaEventRecord(b->freed, stream));
+  b->freed_on = stream;
+  b->freed_epoch = epoch_;
+  b->released = true;
+  free_.push_back(b);
 }
 
 void RunPool::release_all_free(cudaStream_t stream) {
   for (RunBuffer *f : free_) {
+    if (f->released && f->freed_on != stream) cudaStreamWaitEvent(stream, f->freed, 0);
     cudaFreeAsync(f->block, stream);
     if (f->model) cudaFreeAsync(f->model, stream);
     f->model = nullptr;
+    if (f->freed) cudaEventDestroy(f->freed);
+    f->freed = nullptr;
     bytes_ -= f->bytes + f->model_cap;
     for (size_t i = 0; i < all_.size(); ++i)
       if (all_[i].get() == f) {
@@ -190,6 +222,9 @@ LsmDictionary::LsmDictionary(const DictConfig &config)
   GPULSM_CUDA(cudaMallocHost(&width_host_, 8));
   GPULSM_CUDA(cudaEventCreateWithFlags(&op_done_, cudaEventDisableTiming));
   GPULSM_CUDA(cudaEventRecord(op_done_, 0));
+  GPULSM_CUDA(cudaStreamCreateWithFlags(&merge_stream_, cudaStreamNonBlocking));
+  GPULSM_CUDA(cudaEventCreateWithFlags(&adm_done_, cudaEventDisableTiming));
+  GPULSM_CUDA(cudaEventCreateWithFlags(&merge_done_, cudaEventDisableTiming));
 }
 
 LsmDictionary::~LsmDictionary() {
@@ -212,21 +247,59 @@ LsmDictionary::~LsmDictionary() {
     if (lp.p) cudaFree(lp.p);
   if (width_) cudaFree(width_);
   if (width_host_) cudaFreeHost(width_host_);
+  if (ascratch_) cudaFree(ascratch_);
   if (op_done_) cudaEventDestroy(op_done_);
+  if (adm_done_) cudaEventDestroy(adm_done_);
+  if (merge_done_) cudaEventDestroy(merge_done_);
+  if (merge_stream_) cudaStreamDestroy(merge_stream_);
 }
 
 // Operations are ordered by op_done_ across streams; on the stream of the
 // previous operation the stream order already holds (not for the per-thread
 // default stream, whose handle names a different stream in every thread).
-void LsmDictionary::begin_op(cudaStream_t s) {
-  if (last_stream_known_ && s == last_stream_ && s != cudaStreamPerThread) return;
-  GPULSM_CUDA(cudaStreamWaitEvent(s, op_done_, 0));
+void LsmDictionary::begin_op(cudaStream_t s, bool update) {
+  if (!(last_stream_known_ && s == last_stream_ && s != cudaStreamPerThread))
+    GPULSM_CUDA(cudaStreamWaitEvent(s, op_done_, 0));
+  if (!update && merges_pending_) {  // everything but an update reads the merged levels
+    GPULSM_CUDA(cudaStreamWaitEvent(s, merge_done_, 0));
+    merges_pending_ = false;
+  }
 }
 
 void LsmDictionary::end_op(cudaStream_t s) {
   GPULSM_CUDA(cudaEventRecord(op_done_, s));
   last_stream_ = s;
   last_stream_known_ = true;
+}
+
+// Completion of every operation enqueued so far, merges included, on the host.
+void LsmDictionary::host_sync() {
+  GPULSM_CUDA(cudaEventSynchronize(op_done_));
+  if (merges_pending_) GPULSM_CUDA(cudaEventSynchronize(merge_done_));
+}
+
+void LsmDictionary::join(cudaStream_t s) {
+  std::lock_guard<std::mutex> g(mu_);
+  begin_op(s);
+  end_op(s);
+}
+
+// Admission's own scratch: the next batch is admitted while the merges of the
+// previous one still use scratch_.
+void *LsmDictionary::admit_scratch(size_t bytes, cudaStream_t s) {
+  bytes = align_up(std::max<size_t>(bytes, kAlign));
+  if (bytes > ascratch_bytes_) {
+    if (ascratch_) GPULSM_CUDA(cudaFreeAsync(ascratch_, s));
+    size_t grow = std::max(bytes, ascratch_bytes_ * 2);
+    if (cudaMallocAsync(&ascratch_, grow, s) != cudaSuccess) {
+      (void)cudaGetLastError();
+      ascratch_ = nullptr;
+      ascratch_bytes_ = 0;
+      throw std::bad_alloc();
+    }
+    ascratch_bytes_ = grow;
+  }
+  return ascratch_;
 }
 
 void *LsmDictionary::scratch(size_t bytes, cudaStream_t s) {
@@ -306,7 +379,7 @@ void LsmDictionary::apply_receipt(bool wait) {
     if (!wait) return;
     // the receipt may belong to an earlier batch of the operation in progress:
     // wait for the operations before it, then for the receipt itself
-    GPULSM_CUDA(cudaEventSynchronize(op_done_));
+    host_sync();
     const auto t0 = std::chrono::steady_clock::now();
     while (!landed()) {
       if (std::chrono::steady_clock::now() - t0 > std::chrono::seconds(60))
@@ -351,9 +424,9 @@ void LsmDictionary::reject_if_failed() const {
   if (failed_) throw std::runtime_error(failure_);
 }
 
-void LsmDictionary::release_levels(cudaStream_t) {
+void LsmDictionary::release_levels(cudaStream_t s) {
   for (auto &l : levels_) {
-    pool_.release(l.run);
+    pool_.release(l.run, s);
     l = Level{};
     l.gen = next_gen_++;
   }
@@ -361,14 +434,14 @@ void LsmDictionary::release_levels(cudaStream_t) {
 
 // ----------------------------------------------------------------------------
 RunBuffer *LsmDictionary::sort_dedup(const uint32_t *keys, const uint32_t *values, uint64_t n,
-                                     bool tombstone, cudaStream_t s, const lsm::ReceiptSrc *rcpt) {
+                                     bool tombstone, cudaStream_t s) {
   ensure_sort_space(n, s);
-  if (n <= lsm::admit::kMaxKeys) return bucket_admit(keys, values, n, tombstone, s, rcpt);
+  if (n <= lsm::admit::kMaxKeys) return bucket_admit(keys, values, n, tombstone, s);
   const uint32_t nn = uint32_t(n);
   const size_t radix_bytes = align_up(radix::workspace_bytes(n, 4));
   const uint64_t dtiles = (n + lsm::kCompactTile - 1) / lsm::kCompactTile;
   const size_t total = radix_bytes + align_up(8) + align_up((dtiles + 1) * 8);
-  Bump bump{static_cast<char *>(scratch(total, s))};
+  Bump bump{static_cast<char *>(admit_scratch(total, s))};
   GPULSM_CUDA(cudaMemsetAsync(bump.p, 0, total, s));
   uint32_t *ws = bump.take<uint32_t>(radix_bytes / 4);
   uint32_t *counter = bump.take<uint32_t>(2);
@@ -379,7 +452,7 @@ RunBuffer *LsmDictionary::sort_dedup(const uint32_t *keys, const uint32_t *value
   unsigned long long *bufs[2] = {words_[0], words_[1]};
   const int cur = radix::run_passes<unsigned long long, false>(bufs, nullptr, nn, 32, 64, ws,
                                                                dev_status_, s);
-  RunBuffer *carry = pool_.acquire(n, s);
+  RunBuffer *carry = pool_.acquire(n, s, true);
   lsm::dedup_last_kernel<<<unsigned(dtiles), lsm::kCompactThreads, 0, s>>>(
       bufs[cur], nn, tombstone ? 1 : 0, carry->keys, carry->vals, carry->flags, carry->desc, carry->dir,
       carry->dir_bits, rows_log2_, lb, counter, dev_status_); note_launch();
@@ -391,14 +464,15 @@ RunBuffer *LsmDictionary::sort_dedup(const uint32_t *keys, const uint32_t *value
 // (histogram, scan, scatter - no look-back chain), then one CTA per top-byte
 // bucket sorts, deduplicates and writes the level rows (lsm_admit.cuh).
 RunBuffer *LsmDictionary::bucket_admit(const uint32_t *keys, const uint32_t *values, uint64_t n,
-                                       bool tombstone, cudaStream_t s, const lsm::ReceiptSrc *rcpt) {
+                                       bool tombstone, cudaStream_t s) {
   namespace ad = lsm::admit;
   const uint32_t nn = uint32_t(n);
   const uint32_t tiles = ad::part_tiles(n);
   const size_t zero_bytes = align_up(8) + align_up((ad::kBuckets + 1) * 8);
   const size_t total = zero_bytes + 2 * align_up(size_t(tiles) * 256 * 4) + align_up(256 * 4);
-  Bump bump{static_cast<char *>(scratch(total, s))};
-  RunBuffer *carry = pool_.acquire(n, s);  // before the chain: a fresh buffer is a stream-ordered allocation
+  Bump bump{static_cast<char *>(admit_scratch(total, s))};
+  // before the chain: a fresh buffer is a stream-ordered allocation
+  RunBuffer *carry = pool_.acquire(n, s, true);
   unsigned long long *zero = reinterpret_cast<unsigned long long *>(bump.p);  // zeroed by part_hist_kernel
   uint32_t *counter = bump.take<uint32_t>(2);
   unsigned long long *lb = bump.take<unsigned long long>(ad::kBuckets + 1);
@@ -412,8 +486,7 @@ RunBuffer *LsmDictionary::bucket_admit(const uint32_t *keys, const uint32_t *val
                  tiles, static_cast<const uint32_t *>(prefix), static_cast<const uint32_t *>(top), words_[1]);
   launch_chained(ad::admit_bucket_kernel, ad::kBuckets, ad::kThreads, ad::kBucketSmemBytes, s, words_[1], words_[0],
                  static_cast<const uint32_t *>(top), nn, tombstone ? 1 : 0, carry->keys, carry->vals, carry->flags,
-                 carry->desc, carry->dir, carry->dir_bits, rows_log2_, lb, counter, dev_status_,
-                 rcpt ? *rcpt : lsm::ReceiptSrc{});
+                 carry->desc, carry->dir, carry->dir_bits, rows_log2_, lb, counter, dev_status_);
   return carry;
 }
 
@@ -459,8 +532,8 @@ RunBuffer *LsmDictionary::merge(RunBuffer *newer, RunBuffer *older, uint64_t out
     GPULSM_CUDA(cudaEventRecord(tr.stop, s));
     traces_.push_back(tr);
   }
-  pool_.release(newer);
-  pool_.release(older);
+  pool_.release(newer, s);
+  pool_.release(older, s);
   return out;
 }
 
@@ -699,17 +772,29 @@ void LsmDictionary::admit(const uint32_t *keys, const uint32_t *values, uint64_t
       apply_receipt(true);
       reject_if_failed();
     }
-    // a batch that lands in the empty level 0 without a merge has its
-    // receipt written by the admission kernel; otherwise the cascade's
-    // final merge writes it
-    const bool embed = levels_[0].run == nullptr && m <= lsm::admit::kMaxKeys;
-    lsm::ReceiptSrc rcpt{};
-    if (embed) rcpt = next_receipt(0);
-    RunBuffer *carry = sort_dedup(keys + off, values ? values + off : nullptr, m, tombstone, s,
-                                  embed ? &rcpt : nullptr);
-    cascade(carry, m, tombstone, s, !embed);
+    // The batch is admitted on s, which orders the reads of the caller's
+    // input; its merges run on merge_stream_ after the admission and after
+    // the previous batch's merges, while s goes on to admit the next batch.
+    // The receipt comes from the merge stream (the final merge, or a receipt
+    // kernel when nothing merges), so receipts land in batch order.
+    RunBuffer *carry = sort_dedup(keys + off, values ? values + off : nullptr, m, tombstone, s);
+    GPULSM_CUDA(cudaEventRecord(adm_done_, s));
+    GPULSM_CUDA(cudaStreamWaitEvent(merge_stream_, adm_done_, 0));
+    cascade(carry, m, tombstone, merge_stream_, true);
+    GPULSM_CUDA(cudaEventRecord(merge_done_, merge_stream_));
+    merges_pending_ = true;
+    pool_.advance();
     receipt_posted();
   }
+}
+
+// Updates return while their merges run on the dictionary's stream; a CUDA
+// graph capture would leave that stream unjoined, so updates refuse capture.
+static void refuse_capture(cudaStream_t s) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  GPULSM_CUDA(cudaStreamIsCapturing(s, &cs));
+  if (cs != cudaStreamCaptureStatusNone)
+    throw std::invalid_argument("GPU dictionary updates cannot be captured into a CUDA graph");
 }
 
 // ----------------------------------------------------------------------------
@@ -739,7 +824,7 @@ void LsmDictionary::bulk_build(const uint32_t *keys, const uint32_t *values, uin
   failure_.clear();
   receipt_pending_ = false;
   if (n) {
-    RunBuffer *run = sort_dedup(keys, values, n, false, s, nullptr);
+    RunBuffer *run = sort_dedup(keys, values, n, false, s);
     Level &top = levels_.back();
     top.run = run;
     top.upper = n;
@@ -756,9 +841,10 @@ void LsmDictionary::insert(const uint32_t *keys, const uint32_t *values, uint64_
   std::lock_guard<std::mutex> g(mu_);
   if (!n) return;
   if (!keys || !values) throw std::invalid_argument("invalid GPU dictionary update batch");
+  refuse_capture(s);
   apply_receipt(false);
   reject_if_failed();
-  begin_op(s);
+  begin_op(s, true);
   admit(keys, values, n, false, s);  // every batch's finishing kernel writes the receipt
   end_op(s);
 }
@@ -767,9 +853,10 @@ void LsmDictionary::erase(const uint32_t *keys, uint64_t n, cudaStream_t s) {
   std::lock_guard<std::mutex> g(mu_);
   if (!n) return;
   if (!keys) throw std::invalid_argument("invalid GPU dictionary update batch");
+  refuse_capture(s);
   apply_receipt(false);
   reject_if_failed();
-  begin_op(s);
+  begin_op(s, true);
   admit(keys, nullptr, n, true, s);  // every batch's finishing kernel writes the receipt
   end_op(s);
 }
@@ -951,7 +1038,7 @@ void LsmDictionary::successor(const uint32_t *queries, uint64_t n, uint32_t *out
 
 uint32_t LsmDictionary::status() {
   std::lock_guard<std::mutex> g(mu_);
-  GPULSM_CUDA(cudaEventSynchronize(op_done_));
+  host_sync();
   apply_receipt(true);
   uint32_t bits = 0;
   GPULSM_CUDA(cudaMemcpy(&bits, dev_status_, 4, cudaMemcpyDeviceToHost));
@@ -1024,7 +1111,7 @@ uint64_t LsmDictionary::resident_bytes() {
 
 void LsmDictionary::size(uint64_t *rows, uint32_t *levels) {
   std::lock_guard<std::mutex> g(mu_);
-  GPULSM_CUDA(cudaEventSynchronize(op_done_));
+  host_sync();
   uint64_t total = 0;
   uint32_t count = 0;
   for (auto &l : levels_) {

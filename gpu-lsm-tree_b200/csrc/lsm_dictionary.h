@@ -47,15 +47,25 @@ struct RunBuffer {
   uint32_t model_segments = 0;
   uint64_t model_rows = 0;  // rows bound of a level that wants a model before its next read (0: none)
   bool model_ok = false;
+  // Last release: an event recorded on the releasing stream after the
+  // launches that read the buffer; a reuse on another stream waits for it.
+  cudaEvent_t freed = nullptr;
+  cudaStream_t freed_on = nullptr;
+  uint64_t freed_epoch = 0;
+  bool released = false;
 };
 
 class RunPool {
  public:
   explicit RunPool(uint32_t rows_log2) : rows_log2_(rows_log2) {}
   ~RunPool();
-  RunBuffer *acquire(uint64_t min_rows, cudaStream_t stream);
-  void release(RunBuffer *b);
+  // settled_only: skip buffers released on another stream during the last
+  // two epochs (allocating instead), so that the acquiring stream does not
+  // wait for the launches still reading them
+  RunBuffer *acquire(uint64_t min_rows, cudaStream_t stream, bool settled_only = false);
+  void release(RunBuffer *b, cudaStream_t stream);
   void release_all_free(cudaStream_t stream);
+  void advance() { ++epoch_; }
   size_t bytes() const { return bytes_; }
   void account(int64_t delta) { bytes_ = size_t(int64_t(bytes_) + delta); }
 
@@ -64,6 +74,7 @@ class RunPool {
   std::vector<std::unique_ptr<RunBuffer>> all_;
   std::vector<RunBuffer *> free_;
   size_t bytes_ = 0;
+  uint64_t epoch_ = 0;  // advanced once per admitted batch
 };
 
 class LsmDictionary {
@@ -99,6 +110,10 @@ class LsmDictionary {
   void enqueue_table_lookup(const uint32_t *queries, uint64_t n, uint32_t *out_values, uint8_t *out_found,
                             cudaStream_t capturing);
   void launch_read_graph(cudaGraphExec_t exec, cudaStream_t s);
+  // Makes s wait for every update enqueued so far, merges included (updates
+  // return once their batch is admitted; their merges run on the
+  // dictionary's own stream, overlapping the next batch's admission).
+  void join(cudaStream_t s);
   // Kernel timing of the merge launches (CUDA events on the launching stream
   // around each merge kernel, plus the rows it read and wrote).
   void set_kernel_timing(bool on);
@@ -118,8 +133,9 @@ class LsmDictionary {
   };
   struct Receipt;
 
-  void begin_op(cudaStream_t s);
+  void begin_op(cudaStream_t s, bool update = false);
   void end_op(cudaStream_t s);
+  void host_sync();
   void apply_receipt(bool wait);
   void post_receipt(cudaStream_t s);
   lsm::ReceiptSrc next_receipt(int dest);
@@ -128,9 +144,9 @@ class LsmDictionary {
   void admit(const uint32_t *keys, const uint32_t *values, uint64_t n, bool tombstone,
              cudaStream_t s);
   RunBuffer *sort_dedup(const uint32_t *keys, const uint32_t *values, uint64_t n, bool tombstone,
-                        cudaStream_t s, const lsm::ReceiptSrc *rcpt);
+                        cudaStream_t s);
   RunBuffer *bucket_admit(const uint32_t *keys, const uint32_t *values, uint64_t n, bool tombstone,
-                          cudaStream_t s, const lsm::ReceiptSrc *rcpt);
+                          cudaStream_t s);
   void cascade(RunBuffer *carry, uint64_t carry_upper, bool carry_tombs, cudaStream_t s, bool want_receipt);
   RunBuffer *merge(RunBuffer *newer, RunBuffer *older, uint64_t out_upper, bool drop_tombstones,
                    cudaStream_t s, const lsm::ReceiptSrc *rcpt = nullptr);
@@ -146,6 +162,7 @@ class LsmDictionary {
   void fit_now(RunBuffer *run, uint64_t upper, cudaStream_t s);
   void ensure_models(cudaStream_t s);
   void *scratch(size_t bytes, cudaStream_t s);
+  void *admit_scratch(size_t bytes, cudaStream_t s);
   void ensure_sort_space(uint64_t n, cudaStream_t s);
   void level_set(void *out) const;
   lsm::LevelView view_of(int level) const;
@@ -164,8 +181,10 @@ class LsmDictionary {
   // sort space for admission: two u64 word buffers + radix workspace
   unsigned long long *words_[2] = {nullptr, nullptr};
   uint64_t words_cap_ = 0;
-  void *scratch_ = nullptr;
+  void *scratch_ = nullptr;  // merges and reads
   size_t scratch_bytes_ = 0;
+  void *ascratch_ = nullptr;  // admission (runs while the previous batch merges)
+  size_t ascratch_bytes_ = 0;
   uint32_t *dev_status_ = nullptr;
 
   // receipts (pinned host copy of the level row counts and status)
@@ -205,6 +224,13 @@ class LsmDictionary {
   void *table_dev_ = nullptr;  // device copy of the level set (graph-replayed lookups)
   uint64_t table_gen_ = ~0ull;            // next_gen_ when the table was last written
   cudaEvent_t op_done_ = nullptr;
+  // Merges of admitted batches run on merge_stream_: each waits for its
+  // batch's admission (adm_done_); reads and every other operation wait for
+  // merge_done_ when merges are pending.
+  cudaStream_t merge_stream_ = nullptr;
+  cudaEvent_t adm_done_ = nullptr;
+  cudaEvent_t merge_done_ = nullptr;
+  bool merges_pending_ = false;
   cudaStream_t last_stream_ = nullptr;  // stream of the last operation (op_done_ was recorded there)
   bool last_stream_known_ = false;
   mutable std::mutex mu_;

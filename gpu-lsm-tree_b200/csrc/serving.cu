@@ -329,6 +329,10 @@ void Server::launch_round(Slot &slot) {
       r.status = status_of(e);
     }
   }
+  // an update request completes when its merges have completed
+  bool updates = false;
+  for (const Run &r : slot.runs) updates = updates || is_update(r.kind);
+  if (updates) dict_.join(compute_);
   GPULSM_CUDA(cudaEventRecord(slot.computed, compute_));
   GPULSM_CUDA(cudaStreamWaitEvent(download_, slot.computed, 0));
   if (slot.out_words) {

@@ -80,6 +80,11 @@ class GPULSMOpt:
     def clear(self, stream=None):
         N.check(self._lib.gpulsm_dict_clear(self._h, _stream(stream)))
 
+    def join(self, stream=None):
+        """Make `stream` wait until every update enqueued so far has been merged
+        (updates return once admitted; reads join by themselves)."""
+        N.check(self._lib.gpulsm_dict_join(self._h, _stream(stream)))
+
     def bulk_build(self, keys, values, count: int | None = None, stream=None):
         n = keys.numel() if count is None else count
         N.check(self._lib.gpulsm_dict_bulk_build(self._h, _ptr(keys, "keys", count=n),

@@ -127,7 +127,7 @@ def run_batch_log(gl, torch, b: int, args) -> dict:
         begin = (r - 1) * batch
         keys = up(key_for_index(np.arange(begin, begin + batch, dtype=np.uint64)))
         torch.cuda.synchronize()
-        ms = timed(lambda: d.insert(keys, ones))
+        ms = timed(lambda: (d.insert(keys, ones), d.join()))  # admitted and merged
         cumulative += ms
         resident = r * batch
         ins_f.write(f"{SYSTEM},{b},{r},{resident},{ms:.12g},{batch / ms / 1e3:.12g},{cumulative:.12g},"

@@ -78,6 +78,13 @@ int gpulsm_dict_create(const gpulsm_dict_config *config, gpulsm_dict **out);
 int gpulsm_dict_destroy(gpulsm_dict *dict);
 /* GPULSMOpt::clear  GPULSMOpt.cuh:5731 */
 int gpulsm_dict_clear(gpulsm_dict *dict, void *stream);
+/* No GPULSMOpt counterpart (its updates complete in the caller's stream):
+ * makes `stream` wait until every update enqueued so far has been merged.
+ * insert/erase return once their batch is admitted (its input has been read
+ * in `stream`'s order); the merges run on the dictionary's own stream while
+ * the next batch is admitted.  Every read operation joins by itself; join is
+ * for callers that time or order updates against their own work. */
+int gpulsm_dict_join(gpulsm_dict *dict, void *stream);
 /* GPULSMOpt::bulk_build  GPULSMOpt.cuh:5738 (last duplicate wins) */
 int gpulsm_dict_bulk_build(gpulsm_dict *dict, const uint32_t *keys, const uint32_t *values,
                            uint64_t count, void *stream);

@@ -74,6 +74,8 @@ def main():
             d.clear()
             for kind, k, v in ops:
                 d.insert(k, v) if kind == "insert" else d.erase(k)
+            if hasattr(d, "join"):  # ours: the last batches' merges complete
+                d.join()
 
         t_upd = timed(updates)
         ov = torch.empty(nq, dtype=torch.int32, device="cuda")

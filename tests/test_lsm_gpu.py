@@ -273,6 +273,42 @@ def test_streams_are_ordered(gl, cuda):
     assert np.array_equal(to_host(out), t.o.lookup(k))
 
 
+def test_updates_overlap_merges_and_release_their_input(gl, cuda):
+    """insert/erase return once the batch is admitted (its merges run on the
+    dictionary's stream, overlapping the next admission): the caller may
+    overwrite the batch in stream order right away, and a read on any stream
+    sees every merge."""
+    import torch
+
+    t = Twin(gl, max_elements=1 << 18, batch_capacity=1 << 12, level_zero_capacity=1 << 13)
+    rng = np.random.default_rng(21)
+    s = torch.cuda.Stream()
+    kbuf = torch.empty(1 << 12, dtype=torch.int32, device="cuda")
+    vbuf = torch.empty(1 << 12, dtype=torch.int32, device="cuda")
+    with torch.cuda.stream(s):
+        for i in range(40):  # one staging buffer, refilled in stream order after every update
+            k = rng.integers(0, 1 << 16, 1 << 12, dtype=np.uint64).astype(np.uint32)
+            v = rng.integers(0, 1 << 32, 1 << 12, dtype=np.uint64).astype(np.uint32)
+            kbuf.copy_(to_dev(k), non_blocking=True)
+            if i % 5 == 4:
+                t.d.erase(kbuf, stream=s)
+                t.o.erase(k)
+            else:
+                vbuf.copy_(to_dev(v), non_blocking=True)
+                t.d.insert(kbuf, vbuf, stream=s)
+                t.o.insert(k, v)
+            kbuf.fill_(-1)  # the batch was read before this runs
+            vbuf.fill_(-1)
+        t.d.join(stream=s)
+    s.synchronize()
+    probe = np.arange(1 << 16, dtype=np.uint32)
+    out = empty_u32(probe.size)
+    t.d.lookup(to_dev(probe), out)  # another stream: the read joins the merges itself
+    torch.cuda.synchronize()
+    assert np.array_equal(to_host(out), t.o.lookup(probe))
+    assert t.d.canonical_carry_status() == 0
+
+
 def test_lsm_small_configuration(gl, cuda, workloads):
     w = workloads.lsm_small()
     t = Twin(gl, max_elements=1 << 20, batch_capacity=1 << 16)
