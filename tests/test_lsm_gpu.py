@@ -460,3 +460,28 @@ def test_paper_sweep_runner_writes_reference_csvs(gl, cuda, tmp_path):
         want = range_digest(o.range_sum(lo, hi))
         row = [r for r in rng if r["r"] == "1" and r["operation"] == "range" and r["expected_hits"] == str(expected)]
         assert (int(row[0]["checksum_sum"]), int(row[0]["checksum_xor"])) == want
+
+
+@pytest.mark.parametrize("index,key_bits", [("flix", 64), ("flix", 32), ("gpulsmopt", 32)])
+def test_updates_runner_writes_reference_result_file(gl, cuda, tmp_path, index, key_bits):
+    """The updates runner (gpu-lsm-tree_b200/updates_runner.py) on a reduced
+    protocol: every probe, miss and successor validated on the host, and the
+    result file in the reference's long form with its record names."""
+    import csv
+    import importlib
+
+    ur = importlib.import_module("gpu-lsm-tree_b200.updates_runner")
+    out = tmp_path / "updates.csv"
+    assert ur.main(["--out", str(out), "--index", index, "--key-bits", str(key_bits), "--build-size-log", "16",
+                    "--probe-size-log", "14", "--batch-count", "2", "--rebuild"]) == 0
+    rows = list(csv.reader(open(out), skipinitialspace=True))
+    header = rows[0]
+    assert header[:5] == ["EXPERIMENT", "index_type", "index_parameters", "index_id", "run"]
+    assert header[-2:] == ["DESCRIPTION", "VALUE"] and "after_update_size" in header
+    body = [dict(zip(header, r)) for r in rows[1:]]
+    steps = {r["step"] for r in body}
+    assert steps == {str(s) for s in range(5)}
+    assert {r["DESCRIPTION"] for r in body} >= {"insert_or_delete_time_ms", "probe_time_ms", "probe_miss_time_ms",
+                                                "before_update_bytes", "after_update_bytes"}
+    sizes = {int(r["step"]): (int(r["before_update_size"]), int(r["after_update_size"])) for r in body}
+    assert sizes[0] == (1 << 16, 1 << 16) and sizes[2][1] == 1 << 17 and sizes[4][1] == 1 << 16

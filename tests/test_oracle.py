@@ -169,3 +169,30 @@ def test_sweep_runner_inputs_match_the_sweep_protocol():
     assert np.array_equal(lo, lo2) and np.array_equal(hi, hi2)
     r = np.random.default_rng(3).integers(0, 1 << 32, 5000, dtype=np.uint64).astype(np.uint32)
     assert sw.range_digest(r, 77) == sc.range_digest(r, 77)
+
+
+def test_updates_runner_writes_result_collector_long_form():
+    """The updates runner's writer lays a table out as result_collector's
+    write_csv(first_line_header, long_form, pack_columns) does
+    (FliX/result_collector.h:172-296): the parameter columns in first-seen
+    order, then DESCRIPTION and VALUE; one line per measurement, repeating the
+    row's parameters, an empty field for a parameter the row lacks, values
+    printed at precision 16 and booleans as 1/0."""
+    import importlib
+
+    ur = importlib.import_module("gpu-lsm-tree_b200.updates_runner")
+    rc = ur.ResultCollector()
+    rc.commit([("EXPERIMENT", "batches"), ("step", 0), ("do_insert", True)],
+              [("probe_time_ms", 0.125), ("after_update_bytes", 4096)])
+    rc.commit([("EXPERIMENT", "batches"), ("run", 1)], [("probe_time_ms", 1 / 3)])
+    assert rc.long_form_packed() == (
+        "EXPERIMENT, step, do_insert, run, DESCRIPTION, VALUE\n"
+        "batches, 0, 1, , probe_time_ms, 0.125\n"
+        "batches, 0, 1, , after_update_bytes, 4096\n"
+        "batches, , , 1, probe_time_ms, 0.3333333333333333\n")
+    try:
+        rc.commit([("probe_time_ms", 1)], [])
+    except ValueError:
+        pass
+    else:
+        raise AssertionError("a measurement column reused as a parameter must be refused")
