@@ -63,7 +63,7 @@ def parse():
     p.add_argument("--flix-rounds", type=int, default=3)
     p.add_argument("--tenant-rounds", type=int, default=4)
     p.add_argument("--serving-seconds", type=float, default=2.0)
-    p.add_argument("--case", default=None, choices=["merge", "admit", "serving-mix", "flix"],
+    p.add_argument("--case", default=None, choices=["merge", "admit", "serving-mix", "flix", "lookup"],
                    help="run one small profiling case instead of the benchmark (see profile_case)")
     return p.parse_args()
 
@@ -713,7 +713,9 @@ def profile_case(args):
                 the default request mix;
     flix        FliX at 1/4 of its sizes: 2^26 sorted u64 keys built, then 2
                 rounds of 2^20 sorted inserts, 2^19 sorted deletes and 2^22
-                sorted successor probes (plain bucket routing)."""
+                sorted successor probes (plain bucket routing);
+    lookup      the at-scale step's 2^24 lookups (70% Zipf hits) against one
+                level bulk-built from its 2^26 inserted pairs, twice."""
     import torch
 
     gl = importlib.import_module("gpu-lsm-tree_b200")
@@ -752,6 +754,23 @@ def profile_case(args):
         e1.record()
         torch.cuda.synchronize()
         print(json.dumps({"case": "admit", "ms_per_batch": round(e0.elapsed_time(e1) / 64, 4),
+                          "status": d.canonical_carry_status()}))
+    elif args.case == "lookup":
+        # the at-scale step's 2^24 lookups against one level bulk-built from its
+        # 2^26 inserted pairs (the erases are not applied)
+        W = importlib.import_module("gpu-lsm-tree_b200.workloads")
+        w = W.lsm_scale(0)
+        ks = np.concatenate([o[1] for o in w.ops if o[0] == "insert"])
+        vs = np.concatenate([o[2] for o in w.ops if o[0] == "insert"])
+        d = gl.GPULSMOpt(gl.DictionaryConfig(max_elements=ks.size))
+        d.bulk_build(dev(ks), dev(vs))
+        q = dev(w.lookups)
+        out_v = torch.empty(q.numel(), dtype=torch.int32, device="cuda")
+        out_f = torch.empty(q.numel(), dtype=torch.uint8, device="cuda")
+        for _ in range(2):
+            d.lookup(q, out_v, out_f)
+        torch.cuda.synchronize()
+        print(json.dumps({"case": "lookup", "queries": q.numel(), "hits": int(out_f.sum().item()),
                           "status": d.canonical_carry_status()}))
     elif args.case == "flix":
         W = importlib.import_module("gpu-lsm-tree_b200.workloads")

@@ -780,9 +780,14 @@ void LsmDictionary::admit(const uint32_t *keys, const uint32_t *values, uint64_t
     RunBuffer *carry = sort_dedup(keys + off, values ? values + off : nullptr, m, tombstone, s);
     GPULSM_CUDA(cudaEventRecord(adm_done_, s));
     GPULSM_CUDA(cudaStreamWaitEvent(merge_stream_, adm_done_, 0));
-    cascade(carry, m, tombstone, merge_stream_, true);
-    GPULSM_CUDA(cudaEventRecord(merge_done_, merge_stream_));
     merges_pending_ = true;
+    try {
+      cascade(carry, m, tombstone, merge_stream_, true);
+    } catch (...) {  // reads still wait for whatever the cascade enqueued
+      cudaEventRecord(merge_done_, merge_stream_);
+      throw;
+    }
+    GPULSM_CUDA(cudaEventRecord(merge_done_, merge_stream_));
     pool_.advance();
     receipt_posted();
   }
@@ -1106,7 +1111,7 @@ void LsmDictionary::kernel_timing(uint64_t *launches, double *total_ms, double *
 
 uint64_t LsmDictionary::resident_bytes() {
   std::lock_guard<std::mutex> g(mu_);
-  return pool_.bytes() + words_cap_ * 16 + scratch_bytes_ + live_bytes_ + sizeof(Receipt) + 256;
+  return pool_.bytes() + words_cap_ * 16 + scratch_bytes_ + ascratch_bytes_ + live_bytes_ + sizeof(Receipt) + 256;
 }
 
 void LsmDictionary::size(uint64_t *rows, uint32_t *levels) {
