@@ -656,6 +656,95 @@ __global__ void __launch_bounds__(256) successor_direct_kernel(
 }
 
 // ---------------------------------------------------------------------------
+// Unsorted probes without sorting them (small batches): a fence tree over the
+// bucket maxima.  Level 0 is bmax itself; level l + 1 holds the maximum of
+// every group of kFenceFan entries of level l (its last entry), up to a level
+// of at most kFenceFan entries.  A probe descends from the top, searching one
+// group (kFenceFan keys: one or two cache lines) per level; the upper levels
+// stay in L2.  The answer equals bucket_of: a group's maximum bounds every key
+// in it, and a key above every maximum falls into the last group at every
+// level.  For large batches sorting the probes is faster (neighbouring threads
+// then read the same nodes), so the host picks by batch size.
+constexpr uint32_t kFenceFan = 32;
+constexpr int kMaxFenceLevels = 8;
+
+template <typename K>
+struct FenceTree {
+  const K *level[kMaxFenceLevels];
+  uint32_t size[kMaxFenceLevels];
+  uint32_t levels;  // including level 0 (bmax)
+};
+
+template <typename K>
+__global__ void fence_level_kernel(const K *__restrict__ src, uint32_t src_n, K *__restrict__ dst, uint32_t dst_n) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < dst_n) dst[i] = src[min((i + 1) * kFenceFan, src_n) - 1];
+}
+
+template <typename K>
+__device__ __forceinline__ uint32_t route_fence(const FenceTree<K> &t, K k) {
+  int l = int(t.levels) - 1;
+  uint32_t pos = bucket_in(t.level[l], 0u, t.size[l] - 1, k);
+  for (--l; l >= 0; --l) {
+    const uint32_t lo = pos * kFenceFan;
+    pos = bucket_in(t.level[l], lo, min(lo + kFenceFan, t.size[l]) - 1, k);
+  }
+  return pos;
+}
+
+// value or not_found of unsorted probes, one thread each (results in input order)
+template <typename K>
+__global__ void __launch_bounds__(256) lookup_fence_kernel(
+    const K *__restrict__ probes, uint32_t n, FenceTree<K> tree, const learned::ModelHeader *__restrict__ model,
+    const learned::Segment *__restrict__ segs, const Node<K> *__restrict__ nodes, uint32_t *__restrict__ out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const K k = probes[i];
+  uint32_t id = model ? bucket_of_model<K>(*model, segs, tree.level[0], k) : route_fence<K>(tree, k);
+  uint32_t result = kNotFound;
+  for (uint32_t hops = 0; id != kNone && hops < (1u << 20); ++hops) {
+    const Node<K> *p = nodes + id;
+    const uint32_t count = p->count;
+    if (count && k <= p->max) {
+      const uint32_t pos = node_lower_bound(p, count, k);
+      if (pos < count && p->keys[pos] == k) result = p->vals[pos];
+      if (pos < count) break;
+    }
+    id = p->next;
+  }
+  out[i] = result;
+}
+
+// first key >= probe of unsorted probes, one thread each (results in input order)
+template <typename K>
+__global__ void __launch_bounds__(256) successor_fence_kernel(
+    const K *__restrict__ probes, uint32_t n, FenceTree<K> tree, const learned::ModelHeader *__restrict__ model,
+    const learned::Segment *__restrict__ segs, const Node<K> *__restrict__ nodes, K *__restrict__ out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const K k = probes[i];
+  const uint32_t b = model ? bucket_of_model<K>(*model, segs, tree.level[0], k) : route_fence<K>(tree, k);
+  uint32_t id = b;
+  bool found = false;
+  K result = successor_miss<K>();
+  for (uint32_t hops = 0; id != kNone && hops < (1u << 20); ++hops) {
+    const Node<K> *p = nodes + id;
+    const uint32_t count = p->count;
+    if (count && k <= p->max) {
+      const uint32_t pos = node_lower_bound(p, count, k);
+      if (pos < count) {
+        result = p->keys[pos];
+        found = true;
+        break;
+      }
+    }
+    id = p->next;
+  }
+  if (!found) result = first_key_from_bucket(nodes, b + 1, tree.size[0]);
+  out[i] = result;
+}
+
+// ---------------------------------------------------------------------------
 // helpers for sorting / dedup of batches
 template <typename K>
 __global__ void set_u32_kernel(uint32_t *__restrict__ p, uint32_t v) {

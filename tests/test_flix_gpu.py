@@ -49,6 +49,14 @@ class FlixTwin:
         sk = empty_keys(n, self.bits)
         self.f.successor(keys_t(probes, self.bits), sk, n)
         assert np.array_equal(host_keys(sk, self.bits, n), self.o.successor(probes))
+        # unsorted batches up to 2^20 probes take the fence tree, larger ones are sorted first
+        big = np.tile(probes, (1 << 20) // max(n, 1) + 2)
+        nb = big.size
+        outb, skb = empty_u32(nb), empty_keys(nb, self.bits)
+        self.f.lookup(keys_t(big, self.bits), outb, nb)
+        assert np.array_equal(to_host(outb)[:nb], self.o.lookup(big))
+        self.f.successor(keys_t(big, self.bits), skb, nb)
+        assert np.array_equal(host_keys(skb, self.bits, nb), self.o.successor(big))
         sp = np.sort(probes)
         self.f.lookups_ordered(keys_t(sp, self.bits), out, n)
         assert np.array_equal(to_host(out)[:n], self.o.lookup(sp))
