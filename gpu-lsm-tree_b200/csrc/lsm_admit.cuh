@@ -523,6 +523,8 @@ __global__ void __launch_bounds__(kThreads, 2) admit_bucket_kernel(
   extern __shared__ __align__(16) unsigned char dyn[];
   BucketSmem &sm = *reinterpret_cast<BucketSmem *>(dyn);
   chain_wait();
+  // the top-byte counts load while the ticket is taken
+  const uint32_t c = threadIdx.x < kBuckets ? top_hist[threadIdx.x] : 0u;
   if (threadIdx.x == 0) {
     sm.tile = atomicAdd(tile_counter, 1u);
     sm.first = kBuckets;
@@ -530,7 +532,6 @@ __global__ void __launch_bounds__(kThreads, 2) admit_bucket_kernel(
   }
   __syncthreads();
   // bucket starts (exclusive scan of the top-byte counts) and the nonempty span
-  const uint32_t c = threadIdx.x < kBuckets ? top_hist[threadIdx.x] : 0u;
   const uint32_t ex = block_exclusive_scan<kThreads>(c, sm.rank.scan, &sm.rank.total);
   if (threadIdx.x < kBuckets) {
     sm.start[threadIdx.x] = ex;
