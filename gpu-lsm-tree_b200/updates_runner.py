@@ -16,11 +16,12 @@ uniformly without replacement (sorted).  Every step times its update (CUDA
 events, then a device synchronise; a GPULSMOpt update is joined, so its
 merges are inside the time), an optional rebuild, the probe sort, the probe
 of 2^probe_size_log live keys (checked against their values), the probe of as
-many absent keys (checked as misses) and, for the FliX index, successor
+many keys the run never inserts (checked as misses) and, for the FliX index, successor
 probes of live keys (checked equal to themselves) and of absent keys
 (checked against the ceiling in the live set).  Key draws are this runner's
 own, seeded: unique keys in [2, 2^key_bits - 2] (FliX reserves 0 and 1, and a
-64-bit successor miss reads 2^32 - 1 widened).  This index has no separate
+64-bit successor miss reads 2^32 - 1 widened).  The file is rewritten after
+every step, so a run cut short keeps the steps it finished.  This index has no separate
 index layer: index_layer_time_ms is 0 and bucket_layer_time_ms is the probe.
 
 Usage: python gpu-lsm-tree_b200/updates_runner.py --out updates.csv [--index flix|gpulsmopt]
@@ -100,7 +101,7 @@ def ceiling(live_sorted: np.ndarray, q: np.ndarray, miss: int) -> np.ndarray:
     return out
 
 
-def run(gl, torch, args, rc: ResultCollector, run_id: int) -> int:
+def run(gl, torch, args, rc: ResultCollector, run_id: int, save=None) -> int:
     dev = torch.device("cuda")
     kb = args.key_bits
     kdt = np.uint32 if kb == 32 else np.uint64
@@ -118,13 +119,17 @@ def run(gl, torch, args, rc: ResultCollector, run_id: int) -> int:
     rng = np.random.default_rng(0x1D5 + run_id)
     hi = (1 << kb) - 2 if kb == 32 else (1 << 40)
     # unique keys: draw with slack, deduplicate, keep the generation order
-    draw = rng.integers(2, hi, int(gen_size * 1.1) + 1024, dtype=np.uint64)
+    # gen_size keys to insert, then probe_size keys that are never inserted
+    # (the miss probes): unique, in a shuffled order
+    total = gen_size + probe_size
+    draw = rng.integers(2, hi, int(total * 1.1) + 1024, dtype=np.uint64)
     draw = draw[draw != NOT_FOUND]  # a 64-bit successor miss reads 2^32 - 1
-    _, first = np.unique(draw, return_index=True)
-    generated = draw[np.sort(first)][:gen_size].astype(kdt)
-    if generated.size < gen_size:
+    uniq = np.unique(draw)
+    if uniq.size < total:
         raise RuntimeError("key space too small for the generated key set")
-    rng.shuffle(generated)
+    generated = rng.permutation(uniq)[:total].astype(kdt)
+    absent = np.sort(generated[gen_size:])
+    generated = generated[:gen_size]
     live_k = generated[:build_size].copy()  # live keys and their values, unordered
     live_v = np.arange(build_size, dtype=np.uint32)
     inserted_end = build_size
@@ -215,8 +220,6 @@ def run(gl, torch, args, rc: ResultCollector, run_id: int) -> int:
             got = res.cpu().numpy().view(np.uint32)
         errors += int(np.count_nonzero(got != hit_vals))
         m["bucket_layer_time_ms"] = m["probe_time_ms"]
-        absent = np.setdiff1d(rng.integers(2, hi, probe_size * 2, dtype=np.uint64).astype(kdt), live_sorted)
-        absent = np.sort(absent[:probe_size])
         ad = up(absent)
         mres = torch.empty(absent.size, dtype=torch.int32, device=dev)
         if args.index == "flix":
@@ -247,6 +250,8 @@ def run(gl, torch, args, rc: ResultCollector, run_id: int) -> int:
         measurements = [(k, v) for k, v in m.items()] + [("before_update_bytes", before_bytes),
                                                          ("after_update_bytes", after_bytes)]
         rc.commit(parameters, measurements)
+        if save:
+            save()  # the file is complete after every step
     close = getattr(index, "close", None)
     if close:
         close()
@@ -274,9 +279,13 @@ def main(argv=None) -> int:
     sys.path.insert(0, os.path.dirname(here))
     gl = importlib.import_module(os.path.basename(here))
     rc = ResultCollector()
-    errors = sum(run(gl, torch, args, rc, r) for r in range(args.runs))
-    with open(args.out, "w") as f:
-        f.write(rc.long_form_packed())
+
+    def save():
+        with open(args.out, "w") as f:
+            f.write(rc.long_form_packed())
+
+    errors = sum(run(gl, torch, args, rc, r, save) for r in range(args.runs))
+    save()
     print({"out": args.out, "rows": len(rc.rows), "errors": errors}, flush=True)
     return 1 if errors else 0
 
