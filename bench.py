@@ -13,9 +13,9 @@ per-phase rates (inserted keys/s, lookups/s, range queries/s) and per-batch
 p50/p99 latencies ride along.  Inputs live in HBM before the timed region;
 together they exceed the 126 MB L2, so no flush is needed between steps.
 
---impl reference times the reference path's CPU implementation (the oracle
-restatement, all host threads; the reference has no CPU engine of its own) on
-a bounded sample of the same workload.  Under torchrun (N > 1) each rank runs
+--impl reference times a CPU implementation of the path (the reference has no
+CPU engine of its own): a multi-threaded leveled LSM with the path's semantics
+on every host thread, on the same workload at the same size.  Under torchrun (N > 1) each rank runs
 an independent dictionary on its own seeded data (replicas: the path has no
 exchange step), rank 0 prints the aggregate.
 """
@@ -139,6 +139,26 @@ class ClockSampler:
                     reasons.add(nm)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx or None,
                 "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def step_config(args, w, world):
+    """The workload description both arms print (the same dict for the GPU arm
+    and the CPU reference arm on the same configuration)."""
+    return {"workload": w.name, "global_batch": (w.inserted_keys + w.erased_keys) * world,
+            "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (no flush)",
+            "value_definition": "(updated keys + lookups + range queries) per step / step time",
+            "scale": args.scale}
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 def peaks():
@@ -303,12 +323,10 @@ def run_ours(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
         "data": "synthetic (seeded PCG64; shapes of the at-scale LSM configuration)",
-        "config": {"workload": f"{args.workload}: " + w.name, "global_batch": upd_keys * world,
-                   "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (no flush)",
-                   "value_definition": "(updated keys + lookups + range queries) per step / step time",
-                   "scale": args.scale},
+        "config": step_config(args, w, world),
         "parts": {
-            "insert_mkeys_s": round(upd_keys / (upd * 1e-3) / 1e6, 1),
+            "update_mkeys_s": round(upd_keys / (upd * 1e-3) / 1e6, 1),
+            "inserted_mkeys_s": round(w.inserted_keys / (upd * 1e-3) / 1e6, 1),
             "lookup_mops_s": round(nq / (look * 1e-3) / 1e6, 1),
             "range_mqueries_s": round(nr / (rng_ms * 1e-3) / 1e6, 2),
             "range_pairs_per_step": total_pairs,
@@ -332,7 +350,7 @@ def run_ours(args):
         torch.cuda.empty_cache()
         result["serving"] = serving_leg(args, gl, w, dev)
     if rank == 0 and not args.no_cpu:
-        result["cpu_baseline"] = cpu_baseline(args, W)
+        result["cpu_baseline"] = cpu_baseline(args, W, w)
     if world > 1:
         import torch.distributed as dist
 
@@ -637,26 +655,36 @@ def e2e_ours(args, gl, w, dev, total_pairs, max_el):
             "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": steps}
 
 
-def cpu_baseline(args, W, threads: int = 1, scale_extra: int = 4):
-    """The oracle on a bounded sample of the workload (1/16 of every size)."""
-    from oracle import OracleLSM, oracle_threads
-
-    used = oracle_threads(threads)
-    w = W.lsm_scale(args.scale + scale_extra) if args.workload == "lsm_scale" else W.lsm_small(args.scale + 2)
-    o = OracleLSM()
-    t = time.perf_counter()
+def cpu_step(w, engine):
+    """One pass of the workload through a CPU engine with the path's semantics
+    (updates, lookups with found flags, range pairs)."""
     for op in w.ops:
-        o.insert(op[1], op[2]) if op[0] == "insert" else o.erase(op[1])
-    o.lookup(w.lookups, with_found=True)
-    if w.range_kind == "pairs":
-        o.range_pairs(w.range_lo, w.range_hi)
-    else:
-        o.range_count(w.range_lo, w.range_hi)
+        engine.insert(op[1], op[2]) if op[0] == "insert" else engine.erase(op[1])
+    engine.lookup(w.lookups, with_found=True)
+    engine.range_pairs(w.range_lo, w.range_hi)
+
+
+def cpu_baseline(args, W, w):
+    """The CPU baselines over the same workload: the multi-threaded leveled LSM
+    on every host thread at full size (one pass, seconds), and a single-thread
+    std::map over a 1/16-size sample of the same shape."""
+    from oracle import CpuLsm, CpuMap
+
+    threads = os.cpu_count() or 1
+    t = time.perf_counter()
+    cpu_step(w, CpuLsm())
     dt = time.perf_counter() - t
     ops = w.inserted_keys + w.erased_keys + w.lookups.size + w.range_lo.size
-    return {"value": round(ops / dt / 1e6, 3), "unit": "M ops/s", "cores": used, "kind": "port",
-            "sample": f"same workload shape at 1/{1 << (args.scale + scale_extra)} of every size, one pass, "
-                      f"{dt:.1f} s"}
+    ws = W.lsm_scale(args.scale + 4) if args.workload == "lsm_scale" else W.lsm_small(args.scale + 4)
+    t = time.perf_counter()
+    cpu_step(ws, CpuMap())
+    dts = time.perf_counter() - t
+    ops_s = ws.inserted_keys + ws.erased_keys + ws.lookups.size + ws.range_lo.size
+    return {"value": round(ops / dt / 1e6, 3), "unit": "M ops/s", "cores": threads, "kind": "port",
+            "cpu_model": cpu_model(),
+            "sample": f"the same workload at full size, one pass, {dt:.1f} s (multi-threaded leveled CPU LSM)",
+            "std_map_single_thread": {"value": round(ops_s / dts / 1e6, 3), "unit": "M ops/s", "cores": 1,
+                                      "sample": f"same shape at 1/16 of every size, one pass, {dts:.1f} s"}}
 
 
 def run_reference(args):
@@ -664,40 +692,28 @@ def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    from oracle import OracleLSM, oracle_threads
+    from oracle import CpuLsm
 
     W = importlib.import_module("gpu-lsm-tree_b200.workloads")
-    used = oracle_threads(0)
-    extra = 2
-    w = W.lsm_scale(args.scale + extra) if args.workload == "lsm_scale" else W.lsm_small(args.scale)
-
-    def step():
-        o = OracleLSM()
-        for op in w.ops:
-            o.insert(op[1], op[2]) if op[0] == "insert" else o.erase(op[1])
-        o.lookup(w.lookups, with_found=True)
-        if w.range_kind == "pairs":
-            o.range_pairs(w.range_lo, w.range_hi)
-        else:
-            o.range_count(w.range_lo, w.range_hi)
-
+    used = os.cpu_count() or 1
+    w = make_workload(W, args.workload, args.scale, 0)
     for _ in range(args.warmup):
-        step()
+        cpu_step(w, CpuLsm())
     t = time.perf_counter()
     for _ in range(args.steps):
-        step()
+        cpu_step(w, CpuLsm())
     dt = (time.perf_counter() - t) / args.steps
     ops = w.inserted_keys + w.erased_keys + w.lookups.size + w.range_lo.size
     value = ops / dt / 1e6
-    sample = (f"{args.workload} shape at 1/{1 << (args.scale + extra)} of every size per step "
-              f"(oracle: sorted-array restatement, OpenMP)")
+    sample = ("the whole workload every step at full size, on a fresh multi-threaded leveled CPU LSM "
+              "(parallel-mode std::sort of each batch, OpenMP run merges and query batches)")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "M ops/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": args.workload, "parallelism": "cpu", "sample": sample},
+        "config": step_config(args, w, 1),
         "cpu_baseline": {"value": round(value, 3), "unit": "M ops/s", "cores": used, "kind": "port",
-                         "sample": sample},
+                         "cpu_model": cpu_model(), "sample": sample},
         "e2e": {"value": round(value, 3), "unit": "M ops/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 

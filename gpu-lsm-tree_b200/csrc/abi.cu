@@ -99,6 +99,25 @@ void device_accessible(std::initializer_list<std::pair<const void *, const char 
   for (const auto &p : ptrs) device_accessible(p.first, p.second);
 }
 
+// The sort entries accept an output equal to its input (in place) but no
+// partial overlap between any two of the four buffers.
+bool ranges_overlap(const void *a, size_t an, const void *b, size_t bn) {
+  if (!a || !b || !an || !bn) return false;
+  const uintptr_t x = reinterpret_cast<uintptr_t>(a), y = reinterpret_cast<uintptr_t>(b);
+  return x < y + bn && y < x + an;
+}
+
+void no_partial_overlap(const void *ki, const void *ko, size_t kbytes, const void *vi, const void *vo,
+                        size_t vbytes) {
+  if (ki != ko && ranges_overlap(ki, kbytes, ko, kbytes))
+    throw std::invalid_argument("keys_in and keys_out overlap partially (only keys_in == keys_out is allowed)");
+  if (vi != vo && ranges_overlap(vi, vbytes, vo, vbytes))
+    throw std::invalid_argument("values_in and values_out overlap partially (only values_in == values_out is allowed)");
+  if (ranges_overlap(ko, kbytes, vo, vbytes) || ranges_overlap(ki, kbytes, vo, vbytes) ||
+      ranges_overlap(ko, kbytes, vi, vbytes))
+    throw std::invalid_argument("a key buffer overlaps a value buffer");
+}
+
 gpulsm::DictConfig dict_config(const gpulsm_dict_config &config) {
   gpulsm::DictConfig c;
   c.max_elements = config.max_elements;
@@ -551,6 +570,7 @@ int gpulsm_sort_pairs(const void *keys_in, const uint32_t *values_in, void *keys
     need(keys_in, "keys_in");
     need(keys_out, "keys_out");
     if (values_in) need(values_out, "values_out");
+    no_partial_overlap(keys_in, keys_out, count * (key_bits / 8), values_in, values_out, values_in ? count * 4 : 0);
     device_accessible({{keys_in, "keys_in"}, {values_in, "values_in"}, {keys_out, "keys_out"}, {values_out, "values_out"}});
     gpulsm::sort_pairs_any(keys_in, values_in, keys_out, values_out, count, key_bits, begin_bit,
                            end_bit, S(stream));
@@ -677,6 +697,7 @@ extern "C" int gpulsm_sort_pairs_noalloc(const void *keys_in, const uint32_t *va
     need(keys_in, "keys_in");
     need(keys_out, "keys_out");
     if (values_in) need(values_out, "values_out");
+    no_partial_overlap(keys_in, keys_out, count * (key_bits / 8), values_in, values_out, values_in ? count * 4 : 0);
     device_accessible({{keys_in, "keys_in"}, {values_in, "values_in"}, {keys_out, "keys_out"},
                        {values_out, "values_out"}});
     gpulsm::sort_pairs_noalloc(keys_in, values_in, keys_out, values_out, count, key_bits, begin_bit, end_bit,

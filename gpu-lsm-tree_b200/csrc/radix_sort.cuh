@@ -32,17 +32,24 @@ inline size_t workspace_words(uint64_t n, int passes) {
 }
 inline size_t workspace_bytes(uint64_t n, int passes) { return workspace_words(n, passes) * 4; }
 
+// Digit mask of pass p over bits [begin_bit, end_bit): 8 bits, except a last
+// pass that reaches past end_bit, which sorts only the bits below end_bit.
+__host__ __device__ inline uint32_t digit_mask(uint32_t begin_bit, uint32_t end_bit, uint32_t p) {
+  const uint32_t width = end_bit - (begin_bit + 8 * p);
+  return width >= 8 ? 0xffu : ((1u << width) - 1u);
+}
+
 template <typename KeyT>
 __global__ void __launch_bounds__(kThreads) histogram_kernel(const KeyT *__restrict__ keys, uint32_t n,
-                                                             uint32_t begin_bit, uint32_t passes,
-                                                             uint32_t *__restrict__ hist) {
+                                                             uint32_t begin_bit, uint32_t end_bit,
+                                                             uint32_t passes, uint32_t *__restrict__ hist) {
   __shared__ uint32_t s[kMaxPasses][kDigits];
   for (uint32_t i = threadIdx.x; i < kMaxPasses * kDigits; i += kThreads) (&s[0][0])[i] = 0;
   __syncthreads();
   for (uint32_t i = blockIdx.x * kThreads + threadIdx.x; i < n; i += gridDim.x * kThreads) {
     const KeyT k = keys[i];
     for (uint32_t p = 0; p < passes; ++p)
-      atomicAdd(&s[p][uint32_t(k >> (begin_bit + 8 * p)) & 0xffu], 1u);
+      atomicAdd(&s[p][uint32_t(k >> (begin_bit + 8 * p)) & digit_mask(begin_bit, end_bit, p)], 1u);
   }
   __syncthreads();
   for (uint32_t p = 0; p < passes; ++p) {
@@ -59,7 +66,8 @@ struct OnesweepSmem {
 template <typename KeyT, bool kValues>
 __global__ void __launch_bounds__(kThreads) onesweep_kernel(
     const KeyT *__restrict__ kin, const uint32_t *__restrict__ vin, KeyT *__restrict__ kout,
-    uint32_t *__restrict__ vout, uint32_t n_host, uint32_t shift, const uint32_t *__restrict__ pass_hist,
+    uint32_t *__restrict__ vout, uint32_t n_host, uint32_t shift, uint32_t dmask,
+    const uint32_t *__restrict__ pass_hist,
     uint32_t *__restrict__ lookback, uint32_t *__restrict__ tile_counter,
     uint32_t *__restrict__ status, const uint32_t *__restrict__ n_dev) {
   // n_dev (optional) carries a count produced on the device; the grid is then
@@ -94,7 +102,7 @@ __global__ void __launch_bounds__(kThreads) onesweep_kernel(
     const bool valid = idx < n;
     keys[i] = valid ? kin[idx] : KeyT(0);
     if (kValues) vals[i] = valid ? vin[idx] : 0u;
-    digits[i] = valid ? (uint32_t(keys[i] >> shift) & 0xffu) : 256u;
+    digits[i] = valid ? (uint32_t(keys[i] >> shift) & dmask) : 256u;
   }
   uint32_t *my_hist = warp_hist + warp * kDigits;
   const uint32_t lt = lanemask_lt();
@@ -166,7 +174,7 @@ __global__ void __launch_bounds__(kThreads) onesweep_kernel(
   const uint32_t valid_count = min(kTile, n - tile_base);
   for (uint32_t j = threadIdx.x; j < valid_count; j += kThreads) {
     const KeyT k = s_keys[j];
-    const uint32_t o = s_offset[uint32_t(k >> shift) & 0xffu] + j;
+    const uint32_t o = s_offset[uint32_t(k >> shift) & dmask] + j;
     if (o < n) {  // always true unless a look-back wait timed out (status bit set)
       kout[o] = k;
       if (kValues) vout[o] = s_vals[j];
@@ -175,8 +183,8 @@ __global__ void __launch_bounds__(kThreads) onesweep_kernel(
 }
 
 // Runs the digit passes over [begin_bit, end_bit).  The workspace must be
-// zeroed and its histogram filled (histogram_kernel, or a fused producer)
-// before the call.  keys[0]/vals[0] hold the input; returns the index of the
+// zeroed and its histogram filled (histogram_kernel, or a fused producer that
+// counts the same digits, digit_mask included) before the call.  keys[0]/vals[0] hold the input; returns the index of the
 // buffer that holds the sorted output.
 template <typename KeyT, bool kValues>
 int run_passes(KeyT *keys[2], uint32_t *vals[2], uint32_t n, int begin_bit, int end_bit,
@@ -194,7 +202,8 @@ int run_passes(KeyT *keys[2], uint32_t *vals[2], uint32_t n, int begin_bit, int 
   for (int p = 0; p < passes; ++p) {
     onesweep_kernel<KeyT, kValues><<<tiles, kThreads, smem, stream>>>(
         keys[cur], kValues ? vals[cur] : nullptr, keys[cur ^ 1], kValues ? vals[cur ^ 1] : nullptr,
-        n, uint32_t(begin_bit + 8 * p), hist + p * kDigits, lookback + size_t(p) * tiles * kDigits,
+        n, uint32_t(begin_bit + 8 * p), digit_mask(uint32_t(begin_bit), uint32_t(end_bit), uint32_t(p)),
+        hist + p * kDigits, lookback + size_t(p) * tiles * kDigits,
         counters + p, status, n_dev); note_launch();
     cur ^= 1;
   }
@@ -210,7 +219,7 @@ int sort(KeyT *keys[2], uint32_t *vals[2], uint32_t n, int begin_bit, int end_bi
   const int passes = (end_bit - begin_bit + 7) / 8;
   GPULSM_CUDA(cudaMemsetAsync(workspace, 0, workspace_bytes(n, passes), stream));
   const unsigned blocks = std::min<unsigned>(grid_for(n, kTile), unsigned(num_sms) * 4u);
-  histogram_kernel<KeyT><<<blocks, kThreads, 0, stream>>>(keys[0], n, uint32_t(begin_bit),
+  histogram_kernel<KeyT><<<blocks, kThreads, 0, stream>>>(keys[0], n, uint32_t(begin_bit), uint32_t(end_bit),
                                                           uint32_t(passes), workspace); note_launch();
   return run_passes<KeyT, kValues>(keys, vals, n, begin_bit, end_bit, workspace, status, stream);
 }

@@ -1,4 +1,5 @@
-// Standalone entry to the onesweep radix sort (gpulsm_sort_pairs).
+// Standalone entry to the onesweep radix sort (gpulsm_sort_pairs).  The call
+// returns once the sort has finished: it reads back the passes' status word.
 #include <algorithm>
 #include <stdexcept>
 
@@ -46,7 +47,14 @@ void sort_typed(const void *keys_in, const uint32_t *values_in, void *keys_out,
                                    status, sms, s);
   GPULSM_CUDA(cudaMemcpyAsync(keys_out, kk[cur], kb, cudaMemcpyDeviceToDevice, s));
   if (vals) GPULSM_CUDA(cudaMemcpyAsync(values_out, vv[cur], vb, cudaMemcpyDeviceToDevice, s));
+  // the passes' status word: a look-back wait that gave up leaves the output
+  // unsorted, so the call waits for the sort and reports it
+  uint32_t status_word = 0;
+  GPULSM_CUDA(cudaMemcpyAsync(&status_word, status, 4, cudaMemcpyDeviceToHost, s));
   GPULSM_CUDA(cudaFreeAsync(block, s));
+  GPULSM_CUDA(cudaStreamSynchronize(s));
+  if (status_word & kDevWaitTimeout)
+    throw std::runtime_error("gpulsm_sort_pairs: a radix pass timed out waiting on its look-back; output invalid");
 }
 }  // namespace
 

@@ -18,7 +18,12 @@
 //   - the first call on a device looks up the array's device address with
 //     cudaGetSymbolAddress (host code cannot use the symbol itself: in host
 //     code it is only a stand-in for the device array) - make that first call
-//     before any stream capture on that device.
+//     before any stream capture on that device;
+//   - keys_in may be keys_out (and values_in values_out): the sort then runs
+//     in place; a partial overlap of an input with an output is rejected;
+//   - the call returns once the sort has finished: it copies the passes'
+//     status word into a host variable and reports a look-back wait that gave
+//     up as GPULSM_ERR_TIMEOUT (the output is then not sorted).
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -78,10 +83,13 @@ void sort_in_static_scratch(const void *keys_in, const uint32_t *values_in, void
   GPULSM_CUDA(cudaGetDevice(&dev));
   GPULSM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   const bool vals = values_in != nullptr;
-  // the sort ping-pongs between the caller's output and the static scratch
+  // the sort ping-pongs between the caller's output and the static scratch;
+  // an in-place call (input == output) needs no first copy
   GPULSM_CUDA(cudaMemsetAsync(status, 0, 4, s));
-  GPULSM_CUDA(cudaMemcpyAsync(keys_out, keys_in, size_t(n) * sizeof(KeyT), cudaMemcpyDeviceToDevice, s));
-  if (vals) GPULSM_CUDA(cudaMemcpyAsync(values_out, values_in, size_t(n) * 4, cudaMemcpyDeviceToDevice, s));
+  if (keys_out != keys_in)
+    GPULSM_CUDA(cudaMemcpyAsync(keys_out, keys_in, size_t(n) * sizeof(KeyT), cudaMemcpyDeviceToDevice, s));
+  if (vals && values_out != values_in)
+    GPULSM_CUDA(cudaMemcpyAsync(values_out, values_in, size_t(n) * 4, cudaMemcpyDeviceToDevice, s));
   KeyT *kk[2] = {static_cast<KeyT *>(keys_out), scratch_keys};
   uint32_t *vv[2] = {values_out, scratch_vals};
   // radix::sort zeroes the histogram / look-back words it needs (kept from the previous call)
@@ -91,6 +99,14 @@ void sort_in_static_scratch(const void *keys_in, const uint32_t *values_in, void
     GPULSM_CUDA(cudaMemcpyAsync(keys_out, scratch_keys, size_t(n) * sizeof(KeyT), cudaMemcpyDeviceToDevice, s));
     if (vals) GPULSM_CUDA(cudaMemcpyAsync(values_out, scratch_vals, size_t(n) * 4, cudaMemcpyDeviceToDevice, s));
   }
+  // the status word lives in the shared array; it is copied into a host
+  // variable on this thread's stack (no allocation) and the call waits for it
+  uint32_t status_word = 0;
+  GPULSM_CUDA(cudaMemcpyAsync(&status_word, status, 4, cudaMemcpyDeviceToHost, s));
+  GPULSM_CUDA(cudaStreamSynchronize(s));
+  if (status_word & kDevWaitTimeout)
+    throw std::runtime_error(
+        "gpulsm_sort_pairs_noalloc: a radix pass timed out waiting on its look-back; output invalid");
 }
 }  // namespace
 

@@ -198,16 +198,11 @@ def run(gl, torch, args, rc: ResultCollector, run_id: int, save=None) -> int:
         hits, hit_vals = live_k[pick], live_v[pick]
         hd = up(hits)
         sorted_hd = torch.empty_like(hd)
-        perm = torch.empty(probe_size, dtype=torch.int64, device=dev)
+        idx = torch.arange(probe_size, dtype=torch.int32, device=dev)
+        perm = torch.empty(probe_size, dtype=torch.int32, device=dev)
 
-        def sort_probes():  # unsigned order: 32-bit keys sort with their sign bit flipped
-            if kb == 32:
-                s, p = torch.sort(hd ^ -(1 << 31))
-                s = s ^ -(1 << 31)
-            else:
-                s, p = torch.sort(hd)  # 64-bit keys stay below 2^63
-            sorted_hd.copy_(s)
-            perm.copy_(p)
+        def sort_probes():  # this library's onesweep radix sort of (probe, input index)
+            gl.sort_pairs(hd, idx, sorted_hd, perm)
 
         m["sort_time_ms"] = timed(sort_probes)
         res = torch.empty(probe_size, dtype=torch.int32, device=dev)

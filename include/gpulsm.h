@@ -295,9 +295,13 @@ int gpulsm_binary_lower_bound(const void *sorted_keys, uint64_t count, uint32_t 
                               uint64_t query_count, uint64_t *out, void *stream);
 
 /* ===================== building blocks ==================================== */
-/* Stable LSD radix sort of (key, u32 value) pairs by key bits [begin_bit, end_bit).
- * key_bits 32 or 64; values may be NULL. keys_out/values_out receive the result;
- * the inputs are not modified. Allocates its scratch on the stream. */
+/* Stable LSD radix sort of (key, u32 value) pairs by key bits [begin_bit, end_bit)
+ * (bits outside the range do not affect the order).  key_bits 32 or 64; values
+ * may be NULL.  keys_out/values_out receive the result; keys_out may equal
+ * keys_in (values_out values_in), a partial overlap of any two buffers is
+ * rejected with GPULSM_ERR_INVALID_ARGUMENT.  Allocates its scratch on the
+ * stream.  Returns once the sort has finished (it reads the passes' status
+ * word back); a device look-back wait that gave up gives GPULSM_ERR_TIMEOUT. */
 int gpulsm_sort_pairs(const void *keys_in, const uint32_t *values_in, void *keys_out,
                       uint32_t *values_out, uint64_t count, uint32_t key_bits, uint32_t begin_bit,
                       uint32_t end_bit, void *stream);
@@ -308,9 +312,13 @@ int gpulsm_sort_pairs(const void *keys_in, const uint32_t *values_in, void *keys
  * cudaFree or allocating library routine.  Its scratch is one static device
  * array (about 14 MiB, see gpulsm_sort_noalloc_scratch_bytes) that every GPU
  * loading the library holds until exit.  At most 2^20 keys per call; more
- * gives GPULSM_ERR_LENGTH.  All calls on a device share that array: calls that
- * overlap on the GPU race, so serialise them.  The first call on a device
- * resolves the array's address - make it before any stream capture. */
+ * gives GPULSM_ERR_LENGTH.  All calls on a device share that array, which keeps
+ * the previous call's contents (each call clears what must start at zero):
+ * calls that overlap on the GPU race, so serialise them.  The first call on a
+ * device resolves the array's address - make it before any stream capture.
+ * Aliasing, the bit range and the status read-back (the call returns once the
+ * sort has finished; GPULSM_ERR_TIMEOUT if a look-back wait gave up) are as
+ * for gpulsm_sort_pairs. */
 int gpulsm_sort_pairs_noalloc(const void *keys_in, const uint32_t *values_in, void *keys_out,
                               uint32_t *values_out, uint64_t count, uint32_t key_bits, uint32_t begin_bit,
                               uint32_t end_bit, void *stream);

@@ -21,10 +21,14 @@ _u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
 _u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
 
 
-def build_oracle(reference: bool = True) -> None:
-    """Compile liboracle.so (and oracle/_ref when the reference checkout exists)."""
-    target = "all" if reference else os.path.join(_HERE, "liboracle.so")
-    subprocess.run(["make", "-s", "-C", _HERE, target], check=True)
+def build_oracle(reference: str | None = None) -> None:
+    """Compile liboracle.so and, when `reference` names a reference checkout,
+    the reference engines under oracle/_ref (read in place, never copied)."""
+    if reference:
+        subprocess.run(["make", "-s", "-C", _HERE, "all", f"REFERENCE={reference}"], check=True)
+    else:
+        subprocess.run(["make", "-s", "-C", _HERE, os.path.join(_HERE, "liboracle.so"),
+                        os.path.join(_HERE, "libcpubaselines.so")], check=True)
 
 
 def _load():
@@ -32,7 +36,7 @@ def _load():
     if _lib is not None:
         return _lib
     if not os.path.exists(_LIB_PATH):
-        build_oracle(reference=False)
+        build_oracle()
     lib = C.CDLL(_LIB_PATH)
     vp = C.c_void_p
     u64 = C.c_uint64
@@ -229,3 +233,94 @@ def model_gradients(keys, kmin: int, shift: int, nseg: int, a, b):
     fn(k, k.size, kmin, shift, nseg, np.ascontiguousarray(a, np.float32), np.ascontiguousarray(b, np.float32),
        ga, gb, C.byref(loss))
     return ga, gb, loss.value
+
+
+# ----------------------------------------------------------------------------
+# CPU baselines (libcpubaselines.so, cpu_baselines.cpp): engines with the same
+# semantics as OracleLSM, timed beside the GPU.  Test infrastructure only.
+_CPU_LIB_PATH = os.path.join(_HERE, "libcpubaselines.so")
+_cpu = None
+
+
+def _load_cpu():
+    global _cpu
+    if _cpu is not None:
+        return _cpu
+    if not os.path.exists(_CPU_LIB_PATH):
+        subprocess.run(["make", "-s", "-C", _HERE, _CPU_LIB_PATH], check=True)
+    lib = C.CDLL(_CPU_LIB_PATH)
+    vp, u64 = C.c_void_p, C.c_uint64
+    sig = {}
+    for pre in ("cpumap", "cpulsm"):
+        sig.update({
+            f"{pre}_destroy": (None, [vp]),
+            f"{pre}_insert": (None, [vp, _u32p, _u32p, u64]),
+            f"{pre}_erase": (None, [vp, _u32p, u64]),
+            f"{pre}_lookup": (None, [vp, _u32p, u64, _u32p, vp]),
+            f"{pre}_range_offsets": (u64, [vp, _u32p, _u32p, u64, _u64p]),
+            f"{pre}_range_pairs": (None, [vp, _u32p, _u32p, u64, _u64p, _u32p, _u32p]),
+        })
+    sig["cpumap_create"] = (vp, [])
+    sig["cpulsm_create"] = (vp, [u64, C.c_uint32])
+    sig["cpulsm_levels"] = (C.c_uint32, [vp])
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _cpu = lib
+    return lib
+
+
+class _CpuBaseline:
+    _pre = ""
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            getattr(self._lib, f"{self._pre}_destroy")(self._h)
+            self._h = None
+
+    def insert(self, keys, values):
+        k, v = _u32(keys), _u32(values)
+        getattr(self._lib, f"{self._pre}_insert")(self._h, k, v, k.size)
+
+    def erase(self, keys):
+        k = _u32(keys)
+        getattr(self._lib, f"{self._pre}_erase")(self._h, k, k.size)
+
+    def lookup(self, queries, with_found: bool = False):
+        q = _u32(queries)
+        out = np.empty(q.size, np.uint32)
+        found = np.empty(q.size, np.uint8) if with_found else None
+        getattr(self._lib, f"{self._pre}_lookup")(self._h, q, q.size, out,
+                                                  found.ctypes.data_as(C.c_void_p) if with_found else None)
+        return (out, found) if with_found else out
+
+    def range_pairs(self, lo, hi):
+        lo, hi = _u32(lo), _u32(hi)
+        offsets = np.empty(lo.size + 1, np.uint64)
+        total = int(getattr(self._lib, f"{self._pre}_range_offsets")(self._h, lo, hi, lo.size, offsets))
+        keys = np.empty(total, np.uint32)
+        vals = np.empty(total, np.uint32)
+        getattr(self._lib, f"{self._pre}_range_pairs")(self._h, lo, hi, lo.size, offsets, keys, vals)
+        return offsets, keys, vals
+
+
+class CpuMap(_CpuBaseline):
+    """Single-thread std::map with GPULSMOpt's semantics."""
+    _pre = "cpumap"
+
+    def __init__(self):
+        self._lib = _load_cpu()
+        self._h = self._lib.cpumap_create()
+
+
+class CpuLsm(_CpuBaseline):
+    """Multi-threaded leveled LSM on every host core (OpenMP), GPULSMOpt's semantics."""
+    _pre = "cpulsm"
+
+    def __init__(self, cap0: int = 1 << 22, fan_in: int = 4):
+        self._lib = _load_cpu()
+        self._h = self._lib.cpulsm_create(cap0, fan_in)
+
+    def levels(self) -> int:
+        return int(self._lib.cpulsm_levels(self._h))

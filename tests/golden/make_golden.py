@@ -1,8 +1,9 @@
 """Generates the golden fixtures in this folder by running the REFERENCE's own
-GPULSMOpt engine (oracle/_ref/libref_gpulsmopt.so, compiled from the
-reference header GPULSMOpt.cuh) on a CUDA GPU.
+engines on a CUDA GPU: GPULSMOpt (oracle/_ref/libref_gpulsmopt.so, compiled
+from the reference header GPULSMOpt.cuh) and FliX's bucket layer
+(oracle/_ref/libref_flix.so, compiled from FliX/impl_cg_rtx_index_updates.cuh).
 
-    python tests/golden/make_golden.py [--out DIR]   # on a machine with a GPU
+    python tests/golden/make_golden.py [--out DIR] [--only lsm,bulk,flix]
 
 Each fixture stores the scenario's inputs (or the seed that regenerates them)
 and the reference's outputs.  tests/test_golden.py checks the CPU oracle
@@ -23,9 +24,10 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "tests"))
 
-from oracle.refgpu import RefError, RefGPULSMOpt  # noqa: E402
-from scenarios import (capacity_ops, forced_validation_steps, key_for_index, rollover_ops,  # noqa: E402
-                       sweep_lookup_queries, sweep_range_queries, validation_queries)
+from oracle.refgpu import RefError, RefFlix, RefGPULSMOpt  # noqa: E402
+from scenarios import (bulk_build_stages, capacity_ops, forced_validation_steps, key_for_index,  # noqa: E402
+                       rollover_ops, sweep_lookup_queries, sweep_range_queries, validation_queries)
+import flix_scenarios as FS  # noqa: E402
 
 W = importlib.import_module("gpu-lsm-tree_b200.workloads")
 
@@ -93,12 +95,84 @@ def random_ops(seed, batch_capacity, steps=40):
     return ops, q, lo, hi
 
 
+def dev_keys(a):
+    a = np.ascontiguousarray(a)
+    view = {np.dtype(np.uint32): np.int32, np.dtype(np.uint64): np.int64}[a.dtype]
+    return torch.from_numpy(a.view(view)).cuda()
+
+
+def make_bulk():
+    """GPULSMOpt bulk_build with duplicate keys, updates after it, a bulk build
+    over a dictionary holding updates, and an empty bulk build."""
+    ref = RefGPULSMOpt(1 << 17, 1 << 12)
+    data = {}
+    for i, (op, q, lo, hi) in enumerate(bulk_build_stages()):
+        if op[0] == "bulk":
+            ref.bulk_build(dev(op[1]), dev(op[2]))
+        elif op[0] == "insert":
+            ref.insert(dev(op[1]), dev(op[2]))
+        else:
+            ref.erase(dev(op[1]))
+        for k2, v2 in queries(ref, q, lo, hi).items():
+            data[f"s{i}_{k2}"] = v2
+    data["status"] = np.array([ref.status()], np.uint32)
+    np.savez_compressed(os.path.join(HERE, "bulk_build.npz"), **data)
+    ref.close()
+
+
+def make_flix():
+    """FliX bucket-layer scenarios (tests/flix_scenarios.py) through the
+    reference's own FliX kernels: every probe stage records the ordered lookup
+    and successor answers and the key count the reference reports."""
+    for sc in FS.scenarios():
+        kdt = np.uint32 if sc.key_bits == 32 else np.uint64
+        tdt = torch.int32 if sc.key_bits == 32 else torch.int64
+        ref = RefFlix(sc.key_bits)
+        ref.build_bucket_layer_only(dev_keys(sc.build_keys), sc.max_size)
+        torch.cuda.synchronize()
+        data = {"digest": np.array([FS.digest(sc)]), "build_total_keys": np.array([ref.total_keys()], np.uint64)}
+        p = 0
+        for st in sc.stages:
+            if st.kind == "insert":
+                ref.insert(dev_keys(st.keys), dev(st.values))
+            elif st.kind == "remove":
+                ref.remove(dev_keys(st.keys))
+            elif st.kind == "rebuild":
+                ref.rebuild_bucket_layer_only()
+            else:
+                if st.lookup_probes is not None:
+                    probes = st.lookup_probes
+                    out = torch.empty(max(probes.size, 1), dtype=torch.int32, device="cuda")
+                    ref.lookups_ordered(dev_keys(probes), out)
+                    data[f"p{p}_lookup"] = host(out)[: probes.size].copy()
+                probes = st.successor_probes
+                out = torch.empty(max(probes.size, 1), dtype=tdt, device="cuda")
+                ref.lookups_successor(dev_keys(probes), out)
+                data[f"p{p}_successor"] = host(out, kdt)[: probes.size].copy()
+                torch.cuda.synchronize()
+                data[f"p{p}_total_keys"] = np.array([ref.total_keys()], np.uint64)
+                p += 1
+        torch.cuda.synchronize()
+        data["allocation_state"] = np.array(ref.allocation_state(), np.uint64)
+        np.savez_compressed(os.path.join(HERE, f"{sc.name}.npz"), **data)
+        ref.close()
+
+
 def main():
     global HERE
     if "--out" in sys.argv:
         HERE = sys.argv[sys.argv.index("--out") + 1]
         os.makedirs(HERE, exist_ok=True)
+    only = set(sys.argv[sys.argv.index("--only") + 1].split(",")) if "--only" in sys.argv else {"lsm", "bulk", "flix"}
     torch.cuda.init()
+    if "bulk" in only:
+        make_bulk()
+    if "flix" in only:
+        make_flix()
+    if "lsm" not in only:
+        torch.cuda.synchronize()
+        print("golden fixtures written to", HERE)
+        return
     # 1. forced validation (cumulative, one dictionary)
     ref = RefGPULSMOpt(1 << 20)
     data = {}

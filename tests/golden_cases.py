@@ -1,7 +1,7 @@
 """Loads the reference-generated golden fixtures (tests/golden/*.npz, written by
-tests/golden/make_golden.py from the reference's own GPULSMOpt engine) as
-replayable cases: the update operations, the dictionary configuration, the
-queries and the reference's answers."""
+tests/golden/make_golden.py from the reference's own GPULSMOpt engine and
+FliX bucket layer) as replayable cases: the update operations, the
+configuration, the queries and the reference's answers."""
 from __future__ import annotations
 
 import importlib
@@ -10,7 +10,8 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from scenarios import forced_validation_steps, key_for_index, rollover_ops, capacity_ops, \
+import flix_scenarios as FS
+from scenarios import bulk_build_stages, forced_validation_steps, key_for_index, rollover_ops, capacity_ops, \
     sweep_lookup_queries, sweep_range_queries, validation_queries
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
@@ -104,3 +105,34 @@ def capacity_case():
     return {"accepted": int(z["accepted"][0]), "status": int(z["status"][0]),
             "loop_error": str(z["loop_error"][0]), "after_error": str(z["after_error"][0]),
             "queries": z["queries"], "lookup": z["lookup"], "ops": capacity_ops()}
+
+
+def bulk_available() -> bool:
+    return os.path.exists(os.path.join(GOLDEN, "bulk_build.npz"))
+
+
+def bulk_case():
+    """[(op, Probe)] for the bulk-build fixture; op is ("bulk"|"insert", keys,
+    values) or ("erase", keys)."""
+    z = _load("bulk_build.npz")
+    out = []
+    for i, (op, q, lo, hi) in enumerate(bulk_build_stages()):
+        out.append((op, Probe(q, {k: z[f"s{i}_{k}"] for k in ("lookup", "lookup_found_values", "lookup_found",
+                                                                "successor", "range_sum")}, lo, hi)))
+    return out
+
+
+def flix_available() -> bool:
+    return all(os.path.exists(os.path.join(GOLDEN, f"{sc}.npz"))
+               for sc in ("flix32_main", "flix64_insert", "flix32_edge"))
+
+
+def flix_cases():
+    """[(FlixScenario, {answer name: reference output})]; the recorded input
+    digest must match the regenerated scenario."""
+    out = []
+    for sc in FS.scenarios():
+        z = _load(f"{sc.name}.npz")
+        assert str(z["digest"][0]) == FS.digest(sc), f"{sc.name}: regenerated inputs differ from the fixture's"
+        out.append((sc, {k: z[k] for k in z.files}))
+    return out

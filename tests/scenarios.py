@@ -159,3 +159,40 @@ def range_digest(results, query_offset: int = 0):
         v = (v ^ (v >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
         v = v ^ (v >> np.uint64(31))
     return int(r.sum(dtype=np.uint64)), int(np.bitwise_xor.reduce(v)) if v.size else 0
+
+
+def bulk_build_stages(seed: int = 21):
+    """Stages for the bulk-build fixture (GPULSMOpt.cuh:5738-5834: reset, stable
+    radix sort of the pairs, keep the LAST duplicate, mark_last_key_kernel
+    :2633-2638).  Yields (op, probe_queries, lo, hi) where op is
+    ("bulk", keys, values) | ("insert", keys, values) | ("erase", keys).
+    Keys repeat heavily and include 0, 1 and 0xffffffff; the third bulk build
+    replaces a dictionary that already holds updates, and the last one is
+    empty (the reference returns after the reset, leaving no keys)."""
+    rng = np.random.default_rng(seed)
+    universe = rng.integers(0, 1 << 32, 1 << 13, dtype=np.uint64).astype(np.uint32)
+    universe[:4] = [0, 1, 0xFFFFFFFF, 0xFFFFFFFE]
+
+    def vals(n):
+        return rng.integers(0, 1 << 32, n, dtype=np.uint64).astype(np.uint32)
+
+    def probes():
+        q = np.concatenate([universe, rng.integers(0, 1 << 32, 2048, dtype=np.uint64).astype(np.uint32)])
+        lo = universe[rng.integers(0, universe.size, 512)]
+        hi = np.minimum(lo.astype(np.uint64) + rng.integers(0, 1 << 28, 512, dtype=np.uint64),
+                        0xFFFFFFFF).astype(np.uint32)
+        lo[:2] = [7, 0]
+        hi[:2] = [3, 0xFFFFFFFF]
+        return q, lo, hi
+
+    stages = []
+    k = universe[rng.integers(0, universe.size, 1 << 16)]
+    stages.append((("bulk", k, vals(k.size)),) + probes())
+    k = universe[rng.integers(0, universe.size, 3000)]
+    stages.append((("insert", k, vals(k.size)),) + probes())
+    k = universe[rng.integers(0, universe.size, 1500)]
+    stages.append((("erase", k),) + probes())
+    k = universe[rng.integers(0, universe.size // 2, 20000)]
+    stages.append((("bulk", k, vals(k.size)),) + probes())
+    stages.append((("bulk", np.zeros(0, np.uint32), np.zeros(0, np.uint32)),) + probes())
+    return stages

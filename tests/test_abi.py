@@ -68,3 +68,19 @@ def test_no_cpu_fallback_when_library_missing(tmp_path):
             "\ntry:\n  m.load()\nexcept ImportError as e:\n  print('LOUD', e)" % str(tmp_path))
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True)
     assert "LOUD" in r.stdout and "no CPU fallback" in r.stdout
+
+
+def test_sort_entries_reject_partial_overlap_before_touching_memory(gl):
+    """Both sort entries allow keys_out == keys_in (in place) but reject a
+    partial overlap of any two buffers; the check is pointer arithmetic only,
+    made before any pointer is dereferenced, so fake addresses are safe here."""
+    lib = gl.load()
+    N = gl._native
+    base = 1 << 40
+    for fn in (lib.gpulsm_sort_pairs, lib.gpulsm_sort_pairs_noalloc):
+        # keys_out starts 4 bytes into keys_in: partial overlap
+        assert fn(base, None, base + 4, None, 100, 32, 0, 32, None) == N.ERR_INVALID_ARGUMENT
+        assert b"overlap" in lib.gpulsm_last_error()
+        # values_out overlapping keys_out
+        assert fn(base, base + 4096, base + 8192, base + 8192 + 64, 100, 32, 0, 32, None) == N.ERR_INVALID_ARGUMENT
+        assert b"overlap" in lib.gpulsm_last_error()

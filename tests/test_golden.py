@@ -4,7 +4,7 @@ import numpy as np
 import pytest
 
 import golden_cases as G
-from oracle import OracleLSM
+from oracle import OracleFlix, OracleLSM
 
 pytestmark = pytest.mark.skipif(not G.available(), reason="golden fixtures not generated")
 
@@ -46,3 +46,76 @@ def test_oracle_matches_reference_after_capacity_failure():
     got = o.lookup(c["queries"])
     # keys of the failed 16-batch epoch stay readable in the reference ("pending updates were preserved")
     assert np.array_equal(got, c["lookup"])
+
+
+@pytest.mark.skipif(not G.bulk_available(), reason="bulk-build fixture not generated")
+def test_oracle_matches_reference_bulk_build():
+    """Keep-last-duplicate bulk build, updates after it, a bulk build over a
+    dictionary holding updates and an empty bulk build (GPULSMOpt.cuh:5738-5834)."""
+    o = OracleLSM()
+    for i, (op, probe) in enumerate(G.bulk_case()):
+        if op[0] == "bulk":
+            o.bulk_build(op[1], op[2])
+        elif op[0] == "insert":
+            o.insert(op[1], op[2])
+        else:
+            o.erase(op[1])
+        for name, want in probe.expect.items():
+            assert np.array_equal(answer(o, probe, name), want), f"stage {i}: {name}"
+
+
+def flix_replay(sc, z, apply, probe, exact=None):
+    """Replays a FliX scenario: apply(stage) for updates; probe(stage) -> dict of
+    answers, compared with the reference's p<k>_* arrays.  A difference is
+    accepted only where flix_scenarios.allowed() names a documented reference
+    deviation of that stage, and only if the answer there equals exact(stage)
+    (the std::map answers; by default the answers under test are taken as
+    exact, which holds for the oracle)."""
+    import flix_scenarios as FS
+
+    p = 0
+    for st in sc.stages:
+        if st.kind != "probe":
+            apply(st)
+            continue
+        got = probe(st)
+        ex = exact(st) if exact else got
+        for name, val in got.items():
+            want = z[f"p{p}_{name}"]
+            if name == "total_keys":
+                if "lost_in_rebuild" in st.quirks:
+                    assert int(want[0]) <= int(val), f"{sc.name} probe {p}: {name}"
+                else:
+                    assert int(val) == int(want[0]), f"{sc.name} probe {p}: {name}"
+                continue
+            ok = FS.allowed(st, name, ex[name], want)
+            bad = np.flatnonzero((val != want) & ~(ok & (val == ex[name])))
+            assert bad.size == 0, (f"{sc.name} probe {p}: {name} differs at {bad.size} of {want.size} "
+                                   f"(first index {bad[:1]}: got {val[bad[:1]]}, reference {want[bad[:1]]})")
+        p += 1
+
+
+@pytest.mark.skipif(not G.flix_available(), reason="FliX fixtures not generated")
+@pytest.mark.parametrize("case", G.flix_cases() if G.flix_available() else [], ids=lambda c: c[0].name)
+def test_flix_oracle_matches_reference_fixture(case):
+    """flix_oracle.c against the reference's own FliX kernels: build (values =
+    input index), insert-if-absent, physical delete, rebuild, ordered lookups and
+    successors (FliX/impl_cg_rtx_index_updates.cuh:1711-2677)."""
+    sc, z = case
+    o = OracleFlix(sc.key_bits)
+    o.build(sc.build_keys)
+    assert len(o) == int(z["build_total_keys"][0])
+
+    def apply(st):
+        if st.kind == "insert":
+            o.insert(st.keys, st.values)
+        elif st.kind == "remove":
+            o.remove(st.keys)
+
+    def probe(st):
+        got = {"successor": o.successor(st.successor_probes), "total_keys": len(o)}
+        if st.lookup_probes is not None:
+            got["lookup"] = o.lookup(st.lookup_probes)
+        return got
+
+    flix_replay(sc, z, apply, probe)

@@ -196,3 +196,41 @@ def test_updates_runner_writes_result_collector_long_form():
         pass
     else:
         raise AssertionError("a measurement column reused as a parameter must be refused")
+
+
+@pytest.mark.parametrize("engine", ["map", "lsm"])
+def test_cpu_baselines_match_oracle(engine):
+    """The CPU baselines timed beside the GPU (std::map, leveled OpenMP LSM)
+    give the oracle's answers: upserts with the last write of a batch winning,
+    erases, lookups with and without found flags, range pairs."""
+    from oracle import CpuLsm, CpuMap, OracleLSM
+
+    rng = np.random.default_rng(5)
+    o = OracleLSM()
+    e = CpuMap() if engine == "map" else CpuLsm(cap0=512, fan_in=3)
+    universe = rng.integers(0, 1 << 32, 5000, dtype=np.uint64).astype(np.uint32)
+    universe[:3] = [0, 0xFFFFFFFF, 1]
+    for step in range(60):
+        n = int(rng.integers(1, 700))
+        k = universe[rng.integers(0, universe.size, n)]
+        if rng.random() < 0.3:
+            o.erase(k)
+            e.erase(k)
+        else:
+            v = rng.integers(0, 1 << 32, n, dtype=np.uint64).astype(np.uint32)
+            o.insert(k, v)
+            e.insert(k, v)
+        if step % 10 == 9:
+            q = np.concatenate([universe, rng.integers(0, 1 << 32, 500, dtype=np.uint64).astype(np.uint32)])
+            assert np.array_equal(e.lookup(q), o.lookup(q))
+            ev, ef = e.lookup(q, with_found=True)
+            ov, of = o.lookup(q, with_found=True)
+            assert np.array_equal(ev, ov) and np.array_equal(ef, of)
+            lo = universe[rng.integers(0, universe.size, 300)]
+            hi = np.minimum(lo.astype(np.uint64) + rng.integers(0, 1 << 30, 300, dtype=np.uint64),
+                            0xFFFFFFFF).astype(np.uint32)
+            lo[:2], hi[:2] = [9, 0], [3, 0xFFFFFFFF]
+            for a, b in zip(e.range_pairs(lo, hi), o.range_pairs(lo, hi)):
+                assert np.array_equal(a, b)
+    if engine == "lsm":
+        assert e.levels() >= 2  # the run carried down several levels

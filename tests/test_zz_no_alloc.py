@@ -69,3 +69,31 @@ def test_noalloc_sort_rejects_counts_beyond_its_scratch(gl, cuda):
     with pytest.raises(gl.LengthError, match="at most"):
         N.check(lib.gpulsm_sort_pairs_noalloc(k.data_ptr(), None, k.data_ptr(), None, (1 << 20) + 1, 32, 0, 32,
                                               None))
+
+
+@pytest.mark.parametrize("bits", [32, 64])
+def test_noalloc_sort_partial_digit_range_and_in_place(gl, cuda, bits):
+    """A bit range that is not a whole number of 8-bit digits ([3, 13) here) on
+    full-width keys: both entries order by those 10 bits only, stably, like a
+    stable argsort of (key >> 3) & 0x3ff; then the same sort in place (input
+    buffers passed as outputs) gives the same result."""
+    import torch
+
+    lib = gl.load()
+    N = gl._native
+    rng = np.random.default_rng(bits)
+    n = 200_003
+    k = rng.integers(0, 1 << bits, n, dtype=np.uint64)
+    k = k.astype(np.uint32) if bits == 32 else k
+    v = np.arange(n, dtype=np.uint32)
+    order = np.argsort((k >> k.dtype.type(3)) & k.dtype.type(0x3FF), kind="stable")
+    for fn in (lib.gpulsm_sort_pairs, lib.gpulsm_sort_pairs_noalloc):
+        for call in range(2):
+            got_k, got_v = _sort(lib, N, fn, _dev(k), _dev(v), bits, 3, 13)
+            assert np.array_equal(got_k.cpu().numpy().view(k.dtype), k[order]), f"{fn.__name__} call {call}"
+            assert np.array_equal(got_v.cpu().numpy().view(np.uint32), v[order]), f"{fn.__name__} call {call}"
+        kd, vd = _dev(k), _dev(v)
+        N.check(fn(kd.data_ptr(), vd.data_ptr(), kd.data_ptr(), vd.data_ptr(), n, bits, 3, 13, None))
+        torch.cuda.synchronize()
+        assert np.array_equal(kd.cpu().numpy().view(k.dtype), k[order]), f"{fn.__name__} in place"
+        assert np.array_equal(vd.cpu().numpy().view(np.uint32), v[order]), f"{fn.__name__} in place"
