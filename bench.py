@@ -60,7 +60,7 @@ def parse():
     p.add_argument("--no-serving", action="store_true")
     p.add_argument("--no-tenants", action="store_true")
     p.add_argument("--no-flix", action="store_true")
-    p.add_argument("--flix-rounds", type=int, default=3)
+    p.add_argument("--flix-rounds", type=int, default=32)
     p.add_argument("--tenant-rounds", type=int, default=4)
     p.add_argument("--serving-seconds", type=float, default=2.0)
     p.add_argument("--case", default=None, choices=["merge", "admit", "serving-mix", "flix", "lookup"],
@@ -339,6 +339,7 @@ def run_ours(args):
         "clocks": clocks.summary(),
     }
 
+    result["lookup_modes"] = lookup_modes(gl, ops_dev, q, out_v, out_f, max_el, look, stream)
     if not args.no_e2e:
         result["e2e"] = e2e_ours(args, gl, w, dev, total_pairs, max_el)
     if not args.no_tenants:
@@ -360,13 +361,45 @@ def run_ours(args):
         print(json.dumps(result), flush=True)
 
 
+def lookup_modes(gl, ops_dev, q, out_v, out_f, max_el, directory_ms, stream):
+    """The step's 2^24 lookups over the same final dictionary in each search
+    mode: radix directory (the plain form, timed in the step), learned position
+    models (levels of >= 2^22 rows), plain binary search.  Best of three
+    launches, CUDA events on the launching stream; answers compared with the
+    directory mode's."""
+    import torch
+
+    res = {"directory_ms": round(directory_ms, 4)}
+    ref_v, ref_f = out_v.clone(), out_f.clone()
+    for name, mode in (("learned", 1), ("binary", 2)):
+        d = gl.GPULSMOpt(gl.DictionaryConfig(max_elements=max_el, search_mode=mode))
+        for kind, k, v in ops_dev:
+            d.insert(k, v) if kind == "insert" else d.erase(k)
+        d.join()
+        best = float("inf")
+        for _ in range(4):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            d.lookup(q, out_v, out_f)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))  # the first launch also fits the models
+        res[f"{name}_ms"] = round(best, 4)
+        res[f"{name}_same_answers"] = bool(torch.equal(out_v, ref_v) and torch.equal(out_f, ref_f))
+        d.close()
+    res["learned_speedup_vs_directory"] = round(directory_ms / res["learned_ms"], 3)
+    res["learned_speedup_vs_binary"] = round(res["binary_ms"] / res["learned_ms"], 3)
+    return res
+
+
 def flix_leg(args, gl, W, dev):
-    """FliX-style updatable sorted index: bulk build of 2^28 sorted u64 keys
-    (geometric gaps, mean 16), then rounds of 2^22 inserts (half uniform, half
-    in 1024 hot ranges), 2^21 deletes and 2^24 uniform successor probes; bucket
-    routing by binary search over the bucket maxima (plain) against the learned
-    piecewise-linear model with 4096 segments (learned).  The first round of
-    each run warms up; the others are timed with CUDA events."""
+    """FliX-style updatable sorted index at its configured size: bulk build of
+    2^28 sorted u64 keys (geometric gaps, mean 16), then 32 rounds of 2^22
+    inserts (half uniform, half in 1024 hot ranges), 2^21 deletes and 2^24
+    uniform successor probes, after one untimed warm-up round; bucket routing
+    by binary search over the bucket maxima (plain) against the learned
+    piecewise-linear model with 4096 segments (learned).  Every round is timed
+    with CUDA events; the allocation region's use is read after each round."""
     import torch
 
     w = W.flix_fast(0, rounds=args.flix_rounds + 1)
@@ -384,7 +417,7 @@ def flix_leg(args, gl, W, dev):
     cap = n_build + len(w.rounds) * rounds[0][0].numel()
     out = torch.empty(rounds[0][3].numel(), dtype=torch.int64, device=dev)
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
-    res = {}
+    res = {"rounds_timed": args.flix_rounds, "build_keys": int(n_build)}
     warm = gl.FlixIndex(key_bits=64, max_elements=1 << 20)
     warm.build(keys[: 1 << 20])
     torch.cuda.synchronize()
@@ -399,7 +432,8 @@ def flix_leg(args, gl, W, dev):
         e1.record()
         torch.cuda.synchronize()
         build_ms = e0.elapsed_time(e1)
-        t_ins = t_del = t_ord = t_suc = 0.0
+        per = {"insert_ms": [], "delete_ms": [], "ordered_successor_ms": [], "unsorted_successor_ms": [],
+               "region_used_nodes": []}
         n_ins = n_del = n_suc = 0
         for r, (ins, vals, dels, sprobes, probes) in enumerate(rounds):
             a, b, c, d, e = ev(), ev(), ev(), ev(), ev()
@@ -415,21 +449,32 @@ def flix_leg(args, gl, W, dev):
             torch.cuda.synchronize()
             if r == 0:
                 continue
-            t_ins += a.elapsed_time(b)
-            t_del += b.elapsed_time(c)
-            t_ord += c.elapsed_time(d)
-            t_suc += d.elapsed_time(e)
+            per["insert_ms"].append(a.elapsed_time(b))
+            per["delete_ms"].append(b.elapsed_time(c))
+            per["ordered_successor_ms"].append(c.elapsed_time(d))
+            per["unsorted_successor_ms"].append(d.elapsed_time(e))
+            per["region_used_nodes"].append(idx.allocation_state()["used_nodes"])
             n_ins += ins.numel()
             n_del += dels.numel()
             n_suc += probes.numel()
+        alloc = idx.allocation_state()
+        t_ins, t_del = sum(per["insert_ms"]), sum(per["delete_ms"])
+        t_ord, t_suc = sum(per["ordered_successor_ms"]), sum(per["unsorted_successor_ms"])
+        ni, nd, ns = rounds[0][0].numel(), rounds[0][2].numel(), rounds[0][4].numel()
         res[name] = {"build_ms": round(build_ms, 2), "build_mkeys_s": round(n_build / build_ms / 1e3, 1),
                      "insert_mkeys_s": round(n_ins / t_ins / 1e3, 1), "delete_mkeys_s": round(n_del / t_del / 1e3, 1),
                      "ordered_successor_mops_s": round(n_suc / t_ord / 1e3, 1),
                      "unsorted_successor_mops_s": round(n_suc / t_suc / 1e3, 1), "status": idx.status(),
-                     "resident_gb": round(idx.gpu_resident_bytes() / 1e9, 2)}
+                     "keys_after": idx.size(), "resident_gb": round(idx.gpu_resident_bytes() / 1e9, 2),
+                     "allocation_region": alloc,
+                     # per timed round, in order: G keys/s (or G probes/s) and region nodes used
+                     "per_round": {
+                         "insert_gkeys_s": [round(ni / t / 1e6, 2) for t in per["insert_ms"]],
+                         "delete_gkeys_s": [round(nd / t / 1e6, 2) for t in per["delete_ms"]],
+                         "ordered_successor_gops_s": [round(ns / t / 1e6, 1) for t in per["ordered_successor_ms"]],
+                         "region_used_nodes": per["region_used_nodes"]}}
         idx.close()
         torch.cuda.synchronize()
-    res["rounds_timed"] = args.flix_rounds
     res["learned_successor_speedup"] = round(res["learned"]["ordered_successor_mops_s"] /
                                              res["plain"]["ordered_successor_mops_s"], 3)
     res["learned_insert_speedup"] = round(res["learned"]["insert_mkeys_s"] / res["plain"]["insert_mkeys_s"], 3)

@@ -194,6 +194,8 @@ def load() -> C.CDLL:
         "gpulsm_flix_resident_bytes": (i32, [vp, C.POINTER(u64)]),
         "gpulsm_flix_size": (i32, [vp, C.POINTER(u64)]),
         "gpulsm_flix_status": (i32, [vp, C.POINTER(u32)]),
+        "gpulsm_flix_allocation_state": (i32, [vp, C.POINTER(u64), C.POINTER(u64), C.POINTER(u64),
+                                               C.POINTER(u32)]),
         "gpulsm_sort_pairs": (i32, [vp, vp, vp, vp, u64, u32, u32, u32, vp]),
         "gpulsm_sort_pairs_noalloc": (i32, [vp, vp, vp, vp, u64, u32, u32, u32, vp]),
         "gpulsm_sort_noalloc_scratch_bytes": (u64, []),

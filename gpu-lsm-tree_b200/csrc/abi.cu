@@ -401,6 +401,18 @@ int gpulsm_flix_size(gpulsm_flix *f, uint64_t *out_keys) {
   });
 }
 
+int gpulsm_flix_allocation_state(gpulsm_flix *f, uint64_t *out_used_nodes, uint64_t *out_region_nodes,
+                                 uint64_t *out_buckets, uint32_t *out_grows) {
+  return guarded([&] {
+    need(f, "index");
+    need(out_used_nodes, "out_used_nodes");
+    need(out_region_nodes, "out_region_nodes");
+    need(out_buckets, "out_buckets");
+    need(out_grows, "out_grows");
+    f->impl.allocation_state(out_used_nodes, out_region_nodes, out_buckets, out_grows);
+  });
+}
+
 int gpulsm_flix_status(gpulsm_flix *f, uint32_t *out_status) {
   return guarded([&] {
     need(f, "index");

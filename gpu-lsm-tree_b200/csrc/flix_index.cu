@@ -73,6 +73,7 @@ struct FlixIndex::Impl {
   virtual uint64_t resident_bytes() = 0;
   virtual uint64_t size() = 0;
   virtual uint32_t status() = 0;
+  virtual void allocation_state(uint64_t *used, uint64_t *total, uint64_t *buckets, uint32_t *grows) = 0;
 };
 
 template <typename K>
@@ -280,6 +281,18 @@ class FlixImpl final : public FlixIndex::Impl {
     return ctr_host_->status | status_bits_;
   }
 
+  // allocation region: nodes taken by splits, nodes it holds, head buckets,
+  // and how often it was grown (a rebuild into a larger region)
+  void allocation_state(uint64_t *used, uint64_t *total, uint64_t *buckets, uint32_t *grows) override {
+    GPULSM_CUDA(cudaEventSynchronize(op_done_));
+    GPULSM_CUDA(cudaMemcpy(ctr_host_, ctr_, sizeof(DevCounters), cudaMemcpyDeviceToHost));
+    const uint64_t top = std::min<uint64_t>(ctr_host_->alloc_top, capacity_);
+    *used = top > buckets_ ? top - buckets_ : 0;
+    *total = capacity_ > buckets_ ? capacity_ - buckets_ : 0;
+    *buckets = buckets_;
+    *grows = grows_;
+  }
+
  private:
   void begin(cudaStream_t s) { GPULSM_CUDA(cudaStreamWaitEvent(s, op_done_, 0)); }
   void end(cudaStream_t s) { GPULSM_CUDA(cudaEventRecord(op_done_, s)); }
@@ -422,6 +435,7 @@ class FlixImpl final : public FlixIndex::Impl {
   // least `need` more nodes (FliX's rebuild, plus growth).
   void grow(uint64_t need, cudaStream_t s) {
     min_region_ = std::max<uint64_t>({min_region_, 2ull * (capacity_ - buckets_), need + 1024});
+    ++grows_;
     rebuild(s);
   }
 
@@ -592,6 +606,7 @@ class FlixImpl final : public FlixIndex::Impl {
   uint32_t capacity_ = 0;
   uint32_t used_upper_ = 0;
   uint64_t min_region_ = 0;
+  uint32_t grows_ = 0;
   bool built_ = false;
   DevCounters *ctr_ = nullptr;
   char *model_ = nullptr;  // learned routing model over bmax (search_mode 1)
@@ -658,6 +673,10 @@ uint64_t FlixIndex::size() {
 uint32_t FlixIndex::status() {
   std::lock_guard<std::mutex> g(mu_);
   return impl_->status();
+}
+void FlixIndex::allocation_state(uint64_t *used, uint64_t *total, uint64_t *buckets, uint32_t *grows) {
+  std::lock_guard<std::mutex> g(mu_);
+  impl_->allocation_state(used, total, buckets, grows);
 }
 
 }  // namespace gpulsm

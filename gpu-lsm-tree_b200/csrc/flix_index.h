@@ -37,6 +37,7 @@ class FlixIndex {
   uint64_t resident_bytes();
   uint64_t size();
   uint32_t status();
+  void allocation_state(uint64_t *used, uint64_t *total, uint64_t *buckets, uint32_t *grows);
 
   struct Impl;
 

@@ -106,3 +106,13 @@ class FlixIndex:
         v = C.c_uint32()
         N.check(self._lib.gpulsm_flix_status(self._h, C.byref(v)))
         return int(v.value)
+
+    def allocation_state(self) -> dict:
+        """Allocation region: nodes taken by splits, nodes it holds, head
+        buckets, and how often it was grown (allocation_buffer_next_free /
+        allocation_buffer_total_nodes in the reference)."""
+        used, total, buckets, grows = C.c_uint64(), C.c_uint64(), C.c_uint64(), C.c_uint32()
+        N.check(self._lib.gpulsm_flix_allocation_state(self._h, C.byref(used), C.byref(total), C.byref(buckets),
+                                                       C.byref(grows)))
+        return {"used_nodes": int(used.value), "region_nodes": int(total.value), "buckets": int(buckets.value),
+                "grows": int(grows.value)}

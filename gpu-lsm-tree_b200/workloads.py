@@ -142,6 +142,9 @@ class FlixWorkload:
     build_keys: np.ndarray
     rounds: list  # (insert_keys, insert_values, delete_keys, successor_probes)
     span: tuple
+    # flix_fast only: which build keys the rounds deleted (the live set after
+    # the last round is build_keys[~build_deleted] plus every round's inserts)
+    build_deleted: np.ndarray | None = None
 
 
 def flix(scale: int = 0, rounds: int = 32, key_bits: int = 64) -> FlixWorkload:
@@ -185,13 +188,29 @@ def flix(scale: int = 0, rounds: int = 32, key_bits: int = 64) -> FlixWorkload:
     return w
 
 
+def _bitmap_set(bm: np.ndarray, sorted_unique: np.ndarray) -> None:
+    """Sets the bits of sorted unique keys in a byte bitmap (vectorised: the
+    bits of keys sharing a byte are OR-reduced first)."""
+    if not sorted_unique.size:
+        return
+    byte = sorted_unique >> np.uint64(3)
+    bit = (np.uint8(1) << (sorted_unique & np.uint64(7)).astype(np.uint8)).astype(np.uint8)
+    starts = np.flatnonzero(np.concatenate([[True], byte[1:] != byte[:-1]]))
+    bm[byte[starts]] |= np.bitwise_or.reduceat(bit, starts)
+
+
+def _bitmap_has(bm: np.ndarray, keys: np.ndarray) -> np.ndarray:
+    return ((bm[keys >> np.uint64(3)] >> (keys & np.uint64(7)).astype(np.uint8)) & np.uint8(1)).astype(bool)
+
+
 def flix_fast(scale: int = 0, rounds: int = 4, key_bits: int = 64) -> FlixWorkload:
     """The FliX configuration's shapes without re-sorting the whole live set
-    every round (for timing at full size): 2^28 sorted keys with geometric
-    gaps (mean 16), then per round 2^22 unique absent keys (half uniform over
-    the span, half in 1024 hot ranges), a 2^21-key delete batch drawn from the
-    initial keys not yet deleted (all live), and 2^24 uniform successor
-    probes (sizes / 2^scale)."""
+    every round (fast enough for all 32 rounds at full size): 2^28 sorted keys
+    with geometric gaps (mean 16), then per round 2^22 unique keys absent from
+    the index so far (half uniform over the span, half in 1024 hot ranges of
+    2^17 key units; presence is read from a bitmap of every key ever stored), a
+    2^21-key delete batch drawn from the build keys not yet deleted (all live),
+    and 2^24 uniform successor probes (sizes / 2^scale)."""
     rng = rng_for(3)
     n = 1 << (28 - scale)
     keys = np.cumsum(rng.geometric(1.0 / 16.0, n).astype(np.uint64), dtype=np.uint64) + np.uint64(1)
@@ -204,7 +223,8 @@ def flix_fast(scale: int = 0, rounds: int = 4, key_bits: int = 64) -> FlixWorklo
                      "2^24 successor probes", keys, [], (lo_span, hi_span))
     n_ins, n_del, n_succ = 1 << (22 - scale), 1 << (21 - scale), 1 << (24 - scale)
     hot_starts = rng.integers(lo_span, hi_span - (1 << 17), 1024, dtype=np.uint64)
-    inserted = np.empty(0, np.uint64)
+    bm = np.zeros((hi_span >> 3) + 2, np.uint8)  # every key ever stored (hot ranges end below hi_span)
+    _bitmap_set(bm, keys)
     deleted = np.zeros(n, bool)
     for _ in range(rounds):
         cand_u = rng.integers(lo_span, hi_span, n_ins, dtype=np.uint64)
@@ -216,15 +236,9 @@ def flix_fast(scale: int = 0, rounds: int = 4, key_bits: int = 64) -> FlixWorklo
         keep[0] = True
         np.not_equal(cand[1:], cand[:-1], out=keep[1:])
         cand = cand[keep & (cand >= 2) & (cand != 0xFFFFFFFF)]
-        p = np.searchsorted(keys, cand)
-        present = (p < n) & (keys[np.minimum(p, n - 1)] == cand)
-        if inserted.size:
-            q = np.searchsorted(inserted, cand)
-            present |= (q < inserted.size) & (inserted[np.minimum(q, inserted.size - 1)] == cand)
-        ins = cand[~present]
-        rng.shuffle(ins)
-        ins = ins[:n_ins]
-        inserted = np.sort(np.concatenate([inserted, ins]))
+        ins = cand[~_bitmap_has(bm, cand)]
+        ins = ins[rng.permutation(ins.size)[:n_ins]]
+        _bitmap_set(bm, np.sort(ins))
         ins_vals = rng.integers(0, 1 << 32, ins.size, dtype=np.uint64).astype(np.uint32)
         pick = rng.integers(0, n, 2 * n_del)
         pick.sort()
@@ -237,4 +251,5 @@ def flix_fast(scale: int = 0, rounds: int = 4, key_bits: int = 64) -> FlixWorklo
         dels = keys[pick]
         probes = rng.integers(lo_span, hi_span + 2, n_succ, dtype=np.uint64)
         w.rounds.append((ins, ins_vals, dels, probes))
+    w.build_deleted = deleted
     return w

@@ -176,6 +176,12 @@ int gpulsm_flix_rebuild(gpulsm_flix *index, void *stream);
 int gpulsm_flix_resident_bytes(gpulsm_flix *index, uint64_t *out_bytes);
 int gpulsm_flix_size(gpulsm_flix *index, uint64_t *out_keys);
 int gpulsm_flix_status(gpulsm_flix *index, uint32_t *out_status);
+/* allocation_buffer_next_free / allocation_buffer_total_nodes
+ * FliX/impl_cg_rtx_index_updates.cuh:1690-1700 (synchronises): allocation-region
+ * nodes taken by splits, nodes the region holds, head buckets, and how many
+ * times the region was grown by a rebuild before a batch that could exhaust it. */
+int gpulsm_flix_allocation_state(gpulsm_flix *index, uint64_t *out_used_nodes, uint64_t *out_region_nodes,
+                                 uint64_t *out_buckets, uint32_t *out_grows);
 
 /* ===================== multi-tenant batched dictionary ==================== */
 /* Many independent u32 dictionaries (GPULSMOpt upsert semantics, inserts and

@@ -136,3 +136,69 @@ def test_flix_workload_shape_small(gl, cuda, workloads, mode):
         t.f.successor(keys_t(probes, 64), sk, n)
         assert np.array_equal(host_keys(sk, 64, n), t.o.successor(probes))
     assert t.f.size() == len(t.o)
+
+
+@pytest.mark.slow
+def test_flix_configuration_at_size_after_32_rounds(gl, cuda, workloads):
+    """The updatable-index configuration at its stated size: bulk build of 2^28
+    sorted u64 keys (geometric gaps, mean 16), 32 rounds of 2^22 inserts (half
+    in 1024 hot ranges), 2^21 deletes and 2^24 unsorted successor probes.  Every
+    round: status clean and the key count exact.  After round 32: 2^20 uniform
+    probes, 2^18 sampled live keys and 2^16 deleted keys checked bit-exact for
+    successor and lookup against the std::map answers (the live set and its
+    values rebuilt from the generator's record), both through the unsorted
+    entry points (sorted inside) and the ordered ones."""
+    import torch
+
+    w = workloads.flix_fast(0, rounds=32)
+    n0 = w.build_keys.size
+    cap = n0 + sum(r[0].size for r in w.rounds)
+    f = gl.FlixIndex(key_bits=64, max_elements=cap)
+    f.build_bucket_layer_only(keys_t(w.build_keys, 64), n0, max_size=cap)
+    expect = n0
+    out = empty_keys(w.rounds[0][3].size, 64)
+    for r, (ins, vals, dels, probes) in enumerate(w.rounds):
+        f.insert(keys_t(ins, 64), to_dev(vals), ins.size)
+        f.remove(keys_t(dels, 64), dels.size)
+        f.successor(keys_t(probes, 64), out, probes.size)  # the round's probes (timed in bench.py)
+        expect += ins.size - dels.size
+        assert f.status() == 0, f"round {r}"
+        assert f.size() == expect, f"round {r}"
+    torch.cuda.synchronize()
+    # the exact live set after the last round, with values
+    live_b = ~w.build_deleted
+    bk = w.build_keys[live_b]
+    bv = np.flatnonzero(live_b).astype(np.uint32)  # build values are input positions
+    ik = np.concatenate([r[0] for r in w.rounds])
+    iv = np.concatenate([r[1] for r in w.rounds])
+    o = np.argsort(ik)
+    ik, iv = ik[o], iv[o]
+    pos = np.searchsorted(bk, ik)
+    live_k = np.insert(bk, pos, ik)
+    live_v = np.insert(bv, pos, iv)
+    assert live_k.size == expect
+    rng = np.random.default_rng(32)
+    lo, hi = w.span
+    dead = w.build_keys[w.build_deleted]
+    probes = np.concatenate([rng.integers(lo, hi + 2, 1 << 20, dtype=np.uint64),
+                             live_k[rng.integers(0, live_k.size, 1 << 18)],
+                             dead[rng.integers(0, dead.size, 1 << 16)]])
+    p = np.searchsorted(live_k, probes)
+    inb = p < live_k.size
+    exact_succ = np.where(inb, live_k[np.minimum(p, live_k.size - 1)], np.uint64(0xFFFFFFFF))
+    hit = inb & (live_k[np.minimum(p, live_k.size - 1)] == probes)
+    exact_val = np.where(hit, live_v[np.minimum(p, live_v.size - 1)], np.uint32(0xFFFFFFFF)).astype(np.uint32)
+    n = probes.size
+    sk, lv = empty_keys(n, 64), empty_u32(n)
+    f.successor(keys_t(probes, 64), sk, n)
+    f.lookup(keys_t(probes, 64), lv, n)
+    assert np.array_equal(host_keys(sk, 64, n), exact_succ)
+    assert np.array_equal(to_host(lv)[:n], exact_val)
+    sp = np.unique(probes)
+    q = np.searchsorted(live_k, sp)
+    qb = q < live_k.size
+    f.lookups_successor(keys_t(sp, 64), sk, sp.size)
+    assert np.array_equal(host_keys(sk, 64, sp.size),
+                          np.where(qb, live_k[np.minimum(q, live_k.size - 1)], np.uint64(0xFFFFFFFF)))
+    assert f.status() == 0
+    f.close()
