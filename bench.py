@@ -630,6 +630,13 @@ def serving_leg(args, gl, w, dev):
             "peak_mean_round_keys": round(peak["mean_round_keys"], 1),
             "peak_gpu_busy_frac": round(peak["gpu_busy_s"] / max(peak["wall_s"], 1e-9), 3),
             "peak_host_launch_frac": round(peak["host_launch_s"] / max(peak["wall_s"], 1e-9), 3),
+            # where a peak round's time goes: device time per request kind (the
+            # merges still running when a round ends are charged to insert),
+            # worker copy into pinned staging, result scatter
+            "peak_kind_gpu_frac": {k: round(v / max(peak["wall_s"], 1e-9), 3)
+                                   for k, v in zip(("lookup", "insert", "erase", "range"), peak["kind_gpu_s"])},
+            "peak_host_copy_frac": round(peak["host_copy_s"] / max(peak["wall_s"], 1e-9), 3),
+            "peak_host_scatter_frac": round(peak["host_scatter_s"] / max(peak["wall_s"], 1e-9), 3),
             "requests": int(half["completed"]), "rejected": int(half["rejected"] + peak["rejected"]),
         }
     return out

@@ -117,7 +117,19 @@ class ServeStats(C.Structure):
         ("gpu_busy_s", C.c_double),
         ("host_launch_s", C.c_double),
         ("graph_rounds", C.c_uint64),
+        ("kind_gpu_s", C.c_double * 4),
+        ("host_copy_s", C.c_double),
+        ("host_scatter_s", C.c_double),
     ]
+
+
+def stats_dict(s: ServeStats) -> dict:
+    """A ServeStats as a dict (array fields as lists)."""
+    out = {}
+    for k, _ in ServeStats._fields_:
+        v = getattr(s, k)
+        out[k] = list(v) if isinstance(v, C.Array) else v
+    return out
 
 
 class LoadSpec(C.Structure):
@@ -181,6 +193,7 @@ def load() -> C.CDLL:
         "gpulsm_dict_kernel_timing": (i32, [vp, i32]),
         "gpulsm_dict_kernel_timing_read": (i32, [vp, C.POINTER(u64), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
         "gpulsm_dict_size": (i32, [vp, C.POINTER(u64), C.POINTER(u32)]),
+        "gpulsm_dict_cleanup": (i32, [vp, vp, C.POINTER(u64)]),
         "gpulsm_flix_create": (i32, [C.POINTER(FlixConfig), pvp]),
         "gpulsm_flix_destroy": (i32, [vp]),
         "gpulsm_flix_build": (i32, [vp, vp, vp, u64, u64, vp]),

@@ -143,6 +143,9 @@ void copy_stats(const gpulsm::ServeStats &s, gpulsm_serve_stats *o) {
   o->gpu_busy_s = s.gpu_busy_s;
   o->host_launch_s = s.host_launch_s;
   o->graph_rounds = s.graph_rounds;
+  for (int k = 0; k < 4; ++k) o->kind_gpu_s[k] = s.kind_gpu_s[k];
+  o->host_copy_s = s.host_copy_s;
+  o->host_scatter_s = s.host_scatter_s;
 }
 }  // namespace
 
@@ -287,6 +290,14 @@ int gpulsm_dict_kernel_timing_read(gpulsm_dict *d, uint64_t *out_launches, doubl
   return guarded([&] {
     need(d, "dict");
     d->impl.kernel_timing(out_launches, out_ms, out_bytes);
+  });
+}
+
+int gpulsm_dict_cleanup(gpulsm_dict *d, void *stream, uint64_t *out_live_keys) {
+  return guarded([&] {
+    need(d, "dict");
+    const uint64_t n = d->impl.cleanup(S(stream));
+    if (out_live_keys) *out_live_keys = n;
   });
 }
 

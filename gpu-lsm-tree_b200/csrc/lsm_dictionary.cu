@@ -1114,6 +1114,22 @@ uint64_t LsmDictionary::resident_bytes() {
   return pool_.bytes() + words_cap_ * 16 + scratch_bytes_ + ascratch_bytes_ + live_bytes_ + sizeof(Receipt) + 256;
 }
 
+uint64_t LsmDictionary::cleanup(cudaStream_t s) {
+  std::lock_guard<std::mutex> g(mu_);
+  apply_receipt(false);
+  reject_if_failed();
+  begin_op(s);
+  compact_all(s);
+  unsigned long long n = 0;
+  for (auto &l : levels_)
+    if (l.run) GPULSM_CUDA(cudaMemcpyAsync(&n, &l.run->desc->n, 8, cudaMemcpyDeviceToHost, s));
+  GPULSM_CUDA(cudaStreamSynchronize(s));
+  for (auto &l : levels_)
+    if (l.run) l.upper = n;  // the exact count of the one remaining level
+  end_op(s);
+  return n;
+}
+
 void LsmDictionary::size(uint64_t *rows, uint32_t *levels) {
   std::lock_guard<std::mutex> g(mu_);
   host_sync();

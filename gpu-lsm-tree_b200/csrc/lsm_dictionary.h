@@ -119,6 +119,10 @@ class LsmDictionary {
   void set_kernel_timing(bool on);
   void kernel_timing(uint64_t *launches, double *total_ms, double *bytes);
   void size(uint64_t *rows, uint32_t *levels);
+  // LSMu's explicit cleanup (FliX/impl_lsm_tree.cuh:1256-1400): every level
+  // merged into one run of the newest live versions, tombstones and shadowed
+  // versions dropped; returns the live key count (synchronises).
+  uint64_t cleanup(cudaStream_t s);
 
   // Introspection for tests and benchmarks.
   uint32_t level_count() const { return uint32_t(caps_.size()); }

@@ -665,26 +665,64 @@ __device__ __forceinline__ bool row_is_tomb(const LevelView &L, uint64_t p, uint
 }
 
 // ---------------------------------------------------------------------------
+// L2 eviction priorities for random point reads: a level's radix directory
+// (4 B per ~8 rows, 32 MB for 2^26 rows) is read by every lookup that reaches
+// the level, so its lines are kept (evict_last); the key and value sectors a
+// lookup touches are read once and go first (evict_first), so that they do
+// not push the directory out of the 126 MB L2.
+__device__ __forceinline__ uint64_t l2_keep_policy() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t l2_stream_policy() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint32_t ld_hint(const uint32_t *a, uint64_t policy) {
+  uint32_t v;
+  asm volatile("ld.global.nc.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(policy));
+  return v;
+}
+
+// bucket_lower_bound with every key read under an L2 policy
+__device__ __forceinline__ uint32_t bucket_lower_bound_hint(const uint32_t *keys, uint32_t s, uint32_t e,
+                                                            uint32_t key, uint64_t policy) {
+  while (e - s > 8) {
+    const uint32_t mid = s + ((e - s) >> 1);
+    if (ld_hint(keys + mid, policy) < key) s = mid + 1;
+    else e = mid;
+  }
+  while (s < e && ld_hint(keys + s, policy) < key) ++s;
+  return s;
+}
+
 // Point lookup: newest level first; miss value follows GPULSMOpt.cuh:4742-4749.
 __device__ __forceinline__ void lookup_one(const LevelSet &set, uint64_t i, const uint32_t *__restrict__ queries,
                                            uint32_t *__restrict__ out_values, uint8_t *__restrict__ out_found) {
   const uint32_t q = queries[i];
   const uint32_t miss = out_found ? 0u : kNotFound;
+  const uint64_t keep = l2_keep_policy(), stream = l2_stream_policy();
   for (uint32_t l = 0; l < set.count; ++l) {
     const LevelView &L = set.lv[l];
     const LevelDesc d = load_desc(L.desc);
     if (q < d.kmin || q > d.kmax) continue;
     uint64_t p, e;
+    uint32_t kp = 0;
     if (L.dir && !L.ms) {  // radix directory: the bucket's rows only
       const uint32_t b = (q - d.kmin) >> d.shift;
-      e = L.dir[b + 1];
-      p = bucket_lower_bound(L.keys, L.dir[b], uint32_t(e), q);
+      const uint32_t s = ld_hint(L.dir + b, keep);
+      e = ld_hint(L.dir + b + 1, keep);
+      p = bucket_lower_bound_hint(L.keys, s, uint32_t(e), q, stream);
+      if (p < e) kp = ld_hint(L.keys + p, stream);
     } else {  // learned model window or binary search
       p = level_lower_bound(L, d, q);
       e = d.n;
+      if (p < e) kp = L.keys[p];
     }
-    if (p < e && L.keys[p] == q) {
-      const uint32_t v = L.vals[p];
+    if (p < e && kp == q) {
+      const uint32_t v = ld_hint(L.vals + p, stream);
       const bool live = !row_is_tomb(L, p, v);
       out_values[i] = live ? v : miss;
       if (out_found) out_found[i] = live;

@@ -94,6 +94,7 @@ Server::~Server() {
     cudaEventDestroy(s.computed);
     cudaEventDestroy(s.downloaded);
     for (auto &g : s.graphs) cudaGraphExecDestroy(g.second);
+    for (cudaEvent_t e : s.marks) cudaEventDestroy(e);
   }
   cudaStreamDestroy(capture_);
   cudaStreamDestroy(compute_);
@@ -151,6 +152,8 @@ void Server::reset_stats() {
   st_completed_ = st_rejected_ = st_rounds_ = st_keys_ = st_round_keys_ = st_graph_rounds_ = 0;
   st_first_ = -1;
   st_last_ = st_gpu_s_ = st_launch_s_ = 0;
+  for (double &k : st_kind_gpu_s_) k = 0;
+  st_copy_s_ = st_scatter_s_ = 0;
 }
 
 ServeStats Server::stats() {
@@ -168,6 +171,9 @@ ServeStats Server::stats() {
     s.gpu_busy_s = st_gpu_s_;
     s.host_launch_s = st_launch_s_;
     s.graph_rounds = st_graph_rounds_;
+    for (int k = 0; k < 4; ++k) s.kind_gpu_s[k] = st_kind_gpu_s_[k];
+    s.host_copy_s = st_copy_s_;
+    s.host_scatter_s = st_scatter_s_;
   }
   if (!lat.empty()) {
     auto pct = [&](double p) {
@@ -279,13 +285,30 @@ cudaGraphExec_t Server::lookup_graph(Slot &slot, uint32_t size_class) {
   return exec;
 }
 
+// The next free pair of timing events of a slot (created on first use).
+static uint32_t next_mark_pair(std::vector<cudaEvent_t> &marks, size_t used) {
+  while (marks.size() < used + 2) {
+    cudaEvent_t e;
+    GPULSM_CUDA(cudaEventCreate(&e));
+    marks.push_back(e);
+  }
+  return uint32_t(used);
+}
+
 void Server::launch_round(Slot &slot) {
+  const double c0 = now_s();
   for (const Run &r : slot.runs)
     for (uint64_t i = 0; i < r.parts; ++i) {
       const Part &p = slot.parts[r.first_part + i];
       std::memcpy(slot.h_in + r.in_off + p.off, p.keys, p.n * 4);
       if (has_aux(r.kind)) std::memcpy(slot.h_in + r.in_off + r.n + p.off, p.aux, p.n * 4);
     }
+  const double c1 = now_s();
+  slot.timed.clear();
+  {
+    std::lock_guard<std::mutex> g(mu_);
+    st_copy_s_ += c1 - c0;
+  }
   if (slot.runs.size() == 1 && slot.runs[0].kind == kServeLookup) {
     // lookup-only round: one graph launch (size classes are powers of two
     // from 1024 keys, the last one the round limit)
@@ -310,6 +333,8 @@ void Server::launch_round(Slot &slot) {
   GPULSM_CUDA(cudaStreamWaitEvent(compute_, slot.uploaded, 0));
   for (Run &r : slot.runs) {
     const uint32_t *in = slot.d_in + r.in_off;
+    const uint32_t m = next_mark_pair(slot.marks, slot.timed.size() * 2);
+    GPULSM_CUDA(cudaEventRecord(slot.marks[m], compute_));
     try {
       switch (r.kind) {
         case kServeLookup:
@@ -328,11 +353,19 @@ void Server::launch_round(Slot &slot) {
     } catch (const std::exception &e) {
       r.status = status_of(e);
     }
+    GPULSM_CUDA(cudaEventRecord(slot.marks[m + 1], compute_));
+    slot.timed.emplace_back(r.kind, m);
   }
   // an update request completes when its merges have completed
   bool updates = false;
   for (const Run &r : slot.runs) updates = updates || is_update(r.kind);
-  if (updates) dict_.join(compute_);
+  if (updates) {
+    const uint32_t m = next_mark_pair(slot.marks, slot.timed.size() * 2);
+    GPULSM_CUDA(cudaEventRecord(slot.marks[m], compute_));
+    dict_.join(compute_);
+    GPULSM_CUDA(cudaEventRecord(slot.marks[m + 1], compute_));
+    slot.timed.emplace_back(kServeInsert, m);  // the merges still running: charged to updates
+  }
   GPULSM_CUDA(cudaEventRecord(slot.computed, compute_));
   GPULSM_CUDA(cudaStreamWaitEvent(download_, slot.computed, 0));
   if (slot.out_words) {
@@ -400,6 +433,16 @@ void Server::completer() {
       (void)cudaGetLastError();
       gpu_ms = 0.f;
     }
+    double kind_s[4] = {0, 0, 0, 0};
+    if (slot.launched && !fail)
+      for (const auto &t : slot.timed) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, slot.marks[t.second], slot.marks[t.second + 1]) == cudaSuccess)
+          kind_s[t.first & 3u] += double(ms) * 1e-3;
+        else
+          (void)cudaGetLastError();
+      }
+    const double s0 = now_s();
     if (!fail)
       for (const Run &r : slot.runs) {
         if (r.status || !has_out(r.kind)) continue;
@@ -409,7 +452,10 @@ void Server::completer() {
           if (r.kind == kServeLookup && p.found) std::memcpy(p.found, slot.h_found + r.out_off + p.off, p.n);
         }
       }
+    const double s1 = now_s();
     lk.lock();
+    for (int k = 0; k < 4; ++k) st_kind_gpu_s_[k] += kind_s[k];
+    st_scatter_s_ += s1 - s0;
     inflight_.pop_front();
     inflight_bytes_ -= slot.bytes;
     for (const Run &r : slot.runs)

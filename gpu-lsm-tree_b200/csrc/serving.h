@@ -48,6 +48,9 @@ struct ServeStats {
   double gpu_busy_s = 0;      // device time of the rounds (upload done -> kernels done)
   double host_launch_s = 0;   // worker time staging and launching rounds
   uint64_t graph_rounds = 0;  // lookup-only rounds replayed from a captured CUDA graph
+  double kind_gpu_s[4] = {0, 0, 0, 0};  // device time per request kind (updates: merges included)
+  double host_copy_s = 0;     // worker time copying request data into pinned staging
+  double host_scatter_s = 0;  // completion time copying results into the requests' buffers
 };
 
 // Open-loop load: Poisson arrivals, kind mix, log-uniform sizes, Zipf keys.
@@ -127,6 +130,10 @@ class Server {
     // lookup-only rounds replay a CUDA graph per size class (copy in, lookup
     // against the device level table, copy out) captured on first use
     std::vector<std::pair<uint32_t, cudaGraphExec_t>> graphs;
+    // device time per run: events bracketing each timed call on the compute
+    // stream (the stream is serial, so a pair spans that call's work alone)
+    std::vector<cudaEvent_t> marks;
+    std::vector<std::pair<uint32_t, uint32_t>> timed;  // (kind, index of the first event of the pair)
   };
 
   void worker();
@@ -160,6 +167,7 @@ class Server {
   std::vector<float> lat_us_;
   uint64_t st_completed_ = 0, st_rejected_ = 0, st_rounds_ = 0, st_keys_ = 0, st_round_keys_ = 0;
   double st_first_ = -1, st_last_ = 0, st_gpu_s_ = 0, st_launch_s_ = 0;
+  double st_kind_gpu_s_[4] = {0, 0, 0, 0}, st_copy_s_ = 0, st_scatter_s_ = 0;
 
   std::thread worker_, completer_;
 };

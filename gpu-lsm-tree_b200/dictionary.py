@@ -168,6 +168,13 @@ class GPULSMOpt:
         N.check(self._lib.gpulsm_dict_kernel_timing_read(self._h, C.byref(n), C.byref(ms), C.byref(b)))
         return {"launches": int(n.value), "ms": float(ms.value), "bytes": float(b.value)}
 
+    def cleanup(self, stream=None) -> int:
+        """LSMu's explicit cleanup (FliX/impl_lsm_tree.cuh:1256-1400): one level of
+        the newest live versions; returns the live key count."""
+        v = C.c_uint64()
+        N.check(self._lib.gpulsm_dict_cleanup(self._h, _stream(stream), C.byref(v)))
+        return int(v.value)
+
     def size(self) -> tuple[int, int]:
         rows, levels = C.c_uint64(), C.c_uint32()
         N.check(self._lib.gpulsm_dict_size(self._h, C.byref(rows), C.byref(levels)))

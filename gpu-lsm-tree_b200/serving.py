@@ -125,7 +125,7 @@ class Server:
     def stats(self) -> dict:
         s = N.ServeStats()
         N.check(self._lib.gpulsm_server_stats(self._h, C.byref(s)))
-        return {k: getattr(s, k) for k, _ in N.ServeStats._fields_}
+        return N.stats_dict(s)
 
     def reset_stats(self):
         N.check(self._lib.gpulsm_server_reset_stats(self._h))
@@ -145,4 +145,4 @@ class Server:
                           max_keys, range_width_max, seed, u.ctypes.data, u.size)
         s = N.ServeStats()
         N.check(self._lib.gpulsm_server_run_load(self._h, C.byref(spec), C.byref(s)))
-        return {k: getattr(s, k) for k, _ in N.ServeStats._fields_}
+        return N.stats_dict(s)

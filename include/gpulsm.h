@@ -122,6 +122,13 @@ int gpulsm_dict_successor(gpulsm_dict *dict, const uint32_t *queries, uint64_t c
 int gpulsm_dict_status(gpulsm_dict *dict, uint32_t *out_status);
 /* GPULSMOpt::gpu_resident_bytes  GPULSMOpt.cuh:6341 */
 int gpulsm_dict_resident_bytes(gpulsm_dict *dict, uint64_t *out_bytes);
+/* LSMu cleanup  FliX/impl_lsm_tree.cuh:1256-1400 (no GPULSMOpt counterpart):
+ * merges every level into one run that keeps only the newest live version of
+ * each key (tombstones and shadowed versions dropped, as
+ * lsm_mark_cleanup_survivors_kernel :485-500 keeps the first regular entry of
+ * each key segment) and returns the live key count; synchronises.  Answers are
+ * unchanged; later reads search one level. */
+int gpulsm_dict_cleanup(gpulsm_dict *dict, void *stream, uint64_t *out_live_keys);
 /* Number of live rows (synchronises; diagnostics). */
 int gpulsm_dict_size(gpulsm_dict *dict, uint64_t *out_rows, uint32_t *out_levels);
 /* Measurement hook (no reference counterpart): while enabled, every merge
@@ -239,6 +246,9 @@ typedef struct gpulsm_serve_stats {
   double mean_round_keys, wall_s;
   double gpu_busy_s, host_launch_s; /* device time of the rounds; worker time staging + launching */
   uint64_t graph_rounds;            /* lookup-only rounds replayed from a captured CUDA graph */
+  double kind_gpu_s[4];             /* device time of each request kind's calls (updates: merges included) */
+  double host_copy_s;               /* worker time copying request data into pinned staging */
+  double host_scatter_s;            /* completion time copying results into the requests' buffers */
 } gpulsm_serve_stats;
 
 /* Open-loop load: Poisson arrivals at rate_per_s (0 = closed loop with

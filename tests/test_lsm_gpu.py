@@ -485,3 +485,51 @@ def test_updates_runner_writes_reference_result_file(gl, cuda, tmp_path, index, 
                                                 "before_update_bytes", "after_update_bytes"}
     sizes = {int(r["step"]): (int(r["before_update_size"]), int(r["after_update_size"])) for r in body}
     assert sizes[0] == (1 << 16, 1 << 16) and sizes[2][1] == 1 << 17 and sizes[4][1] == 1 << 16
+
+
+def test_cleanup_keeps_answers_and_leaves_one_level(gl, cuda):
+    """LSMu's cleanup (FliX/impl_lsm_tree.cuh:1256-1400): after inserts, upserts
+    and erases spread over several levels, cleanup returns the live key count,
+    leaves one level, and every lookup, range sum, range count and successor
+    answer stays the oracle's; updates after it land as usual."""
+    import torch
+
+    rng = np.random.default_rng(77)
+    d = gl.GPULSMOpt(gl.DictionaryConfig(max_elements=1 << 18, batch_capacity=4096))
+    o = OracleLSM()
+    universe = rng.integers(0, 1 << 32, 40000, dtype=np.uint64).astype(np.uint32)
+    for step in range(30):
+        k = universe[rng.integers(0, universe.size, 3000)]
+        if step % 3 == 2:
+            d.erase(to_dev(k))
+            o.erase(k)
+        else:
+            v = rng.integers(0, 1 << 32, k.size, dtype=np.uint64).astype(np.uint32)
+            d.insert(to_dev(k), to_dev(v))
+            o.insert(k, v)
+    assert d.size()[1] > 1
+    assert d.cleanup() == len(o)
+    rows, levels = d.size()
+    assert (rows, levels) == (len(o), 1)
+    q = np.concatenate([universe[:8000], rng.integers(0, 1 << 32, 2000, dtype=np.uint64).astype(np.uint32)])
+    out = empty_u32(q.size)
+    d.lookup(to_dev(q), out)
+    assert np.array_equal(to_host(out)[: q.size], o.lookup(q))
+    lo = q[:1000]
+    hi = (lo.astype(np.uint64) + (1 << 26)).clip(0, 0xFFFFFFFF).astype(np.uint32)
+    s = empty_u32(lo.size)
+    d.range(to_dev(lo), to_dev(hi), s)
+    assert np.array_equal(to_host(s)[: lo.size], o.range_sum(lo, hi))
+    c = empty_u32(lo.size)
+    d.range_count(to_dev(lo), to_dev(hi), c)
+    assert np.array_equal(to_host(c)[: lo.size], o.range_count(lo, hi))
+    d.successor(to_dev(q), out)
+    assert np.array_equal(to_host(out)[: q.size], o.successor(q))
+    k = universe[:5000]
+    v = np.arange(k.size, dtype=np.uint32)
+    d.insert(to_dev(k), to_dev(v))
+    o.insert(k, v)
+    d.lookup(to_dev(q), out)
+    torch.cuda.synchronize()
+    assert np.array_equal(to_host(out)[: q.size], o.lookup(q))
+    assert d.cleanup() == len(o)
