@@ -52,26 +52,34 @@ def test_flix_adapter_runs_over_the_c_abi(gl, cuda):
     ok(lib.adapter_create(C.byref(h)))
     kd = to_dev(keys)
     ok(lib.adapter_build(h, kd.data_ptr(), keys.size, 4 * n))
+    torch.cuda.synchronize()
     for step in range(3):  # inserts (updates and new keys), then a remove batch
         k = np.concatenate([keys[rng.integers(0, keys.size, 3000)],
                             rng.integers(0, 1 << 31, 3000, dtype=np.uint64).astype(np.uint32)])
         v = rng.integers(0, 1 << 32, k.size, dtype=np.uint64).astype(np.uint32)
-        ok(lib.adapter_insert(h, to_dev(k).data_ptr(), to_dev(v).data_ptr(), k.size, None))
+        # device copies held by name for the duration of each call (a temporary
+        # freed inside the argument list could be reused by the next copy)
+        kd_, vd_ = to_dev(k), to_dev(v)
+        ok(lib.adapter_insert(h, kd_.data_ptr(), vd_.data_ptr(), k.size, None))
         o.insert(k, v)
         e = keys[rng.integers(0, keys.size, 2000)]
-        ok(lib.adapter_remove(h, to_dev(e).data_ptr(), e.size, None))
+        ed = to_dev(e)
+        ok(lib.adapter_remove(h, ed.data_ptr(), e.size, None))
         o.erase(e)
+    torch.cuda.synchronize()
     q = np.concatenate([keys[:5000], rng.integers(0, 1 << 32, 3000, dtype=np.uint64).astype(np.uint32)])
+    qd = to_dev(q)
     out = empty_u32(q.size)
-    ok(lib.adapter_lookup(h, to_dev(q).data_ptr(), out.data_ptr(), q.size, None))
+    ok(lib.adapter_lookup(h, qd.data_ptr(), out.data_ptr(), q.size, None))
     torch.cuda.synchronize()
     assert np.array_equal(to_host(out)[: q.size], o.lookup(q))
     lo = q[:2000]
     hi = (lo.astype(np.uint64) + rng.integers(0, 1 << 24, lo.size, dtype=np.uint64)).clip(0, 0xFFFFFFFF).astype(np.uint32)
+    lod, hid = to_dev(lo), to_dev(hi)
     sums = empty_u32(lo.size)
-    ok(lib.adapter_range_lookup_sum(h, to_dev(lo).data_ptr(), to_dev(hi).data_ptr(), sums.data_ptr(), lo.size, None))
+    ok(lib.adapter_range_lookup_sum(h, lod.data_ptr(), hid.data_ptr(), sums.data_ptr(), lo.size, None))
     succ = empty_u32(q.size)
-    ok(lib.adapter_lookups_successor(h, to_dev(q).data_ptr(), succ.data_ptr(), q.size, None))
+    ok(lib.adapter_lookups_successor(h, qd.data_ptr(), succ.data_ptr(), q.size, None))
     torch.cuda.synchronize()
     assert np.array_equal(to_host(sums)[: lo.size], o.range_sum(lo, hi))
     assert np.array_equal(to_host(succ)[: q.size], o.successor(q))

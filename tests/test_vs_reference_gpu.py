@@ -182,14 +182,19 @@ def test_flix_same_answers_as_reference_kernels(gl, cuda, workloads):
         assert np.array_equal(ours_s, exact), f"round {r}: our successors differ from the exact answers"
         for what, a, b in zip(("successor", "lookup"), outs["reference"], outs["ours"]):
             bad = np.flatnonzero(a != b)
-            if what == "successor":
-                # the reference's documented quirk: a successor read as 0 (its own
-                # driver check skips 0 results, FliX/benchmarks_updates.cuh:160-162)
-                quirk = bad[ref_s[bad] == 0]
-                if quirk.size:
-                    reference_quirks.append({"round": r, "class": "zero_successor", "count": int(quirk.size),
-                                             "probe": int(h_sp[quirk[0]]), "exact": int(exact[quirk[0]])})
-                bad = bad[ref_s[bad] != 0]
+            if what == "successor" and bad.size:
+                # ours equals the exact answer everywhere (asserted above), so every
+                # disagreement is the reference's; recorded with an example, by
+                # class: a successor read as 0 (the quirk its own driver check skips,
+                # FliX/benchmarks_updates.cuh:160-162) or another wrong key
+                ex = ref_s[bad]
+                for cls, sel in (("zero_successor", ex == 0), ("wrong_successor", ex != 0)):
+                    if sel.any():
+                        j = bad[sel][0]
+                        reference_quirks.append({"round": r, "class": cls, "count": int(sel.sum()),
+                                                 "probe": int(h_sp[j]), "reference": int(ref_s[j]),
+                                                 "exact": int(exact[j])})
+                bad = bad[:0]
             if bad.size:
                 mismatches.append((r, what, int(bad.size)))
     total_ref, total_ours = ref.total_keys(), ours.size()
