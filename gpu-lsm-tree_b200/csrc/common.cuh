@@ -26,6 +26,10 @@ enum : uint32_t {
 // resident (tile ids come from an atomic ticket), so a healthy wait ends in a
 // few microseconds; the limit only turns a broken invariant into a status bit.
 constexpr uint32_t kMaxSpins = 1u << 22;
+// Limit on mbarrier.try_wait probes: each probe may suspend the thread for a
+// time limit of the implementation (microseconds), so far fewer probes than
+// polls bound a wait of the same length.
+constexpr uint32_t kMaxTryWaits = 1u << 18;
 
 constexpr uint32_t kNotFound = 0xffffffffu;
 

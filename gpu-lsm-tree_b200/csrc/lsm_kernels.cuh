@@ -373,14 +373,27 @@ __device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
+// One potentially blocking probe of the phase: the thread is suspended in
+// hardware until the phase completes or a time limit of the implementation
+// passes (no polling instructions are issued meanwhile).
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
 // Bounded wait for the input copies; false (and the status bit) on timeout.
+// The probes suspend the waiting warps, so the CTAs that share the SM keep
+// its issue slots while the copies are in flight.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t *status) {
-  for (uint32_t spins = 0; !mbar_test(bar, 0); ++spins) {
-    if (spins > kMaxSpins) {
+  for (uint32_t tries = 0; !mbar_try(bar, 0); ++tries) {
+    if (tries > kMaxTryWaits) {
       atomicOr(status, kDevWaitTimeout);
       return false;
     }
-    __nanosleep(20);
   }
   return true;
 }
@@ -665,19 +678,14 @@ __device__ __forceinline__ bool row_is_tomb(const LevelView &L, uint64_t p, uint
 }
 
 // ---------------------------------------------------------------------------
-// L2 eviction priorities for random point reads: a level's radix directory
-// (4 B per ~8 rows, 32 MB for 2^26 rows) is read by every lookup that reaches
-// the level, so its lines are kept (evict_last); the key and value sectors a
-// lookup touches are read once and go first (evict_first), so that they do
-// not push the directory out of the 126 MB L2.
+// L2 eviction priority for point reads: a level's radix directory (4 B per
+// ~8 rows, 32 MB for 2^26 rows) is read by every lookup that reaches the
+// level, so its lines are kept (evict_last).  (Marking the key and value
+// sectors evict_first as well was measured: it also evicts the sectors of
+// Zipf-popular keys and raised DRAM reads from 147 to 186 B per lookup.)
 __device__ __forceinline__ uint64_t l2_keep_policy() {
   uint64_t p;
   asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
-  return p;
-}
-__device__ __forceinline__ uint64_t l2_stream_policy() {
-  uint64_t p;
-  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
   return p;
 }
 __device__ __forceinline__ uint32_t ld_hint(const uint32_t *a, uint64_t policy) {
@@ -686,24 +694,12 @@ __device__ __forceinline__ uint32_t ld_hint(const uint32_t *a, uint64_t policy) 
   return v;
 }
 
-// bucket_lower_bound with every key read under an L2 policy
-__device__ __forceinline__ uint32_t bucket_lower_bound_hint(const uint32_t *keys, uint32_t s, uint32_t e,
-                                                            uint32_t key, uint64_t policy) {
-  while (e - s > 8) {
-    const uint32_t mid = s + ((e - s) >> 1);
-    if (ld_hint(keys + mid, policy) < key) s = mid + 1;
-    else e = mid;
-  }
-  while (s < e && ld_hint(keys + s, policy) < key) ++s;
-  return s;
-}
-
 // Point lookup: newest level first; miss value follows GPULSMOpt.cuh:4742-4749.
 __device__ __forceinline__ void lookup_one(const LevelSet &set, uint64_t i, const uint32_t *__restrict__ queries,
                                            uint32_t *__restrict__ out_values, uint8_t *__restrict__ out_found) {
   const uint32_t q = queries[i];
   const uint32_t miss = out_found ? 0u : kNotFound;
-  const uint64_t keep = l2_keep_policy(), stream = l2_stream_policy();
+  const uint64_t keep = l2_keep_policy();
   for (uint32_t l = 0; l < set.count; ++l) {
     const LevelView &L = set.lv[l];
     const LevelDesc d = load_desc(L.desc);
@@ -714,15 +710,14 @@ __device__ __forceinline__ void lookup_one(const LevelSet &set, uint64_t i, cons
       const uint32_t b = (q - d.kmin) >> d.shift;
       const uint32_t s = ld_hint(L.dir + b, keep);
       e = ld_hint(L.dir + b + 1, keep);
-      p = bucket_lower_bound_hint(L.keys, s, uint32_t(e), q, stream);
-      if (p < e) kp = ld_hint(L.keys + p, stream);
+      p = bucket_lower_bound(L.keys, s, uint32_t(e), q);
     } else {  // learned model window or binary search
       p = level_lower_bound(L, d, q);
       e = d.n;
-      if (p < e) kp = L.keys[p];
     }
+    if (p < e) kp = L.keys[p];
     if (p < e && kp == q) {
-      const uint32_t v = ld_hint(L.vals + p, stream);
+      const uint32_t v = L.vals[p];
       const bool live = !row_is_tomb(L, p, v);
       out_values[i] = live ? v : miss;
       if (out_found) out_found[i] = live;
