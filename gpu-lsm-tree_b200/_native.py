@@ -120,6 +120,8 @@ class ServeStats(C.Structure):
         ("kind_gpu_s", C.c_double * 4),
         ("host_copy_s", C.c_double),
         ("host_scatter_s", C.c_double),
+        ("graph_updates", C.c_uint64),
+        ("stage_flushes", C.c_uint64),
     ]
 
 

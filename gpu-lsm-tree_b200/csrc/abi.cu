@@ -146,6 +146,8 @@ void copy_stats(const gpulsm::ServeStats &s, gpulsm_serve_stats *o) {
   for (int k = 0; k < 4; ++k) o->kind_gpu_s[k] = s.kind_gpu_s[k];
   o->host_copy_s = s.host_copy_s;
   o->host_scatter_s = s.host_scatter_s;
+  o->graph_updates = s.graph_updates;
+  o->stage_flushes = s.stage_flushes;
 }
 }  // namespace
 

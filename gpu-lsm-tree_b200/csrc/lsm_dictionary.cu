@@ -248,6 +248,10 @@ LsmDictionary::~LsmDictionary() {
   if (width_) cudaFree(width_);
   if (width_host_) cudaFreeHost(width_host_);
   if (ascratch_) cudaFree(ascratch_);
+  if (stage_in_) cudaFree(stage_in_);
+  for (auto &w : stage_words_)
+    if (w) cudaFree(w);
+  if (stage_scratch_) cudaFree(stage_scratch_);
   if (op_done_) cudaEventDestroy(op_done_);
   if (adm_done_) cudaEventDestroy(adm_done_);
   if (merge_done_) cudaEventDestroy(merge_done_);
@@ -463,16 +467,31 @@ RunBuffer *LsmDictionary::sort_dedup(const uint32_t *keys, const uint32_t *value
 // Batches up to 2^20 rows: a stable partition by the key's top byte
 // (histogram, scan, scatter - no look-back chain), then one CTA per top-byte
 // bucket sorts, deduplicates and writes the level rows (lsm_admit.cuh).
+size_t LsmDictionary::bucket_admit_scratch_bytes(uint64_t n) {
+  namespace ad = lsm::admit;
+  const uint32_t tiles = ad::part_tiles(n);
+  const size_t zero_bytes = align_up(8) + align_up((ad::kBuckets + 1) * 8);
+  return zero_bytes + 2 * align_up(size_t(tiles) * 256 * 4) + align_up(256 * 4);
+}
+
 RunBuffer *LsmDictionary::bucket_admit(const uint32_t *keys, const uint32_t *values, uint64_t n,
                                        bool tombstone, cudaStream_t s) {
+  void *scratch = admit_scratch(bucket_admit_scratch_bytes(n), s);
+  // before the chain: a fresh buffer is a stream-ordered allocation
+  RunBuffer *carry = pool_.acquire(n, s, true);
+  bucket_admit_into(keys, values, n, tombstone, s, carry, words_[0], words_[1], scratch);
+  return carry;
+}
+
+// The four admission launches into `carry`, with the given sort words and scratch.
+void LsmDictionary::bucket_admit_into(const uint32_t *keys, const uint32_t *values, uint64_t n, bool tombstone,
+                                      cudaStream_t s, RunBuffer *carry, unsigned long long *w0,
+                                      unsigned long long *w1, void *scratch) {
   namespace ad = lsm::admit;
   const uint32_t nn = uint32_t(n);
   const uint32_t tiles = ad::part_tiles(n);
   const size_t zero_bytes = align_up(8) + align_up((ad::kBuckets + 1) * 8);
-  const size_t total = zero_bytes + 2 * align_up(size_t(tiles) * 256 * 4) + align_up(256 * 4);
-  Bump bump{static_cast<char *>(admit_scratch(total, s))};
-  // before the chain: a fresh buffer is a stream-ordered allocation
-  RunBuffer *carry = pool_.acquire(n, s, true);
+  Bump bump{static_cast<char *>(scratch)};
   unsigned long long *zero = reinterpret_cast<unsigned long long *>(bump.p);  // zeroed by part_hist_kernel
   uint32_t *counter = bump.take<uint32_t>(2);
   unsigned long long *lb = bump.take<unsigned long long>(ad::kBuckets + 1);
@@ -483,15 +502,15 @@ RunBuffer *LsmDictionary::bucket_admit(const uint32_t *keys, const uint32_t *val
                  uint32_t(zero_bytes / 8));
   launch_chained(ad::part_scan_kernel, 256, ad::kPartThreads, 0, s, cnt, tiles, prefix, top);
   launch_chained(ad::part_scatter_kernel, tiles, ad::kPartThreads, 0, s, keys, tombstone ? nullptr : values, nn,
-                 tiles, static_cast<const uint32_t *>(prefix), static_cast<const uint32_t *>(top), words_[1]);
-  launch_chained(ad::admit_bucket_kernel, ad::kBuckets, ad::kThreads, ad::kBucketSmemBytes, s, words_[1], words_[0],
+                 tiles, static_cast<const uint32_t *>(prefix), static_cast<const uint32_t *>(top), w1);
+  launch_chained(ad::admit_bucket_kernel, ad::kBuckets, ad::kThreads, ad::kBucketSmemBytes, s, w1, w0,
                  static_cast<const uint32_t *>(top), nn, tombstone ? 1 : 0, carry->keys, carry->vals, carry->flags,
                  carry->desc, carry->dir, carry->dir_bits, rows_log2_, lb, counter, dev_status_);
-  return carry;
 }
 
 RunBuffer *LsmDictionary::merge(RunBuffer *newer, RunBuffer *older, uint64_t out_upper,
-                                bool drop_tombstones, cudaStream_t s, const lsm::ReceiptSrc *rcpt) {
+                                bool drop_tombstones, cudaStream_t s, const lsm::ReceiptSrc *rcpt,
+                                bool release_newer, bool release_older) {
   RunBuffer *out = pool_.acquire(out_upper, s);
   const uint64_t tiles = std::max<uint64_t>(1, (out_upper + lsm::kMergeTile - 1) / lsm::kMergeTile);
   const size_t zero_bytes = merge_scratch_bytes(out_upper);
@@ -532,8 +551,8 @@ RunBuffer *LsmDictionary::merge(RunBuffer *newer, RunBuffer *older, uint64_t out
     GPULSM_CUDA(cudaEventRecord(tr.stop, s));
     traces_.push_back(tr);
   }
-  pool_.release(newer, s);
-  pool_.release(older, s);
+  if (release_newer) pool_.release(newer, s);
+  if (release_older) pool_.release(older, s);
   return out;
 }
 
@@ -806,6 +825,7 @@ static void refuse_capture(cudaStream_t s) {
 void LsmDictionary::clear(cudaStream_t s) {
   std::lock_guard<std::mutex> g(mu_);
   begin_op(s);
+  drop_staged();
   release_levels(s);
   GPULSM_CUDA(cudaMemsetAsync(dev_status_, 0, 4, s));
   status_bits_ = 0;
@@ -822,6 +842,7 @@ void LsmDictionary::bulk_build(const uint32_t *keys, const uint32_t *values, uin
     throw std::invalid_argument("invalid GPU dictionary initial input");
   if (n > radix::kMaxKeys) throw std::length_error("bulk build limited to 2^30-1 keys per call");
   begin_op(s);
+  drop_staged();
   release_levels(s);
   GPULSM_CUDA(cudaMemsetAsync(dev_status_, 0, 4, s));
   status_bits_ = 0;
@@ -850,6 +871,10 @@ void LsmDictionary::insert(const uint32_t *keys, const uint32_t *values, uint64_
   apply_receipt(false);
   reject_if_failed();
   begin_op(s, true);
+  if (stage_seq_pending()) {  // staged runs are older than this batch: they land first
+    begin_op(s);
+    flush_staged_locked(s);
+  }
   admit(keys, values, n, false, s);  // every batch's finishing kernel writes the receipt
   end_op(s);
 }
@@ -862,12 +887,17 @@ void LsmDictionary::erase(const uint32_t *keys, uint64_t n, cudaStream_t s) {
   apply_receipt(false);
   reject_if_failed();
   begin_op(s, true);
+  if (stage_seq_pending()) {  // staged runs are older than this batch: they land first
+    begin_op(s);
+    flush_staged_locked(s);
+  }
   admit(keys, nullptr, n, true, s);  // every batch's finishing kernel writes the receipt
   end_op(s);
 }
 
-lsm::LevelView LsmDictionary::view_of(int level) const {
-  const RunBuffer *r = levels_[level].run;
+lsm::LevelView LsmDictionary::view_of(int level) const { return view_of_run(levels_[level].run); }
+
+lsm::LevelView LsmDictionary::view_of_run(const RunBuffer *r) const {
   lsm::LevelView v{r->keys, r->vals, r->flags, cfg_.search_mode == 2 ? nullptr : r->dir, r->desc};
   if (cfg_.search_mode == 1 && r->model_ok) {
     v.mh = static_cast<const learned::ModelHeader *>(r->model);
@@ -880,6 +910,12 @@ lsm::LevelView LsmDictionary::view_of(int level) const {
 void LsmDictionary::level_set(void *out) const {
   auto *set = static_cast<lsm::LevelSet *>(out);
   set->count = 0;
+  // staged runs first, newest first: they are newer than every level
+  std::vector<const Staged *> st;
+  for (const Staged &x : staged_)
+    if (x.seq) st.push_back(&x);
+  std::sort(st.begin(), st.end(), [](const Staged *a, const Staged *b) { return a->seq > b->seq; });
+  for (const Staged *x : st) set->lv[set->count++] = view_of_run(x->run);
   for (size_t i = 0; i < levels_.size(); ++i)
     if (levels_[i].run) set->lv[set->count++] = view_of(int(i));
 }
@@ -906,6 +942,7 @@ void LsmDictionary::range_sum(const uint32_t *lo, const uint32_t *hi, uint64_t n
   if (!lo || !hi || !out) throw std::invalid_argument("invalid GPU dictionary range");
   apply_receipt(false);
   begin_op(s);
+  flush_staged_locked(s);  // range paths read the levels only
   ensure_models(s);
   const int single = ranges_on_single_level(lo, hi, n, s);
   ensure_models(s);  // a compaction wrote a new level
@@ -930,6 +967,7 @@ void LsmDictionary::range_sum_kway(const uint32_t *lo, const uint32_t *hi, uint6
   if (!lo || !hi || !out) throw std::invalid_argument("invalid GPU dictionary range");
   apply_receipt(false);
   begin_op(s);
+  flush_staged_locked(s);  // range paths read the levels only
   ensure_models(s);
   lsm::LevelSet set;
   live_level_set(&set, s);
@@ -946,6 +984,7 @@ void LsmDictionary::range_count(const uint32_t *lo, const uint32_t *hi, uint64_t
   if (!lo || !hi || !out) throw std::invalid_argument("invalid GPU dictionary range");
   apply_receipt(false);
   begin_op(s);
+  flush_staged_locked(s);  // range paths read the levels only
   ensure_models(s);
   const int single = ranges_on_single_level(lo, hi, n, s);
   ensure_models(s);  // a compaction wrote a new level
@@ -969,6 +1008,7 @@ void LsmDictionary::range_offsets(const uint32_t *lo, const uint32_t *hi, uint64
   if (n && (!lo || !hi)) throw std::invalid_argument("invalid GPU dictionary range");
   apply_receipt(false);
   begin_op(s);
+  flush_staged_locked(s);  // range paths read the levels only
   ensure_models(s);
   const uint32_t tiles = lsm::scan_tiles(n);
   const size_t count_bytes = align_up(std::max<uint64_t>(n, 1) * 4);
@@ -1007,6 +1047,7 @@ void LsmDictionary::range_pairs(const uint32_t *lo, const uint32_t *hi, uint64_t
     throw std::invalid_argument("invalid GPU dictionary range");
   apply_receipt(false);
   begin_op(s);
+  flush_staged_locked(s);  // range paths read the levels only
   ensure_models(s);
   const int single = ranges_on_single_level(lo, hi, n, s);
   ensure_models(s);  // a compaction wrote a new level
@@ -1111,7 +1152,113 @@ void LsmDictionary::kernel_timing(uint64_t *launches, double *total_ms, double *
 
 uint64_t LsmDictionary::resident_bytes() {
   std::lock_guard<std::mutex> g(mu_);
-  return pool_.bytes() + words_cap_ * 16 + scratch_bytes_ + ascratch_bytes_ + live_bytes_ + sizeof(Receipt) + 256;
+  const uint64_t staging = stage_max_ ? stage_max_ * (8 + 16) + bucket_admit_scratch_bytes(stage_max_) : 0;
+  return pool_.bytes() + words_cap_ * 16 + scratch_bytes_ + ascratch_bytes_ + live_bytes_ + sizeof(Receipt) + 256 +
+         staging;
+}
+
+// ---------------------------------------------------------------- staged updates
+void LsmDictionary::stage_configure(uint32_t slots, uint64_t max_keys, cudaStream_t s) {
+  std::lock_guard<std::mutex> g(mu_);
+  if (!staged_.empty()) throw std::invalid_argument("staged updates are already configured");
+  if (max_keys == 0 || max_keys > lsm::admit::kMaxKeys)
+    throw std::invalid_argument("staged update batches must hold 1 to 2^20 keys");
+  // every staged run is one more level of the level set
+  const uint32_t room = uint32_t(lsm::kMaxLevels) - uint32_t(caps_.size());
+  slots = std::min(slots, room);
+  if (slots == 0) throw std::invalid_argument("no room for staged levels beside the level schedule");
+  begin_op(s);
+  stage_max_ = max_keys;
+  GPULSM_CUDA(cudaMalloc(&stage_in_, 2 * max_keys * 4));
+  for (auto &w : stage_words_) GPULSM_CUDA(cudaMalloc(&w, max_keys * 8));
+  GPULSM_CUDA(cudaMalloc(&stage_scratch_, bucket_admit_scratch_bytes(max_keys)));
+  staged_.resize(slots);
+  for (Staged &x : staged_) x.run = pool_.acquire(max_keys, s);  // owned by the slot from now on
+  end_op(s);
+}
+
+int LsmDictionary::stage_free_slot() const {
+  std::lock_guard<std::mutex> g(mu_);
+  for (size_t i = 0; i < staged_.size(); ++i)
+    if (!staged_[i].seq) return int(i);
+  return -1;
+}
+
+void LsmDictionary::enqueue_stage_admit(uint32_t slot, uint64_t n, bool tombstone, cudaStream_t capturing) {
+  std::lock_guard<std::mutex> g(mu_);
+  if (slot >= staged_.size()) throw std::invalid_argument("no such staging slot");
+  if (n == 0 || n > stage_max_) throw std::length_error("staged update larger than the staging runs");
+  bucket_admit_into(stage_in_, tombstone ? nullptr : stage_in_ + n, n, tombstone, capturing, staged_[slot].run,
+                    stage_words_[0], stage_words_[1], stage_scratch_);
+  GPULSM_CUDA(cudaGetLastError());
+}
+
+void LsmDictionary::launch_stage_graph(cudaGraphExec_t exec, uint32_t slot, uint64_t n, bool tombstone,
+                                       cudaStream_t s) {
+  std::lock_guard<std::mutex> g(mu_);
+  if (slot >= staged_.size() || staged_[slot].seq) throw std::invalid_argument("staging slot is not free");
+  apply_receipt(false);
+  reject_if_failed();
+  begin_op(s, true);  // writes only its staging run: merges of earlier updates may still run
+  GPULSM_CUDA(cudaGraphLaunch(exec, s));
+  note_launch();
+  Staged &x = staged_[slot];
+  x.upper = n;
+  x.seq = ++stage_seq_;
+  x.tombs = tombstone;
+  ++next_gen_;  // the level set changed (device level table, live prefixes)
+  end_op(s);
+}
+
+void LsmDictionary::stage_flush(cudaStream_t s) {
+  std::lock_guard<std::mutex> g(mu_);
+  apply_receipt(false);
+  reject_if_failed();
+  begin_op(s);
+  flush_staged_locked(s);
+  end_op(s);
+}
+
+// Merges the staged runs, newest first, into one run and carries it into the
+// levels like an admitted batch; the staging runs stay with their slots.
+// Called with the lock held and s already ordered after the pending merges.
+void LsmDictionary::flush_staged_locked(cudaStream_t s) {
+  std::vector<Staged *> st;
+  for (Staged &x : staged_)
+    if (x.seq) st.push_back(&x);
+  if (st.empty()) return;
+  std::sort(st.begin(), st.end(), [](const Staged *a, const Staged *b) { return a->seq > b->seq; });
+  uint64_t total_upper = 0;
+  for (const Staged *x : st) total_upper += x->upper;
+  for (auto &l : levels_) total_upper += l.upper;
+  if (total_upper > 2 * budget_ + batch_capacity_ && receipt_pending_) {
+    apply_receipt(true);  // stale bounds: wait for the exact counts before planning more storage
+    reject_if_failed();
+  }
+  RunBuffer *x = st[0]->run;
+  uint64_t xu = st[0]->upper;
+  bool xt = st[0]->tombs, pooled = false;
+  for (size_t i = 1; i < st.size(); ++i) {
+    x = merge(x, st[i]->run, xu + st[i]->upper, false, s, nullptr, pooled, false);
+    xu += st[i]->upper;
+    xt = xt || st[i]->tombs;
+    pooled = true;
+  }
+  if (!pooled) {  // one staged run: copied into a pool run (merged with an empty run)
+    RunBuffer *empty = pool_.acquire(1, s);
+    GPULSM_CUDA(cudaMemsetAsync(empty->desc, 0, sizeof(LevelDesc), s));
+    x = merge(x, empty, xu, false, s, nullptr, false, true);
+  }
+  for (Staged *y : st) {
+    y->seq = 0;
+    y->upper = 0;
+    y->tombs = false;
+  }
+  cascade(x, xu, xt, s, true);
+  pool_.advance();
+  receipt_posted();
+  ++stage_flushes_;
+  ++next_gen_;
 }
 
 uint64_t LsmDictionary::cleanup(cudaStream_t s) {
@@ -1119,6 +1266,7 @@ uint64_t LsmDictionary::cleanup(cudaStream_t s) {
   apply_receipt(false);
   reject_if_failed();
   begin_op(s);
+  flush_staged_locked(s);
   compact_all(s);
   unsigned long long n = 0;
   for (auto &l : levels_)
@@ -1139,6 +1287,13 @@ void LsmDictionary::size(uint64_t *rows, uint32_t *levels) {
     if (!l.run) continue;
     unsigned long long n = 0;
     GPULSM_CUDA(cudaMemcpy(&n, &l.run->desc->n, 8, cudaMemcpyDeviceToHost));
+    total += n;
+    ++count;
+  }
+  for (const Staged &x : staged_) {  // staged runs count as levels
+    if (!x.seq) continue;
+    unsigned long long n = 0;
+    GPULSM_CUDA(cudaMemcpy(&n, &x.run->desc->n, 8, cudaMemcpyDeviceToHost));
     total += n;
     ++count;
   }

@@ -124,6 +124,28 @@ class LsmDictionary {
   // versions dropped; returns the live key count (synchronises).
   uint64_t cleanup(cudaStream_t s);
 
+  // Staged updates, replayable from CUDA graphs (the serving loop).  A staged
+  // update admits a batch of exactly `n` keys (a size class; the caller pads
+  // with copies of its last key and value, which change nothing) into one of
+  // `slots` fixed staging runs with fixed admission buffers, so its four
+  // admission kernels can be captured once and replayed.  Staged runs are the
+  // newest levels of every point lookup, successor and table lookup; they
+  // merge into the levels (the regular cascade) when stage_flush runs - which
+  // every other update, range operation, build and clear does first, and
+  // which the caller runs when no slot is free.
+  void stage_configure(uint32_t slots, uint64_t max_keys, cudaStream_t s);
+  // a free staging slot, or -1 when every slot holds a run
+  int stage_free_slot() const;
+  // records the admission of slot `slot` into a capturing stream: keys (and
+  // values, for inserts) are read from stage_input()
+  void enqueue_stage_admit(uint32_t slot, uint64_t n, bool tombstone, cudaStream_t capturing);
+  // the device buffer a staged graph reads: keys at [0, n), values at [n, 2n)
+  uint32_t *stage_input() const { return stage_in_; }
+  // launches a captured staged-update graph, ordered like an update
+  void launch_stage_graph(cudaGraphExec_t exec, uint32_t slot, uint64_t n, bool tombstone, cudaStream_t s);
+  void stage_flush(cudaStream_t s);
+  uint64_t stage_flushes() const { return stage_flushes_; }
+
   // Introspection for tests and benchmarks.
   uint32_t level_count() const { return uint32_t(caps_.size()); }
   uint64_t level_capacity(uint32_t i) const { return caps_[i]; }
@@ -151,9 +173,24 @@ class LsmDictionary {
                         cudaStream_t s);
   RunBuffer *bucket_admit(const uint32_t *keys, const uint32_t *values, uint64_t n, bool tombstone,
                           cudaStream_t s);
+  void bucket_admit_into(const uint32_t *keys, const uint32_t *values, uint64_t n, bool tombstone,
+                         cudaStream_t s, RunBuffer *out, unsigned long long *w0, unsigned long long *w1,
+                         void *scratch);
+  static size_t bucket_admit_scratch_bytes(uint64_t n);
+  void flush_staged_locked(cudaStream_t s);
+  bool stage_seq_pending() const {
+    for (const Staged &x : staged_)
+      if (x.seq) return true;
+    return false;
+  }
+  void drop_staged() {
+    for (Staged &x : staged_) x.seq = x.upper = 0, x.tombs = false;
+    ++next_gen_;
+  }
   void cascade(RunBuffer *carry, uint64_t carry_upper, bool carry_tombs, cudaStream_t s, bool want_receipt);
   RunBuffer *merge(RunBuffer *newer, RunBuffer *older, uint64_t out_upper, bool drop_tombstones,
-                   cudaStream_t s, const lsm::ReceiptSrc *rcpt = nullptr);
+                   cudaStream_t s, const lsm::ReceiptSrc *rcpt = nullptr, bool release_newer = true,
+                   bool release_older = true);
   // Range batches: merge every level into one tombstone-free run when the
   // rows the batch covers outweigh the merge; returns the single level to
   // answer from, or -1 to use the per-query k-way merge.
@@ -170,6 +207,7 @@ class LsmDictionary {
   void ensure_sort_space(uint64_t n, cudaStream_t s);
   void level_set(void *out) const;
   lsm::LevelView view_of(int level) const;
+  lsm::LevelView view_of_run(const RunBuffer *r) const;
 
   DictConfig cfg_;
   uint64_t batch_capacity_ = 0;
@@ -235,6 +273,20 @@ class LsmDictionary {
   cudaEvent_t adm_done_ = nullptr;
   cudaEvent_t merge_done_ = nullptr;
   bool merges_pending_ = false;
+  // staged updates (serving): fixed staging runs, newest first by seq
+  struct Staged {
+    RunBuffer *run = nullptr;
+    uint64_t upper = 0;
+    uint64_t seq = 0;  // 0 = free
+    bool tombs = false;
+  };
+  std::vector<Staged> staged_;
+  uint64_t stage_seq_ = 0;
+  uint64_t stage_max_ = 0;
+  uint64_t stage_flushes_ = 0;
+  uint32_t *stage_in_ = nullptr;                      // the staged graphs' input (2 * stage_max_ words)
+  unsigned long long *stage_words_[2] = {nullptr, nullptr};
+  void *stage_scratch_ = nullptr;
   cudaStream_t last_stream_ = nullptr;  // stream of the last operation (op_done_ was recorded there)
   bool last_stream_known_ = false;
   mutable std::mutex mu_;

@@ -48,20 +48,29 @@ Server::Server(const DictConfig &cfg, uint64_t budget_bytes, uint32_t max_round_
   GPULSM_CUDA(cudaStreamCreateWithFlags(&download_, cudaStreamNonBlocking));
   GPULSM_CUDA(cudaStreamCreateWithFlags(&capture_, cudaStreamNonBlocking));
   const uint64_t m = max_round_keys_;
-  slot_bytes_ = m * 8 + m * 4 + m;  // inputs (two words a key), outputs, found flags
+  // inputs: two words a key, twice that for the padding of staged update runs
+  in_words_cap_ = 4 * m + 4096;
+  slot_bytes_ = in_words_cap_ * 4 + m * 4 + m;  // inputs, outputs, found flags
   slots_.resize(depth);
   for (uint32_t i = 0; i < depth; ++i) {
     Slot &s = slots_[i];
-    GPULSM_CUDA(cudaMallocHost(&s.h_in, m * 8));
+    GPULSM_CUDA(cudaMallocHost(&s.h_in, in_words_cap_ * 4));
     GPULSM_CUDA(cudaMallocHost(&s.h_out, m * 4));
     GPULSM_CUDA(cudaMallocHost(&s.h_found, m));
-    GPULSM_CUDA(cudaMalloc(&s.d_in, m * 8));
+    GPULSM_CUDA(cudaMalloc(&s.d_in, in_words_cap_ * 4));
     GPULSM_CUDA(cudaMalloc(&s.d_out, m * 4));
     GPULSM_CUDA(cudaMalloc(&s.d_found, m));
     GPULSM_CUDA(cudaEventCreate(&s.uploaded));  // timed: device busy time per round
     GPULSM_CUDA(cudaEventCreate(&s.computed));
     GPULSM_CUDA(cudaEventCreateWithFlags(&s.downloaded, cudaEventDisableTiming));
     free_slots_.push_back(i);
+  }
+  // staged updates: update runs are admitted into fixed staging runs by
+  // captured graphs; 4 staging slots (fewer when the level schedule is deep)
+  if (max_round_keys_ <= (1u << 20)) {
+    dict_.stage_configure(4, max_round_keys_, compute_);
+    GPULSM_CUDA(cudaStreamSynchronize(compute_));
+    staged_updates_ = true;
   }
   worker_ = std::thread(&Server::worker, this);
   completer_ = std::thread(&Server::completer, this);
@@ -96,6 +105,7 @@ Server::~Server() {
     for (auto &g : s.graphs) cudaGraphExecDestroy(g.second);
     for (cudaEvent_t e : s.marks) cudaEventDestroy(e);
   }
+  for (auto &g : update_graphs_) cudaGraphExecDestroy(g.second);
   cudaStreamDestroy(capture_);
   cudaStreamDestroy(compute_);
   cudaStreamDestroy(upload_);
@@ -150,6 +160,7 @@ void Server::reset_stats() {
   std::lock_guard<std::mutex> g(mu_);
   lat_us_.clear();
   st_completed_ = st_rejected_ = st_rounds_ = st_keys_ = st_round_keys_ = st_graph_rounds_ = 0;
+  st_graph_updates_ = 0;
   st_first_ = -1;
   st_last_ = st_gpu_s_ = st_launch_s_ = 0;
   for (double &k : st_kind_gpu_s_) k = 0;
@@ -171,6 +182,8 @@ ServeStats Server::stats() {
     s.gpu_busy_s = st_gpu_s_;
     s.host_launch_s = st_launch_s_;
     s.graph_rounds = st_graph_rounds_;
+    s.graph_updates = st_graph_updates_;
+    s.stage_flushes = dict_.stage_flushes();
     for (int k = 0; k < 4; ++k) s.kind_gpu_s[k] = st_kind_gpu_s_[k];
     s.host_copy_s = st_copy_s_;
     s.host_scatter_s = st_scatter_s_;
@@ -205,10 +218,22 @@ bool Server::form_round(Slot &slot) {
   const uint64_t resident = dict_.resident_bytes();
   const double t = now_s();
   bool any = false;
+  uint64_t words_done = 0;  // input words of the runs before the current one (padding included)
+  auto run_words = [&](uint32_t kind, uint64_t n) {
+    const uint64_t c = (staged_updates_ && is_update(kind)) ? size_class(n) : n;
+    return c * (has_aux(kind) ? 2 : 1);
+  };
   while (!queue_.empty()) {
     const uint64_t tk = queue_.front();
     Req &q = reqs_.at(tk);
     if (keys > 0 && keys + q.n > max_round_keys_) break;
+    if (keys > 0 && q.n) {  // the staging input must hold the round with its padding
+      const bool same = !slot.runs.empty() && slot.runs.back().kind == q.kind;
+      const uint64_t cur = slot.runs.empty() ? 0 : run_words(slot.runs.back().kind, slot.runs.back().n);
+      const uint64_t words = same ? words_done + run_words(q.kind, slot.runs.back().n + q.n)
+                                  : words_done + cur + run_words(q.kind, q.n);
+      if (words > in_words_cap_) break;
+    }
     queue_.pop_front();
     if (q.n == 0) {  // nothing to do: done at once
       q.state = 1;
@@ -228,6 +253,7 @@ bool Server::form_round(Slot &slot) {
       slot.bytes += growth;
     }
     if (slot.runs.empty() || slot.runs.back().kind != q.kind) {
+      if (!slot.runs.empty()) words_done += run_words(slot.runs.back().kind, slot.runs.back().n);
       Run r{};
       r.kind = q.kind;
       r.first_part = slot.parts.size();
@@ -240,13 +266,15 @@ bool Server::form_round(Slot &slot) {
     keys += q.n;
     any = true;
   }
-  // staging layout: each run's keys, then its values / upper bounds
+  // staging layout: each run's keys, then its values / upper bounds; a staged
+  // update run is padded to its size class (copies of its last key and value)
   uint64_t in = 0, out = 0;
   for (Run &r : slot.runs) {
     r.in_off = in;
     r.out_off = out;
     r.status = 0;
-    in += r.n * (has_aux(r.kind) ? 2 : 1);
+    r.cls = (staged_updates_ && is_update(r.kind)) ? size_class(r.n) : r.n;
+    in += r.cls * (has_aux(r.kind) ? 2 : 1);
     if (has_out(r.kind)) out += r.n;
   }
   slot.in_words = in;
@@ -295,14 +323,50 @@ static uint32_t next_mark_pair(std::vector<cudaEvent_t> &marks, size_t used) {
   return uint32_t(used);
 }
 
+// Size classes of staged updates: powers of two from 1024 keys, the last one
+// the round limit.
+uint64_t Server::size_class(uint64_t n) const {
+  uint64_t c = 1024;
+  while (c < n) c <<= 1;
+  return std::min<uint64_t>(c, max_round_keys_);
+}
+
+cudaGraphExec_t Server::update_graph(bool tombstone, uint32_t size_class, uint32_t stage) {
+  const uint64_t key = uint64_t(tombstone) | (uint64_t(size_class) << 1) | (uint64_t(stage) << 40);
+  for (const auto &g : update_graphs_)
+    if (g.first == key) return g.second;
+  cudaGraph_t graph = nullptr;
+  GPULSM_CUDA(cudaStreamBeginCapture(capture_, cudaStreamCaptureModeThreadLocal));
+  try {
+    dict_.enqueue_stage_admit(stage, size_class, tombstone, capture_);
+  } catch (...) {
+    cudaStreamEndCapture(capture_, &graph);
+    if (graph) cudaGraphDestroy(graph);
+    throw;
+  }
+  GPULSM_CUDA(cudaStreamEndCapture(capture_, &graph));
+  cudaGraphExec_t exec = nullptr;
+  const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  GPULSM_CUDA(e);
+  update_graphs_.emplace_back(key, exec);
+  return exec;
+}
+
 void Server::launch_round(Slot &slot) {
   const double c0 = now_s();
-  for (const Run &r : slot.runs)
+  for (const Run &r : slot.runs) {
     for (uint64_t i = 0; i < r.parts; ++i) {
       const Part &p = slot.parts[r.first_part + i];
       std::memcpy(slot.h_in + r.in_off + p.off, p.keys, p.n * 4);
-      if (has_aux(r.kind)) std::memcpy(slot.h_in + r.in_off + r.n + p.off, p.aux, p.n * 4);
+      if (has_aux(r.kind)) std::memcpy(slot.h_in + r.in_off + r.cls + p.off, p.aux, p.n * 4);
     }
+    if (r.cls > r.n && r.n) {  // padding of a staged update: repeats of its last (key, value) change nothing
+      uint32_t *k = slot.h_in + r.in_off;
+      std::fill(k + r.n, k + r.cls, k[r.n - 1]);
+      if (has_aux(r.kind)) std::fill(k + r.cls + r.n, k + 2 * r.cls, k[r.cls + r.n - 1]);
+    }
+  }
   const double c1 = now_s();
   slot.timed.clear();
   {
@@ -341,11 +405,27 @@ void Server::launch_round(Slot &slot) {
           dict_.lookup(in, r.n, slot.d_out + r.out_off, slot.d_found + r.out_off, compute_);
           break;
         case kServeInsert:
-          dict_.insert(in, in + r.n, r.n, compute_);
+        case kServeErase: {
+          const bool tomb = r.kind == kServeErase;
+          if (!staged_updates_) {
+            tomb ? dict_.erase(in, r.n, compute_) : dict_.insert(in, in + r.n, r.n, compute_);
+            break;
+          }
+          // one graph launch: the run's (padded) keys into the staged graphs'
+          // input, then the captured admission into a free staging slot
+          int stage = dict_.stage_free_slot();
+          if (stage < 0) {
+            dict_.stage_flush(compute_);  // the staged runs merge into the levels
+            stage = dict_.stage_free_slot();
+          }
+          GPULSM_CUDA(cudaMemcpyAsync(dict_.stage_input(), in, r.cls * (tomb ? 4 : 8), cudaMemcpyDeviceToDevice,
+                                      compute_));
+          dict_.launch_stage_graph(update_graph(tomb, uint32_t(r.cls), uint32_t(stage)), uint32_t(stage), r.cls,
+                                   tomb, compute_);
+          std::lock_guard<std::mutex> g(mu_);
+          ++st_graph_updates_;
           break;
-        case kServeErase:
-          dict_.erase(in, r.n, compute_);
-          break;
+        }
         default:
           dict_.range_sum_kway(in, in + r.n, r.n, slot.d_out + r.out_off, compute_);
           break;
@@ -359,7 +439,7 @@ void Server::launch_round(Slot &slot) {
   // an update request completes when its merges have completed
   bool updates = false;
   for (const Run &r : slot.runs) updates = updates || is_update(r.kind);
-  if (updates) {
+  if (updates && !staged_updates_) {
     const uint32_t m = next_mark_pair(slot.marks, slot.timed.size() * 2);
     GPULSM_CUDA(cudaEventRecord(slot.marks[m], compute_));
     dict_.join(compute_);

@@ -48,6 +48,8 @@ struct ServeStats {
   double gpu_busy_s = 0;      // device time of the rounds (upload done -> kernels done)
   double host_launch_s = 0;   // worker time staging and launching rounds
   uint64_t graph_rounds = 0;  // lookup-only rounds replayed from a captured CUDA graph
+  uint64_t graph_updates = 0;  // update runs replayed from a captured CUDA graph (staged)
+  uint64_t stage_flushes = 0;  // staged runs merged into the levels
   double kind_gpu_s[4] = {0, 0, 0, 0};  // device time per request kind (updates: merges included)
   double host_copy_s = 0;     // worker time copying request data into pinned staging
   double host_scatter_s = 0;  // completion time copying results into the requests' buffers
@@ -113,6 +115,7 @@ class Server {
     uint64_t in_off = 0;   // words into the staging input: keys, then values / upper bounds
     uint64_t out_off = 0;  // words into the staging output
     uint64_t n = 0;
+    uint64_t cls = 0;      // staged update: keys padded to this size class (values start at in_off + cls)
     size_t first_part = 0, parts = 0;
     int status = 0;        // 0, or the negated gpulsm status of a failed call
   };
@@ -141,6 +144,9 @@ class Server {
   bool form_round(Slot &slot);
   void launch_round(Slot &slot);
   cudaGraphExec_t lookup_graph(Slot &slot, uint32_t size_class);
+  // the graph of a staged update of `size_class` keys into staging slot `stage`
+  cudaGraphExec_t update_graph(bool tombstone, uint32_t size_class, uint32_t stage);
+  uint64_t size_class(uint64_t n) const;
   static double now_s();
 
   LsmDictionary dict_;
@@ -148,12 +154,18 @@ class Server {
   uint64_t budget_;
   uint32_t max_round_keys_;
   uint64_t slot_bytes_ = 0;
+  uint64_t in_words_cap_ = 0;  // staging input words of a slot
   std::vector<Slot> slots_;
   std::deque<uint32_t> free_slots_;
   std::deque<uint32_t> inflight_;
   cudaStream_t compute_ = nullptr, upload_ = nullptr, download_ = nullptr;
   cudaStream_t capture_ = nullptr;  // graphs are captured here (thread-local mode)
   uint64_t st_graph_rounds_ = 0;
+  // staged updates: update runs replayed from captured graphs (admission only;
+  // the staged runs merge into the levels when the staging slots are full)
+  bool staged_updates_ = false;
+  std::vector<std::pair<uint64_t, cudaGraphExec_t>> update_graphs_;  // key: tomb | class << 1 | stage << 40
+  uint64_t st_graph_updates_ = 0;
 
   std::mutex mu_;
   std::condition_variable cv_work_, cv_done_, cv_inflight_;

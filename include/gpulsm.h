@@ -249,6 +249,8 @@ typedef struct gpulsm_serve_stats {
   double kind_gpu_s[4];             /* device time of each request kind's calls (updates: merges included) */
   double host_copy_s;               /* worker time copying request data into pinned staging */
   double host_scatter_s;            /* completion time copying results into the requests' buffers */
+  uint64_t graph_updates;           /* update runs replayed from a captured CUDA graph (staged admission) */
+  uint64_t stage_flushes;           /* merges of the staged runs into the levels */
 } gpulsm_serve_stats;
 
 /* Open-loop load: Poisson arrivals at rate_per_s (0 = closed loop with

@@ -111,8 +111,14 @@ def test_results_same_alone_and_in_mix(gl, cuda):
     ordered = [req for _, _, req in flat]
     srv = fresh_server(gl, base_k, base_v)
     alone = [srv.wait(submit(srv, req)) for req in ordered]
-    # a lookup submitted alone is a lookup-only round: replayed from a CUDA graph
-    assert srv.stats()["graph_rounds"] == sum(1 for r in ordered if r[0] == "lookup")
+    # a lookup submitted alone is a lookup-only round: replayed from a CUDA graph;
+    # an update submitted alone is one staged admission replayed from a graph,
+    # and the staged runs merged into the levels whenever the staging slots filled
+    st = srv.stats()
+    assert st["graph_rounds"] == sum(1 for r in ordered if r[0] == "lookup")
+    n_updates = sum(1 for r in ordered if r[0] in ("insert", "erase"))
+    assert st["graph_updates"] == n_updates
+    assert st["stage_flushes"] >= 1 and st["stage_flushes"] >= n_updates // 4 - 1
     srv.close()
 
     want = oracle_answers(base_k, base_v, ordered)
@@ -147,4 +153,42 @@ def test_load_generator_reports_consistent_stats(gl, cuda):
     rate = 0.3 * closed["completed"] / max(closed["wall_s"], 1e-6)
     opened = srv.run_load(base_k, rate_per_s=rate, seconds=0.3, max_keys=1 << 12, seed=2)
     assert opened["completed"] > 5 and opened["p50_us"] <= opened["p99_us"]
+    srv.close()
+
+
+def test_staged_updates_merge_into_levels_and_stay_exact(gl, cuda):
+    """Update rounds go through the staged path: each admits its (padded)
+    batch into a staging run by one captured graph; when the staging slots are
+    full they merge into the levels.  Many small update rounds of every size
+    class, interleaved with reads of every kind (lookups see the staged runs
+    directly; range sums and the rest merge them first), stay equal to the
+    oracle, and the padding never changes an answer."""
+    rng = np.random.default_rng(23)
+    base_k = rng.integers(0, 1 << 32, 1 << 15, dtype=np.uint64).astype(np.uint32)
+    base_v = np.arange(base_k.size, dtype=np.uint32)
+    universe = np.concatenate([base_k, rng.integers(0, 1 << 32, 1 << 13, dtype=np.uint64).astype(np.uint32)])
+    srv = fresh_server(gl, base_k, base_v)
+    o = OracleLSM()
+    o.bulk_build(base_k, base_v)
+    for step in range(40):
+        n = int(rng.choice([1, 7, 1000, 1025, 3000, 5000]))
+        keys = universe[rng.integers(0, universe.size, n)]
+        if step % 5 == 4:
+            srv.wait(srv.submit_erase(keys))
+            o.erase(keys)
+        else:
+            vals = rng.integers(0, 1 << 32, n, dtype=np.uint64).astype(np.uint32)
+            srv.wait(srv.submit_insert(keys, vals))
+            o.insert(keys, vals)
+        if step % 3 == 0:
+            q = universe[rng.integers(0, universe.size, 4000)]
+            got = srv.wait(srv.submit_lookup(q, with_found=True))
+            want = o.lookup(q, with_found=True)
+            assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1]), f"step {step}"
+        if step % 7 == 6:
+            lo = universe[rng.integers(0, universe.size, 500)]
+            hi = np.minimum(lo.astype(np.uint64) + (1 << 24), 0xFFFFFFFF).astype(np.uint32)
+            assert np.array_equal(srv.wait(srv.submit_range_sum(lo, hi)), o.range_sum(lo, hi)), f"step {step}"
+    st = srv.stats()
+    assert st["graph_updates"] == 40 and st["stage_flushes"] >= 5
     srv.close()
