@@ -601,7 +601,7 @@ void LsmDictionary::fit_now(RunBuffer *run, uint64_t upper, cudaStream_t s) {
 // update's receipt goes into its final merge kernel (or, without a merge, a
 // standalone receipt kernel).
 void LsmDictionary::cascade(RunBuffer *carry, uint64_t carry_upper, bool carry_tombs, cudaStream_t s,
-                            bool want_receipt) {
+                            bool want_receipt, bool carry_owned) {
   const size_t L = levels_.size();
   size_t dest = 0;
   uint64_t acc = carry_upper;
@@ -624,7 +624,8 @@ void LsmDictionary::cascade(RunBuffer *carry, uint64_t carry_upper, bool carry_t
     const bool last = (i + 1 == dest) && !dest_occupied;
     const uint64_t ou = xu + levels_[i].upper;
     const bool drop = last && !deeper;
-    x = merge(x, levels_[i].run, ou, drop, s, (want_receipt && i + 1 == merges) ? &rcpt : nullptr);
+    x = merge(x, levels_[i].run, ou, drop, s, (want_receipt && i + 1 == merges) ? &rcpt : nullptr,
+              carry_owned || x != carry);
     xu = ou;
     xt = !drop && (xt || levels_[i].tombs);
     levels_[i] = Level{};
@@ -632,9 +633,15 @@ void LsmDictionary::cascade(RunBuffer *carry, uint64_t carry_upper, bool carry_t
   }
   if (dest_occupied) {
     const uint64_t ou = xu + levels_[dest].upper;
-    x = merge(x, levels_[dest].run, ou, !deeper, s, want_receipt ? &rcpt : nullptr);
+    x = merge(x, levels_[dest].run, ou, !deeper, s, want_receipt ? &rcpt : nullptr, carry_owned || x != carry);
     xu = ou;
     xt = deeper && (xt || levels_[dest].tombs);
+  }
+  if (x == carry && !carry_owned) {  // the carry lands as it is: a copy of it becomes the level
+    RunBuffer *empty = pool_.acquire(1, s);
+    GPULSM_CUDA(cudaMemsetAsync(empty->desc, 0, sizeof(LevelDesc), s));
+    x = merge(carry, empty, xu, !deeper, s, nullptr, false, true);
+    xt = deeper && xt;
   }
   levels_[dest].run = x;
   levels_[dest].upper = std::min<uint64_t>(xu, x->cap);
@@ -1235,28 +1242,17 @@ void LsmDictionary::flush_staged_locked(cudaStream_t s) {
     apply_receipt(true);  // stale bounds: wait for the exact counts before planning more storage
     reject_if_failed();
   }
-  RunBuffer *x = st[0]->run;
-  uint64_t xu = st[0]->upper;
-  bool xt = st[0]->tombs, pooled = false;
-  for (size_t i = 1; i < st.size(); ++i) {
-    x = merge(x, st[i]->run, xu + st[i]->upper, false, s, nullptr, pooled, false);
-    xu += st[i]->upper;
-    xt = xt || st[i]->tombs;
-    pooled = true;
-  }
-  if (!pooled) {  // one staged run: copied into a pool run (merged with an empty run)
-    RunBuffer *empty = pool_.acquire(1, s);
-    GPULSM_CUDA(cudaMemsetAsync(empty->desc, 0, sizeof(LevelDesc), s));
-    x = merge(x, empty, xu, false, s, nullptr, false, true);
-  }
-  for (Staged *y : st) {
+  // oldest first, each staged run is carried into the levels like an admitted
+  // batch (the cascade reads it and leaves the buffer with its slot)
+  for (size_t i = st.size(); i-- > 0;) {
+    Staged *y = st[i];
+    cascade(y->run, y->upper, y->tombs, s, true, false);
+    receipt_posted();
     y->seq = 0;
     y->upper = 0;
     y->tombs = false;
   }
-  cascade(x, xu, xt, s, true);
   pool_.advance();
-  receipt_posted();
   ++stage_flushes_;
   ++next_gen_;
 }

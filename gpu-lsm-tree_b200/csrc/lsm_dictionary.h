@@ -187,7 +187,10 @@ class LsmDictionary {
     for (Staged &x : staged_) x.seq = x.upper = 0, x.tombs = false;
     ++next_gen_;
   }
-  void cascade(RunBuffer *carry, uint64_t carry_upper, bool carry_tombs, cudaStream_t s, bool want_receipt);
+  // carry_owned = false: the carry belongs to someone else (a staging run);
+  // the cascade reads it but never releases or keeps it
+  void cascade(RunBuffer *carry, uint64_t carry_upper, bool carry_tombs, cudaStream_t s, bool want_receipt,
+               bool carry_owned = true);
   RunBuffer *merge(RunBuffer *newer, RunBuffer *older, uint64_t out_upper, bool drop_tombstones,
                    cudaStream_t s, const lsm::ReceiptSrc *rcpt = nullptr, bool release_newer = true,
                    bool release_older = true);

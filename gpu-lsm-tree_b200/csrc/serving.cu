@@ -323,11 +323,16 @@ static uint32_t next_mark_pair(std::vector<cudaEvent_t> &marks, size_t used) {
   return uint32_t(used);
 }
 
-// Size classes of staged updates: powers of two from 1024 keys, the last one
-// the round limit.
+// Size classes of staged updates: from 1024 keys, four classes per power of
+// two (padding at most a quarter of the batch), the last one the round limit.
 uint64_t Server::size_class(uint64_t n) const {
   uint64_t c = 1024;
-  while (c < n) c <<= 1;
+  if (n > c) {
+    uint64_t p = 1024;
+    while (p * 2 < n) p <<= 1;  // p < n <= 2p
+    const uint64_t step = p / 4;
+    c = (n + step - 1) / step * step;
+  }
   return std::min<uint64_t>(c, max_round_keys_);
 }
 
