@@ -245,6 +245,8 @@ LsmDictionary::~LsmDictionary() {
   for (cudaEvent_t e : spare_events_) cudaEventDestroy(e);
   for (auto &lp : live_)
     if (lp.p) cudaFree(lp.p);
+  for (auto &lp : live_staged_)
+    if (lp.p) cudaFree(lp.p);
   if (width_) cudaFree(width_);
   if (width_host_) cudaFreeHost(width_host_);
   if (ascratch_) cudaFree(ascratch_);
@@ -749,13 +751,37 @@ const unsigned long long *LsmDictionary::value_prefix(int level, cudaStream_t s)
 void LsmDictionary::live_level_set(void *out, cudaStream_t s) {
   auto *set = static_cast<lsm::LevelSet *>(out);
   set->count = 0;
+  // staged runs first, newest first (their prefixes are rebuilt when a slot is refilled)
+  if (live_staged_.size() < staged_.size()) live_staged_.resize(staged_.size());
+  std::vector<size_t> st;
+  for (size_t i = 0; i < staged_.size(); ++i)
+    if (staged_[i].seq) st.push_back(i);
+  std::sort(st.begin(), st.end(), [&](size_t a, size_t b) { return staged_[a].seq > staged_[b].seq; });
+  for (size_t i : st) {
+    LivePrefix &lp = live_staged_[i];
+    refresh_live_prefix(lp, staged_[i].run, staged_[i].upper, staged_[i].seq, s);
+    lsm::LevelView v = view_of_run(staged_[i].run);
+    v.live = lp.p;
+    set->lv[set->count++] = v;
+  }
   if (live_.size() < levels_.size()) live_.resize(levels_.size());
   for (size_t i = 0; i < levels_.size(); ++i) {
     const Level &l = levels_[i];
     if (!l.run) continue;
     LivePrefix &lp = live_[i];
-    if (lp.gen != l.gen || !lp.p) {
-      const uint64_t n = l.upper;
+    refresh_live_prefix(lp, l.run, l.upper, l.gen, s);
+    lsm::LevelView v = view_of(int(i));
+    v.live = lp.p;
+    set->lv[set->count++] = v;
+  }
+}
+
+// The u32 prefix of live values of a run, rebuilt when its generation changed.
+void LsmDictionary::refresh_live_prefix(LivePrefix &lp, RunBuffer *run, uint64_t upper, uint64_t gen,
+                                        cudaStream_t s) {
+  {
+    const uint64_t n = upper;
+    if (lp.gen != gen || !lp.p) {
       if (n + 1 > lp.cap) {
         if (lp.p) GPULSM_CUDA(cudaFreeAsync(lp.p, s));
         live_bytes_ -= lp.cap * 4;
@@ -776,14 +802,11 @@ void LsmDictionary::live_level_set(void *out, cudaStream_t s) {
       GPULSM_CUDA(cudaMemsetAsync(bump.p, 0, bytes, s));
       uint32_t *counter = bump.take<uint32_t>(2);
       unsigned long long *lb = bump.take<unsigned long long>(tiles + 1);
-      lsm::scan_kernel<uint32_t, true><<<tiles, lsm::kScanThreads, 0, s>>>(l.run->vals, l.run->flags, n, lp.p, lb,
+      lsm::scan_kernel<uint32_t, true><<<tiles, lsm::kScanThreads, 0, s>>>(run->vals, run->flags, n, lp.p, lb,
                                                                            counter, dev_status_);
       note_launch();
-      lp.gen = l.gen;
+      lp.gen = gen;
     }
-    lsm::LevelView v = view_of(int(i));
-    v.live = lp.p;
-    set->lv[set->count++] = v;
   }
 }
 
@@ -973,8 +996,7 @@ void LsmDictionary::range_sum_kway(const uint32_t *lo, const uint32_t *hi, uint6
   if (!n) return;
   if (!lo || !hi || !out) throw std::invalid_argument("invalid GPU dictionary range");
   apply_receipt(false);
-  begin_op(s);
-  flush_staged_locked(s);  // range paths read the levels only
+  begin_op(s);  // staged runs take part through their live-value prefixes (no flush)
   ensure_models(s);
   lsm::LevelSet set;
   live_level_set(&set, s);

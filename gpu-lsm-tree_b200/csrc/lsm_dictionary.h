@@ -251,6 +251,8 @@ class LsmDictionary {
     uint64_t gen = ~0ull;
   };
   std::vector<LivePrefix> live_;
+  std::vector<LivePrefix> live_staged_;  // one per staging slot (gen = the staged run's seq)
+  void refresh_live_prefix(LivePrefix &lp, RunBuffer *run, uint64_t upper, uint64_t gen, cudaStream_t s);
   uint64_t live_bytes_ = 0;
   unsigned long long *width_ = nullptr;  // device word for the range-width estimate
   unsigned long long *width_host_ = nullptr;
