@@ -603,12 +603,16 @@ def serving_leg(args, gl, w, dev):
     keys = np.concatenate([o[1] for o in w.ops if o[0] == "insert"])
     secs = args.serving_seconds
     out = {"dictionary_keys": int(keys.size), "budget_gb": 16}
-    for name, mode in (("plain", 0), ("learned", 1)):
+    # plain / learned: search modes of the levels, update runs staged (admitted by
+    # captured graphs, merged when the staging slots fill); plain_direct: update
+    # runs admitted and merged at once, each round waiting for its merges
+    for name, mode, staged in (("plain", 0, True), ("learned", 1, True), ("plain_direct", 0, False)):
         # serving requests are small: a small level 0 (2^17 rows, fan-in 4) keeps
         # a run's merge proportional to the run instead of to a 4M-row level
         srv = gl.Server(gl.DictionaryConfig(max_elements=keys.size + w.erased_keys + (1 << 24), search_mode=mode,
                                             level_zero_capacity=1 << 17),
                         budget_bytes=16 << 30, max_round_keys=1 << 20, depth=3)
+        srv.set_staged_updates(staged)
         kd = torch.from_numpy(keys.view(np.int32)).to(dev)
         vd = torch.arange(keys.size, dtype=torch.int32, device=dev)
         srv.bulk_build(kd, vd)
@@ -638,6 +642,8 @@ def serving_leg(args, gl, w, dev):
             "peak_host_copy_frac": round(peak["host_copy_s"] / max(peak["wall_s"], 1e-9), 3),
             "peak_host_scatter_frac": round(peak["host_scatter_s"] / max(peak["wall_s"], 1e-9), 3),
             "requests": int(half["completed"]), "rejected": int(half["rejected"] + peak["rejected"]),
+            "peak_graph_update_runs": int(peak["graph_updates"]), "peak_stage_flushes": int(peak["stage_flushes"]),
+            "peak_graph_lookup_rounds": int(peak["graph_rounds"]), "peak_rounds": int(peak["rounds"]),
         }
     return out
 

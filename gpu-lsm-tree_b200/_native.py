@@ -232,6 +232,7 @@ def load() -> C.CDLL:
         "gpulsm_server_drain": (i32, [vp]),
         "gpulsm_server_stats": (i32, [vp, C.POINTER(ServeStats)]),
         "gpulsm_server_reset_stats": (i32, [vp]),
+        "gpulsm_server_set_staged_updates": (i32, [vp, C.c_int]),
         "gpulsm_server_run_load": (i32, [vp, C.POINTER(LoadSpec), C.POINTER(ServeStats)]),
         "gpulsm_server_resident_bytes": (i32, [vp, C.POINTER(u64)]),
         "gpulsm_model_bytes": (u64, [u32]),

@@ -670,6 +670,13 @@ int gpulsm_server_stats(gpulsm_server *server, gpulsm_serve_stats *out) {
   });
 }
 
+int gpulsm_server_set_staged_updates(gpulsm_server *server, int staged) {
+  return guarded([&] {
+    need(server, "server");
+    server->impl.set_staged_updates(staged != 0);
+  });
+}
+
 int gpulsm_server_reset_stats(gpulsm_server *server) {
   return guarded([&] {
     need(server, "server");

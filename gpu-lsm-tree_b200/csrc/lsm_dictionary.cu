@@ -1264,12 +1264,21 @@ void LsmDictionary::flush_staged_locked(cudaStream_t s) {
     apply_receipt(true);  // stale bounds: wait for the exact counts before planning more storage
     reject_if_failed();
   }
-  // oldest first, each staged run is carried into the levels like an admitted
-  // batch (the cascade reads it and leaves the buffer with its slot)
-  for (size_t i = st.size(); i-- > 0;) {
-    Staged *y = st[i];
-    cascade(y->run, y->upper, y->tombs, s, true, false);
-    receipt_posted();
+  // the staged runs, newest first, merge into one run (small merges, in L2),
+  // which is carried into the levels like one admitted batch: level 0 is
+  // rewritten once per flush instead of once per staged run.  A lone staged
+  // run is carried as it is (the cascade reads it and leaves it with its slot).
+  RunBuffer *x = st[0]->run;
+  uint64_t xu = st[0]->upper;
+  bool xt = st[0]->tombs;
+  for (size_t i = 1; i < st.size(); ++i) {
+    x = merge(x, st[i]->run, xu + st[i]->upper, false, s, nullptr, i > 1, false);
+    xu += st[i]->upper;
+    xt = xt || st[i]->tombs;
+  }
+  cascade(x, xu, xt, s, true, st.size() > 1);
+  receipt_posted();
+  for (Staged *y : st) {
     y->seq = 0;
     y->upper = 0;
     y->tombs = false;

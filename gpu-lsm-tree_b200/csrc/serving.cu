@@ -70,7 +70,7 @@ Server::Server(const DictConfig &cfg, uint64_t budget_bytes, uint32_t max_round_
   if (max_round_keys_ <= (1u << 20)) {
     dict_.stage_configure(4, max_round_keys_, compute_);
     GPULSM_CUDA(cudaStreamSynchronize(compute_));
-    staged_updates_ = true;
+    stage_ready_ = staged_updates_ = true;
   }
   worker_ = std::thread(&Server::worker, this);
   completer_ = std::thread(&Server::completer, this);
@@ -154,6 +154,17 @@ int Server::wait(uint64_t ticket) {
 void Server::drain() {
   std::unique_lock<std::mutex> lk(mu_);
   cv_done_.wait(lk, [&] { return queue_.empty() && inflight_.empty() && free_slots_.size() == slots_.size(); });
+}
+
+void Server::set_staged_updates(bool on) {
+  drain();
+  std::lock_guard<std::mutex> g(mu_);  // the worker forms no round while this is held
+  if (on && !stage_ready_) throw std::invalid_argument("staged updates need max_round_keys <= 2^20");
+  if (!on && staged_updates_) {
+    dict_.stage_flush(compute_);
+    GPULSM_CUDA(cudaStreamSynchronize(compute_));
+  }
+  staged_updates_ = on;
 }
 
 void Server::reset_stats() {

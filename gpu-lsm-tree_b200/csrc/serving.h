@@ -87,6 +87,8 @@ class Server {
   ServeStats stats();
   void reset_stats();
   void run_load(const LoadSpec &spec, ServeStats *out);
+  // staged (graph-replayed) or direct update runs; waits for the requests in flight
+  void set_staged_updates(bool on);
   LsmDictionary &dict() { return dict_; }
   uint64_t device_bytes() const { return slot_bytes_ * slots_.size(); }
 
@@ -164,6 +166,7 @@ class Server {
   // staged updates: update runs replayed from captured graphs (admission only;
   // the staged runs merge into the levels when the staging slots are full)
   bool staged_updates_ = false;
+  bool stage_ready_ = false;  // the dictionary's staging slots are configured
   std::vector<std::pair<uint64_t, cudaGraphExec_t>> update_graphs_;  // key: tomb | class << 1 | stage << 40
   uint64_t st_graph_updates_ = 0;
 

@@ -57,6 +57,10 @@ class Server:
         except Exception:
             pass
 
+    def set_staged_updates(self, staged: bool) -> None:
+        """Staged (graph-replayed admission, merges deferred) or direct update runs."""
+        N.check(self._lib.gpulsm_server_set_staged_updates(self._h, int(bool(staged))))
+
     def bulk_build(self, keys, values, stream=None):
         """Preload from device tensors (torch), as GPULSMOpt.bulk_build."""
         from .dictionary import _ptr, _stream
