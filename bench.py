@@ -603,10 +603,11 @@ def serving_leg(args, gl, w, dev):
     keys = np.concatenate([o[1] for o in w.ops if o[0] == "insert"])
     secs = args.serving_seconds
     out = {"dictionary_keys": int(keys.size), "budget_gb": 16}
-    # plain / learned: search modes of the levels, update runs staged (admitted by
-    # captured graphs, merged when the staging slots fill); plain_direct: update
-    # runs admitted and merged at once, each round waiting for its merges
-    for name, mode, staged in (("plain", 0, True), ("learned", 1, True), ("plain_direct", 0, False)):
+    # plain / learned: search modes of the levels, update runs direct (admitted
+    # and merged at once, the round waiting for its merges); plain_staged:
+    # update runs admitted into staging runs by captured CUDA graphs and merged
+    # into the levels when the staging slots fill
+    for name, mode, staged in (("plain", 0, False), ("learned", 1, False), ("plain_staged", 0, True)):
         # serving requests are small: a small level 0 (2^17 rows, fan-in 4) keeps
         # a run's merge proportional to the run instead of to a 4M-row level
         srv = gl.Server(gl.DictionaryConfig(max_elements=keys.size + w.erased_keys + (1 << 24), search_mode=mode,

@@ -67,10 +67,12 @@ Server::Server(const DictConfig &cfg, uint64_t budget_bytes, uint32_t max_round_
   }
   // staged updates: update runs are admitted into fixed staging runs by
   // captured graphs; 4 staging slots (fewer when the level schedule is deep)
+  // (staged update runs are off by default: on the serving mix they lowered
+  // peak throughput, see set_staged_updates)
   if (max_round_keys_ <= (1u << 20)) {
     dict_.stage_configure(4, max_round_keys_, compute_);
     GPULSM_CUDA(cudaStreamSynchronize(compute_));
-    stage_ready_ = staged_updates_ = true;
+    stage_ready_ = true;
   }
   worker_ = std::thread(&Server::worker, this);
   completer_ = std::thread(&Server::completer, this);

@@ -287,14 +287,15 @@ int gpulsm_server_stats(gpulsm_server *server, gpulsm_serve_stats *out);
 int gpulsm_server_reset_stats(gpulsm_server *server);
 int gpulsm_server_run_load(gpulsm_server *server, const gpulsm_load_spec *spec, gpulsm_serve_stats *out);
 int gpulsm_server_resident_bytes(gpulsm_server *server, uint64_t *out_bytes);
-/* How update requests run (no reference counterpart).  1 (the default):
- * staged - each update run is admitted into a staging run by one replay of a
- * captured CUDA graph and completes without waiting for merges; the staged
- * runs are the newest levels of point reads and range sums and merge into the
- * levels when the staging slots are full (or before a non-graph update, a
- * range count or a build).  0: direct - each update run is admitted and
- * merged at once and its round waits for the merges.  Waits for the requests
- * in flight; switching to direct merges the staged runs first. */
+/* How update requests run (no reference counterpart).  0 (the default):
+ * direct - each update run is admitted and merged at once and its round waits
+ * for the merges.  1: staged - each update run is admitted into a staging run
+ * by one replay of a captured CUDA graph and completes without waiting for
+ * merges; the staged runs are the newest levels of point reads and range sums
+ * and merge into the levels when the staging slots are full (or before a
+ * non-graph update, a range count or a build).  Staged needs max_round_keys
+ * <= 2^20.  Waits for the requests in flight; switching to direct merges the
+ * staged runs first. */
 int gpulsm_server_set_staged_updates(gpulsm_server *server, int staged);
 
 /* ===================== learned position model ============================ */

@@ -47,9 +47,10 @@ def submit(srv, req):
     return srv.submit_range_sum(keys, aux)
 
 
-def fresh_server(gl, base_k, base_v):
+def fresh_server(gl, base_k, base_v, staged=False):
     srv = gl.Server(gl.DictionaryConfig(max_elements=1 << 20, batch_capacity=1 << 16), budget_bytes=4 << 30,
                     max_round_keys=1 << 16, depth=3)
+    srv.set_staged_updates(staged)
     srv.bulk_build(to_dev(base_k), to_dev(base_v))
     return srv
 
@@ -80,7 +81,8 @@ def same(a, b):
     return np.array_equal(a, b)
 
 
-def test_results_same_alone_and_in_mix(gl, cuda):
+@pytest.mark.parametrize("staged", [False, True], ids=["direct", "staged"])
+def test_results_same_alone_and_in_mix(gl, cuda, staged):
     rng = np.random.default_rng(11)
     base_k = rng.integers(0, 1 << 32, 1 << 16, dtype=np.uint64).astype(np.uint32)
     base_v = np.arange(base_k.size, dtype=np.uint32)
@@ -88,7 +90,7 @@ def test_results_same_alone_and_in_mix(gl, cuda):
     per_thread = [make_requests(np.random.default_rng(100 + t), universe, 60) for t in range(4)]
 
     # in the mix: four threads submit at once, nothing waits until all are in
-    srv = fresh_server(gl, base_k, base_v)
+    srv = fresh_server(gl, base_k, base_v, staged)
     submitted = [[] for _ in range(4)]
 
     def client(t):
@@ -109,7 +111,7 @@ def test_results_same_alone_and_in_mix(gl, cuda):
 
     # alone: one request at a time, in the order the server assigned
     ordered = [req for _, _, req in flat]
-    srv = fresh_server(gl, base_k, base_v)
+    srv = fresh_server(gl, base_k, base_v, staged)
     alone = [srv.wait(submit(srv, req)) for req in ordered]
     # a lookup submitted alone is a lookup-only round: replayed from a CUDA graph;
     # an update submitted alone is one staged admission replayed from a graph,
@@ -117,8 +119,11 @@ def test_results_same_alone_and_in_mix(gl, cuda):
     st = srv.stats()
     assert st["graph_rounds"] == sum(1 for r in ordered if r[0] == "lookup")
     n_updates = sum(1 for r in ordered if r[0] in ("insert", "erase"))
-    assert st["graph_updates"] == n_updates
-    assert st["stage_flushes"] >= 1 and st["stage_flushes"] >= n_updates // 4 - 1
+    if staged:
+        assert st["graph_updates"] == n_updates
+        assert st["stage_flushes"] >= 1 and st["stage_flushes"] >= n_updates // 4 - 1
+    else:
+        assert st["graph_updates"] == 0 and st["stage_flushes"] == 0
     srv.close()
 
     want = oracle_answers(base_k, base_v, ordered)
@@ -167,7 +172,7 @@ def test_staged_updates_merge_into_levels_and_stay_exact(gl, cuda):
     base_k = rng.integers(0, 1 << 32, 1 << 15, dtype=np.uint64).astype(np.uint32)
     base_v = np.arange(base_k.size, dtype=np.uint32)
     universe = np.concatenate([base_k, rng.integers(0, 1 << 32, 1 << 13, dtype=np.uint64).astype(np.uint32)])
-    srv = fresh_server(gl, base_k, base_v)
+    srv = fresh_server(gl, base_k, base_v, staged=True)
     o = OracleLSM()
     o.bulk_build(base_k, base_v)
     for step in range(40):
