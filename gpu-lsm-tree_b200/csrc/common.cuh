@@ -192,10 +192,10 @@ __device__ __forceinline__ T block_exclusive_scan(T value, T *warp_sums, T *tota
 }
 // Decoupled look-back over per-tile counts (u64: flag in the top two bits,
 // 62-bit value).  Tile ids come from an atomic ticket, so every predecessor
-// is resident or done.  Run by one full warp: each round trip reads 32
+// is resident or done.  Run by one full warp: each round trip reads 32 * kPer
 // predecessors, so the walk to the nearest inclusive prefix takes
-// distance / 32 dependent loads instead of distance.  Returns the exclusive
-// prefix on every lane; lb[] must be zeroed before the launch.
+// distance / (32 * kPer) dependent loads instead of distance.  Returns the
+// exclusive prefix on every lane; lb[] must be zeroed before the launch.
 constexpr unsigned long long kLbAgg = 1ull << 62;
 constexpr unsigned long long kLbInc = 2ull << 62;
 constexpr unsigned long long kLbMask = (1ull << 62) - 1ull;
@@ -207,18 +207,35 @@ __device__ __forceinline__ void lookback_publish(unsigned long long *lb, uint32_
 
 // Walk back from a tile whose count is published; run by one full warp.
 // Returns the exclusive prefix on every lane and publishes the inclusive one.
+// A round trip reads the window of 32 * kPer predecessors; only the slots
+// after the newest inclusive prefix in it must be published for it to count.
+template <int kPer = 1>
 __device__ __forceinline__ unsigned long long lookback_walk(unsigned long long *lb, uint32_t tile,
                                                             unsigned long long agg, uint32_t *status) {
+  constexpr int kWin = 32 * kPer;  // predecessors per round trip
   const uint32_t lane = threadIdx.x & 31u;
   if (tile == 0) return 0ull;
   unsigned long long excl = 0;
-  int64_t end = int64_t(tile);  // window [end - 32, end); slots before tile 0 read as inclusive 0
+  int64_t end = int64_t(tile);  // window [end - kWin, end); slots before tile 0 read as inclusive 0
   uint32_t spins = 0;
   while (true) {
-    const int64_t t = end - 32 + int64_t(lane);
-    const unsigned long long v = t >= 0 ? ld_relaxed_u64(lb + t) : kLbInc;
-    const unsigned long long flag = v & ~kLbMask;
-    if (__any_sync(0xffffffffu, flag == 0ull)) {
+    const int64_t t0 = end - kWin + int64_t(lane) * kPer;
+    unsigned long long v[kPer];
+    int my_inc = -1, my_pend = -1;  // this lane's newest inclusive / unpublished window position
+#pragma unroll
+    for (int q = 0; q < kPer; ++q) {
+      v[q] = t0 + q >= 0 ? ld_relaxed_u64(lb + t0 + q) : kLbInc;
+      const unsigned long long f = v[q] & ~kLbMask;
+      if (f == kLbInc) my_inc = int(lane) * kPer + q;
+      if (f == 0ull) my_pend = int(lane) * kPer + q;
+    }
+    int inc = my_inc, pend = my_pend;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+      inc = max(inc, __shfl_xor_sync(0xffffffffu, inc, o));
+      pend = max(pend, __shfl_xor_sync(0xffffffffu, pend, o));
+    }
+    if (pend > inc) {  // a slot after the newest inclusive prefix is not published yet
       if (++spins > kMaxSpins) {
         if (lane == 0) atomicOr(status, kDevWaitTimeout);
         break;
@@ -226,15 +243,17 @@ __device__ __forceinline__ unsigned long long lookback_walk(unsigned long long *
       __nanosleep(32);
       continue;
     }
-    // a published inclusive prefix implies every earlier slot is published
-    const uint32_t inc = __ballot_sync(0xffffffffu, flag == kLbInc);
-    const int hi = inc ? 31 - __clz(int(inc)) : 0;
-    unsigned long long s = int(lane) >= hi ? (v & kLbMask) : 0ull;
+    // sum from the newest inclusive slot (or the window's start) to its end
+    const int lo = inc >= 0 ? inc : 0;
+    unsigned long long s = 0;
+#pragma unroll
+    for (int q = 0; q < kPer; ++q)
+      if (int(lane) * kPer + q >= lo) s += v[q] & kLbMask;
 #pragma unroll
     for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     excl += s;
-    if (inc) break;
-    end -= 32;
+    if (inc >= 0) break;
+    end -= kWin;
   }
   if (lane == 0) st_relaxed_u64(lb + tile, kLbInc | (excl + agg));
   return excl;
