@@ -184,6 +184,7 @@ def load() -> C.CDLL:
         "gpulsm_dict_bulk_build": (i32, [vp, vp, vp, u64, vp]),
         "gpulsm_dict_insert": (i32, [vp, vp, vp, u64, vp]),
         "gpulsm_dict_erase": (i32, [vp, vp, u64, vp]),
+        "gpulsm_dict_update": (i32, [vp, vp, vp, vp, u64, vp]),
         "gpulsm_dict_lookup": (i32, [vp, vp, u64, vp, vp, vp]),
         "gpulsm_dict_range_sum": (i32, [vp, vp, vp, u64, vp, vp]),
         "gpulsm_dict_range_count": (i32, [vp, vp, vp, u64, vp, vp]),
@@ -229,6 +230,7 @@ def load() -> C.CDLL:
         "gpulsm_server_submit": (i32, [vp, u32, vp, vp, u64, vp, vp, C.POINTER(u64)]),
         "gpulsm_server_poll": (i32, [vp, u64, C.POINTER(C.c_int32)]),
         "gpulsm_server_wait": (i32, [vp, u64, C.POINTER(C.c_int32)]),
+        "gpulsm_server_wait_round": (i32, [vp, u64, C.POINTER(C.c_int32), C.POINTER(u64)]),
         "gpulsm_server_drain": (i32, [vp]),
         "gpulsm_server_stats": (i32, [vp, C.POINTER(ServeStats)]),
         "gpulsm_server_reset_stats": (i32, [vp]),

@@ -210,6 +210,15 @@ int gpulsm_dict_erase(gpulsm_dict *d, const uint32_t *keys, uint64_t count, void
   });
 }
 
+int gpulsm_dict_update(gpulsm_dict *d, const uint32_t *keys, const uint32_t *values, const uint8_t *erase,
+                       uint64_t count, void *stream) {
+  return guarded([&] {
+    need(d, "dict");
+    device_accessible({{keys, "keys"}, {values, "values"}, {erase, "erase"}});
+    d->impl.update(keys, values, erase, count, S(stream));
+  });
+}
+
 int gpulsm_dict_lookup(gpulsm_dict *d, const uint32_t *queries, uint64_t count,
                        uint32_t *out_values, uint8_t *out_found, void *stream) {
   return guarded([&] {
@@ -652,6 +661,15 @@ int gpulsm_server_wait(gpulsm_server *server, uint64_t ticket, int32_t *out_stat
     need(server, "server");
     need(out_state, "out_state");
     *out_state = server->impl.wait(ticket);
+  });
+}
+
+int gpulsm_server_wait_round(gpulsm_server *server, uint64_t ticket, int32_t *out_state, uint64_t *out_round) {
+  return guarded([&] {
+    need(server, "server");
+    need(out_state, "out_state");
+    need(out_round, "out_round");
+    *out_state = server->impl.wait(ticket, out_round);
   });
 }
 

@@ -6,7 +6,9 @@
 //   1. part_hist_kernel     per 2048-key tile, the counts of the key's top byte
 //   2. part_scan_kernel     per top byte, the exclusive scan over the tiles
 //   3. part_scatter_kernel  words (key << 32 | value) written to their top-byte
-//                           bucket in input order (a stable partition)
+//                           bucket in input order (a stable partition); a
+//                           batch of inserts and erases packs the input
+//                           position instead of the value
 //   4. admit_bucket_kernel  one CTA per top-byte bucket, in bucket order:
 //                           sorts the bucket by (key, input position) in
 //                           shared memory (a 12-bit counting sort plus an
@@ -112,6 +114,28 @@ __device__ __forceinline__ void load_striped(const unsigned long long *src, uint
   }
 }
 
+// Where a kept row's value and flag come from.  Insert and erase batches
+// packed the value into the sort word (erase: the tombstone value); a mixed
+// batch packed the row's input position instead, and the row reads its value
+// and its erase mark from the batch by that position.
+struct RowSource {
+  const uint32_t *vals;  // mixed batches: the batch's values (erased rows ignore theirs)
+  const uint8_t *erase;  // mixed batches: nonzero = the row erases its key; null otherwise
+  int tombstone;         // erase batches
+};
+
+__device__ __forceinline__ void resolve_row(const RowSource &src, unsigned long long w, uint32_t &v, uint8_t &f) {
+  if (src.erase) {
+    const uint32_t i = uint32_t(w);
+    const bool er = src.erase[i] != 0;
+    v = er ? kTombValue : src.vals[i];
+    f = er ? kFlagTomb : uint8_t(0);
+  } else {
+    v = uint32_t(w);
+    f = src.tombstone ? kFlagTomb : uint8_t(0);
+  }
+}
+
 // at(j): the j-th word of a sorted sequence (an array, or an index into one)
 template <typename At>
 __device__ __forceinline__ bool run_end(const At &at, uint32_t j, uint32_t cnt) {
@@ -136,7 +160,7 @@ __device__ __forceinline__ uint32_t count_distinct(const At &at, uint32_t cnt, R
 // buckets after the bucket of the previous distinct key (bp before the first
 // row) up to its own, pointing at the row (= run ends before the element).
 template <typename At>
-__device__ __forceinline__ void write_rows(const At &at, uint32_t cnt, int tombstone, uint32_t *out_keys,
+__device__ __forceinline__ void write_rows(const At &at, uint32_t cnt, const RowSource &src, uint32_t *out_keys,
                                            uint32_t *out_vals, uint8_t *out_flags, unsigned long long g0,
                                            RankSmem &rs, uint32_t *__restrict__ dir, const DirGeom &g,
                                            int64_t bp) {
@@ -169,9 +193,12 @@ __device__ __forceinline__ void write_rows(const At &at, uint32_t cnt, int tombs
       const unsigned long long w64 = at(e);
       const uint32_t k = word_key(w64);
       if ((ends[i] >> lane) & 1u) {
+        uint32_t v;
+        uint8_t f;
+        resolve_row(src, w64, v, f);
         out_keys[r] = k;
-        out_vals[r] = uint32_t(w64);  // the tombstone value was packed for erase batches
-        out_flags[r] = tombstone ? kFlagTomb : uint8_t(0);
+        out_vals[r] = v;
+        out_flags[r] = f;
       }
       // the first element of a run writes the directory entries its row starts
       const uint32_t kp = e > 0 ? word_key(at(e - 1)) : 0u;
@@ -323,7 +350,8 @@ __global__ void __launch_bounds__(kPartThreads) part_scan_kernel(const uint32_t 
 
 __global__ void __launch_bounds__(kPartThreads) part_scatter_kernel(
     const uint32_t *__restrict__ keys, const uint32_t *__restrict__ vals, uint32_t n, uint32_t tiles,
-    const uint32_t *__restrict__ prefix, const uint32_t *__restrict__ total, unsigned long long *__restrict__ out) {
+    const uint32_t *__restrict__ prefix, const uint32_t *__restrict__ total, unsigned long long *__restrict__ out,
+    int pack_index) {
   __shared__ unsigned long long s_words[kPartTile];
   __shared__ uint32_t warp_hist[kPartWarps][256];
   __shared__ uint32_t s_start[256];   // first staged position of each byte in the tile
@@ -343,7 +371,8 @@ __global__ void __launch_bounds__(kPartThreads) part_scatter_kernel(
     const uint32_t e = wbase + uint32_t(i) * 32u + lane;
     const bool valid = e < n;
     const uint32_t k = valid ? keys[e] : 0u;
-    w[i] = (static_cast<unsigned long long>(k) << 32) | (vals ? (valid ? vals[e] : 0u) : kTombValue);
+    const uint32_t v = pack_index ? e : vals ? (valid ? vals[e] : 0u) : kTombValue;
+    w[i] = (static_cast<unsigned long long>(k) << 32) | v;
     d[i] = valid ? (k >> 24) : 256u;
   }
   const uint32_t tot = total[threadIdx.x];
@@ -516,7 +545,7 @@ constexpr size_t kBucketSmemBytes = sizeof(BucketSmem);
 // same size for oversized buckets; top_hist: rows per top byte.
 __global__ void __launch_bounds__(kThreads, 2) admit_bucket_kernel(
     unsigned long long *__restrict__ words0, unsigned long long *__restrict__ words1,
-    const uint32_t *__restrict__ top_hist, uint32_t n, int tombstone, uint32_t *__restrict__ out_keys,
+    const uint32_t *__restrict__ top_hist, uint32_t n, RowSource src, uint32_t *__restrict__ out_keys,
     uint32_t *__restrict__ out_vals, uint8_t *__restrict__ out_flags, LevelDesc *__restrict__ out_desc,
     uint32_t *__restrict__ out_dir, uint32_t dir_bits, uint32_t rows_log2, unsigned long long *__restrict__ lb,
     uint32_t *__restrict__ tile_counter, uint32_t *__restrict__ status) {
@@ -642,9 +671,12 @@ __global__ void __launch_bounds__(kThreads, 2) admit_bucket_kernel(
       const unsigned long long w64 = w[e];
       const uint32_t k = word_key(w64);
       if ((ends[i] >> lane) & 1u) {
+        uint32_t v;
+        uint8_t f;
+        resolve_row(src, w64, v, f);
         out_keys[r] = k;
-        out_vals[r] = uint32_t(w64);  // the tombstone value was packed for erase batches
-        out_flags[r] = tombstone ? kFlagTomb : uint8_t(0);
+        out_vals[r] = v;
+        out_flags[r] = f;
       }
       // the first element of a run writes the directory entries its row starts
       const uint32_t kp = e > 0 ? word_key(w[e - 1]) : 0u;
@@ -663,7 +695,7 @@ __global__ void __launch_bounds__(kThreads, 2) admit_bucket_kernel(
       atomicOr(status, kDevWaitTimeout);
       return;
     }
-    write_rows(by_array, cnt, tombstone, out_keys, out_vals, out_flags, g0, sm.rank, out_dir, g, int64_t(bp));
+    write_rows(by_array, cnt, src, out_keys, out_vals, out_flags, g0, sm.rank, out_dir, g, int64_t(bp));
   }
   if (threadIdx.x == 0) {
     // an empty bucket between the first and the last one only closes its range

@@ -440,9 +440,12 @@ void LsmDictionary::release_levels(cudaStream_t s) {
 
 // ----------------------------------------------------------------------------
 RunBuffer *LsmDictionary::sort_dedup(const uint32_t *keys, const uint32_t *values, uint64_t n,
-                                     bool tombstone, cudaStream_t s) {
+                                     bool tombstone, cudaStream_t s, const uint8_t *erase) {
   ensure_sort_space(n, s);
-  if (n <= lsm::admit::kMaxKeys) return bucket_admit(keys, values, n, tombstone, s);
+  if (n <= lsm::admit::kMaxKeys) return bucket_admit(keys, values, erase, n, tombstone, s);
+  // update batches are tiled to at most kMaxBatch = 2^20 rows: only a bulk
+  // build (never mixed) takes the four-pass sort
+  if (erase) throw std::logic_error("mixed batches are admitted by top-byte buckets only");
   const uint32_t nn = uint32_t(n);
   const size_t radix_bytes = align_up(radix::workspace_bytes(n, 4));
   const uint64_t dtiles = (n + lsm::kCompactTile - 1) / lsm::kCompactTile;
@@ -476,19 +479,21 @@ size_t LsmDictionary::bucket_admit_scratch_bytes(uint64_t n) {
   return zero_bytes + 2 * align_up(size_t(tiles) * 256 * 4) + align_up(256 * 4);
 }
 
-RunBuffer *LsmDictionary::bucket_admit(const uint32_t *keys, const uint32_t *values, uint64_t n,
-                                       bool tombstone, cudaStream_t s) {
+RunBuffer *LsmDictionary::bucket_admit(const uint32_t *keys, const uint32_t *values, const uint8_t *erase,
+                                       uint64_t n, bool tombstone, cudaStream_t s) {
   void *scratch = admit_scratch(bucket_admit_scratch_bytes(n), s);
   // before the chain: a fresh buffer is a stream-ordered allocation
   RunBuffer *carry = pool_.acquire(n, s, true);
-  bucket_admit_into(keys, values, n, tombstone, s, carry, words_[0], words_[1], scratch);
+  bucket_admit_into(keys, values, erase, n, tombstone, s, carry, words_[0], words_[1], scratch);
   return carry;
 }
 
-// The four admission launches into `carry`, with the given sort words and scratch.
-void LsmDictionary::bucket_admit_into(const uint32_t *keys, const uint32_t *values, uint64_t n, bool tombstone,
-                                      cudaStream_t s, RunBuffer *carry, unsigned long long *w0,
-                                      unsigned long long *w1, void *scratch) {
+// The four admission launches into `carry`, with the given sort words and
+// scratch.  A mixed batch (erase marks given) sorts words of (key, input
+// position); its rows take value and flag from the batch by that position.
+void LsmDictionary::bucket_admit_into(const uint32_t *keys, const uint32_t *values, const uint8_t *erase,
+                                      uint64_t n, bool tombstone, cudaStream_t s, RunBuffer *carry,
+                                      unsigned long long *w0, unsigned long long *w1, void *scratch) {
   namespace ad = lsm::admit;
   const uint32_t nn = uint32_t(n);
   const uint32_t tiles = ad::part_tiles(n);
@@ -503,11 +508,14 @@ void LsmDictionary::bucket_admit_into(const uint32_t *keys, const uint32_t *valu
   launch_chained(ad::part_hist_kernel, tiles, ad::kPartThreads, 0, s, keys, nn, tiles, cnt, zero,
                  uint32_t(zero_bytes / 8));
   launch_chained(ad::part_scan_kernel, 256, ad::kPartThreads, 0, s, cnt, tiles, prefix, top);
-  launch_chained(ad::part_scatter_kernel, tiles, ad::kPartThreads, 0, s, keys, tombstone ? nullptr : values, nn,
-                 tiles, static_cast<const uint32_t *>(prefix), static_cast<const uint32_t *>(top), w1);
+  const bool mixed = erase != nullptr;
+  launch_chained(ad::part_scatter_kernel, tiles, ad::kPartThreads, 0, s, keys,
+                 (tombstone || mixed) ? nullptr : values, nn, tiles, static_cast<const uint32_t *>(prefix),
+                 static_cast<const uint32_t *>(top), w1, mixed ? 1 : 0);
+  const ad::RowSource src{mixed ? values : nullptr, erase, tombstone ? 1 : 0};
   launch_chained(ad::admit_bucket_kernel, ad::kBuckets, ad::kThreads, ad::kBucketSmemBytes, s, w1, w0,
-                 static_cast<const uint32_t *>(top), nn, tombstone ? 1 : 0, carry->keys, carry->vals, carry->flags,
-                 carry->desc, carry->dir, carry->dir_bits, rows_log2_, lb, counter, dev_status_);
+                 static_cast<const uint32_t *>(top), nn, src, carry->keys, carry->vals, carry->flags, carry->desc,
+                 carry->dir, carry->dir_bits, rows_log2_, lb, counter, dev_status_);
 }
 
 RunBuffer *LsmDictionary::merge(RunBuffer *newer, RunBuffer *older, uint64_t out_upper,
@@ -810,8 +818,8 @@ void LsmDictionary::refresh_live_prefix(LivePrefix &lp, RunBuffer *run, uint64_t
   }
 }
 
-void LsmDictionary::admit(const uint32_t *keys, const uint32_t *values, uint64_t n, bool tombstone,
-                          cudaStream_t s) {
+void LsmDictionary::admit(const uint32_t *keys, const uint32_t *values, const uint8_t *erase, uint64_t n,
+                          bool tombstone, cudaStream_t s) {
   for (uint64_t off = 0; off < n; off += batch_capacity_) {
     const uint64_t m = std::min(batch_capacity_, n - off);
     uint64_t total_upper = m;
@@ -826,12 +834,13 @@ void LsmDictionary::admit(const uint32_t *keys, const uint32_t *values, uint64_t
     // the previous batch's merges, while s goes on to admit the next batch.
     // The receipt comes from the merge stream (the final merge, or a receipt
     // kernel when nothing merges), so receipts land in batch order.
-    RunBuffer *carry = sort_dedup(keys + off, values ? values + off : nullptr, m, tombstone, s);
+    RunBuffer *carry = sort_dedup(keys + off, values ? values + off : nullptr, m, tombstone, s,
+                                  erase ? erase + off : nullptr);
     GPULSM_CUDA(cudaEventRecord(adm_done_, s));
     GPULSM_CUDA(cudaStreamWaitEvent(merge_stream_, adm_done_, 0));
     merges_pending_ = true;
     try {
-      cascade(carry, m, tombstone, merge_stream_, true);
+      cascade(carry, m, tombstone || erase, merge_stream_, true);
     } catch (...) {  // reads still wait for whatever the cascade enqueued
       cudaEventRecord(merge_done_, merge_stream_);
       throw;
@@ -905,7 +914,7 @@ void LsmDictionary::insert(const uint32_t *keys, const uint32_t *values, uint64_
     begin_op(s);
     flush_staged_locked(s);
   }
-  admit(keys, values, n, false, s);  // every batch's finishing kernel writes the receipt
+  admit(keys, values, nullptr, n, false, s);  // every batch's finishing kernel writes the receipt
   end_op(s);
 }
 
@@ -921,7 +930,24 @@ void LsmDictionary::erase(const uint32_t *keys, uint64_t n, cudaStream_t s) {
     begin_op(s);
     flush_staged_locked(s);
   }
-  admit(keys, nullptr, n, true, s);  // every batch's finishing kernel writes the receipt
+  admit(keys, nullptr, nullptr, n, true, s);  // every batch's finishing kernel writes the receipt
+  end_op(s);
+}
+
+void LsmDictionary::update(const uint32_t *keys, const uint32_t *values, const uint8_t *erase, uint64_t n,
+                           cudaStream_t s) {
+  std::lock_guard<std::mutex> g(mu_);
+  if (!n) return;
+  if (!keys || !values || !erase) throw std::invalid_argument("invalid GPU dictionary update batch");
+  refuse_capture(s);
+  apply_receipt(false);
+  reject_if_failed();
+  begin_op(s, true);
+  if (stage_seq_pending()) {  // staged runs are older than this batch: they land first
+    begin_op(s);
+    flush_staged_locked(s);
+  }
+  admit(keys, values, erase, n, false, s);  // every batch's finishing kernel writes the receipt
   end_op(s);
 }
 
@@ -1181,7 +1207,7 @@ void LsmDictionary::kernel_timing(uint64_t *launches, double *total_ms, double *
 
 uint64_t LsmDictionary::resident_bytes() {
   std::lock_guard<std::mutex> g(mu_);
-  const uint64_t staging = stage_max_ ? stage_max_ * (8 + 16) + bucket_admit_scratch_bytes(stage_max_) : 0;
+  const uint64_t staging = stage_max_ ? stage_max_ * (9 + 16) + bucket_admit_scratch_bytes(stage_max_) : 0;
   return pool_.bytes() + words_cap_ * 16 + scratch_bytes_ + ascratch_bytes_ + live_bytes_ + sizeof(Receipt) + 256 +
          staging;
 }
@@ -1198,7 +1224,7 @@ void LsmDictionary::stage_configure(uint32_t slots, uint64_t max_keys, cudaStrea
   if (slots == 0) throw std::invalid_argument("no room for staged levels beside the level schedule");
   begin_op(s);
   stage_max_ = max_keys;
-  GPULSM_CUDA(cudaMalloc(&stage_in_, 2 * max_keys * 4));
+  GPULSM_CUDA(cudaMalloc(&stage_in_, 2 * max_keys * 4 + max_keys));  // keys, values, erase marks
   for (auto &w : stage_words_) GPULSM_CUDA(cudaMalloc(&w, max_keys * 8));
   GPULSM_CUDA(cudaMalloc(&stage_scratch_, bucket_admit_scratch_bytes(max_keys)));
   staged_.resize(slots);
@@ -1213,16 +1239,19 @@ int LsmDictionary::stage_free_slot() const {
   return -1;
 }
 
-void LsmDictionary::enqueue_stage_admit(uint32_t slot, uint64_t n, bool tombstone, cudaStream_t capturing) {
+void LsmDictionary::enqueue_stage_admit(uint32_t slot, uint64_t n, int mode, cudaStream_t capturing) {
   std::lock_guard<std::mutex> g(mu_);
   if (slot >= staged_.size()) throw std::invalid_argument("no such staging slot");
   if (n == 0 || n > stage_max_) throw std::length_error("staged update larger than the staging runs");
-  bucket_admit_into(stage_in_, tombstone ? nullptr : stage_in_ + n, n, tombstone, capturing, staged_[slot].run,
+  if (mode < kStageInsert || mode > kStageMixed) throw std::invalid_argument("unknown staged update mode");
+  const bool tombstone = mode == kStageErase;
+  const uint8_t *erase = mode == kStageMixed ? reinterpret_cast<const uint8_t *>(stage_in_ + 2 * n) : nullptr;
+  bucket_admit_into(stage_in_, tombstone ? nullptr : stage_in_ + n, erase, n, tombstone, capturing, staged_[slot].run,
                     stage_words_[0], stage_words_[1], stage_scratch_);
   GPULSM_CUDA(cudaGetLastError());
 }
 
-void LsmDictionary::launch_stage_graph(cudaGraphExec_t exec, uint32_t slot, uint64_t n, bool tombstone,
+void LsmDictionary::launch_stage_graph(cudaGraphExec_t exec, uint32_t slot, uint64_t n, bool tombs,
                                        cudaStream_t s) {
   std::lock_guard<std::mutex> g(mu_);
   if (slot >= staged_.size() || staged_[slot].seq) throw std::invalid_argument("staging slot is not free");
@@ -1234,7 +1263,7 @@ void LsmDictionary::launch_stage_graph(cudaGraphExec_t exec, uint32_t slot, uint
   Staged &x = staged_[slot];
   x.upper = n;
   x.seq = ++stage_seq_;
-  x.tombs = tombstone;
+  x.tombs = tombs;
   ++next_gen_;  // the level set changed (device level table, live prefixes)
   end_op(s);
 }

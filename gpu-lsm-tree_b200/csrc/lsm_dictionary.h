@@ -20,6 +20,9 @@ struct ReceiptSrc;
 struct LevelView;
 }
 
+// Batches of a staged update (LsmDictionary::enqueue_stage_admit).
+enum StageMode : int { kStageInsert = 0, kStageErase = 1, kStageMixed = 2 };
+
 struct DictConfig {
   uint64_t max_elements = 0;
   uint64_t batch_capacity = 0;
@@ -88,6 +91,10 @@ class LsmDictionary {
   void bulk_build(const uint32_t *keys, const uint32_t *values, uint64_t n, cudaStream_t s);
   void insert(const uint32_t *keys, const uint32_t *values, uint64_t n, cudaStream_t s);
   void erase(const uint32_t *keys, uint64_t n, cudaStream_t s);
+  // One batch of inserts and erases: row i erases keys[i] when erase[i] is
+  // nonzero, else inserts (keys[i], values[i]); the last row of a key wins,
+  // as in an insert or erase batch.
+  void update(const uint32_t *keys, const uint32_t *values, const uint8_t *erase, uint64_t n, cudaStream_t s);
   void lookup(const uint32_t *queries, uint64_t n, uint32_t *out_values, uint8_t *out_found,
               cudaStream_t s);
   void range_sum(const uint32_t *lo, const uint32_t *hi, uint64_t n, uint32_t *out, cudaStream_t s);
@@ -136,13 +143,15 @@ class LsmDictionary {
   void stage_configure(uint32_t slots, uint64_t max_keys, cudaStream_t s);
   // a free staging slot, or -1 when every slot holds a run
   int stage_free_slot() const;
-  // records the admission of slot `slot` into a capturing stream: keys (and
-  // values, for inserts) are read from stage_input()
-  void enqueue_stage_admit(uint32_t slot, uint64_t n, bool tombstone, cudaStream_t capturing);
-  // the device buffer a staged graph reads: keys at [0, n), values at [n, 2n)
+  // records the admission of slot `slot` into a capturing stream; `mode` is
+  // kStageInsert, kStageErase or kStageMixed, and the batch is read from
+  // stage_input(): keys at words [0, n), values (insert, mixed) at words
+  // [n, 2n), erase marks (mixed) as bytes from word 2n on
+  void enqueue_stage_admit(uint32_t slot, uint64_t n, int mode, cudaStream_t capturing);
   uint32_t *stage_input() const { return stage_in_; }
-  // launches a captured staged-update graph, ordered like an update
-  void launch_stage_graph(cudaGraphExec_t exec, uint32_t slot, uint64_t n, bool tombstone, cudaStream_t s);
+  // launches a captured staged-update graph, ordered like an update; `tombs`:
+  // the batch may erase keys
+  void launch_stage_graph(cudaGraphExec_t exec, uint32_t slot, uint64_t n, bool tombs, cudaStream_t s);
   void stage_flush(cudaStream_t s);
   uint64_t stage_flushes() const { return stage_flushes_; }
 
@@ -167,15 +176,16 @@ class LsmDictionary {
   lsm::ReceiptSrc next_receipt(int dest);
   void receipt_posted();
   void reject_if_failed() const;
-  void admit(const uint32_t *keys, const uint32_t *values, uint64_t n, bool tombstone,
+  // erase: the erase marks of a mixed batch (null for insert / erase batches)
+  void admit(const uint32_t *keys, const uint32_t *values, const uint8_t *erase, uint64_t n, bool tombstone,
              cudaStream_t s);
   RunBuffer *sort_dedup(const uint32_t *keys, const uint32_t *values, uint64_t n, bool tombstone,
-                        cudaStream_t s);
-  RunBuffer *bucket_admit(const uint32_t *keys, const uint32_t *values, uint64_t n, bool tombstone,
-                          cudaStream_t s);
-  void bucket_admit_into(const uint32_t *keys, const uint32_t *values, uint64_t n, bool tombstone,
-                         cudaStream_t s, RunBuffer *out, unsigned long long *w0, unsigned long long *w1,
-                         void *scratch);
+                        cudaStream_t s, const uint8_t *erase = nullptr);
+  RunBuffer *bucket_admit(const uint32_t *keys, const uint32_t *values, const uint8_t *erase, uint64_t n,
+                          bool tombstone, cudaStream_t s);
+  void bucket_admit_into(const uint32_t *keys, const uint32_t *values, const uint8_t *erase, uint64_t n,
+                         bool tombstone, cudaStream_t s, RunBuffer *out, unsigned long long *w0,
+                         unsigned long long *w1, void *scratch);
   static size_t bucket_admit_scratch_bytes(uint64_t n);
   void flush_staged_locked(cudaStream_t s);
   bool stage_seq_pending() const {

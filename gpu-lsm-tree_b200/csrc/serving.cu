@@ -48,7 +48,8 @@ Server::Server(const DictConfig &cfg, uint64_t budget_bytes, uint32_t max_round_
   GPULSM_CUDA(cudaStreamCreateWithFlags(&download_, cudaStreamNonBlocking));
   GPULSM_CUDA(cudaStreamCreateWithFlags(&capture_, cudaStreamNonBlocking));
   const uint64_t m = max_round_keys_;
-  // inputs: two words a key, twice that for the padding of staged update runs
+  // inputs: at most two words and an erase mark a key, plus the padding of
+  // a staged update batch (form_round checks the exact need)
   in_words_cap_ = 4 * m + 4096;
   slot_bytes_ = in_words_cap_ * 4 + m * 4 + m;  // inputs, outputs, found flags
   slots_.resize(depth);
@@ -144,11 +145,13 @@ int Server::poll(uint64_t ticket) {
   return st;
 }
 
-int Server::wait(uint64_t ticket) {
+int Server::wait(uint64_t ticket, uint64_t *round) {
   std::unique_lock<std::mutex> lk(mu_);
   if (reqs_.find(ticket) == reqs_.end()) throw std::invalid_argument("unknown or already collected ticket");
   cv_done_.wait(lk, [&] { return reqs_.at(ticket).state != 0; });
-  const int st = reqs_.at(ticket).state;
+  const Req &q = reqs_.at(ticket);
+  const int st = q.state;
+  if (round) *round = q.round;
   reqs_.erase(ticket);
   return st;
 }
@@ -221,31 +224,42 @@ ServeStats Server::stats() {
   return s;
 }
 
-// Called with mu_ held: take requests in arrival order into runs of one kind
-// until the round is full; reject updates the budget cannot hold.
+// Staging input words of a round: the update batch (keys, values when any
+// request inserts, erase marks as bytes when it mixes inserts and erases,
+// padded to its size class when staged), the lookup keys, the range bounds.
+uint64_t Server::round_words(uint64_t nu, bool mixed, uint64_t nl, uint64_t nr) const {
+  uint64_t w = nl + 2 * nr;
+  if (nu) {
+    const uint64_t c = staged_updates_ ? size_class(nu) : nu;
+    w += 2 * c + (mixed ? (c + 3) / 4 : 0);
+  }
+  return w;
+}
+
+// Called with mu_ held: take requests in arrival order into the round's
+// three runs until the round is full; reject updates the budget cannot hold.
 bool Server::form_round(Slot &slot) {
-  slot.runs.clear();
+  for (Run &r : slot.runs) r = Run{};
+  slot.runs[kRunUpdate].kind = kServeInsert;
+  slot.runs[kRunLookup].kind = kServeLookup;
+  slot.runs[kRunRange].kind = kServeRangeSum;
   slot.parts.clear();
   slot.bytes = 0;
   uint64_t keys = 0;
   const uint64_t resident = dict_.resident_bytes();
   const double t = now_s();
-  bool any = false;
-  uint64_t words_done = 0;  // input words of the runs before the current one (padding included)
-  auto run_words = [&](uint32_t kind, uint64_t n) {
-    const uint64_t c = (staged_updates_ && is_update(kind)) ? size_class(n) : n;
-    return c * (has_aux(kind) ? 2 : 1);
-  };
+  bool any = false, ins = false, era = false;
+  std::vector<Part> parts[kRuns];
   while (!queue_.empty()) {
     const uint64_t tk = queue_.front();
     Req &q = reqs_.at(tk);
     if (keys > 0 && keys + q.n > max_round_keys_) break;
+    const int ri = is_update(q.kind) ? kRunUpdate : q.kind == kServeLookup ? kRunLookup : kRunRange;
     if (keys > 0 && q.n) {  // the staging input must hold the round with its padding
-      const bool same = !slot.runs.empty() && slot.runs.back().kind == q.kind;
-      const uint64_t cur = slot.runs.empty() ? 0 : run_words(slot.runs.back().kind, slot.runs.back().n);
-      const uint64_t words = same ? words_done + run_words(q.kind, slot.runs.back().n + q.n)
-                                  : words_done + cur + run_words(q.kind, q.n);
-      if (words > in_words_cap_) break;
+      uint64_t n[kRuns] = {slot.runs[0].n, slot.runs[1].n, slot.runs[2].n};
+      n[ri] += q.n;
+      const bool mixed = (ins || q.kind == kServeInsert) && (era || q.kind == kServeErase);
+      if (round_words(n[kRunUpdate], mixed, n[kRunLookup], n[kRunRange]) > in_words_cap_) break;
     }
     queue_.pop_front();
     if (q.n == 0) {  // nothing to do: done at once
@@ -264,36 +278,43 @@ bool Server::form_round(Slot &slot) {
         continue;
       }
       slot.bytes += growth;
+      ins = ins || q.kind == kServeInsert;
+      era = era || q.kind == kServeErase;
     }
-    if (slot.runs.empty() || slot.runs.back().kind != q.kind) {
-      if (!slot.runs.empty()) words_done += run_words(slot.runs.back().kind, slot.runs.back().n);
-      Run r{};
-      r.kind = q.kind;
-      r.first_part = slot.parts.size();
-      slot.runs.push_back(r);
-    }
-    Run &r = slot.runs.back();
-    slot.parts.push_back(Part{tk, r.n, q.n, q.keys, q.aux, q.out, q.found});
-    ++r.parts;
+    Run &r = slot.runs[ri];
+    parts[ri].push_back(Part{tk, q.kind, r.n, q.n, q.keys, q.aux, q.out, q.found});
     r.n += q.n;
     keys += q.n;
     any = true;
   }
-  // staging layout: each run's keys, then its values / upper bounds; a staged
-  // update run is padded to its size class (copies of its last key and value)
+  if (!any) return false;
+  slot.round = next_round_++;
+  // staging layout, runs in execution order: the update batch (keys, values,
+  // erase marks), the lookup keys, the range lower then upper bounds
+  slot.runs[kRunUpdate].mode = (ins && era) ? kStageMixed : era ? kStageErase : kStageInsert;
   uint64_t in = 0, out = 0;
-  for (Run &r : slot.runs) {
+  for (int ri = 0; ri < kRuns; ++ri) {
+    Run &r = slot.runs[ri];
     r.in_off = in;
     r.out_off = out;
-    r.status = 0;
-    r.cls = (staged_updates_ && is_update(r.kind)) ? size_class(r.n) : r.n;
-    in += r.cls * (has_aux(r.kind) ? 2 : 1);
-    if (has_out(r.kind)) out += r.n;
+    r.first_part = slot.parts.size();
+    r.parts = parts[ri].size();
+    slot.parts.insert(slot.parts.end(), parts[ri].begin(), parts[ri].end());
+    for (const Part &p : parts[ri]) reqs_.at(p.ticket).round = slot.round;
+    if (!r.n) continue;
+    if (ri == kRunUpdate) {
+      r.cls = staged_updates_ ? size_class(r.n) : r.n;
+      in += r.mode == kStageErase ? r.cls : 2 * r.cls + (r.mode == kStageMixed ? (r.cls + 3) / 4 : 0);
+    } else {
+      r.cls = r.n;
+      in += r.n * (ri == kRunRange ? 2 : 1);
+      out += r.n;
+    }
   }
   slot.in_words = in;
   slot.out_words = out;
   slot.keys = keys;
-  return any;
+  return true;
 }
 
 // The graph of a lookup-only round of up to `size_class` keys in this slot:
@@ -349,14 +370,14 @@ uint64_t Server::size_class(uint64_t n) const {
   return std::min<uint64_t>(c, max_round_keys_);
 }
 
-cudaGraphExec_t Server::update_graph(bool tombstone, uint32_t size_class, uint32_t stage) {
-  const uint64_t key = uint64_t(tombstone) | (uint64_t(size_class) << 1) | (uint64_t(stage) << 40);
+cudaGraphExec_t Server::update_graph(int mode, uint32_t size_class, uint32_t stage) {
+  const uint64_t key = uint64_t(mode) | (uint64_t(size_class) << 2) | (uint64_t(stage) << 40);
   for (const auto &g : update_graphs_)
     if (g.first == key) return g.second;
   cudaGraph_t graph = nullptr;
   GPULSM_CUDA(cudaStreamBeginCapture(capture_, cudaStreamCaptureModeThreadLocal));
   try {
-    dict_.enqueue_stage_admit(stage, size_class, tombstone, capture_);
+    dict_.enqueue_stage_admit(stage, size_class, mode, capture_);
   } catch (...) {
     cudaStreamEndCapture(capture_, &graph);
     if (graph) cudaGraphDestroy(graph);
@@ -374,15 +395,20 @@ cudaGraphExec_t Server::update_graph(bool tombstone, uint32_t size_class, uint32
 void Server::launch_round(Slot &slot) {
   const double c0 = now_s();
   for (const Run &r : slot.runs) {
+    if (!r.n) continue;
+    uint32_t *k = slot.h_in + r.in_off;
+    uint8_t *marks = reinterpret_cast<uint8_t *>(k + 2 * r.cls);  // update batch: erase marks
     for (uint64_t i = 0; i < r.parts; ++i) {
       const Part &p = slot.parts[r.first_part + i];
-      std::memcpy(slot.h_in + r.in_off + p.off, p.keys, p.n * 4);
-      if (has_aux(r.kind)) std::memcpy(slot.h_in + r.in_off + r.cls + p.off, p.aux, p.n * 4);
+      std::memcpy(k + p.off, p.keys, p.n * 4);
+      if (p.aux) std::memcpy(k + r.cls + p.off, p.aux, p.n * 4);
+      else if (r.mode == kStageMixed) std::memset(k + r.cls + p.off, 0, p.n * 4);  // an erase's values: unused
+      if (r.mode == kStageMixed) std::memset(marks + p.off, p.kind == kServeErase ? 1 : 0, p.n);
     }
-    if (r.cls > r.n && r.n) {  // padding of a staged update: repeats of its last (key, value) change nothing
-      uint32_t *k = slot.h_in + r.in_off;
+    if (r.cls > r.n) {  // padding of a staged update: repeats of its last row change nothing
       std::fill(k + r.n, k + r.cls, k[r.n - 1]);
-      if (has_aux(r.kind)) std::fill(k + r.cls + r.n, k + 2 * r.cls, k[r.cls + r.n - 1]);
+      if (r.mode != kStageErase) std::fill(k + r.cls + r.n, k + 2 * r.cls, k[r.cls + r.n - 1]);
+      if (r.mode == kStageMixed) std::memset(marks + r.n, marks[r.n - 1], r.cls - r.n);
     }
   }
   const double c1 = now_s();
@@ -391,18 +417,18 @@ void Server::launch_round(Slot &slot) {
     std::lock_guard<std::mutex> g(mu_);
     st_copy_s_ += c1 - c0;
   }
-  if (slot.runs.size() == 1 && slot.runs[0].kind == kServeLookup) {
+  Run &ru = slot.runs[kRunUpdate], &rl = slot.runs[kRunLookup], &rr = slot.runs[kRunRange];
+  if (!ru.n && !rr.n) {
     // lookup-only round: one graph launch (size classes are powers of two
     // from 1024 keys, the last one the round limit)
-    Run &r = slot.runs[0];
     uint64_t c = 1024;
-    while (c < r.n) c <<= 1;
+    while (c < rl.n) c <<= 1;
     if (c > max_round_keys_) c = max_round_keys_;
     GPULSM_CUDA(cudaEventRecord(slot.uploaded, compute_));
     try {
       dict_.launch_read_graph(lookup_graph(slot, uint32_t(c)), compute_);
     } catch (const std::exception &e) {
-      r.status = status_of(e);
+      rl.status = status_of(e);
     }
     GPULSM_CUDA(cudaEventRecord(slot.computed, compute_));
     GPULSM_CUDA(cudaEventRecord(slot.downloaded, compute_));
@@ -413,56 +439,59 @@ void Server::launch_round(Slot &slot) {
   GPULSM_CUDA(cudaMemcpyAsync(slot.d_in, slot.h_in, slot.in_words * 4, cudaMemcpyHostToDevice, upload_));
   GPULSM_CUDA(cudaEventRecord(slot.uploaded, upload_));
   GPULSM_CUDA(cudaStreamWaitEvent(compute_, slot.uploaded, 0));
-  for (Run &r : slot.runs) {
-    const uint32_t *in = slot.d_in + r.in_off;
+  // the calls in execution order; each bracketed by a pair of timing events
+  auto timed_call = [&](Run &r, uint32_t kind, auto &&call) {
     const uint32_t m = next_mark_pair(slot.marks, slot.timed.size() * 2);
     GPULSM_CUDA(cudaEventRecord(slot.marks[m], compute_));
     try {
-      switch (r.kind) {
-        case kServeLookup:
-          dict_.lookup(in, r.n, slot.d_out + r.out_off, slot.d_found + r.out_off, compute_);
-          break;
-        case kServeInsert:
-        case kServeErase: {
-          const bool tomb = r.kind == kServeErase;
-          if (!staged_updates_) {
-            tomb ? dict_.erase(in, r.n, compute_) : dict_.insert(in, in + r.n, r.n, compute_);
-            break;
-          }
-          // one graph launch: the run's (padded) keys into the staged graphs'
-          // input, then the captured admission into a free staging slot
-          int stage = dict_.stage_free_slot();
-          if (stage < 0) {
-            dict_.stage_flush(compute_);  // the staged runs merge into the levels
-            stage = dict_.stage_free_slot();
-          }
-          GPULSM_CUDA(cudaMemcpyAsync(dict_.stage_input(), in, r.cls * (tomb ? 4 : 8), cudaMemcpyDeviceToDevice,
-                                      compute_));
-          dict_.launch_stage_graph(update_graph(tomb, uint32_t(r.cls), uint32_t(stage)), uint32_t(stage), r.cls,
-                                   tomb, compute_);
-          std::lock_guard<std::mutex> g(mu_);
-          ++st_graph_updates_;
-          break;
-        }
-        default:
-          dict_.range_sum_kway(in, in + r.n, r.n, slot.d_out + r.out_off, compute_);
-          break;
-      }
+      call();
     } catch (const std::exception &e) {
       r.status = status_of(e);
     }
     GPULSM_CUDA(cudaEventRecord(slot.marks[m + 1], compute_));
-    slot.timed.emplace_back(r.kind, m);
+    slot.timed.emplace_back(kind, m);
+  };
+  // update batches are charged to insert, erase-only batches to erase
+  const uint32_t ukind = ru.mode == kStageErase ? kServeErase : kServeInsert;
+  if (ru.n) {
+    const uint32_t *in = slot.d_in + ru.in_off;
+    timed_call(ru, ukind, [&] {
+      if (!staged_updates_) {
+        if (ru.mode == kStageErase) dict_.erase(in, ru.n, compute_);
+        else if (ru.mode == kStageInsert) dict_.insert(in, in + ru.cls, ru.n, compute_);
+        else dict_.update(in, in + ru.cls, reinterpret_cast<const uint8_t *>(in + 2 * ru.cls), ru.n, compute_);
+        return;
+      }
+      // one graph launch: the batch's (padded) rows into the staged graphs'
+      // input, then the captured admission into a free staging slot
+      int stage = dict_.stage_free_slot();
+      if (stage < 0) {
+        dict_.stage_flush(compute_);  // the staged runs merge into the levels
+        stage = dict_.stage_free_slot();
+      }
+      const uint64_t words = ru.mode == kStageErase ? ru.cls : 2 * ru.cls;
+      const uint64_t bytes = words * 4 + (ru.mode == kStageMixed ? ru.cls : 0);
+      GPULSM_CUDA(cudaMemcpyAsync(dict_.stage_input(), in, bytes, cudaMemcpyDeviceToDevice, compute_));
+      dict_.launch_stage_graph(update_graph(ru.mode, uint32_t(ru.cls), uint32_t(stage)), uint32_t(stage), ru.cls,
+                               ru.mode != kStageInsert, compute_);
+      std::lock_guard<std::mutex> g(mu_);
+      ++st_graph_updates_;
+    });
   }
+  if (rl.n)
+    timed_call(rl, kServeLookup, [&] {
+      dict_.lookup(slot.d_in + rl.in_off, rl.n, slot.d_out + rl.out_off, slot.d_found + rl.out_off, compute_);
+    });
+  if (rr.n)
+    timed_call(rr, kServeRangeSum, [&] {
+      const uint32_t *in = slot.d_in + rr.in_off;
+      dict_.range_sum_kway(in, in + rr.n, rr.n, slot.d_out + rr.out_off, compute_);
+    });
   // an update request completes when its merges have completed
-  bool updates = false;
-  for (const Run &r : slot.runs) updates = updates || is_update(r.kind);
-  if (updates && !staged_updates_) {
-    const uint32_t m = next_mark_pair(slot.marks, slot.timed.size() * 2);
-    GPULSM_CUDA(cudaEventRecord(slot.marks[m], compute_));
-    dict_.join(compute_);
-    GPULSM_CUDA(cudaEventRecord(slot.marks[m + 1], compute_));
-    slot.timed.emplace_back(kServeInsert, m);  // the merges still running: charged to updates
+  if (ru.n && !staged_updates_) {
+    Run none{};
+    timed_call(none, ukind, [&] { dict_.join(compute_); });  // the merges still running
+    if (none.status) ru.status = none.status;
   }
   GPULSM_CUDA(cudaEventRecord(slot.computed, compute_));
   GPULSM_CUDA(cudaStreamWaitEvent(download_, slot.computed, 0));

@@ -4,19 +4,24 @@
 // The reference has no serving facility: GPULSMOpt serialises every call
 // behind a mutex and an operation event (GPULSMOpt.cuh:6852-6858), so a
 // caller batches by hand.  Here requests are submitted from any host thread
-// with host buffers; a worker thread forms rounds in arrival order,
-// coalescing each run of same-kind requests into one dictionary call, and
-// admits a request only while the dictionary's resident bytes plus the
-// rounds in flight stay inside a device-memory budget.  Rounds occupy one of
-// `depth` pipeline slots (pinned staging + device buffers): the upload of
-// round r+1 and the host staging of round r+2 overlap the kernels of round r,
-// and a completion thread returns results and records each request's latency
-// (submit to results in the caller's buffers).
+// with host buffers; a worker thread takes what has queued, in arrival order,
+// into a round of at most three dictionary calls - every insert and erase of
+// the round as one mixed update batch, then every lookup as one lookup, then
+// every range sum as one range sum - and admits an update only while the
+// dictionary's resident bytes plus the rounds in flight stay inside a
+// device-memory budget.  Rounds occupy one of `depth` pipeline slots (pinned
+// staging + device buffers): the upload of round r+1 and the host staging of
+// round r+2 overlap the kernels of round r, and a completion thread returns
+// results and records each request's latency (submit to results in the
+// caller's buffers).
 //
-// Semantics: the outcome equals applying the requests one at a time in
-// submission order (a lookup sees every earlier update and no later one):
-// rounds run in order on one compute stream, runs inside a round in order,
-// and a run of inserts or erases is one batch with keep-last semantics.
+// Semantics (linearizable): rounds apply in order; inside a round the updates
+// apply one at a time in submission order (the update batch keeps the last
+// row of every key), then the reads see the result.  Every request of a round
+// is in flight from before the round is formed until after it completes, so
+// this order is consistent with real time; a read submitted after a round
+// formed sees all of that round's updates.  wait_round reports the round of a
+// request, so a caller can replay the order.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -48,9 +53,11 @@ struct ServeStats {
   double gpu_busy_s = 0;      // device time of the rounds (upload done -> kernels done)
   double host_launch_s = 0;   // worker time staging and launching rounds
   uint64_t graph_rounds = 0;  // lookup-only rounds replayed from a captured CUDA graph
-  uint64_t graph_updates = 0;  // update runs replayed from a captured CUDA graph (staged)
+  uint64_t graph_updates = 0;  // update batches replayed from a captured CUDA graph (staged)
   uint64_t stage_flushes = 0;  // staged runs merged into the levels
-  double kind_gpu_s[4] = {0, 0, 0, 0};  // device time per request kind (updates: merges included)
+  // device time per request kind (updates: merges included; a round's update
+  // batch is charged to insert, or to erase when it only erases)
+  double kind_gpu_s[4] = {0, 0, 0, 0};
   double host_copy_s = 0;     // worker time copying request data into pinned staging
   double host_scatter_s = 0;  // completion time copying results into the requests' buffers
 };
@@ -82,7 +89,9 @@ class Server {
   uint64_t submit(uint32_t kind, const uint32_t *keys, const uint32_t *aux, uint64_t n, uint32_t *out,
                   uint8_t *found);
   int poll(uint64_t ticket);  // 0 pending, 1 done, < 0 failed (negated gpulsm status)
-  int wait(uint64_t ticket);  // 1 done, < 0 failed
+  // 1 done, < 0 failed; *round (optional): the request's round, numbered from
+  // 1 in execution order (0: completed without a round - empty or rejected)
+  int wait(uint64_t ticket, uint64_t *round = nullptr);
   void drain();
   ServeStats stats();
   void reset_stats();
@@ -101,10 +110,12 @@ class Server {
     uint32_t *out;
     uint8_t *found;
     double t_submit;
-    int state;  // 0 queued, 1 done, < 0 failed
+    int state;       // 0 queued, 1 done, < 0 failed
+    uint64_t round;  // the round that ran it (0: none)
   };
   struct Part {  // one request's share of a run
     uint64_t ticket;
+    uint32_t kind;
     uint64_t off;  // first key of this request inside its run
     uint64_t n;
     const uint32_t *keys;
@@ -112,12 +123,17 @@ class Server {
     uint32_t *out;
     uint8_t *found;
   };
+  // The calls of a round, in this order: the update batch, the lookups, the
+  // range sums (each run holds its requests in arrival order).
+  enum RunIndex : int { kRunUpdate = 0, kRunLookup = 1, kRunRange = 2, kRuns = 3 };
   struct Run {
-    uint32_t kind = 0;
+    uint32_t kind = 0;     // kServeInsert for the update batch, kServeLookup, kServeRangeSum
+    int mode = 0;          // update batch: kStageInsert, kStageErase or kStageMixed
     uint64_t in_off = 0;   // words into the staging input: keys, then values / upper bounds
     uint64_t out_off = 0;  // words into the staging output
     uint64_t n = 0;
-    uint64_t cls = 0;      // staged update: keys padded to this size class (values start at in_off + cls)
+    uint64_t cls = 0;      // update batch: keys padded to this size class (staged), else n;
+                           // values at in_off + cls, erase marks (bytes) at word in_off + 2 cls
     size_t first_part = 0, parts = 0;
     int status = 0;        // 0, or the negated gpulsm status of a failed call
   };
@@ -127,8 +143,9 @@ class Server {
     uint32_t *d_in = nullptr, *d_out = nullptr;
     uint8_t *d_found = nullptr;
     cudaEvent_t uploaded = nullptr, computed = nullptr, downloaded = nullptr;
-    std::vector<Run> runs;
-    std::vector<Part> parts;
+    Run runs[kRuns];
+    std::vector<Part> parts;  // grouped by run
+    uint64_t round = 0;
     uint64_t in_words = 0, out_words = 0, keys = 0;
     uint64_t bytes = 0;  // device bytes the round's updates may add (admission budget)
     bool launched = false;
@@ -146,9 +163,11 @@ class Server {
   bool form_round(Slot &slot);
   void launch_round(Slot &slot);
   cudaGraphExec_t lookup_graph(Slot &slot, uint32_t size_class);
-  // the graph of a staged update of `size_class` keys into staging slot `stage`
-  cudaGraphExec_t update_graph(bool tombstone, uint32_t size_class, uint32_t stage);
+  // the graph of a staged update (kStage* mode) of `size_class` keys into staging slot `stage`
+  cudaGraphExec_t update_graph(int mode, uint32_t size_class, uint32_t stage);
   uint64_t size_class(uint64_t n) const;
+  // staging input words of a round with these update / lookup / range-sum key counts
+  uint64_t round_words(uint64_t nu, bool mixed, uint64_t nl, uint64_t nr) const;
   static double now_s();
 
   LsmDictionary dict_;
@@ -167,7 +186,7 @@ class Server {
   // the staged runs merge into the levels when the staging slots are full)
   bool staged_updates_ = false;
   bool stage_ready_ = false;  // the dictionary's staging slots are configured
-  std::vector<std::pair<uint64_t, cudaGraphExec_t>> update_graphs_;  // key: tomb | class << 1 | stage << 40
+  std::vector<std::pair<uint64_t, cudaGraphExec_t>> update_graphs_;  // key: mode | class << 2 | stage << 40
   uint64_t st_graph_updates_ = 0;
 
   std::mutex mu_;
@@ -175,6 +194,7 @@ class Server {
   std::deque<uint64_t> queue_;
   std::unordered_map<uint64_t, Req> reqs_;
   uint64_t next_ticket_ = 1;
+  uint64_t next_round_ = 1;
   uint64_t inflight_bytes_ = 0;
   bool stop_ = false;
 

@@ -99,6 +99,14 @@ class GPULSMOpt:
         n = keys.numel() if count is None else count
         N.check(self._lib.gpulsm_dict_erase(self._h, _ptr(keys, "keys", count=n), n, _stream(stream)))
 
+    def update(self, keys, values, erase, count: int | None = None, stream=None):
+        """One batch of inserts and erases (no GPULSMOpt counterpart): row i
+        erases keys[i] when erase[i] (uint8) is nonzero, else inserts
+        (keys[i], values[i]); the last row of a key wins."""
+        n = keys.numel() if count is None else count
+        N.check(self._lib.gpulsm_dict_update(self._h, _ptr(keys, "keys", count=n), _ptr(values, "values", count=n),
+                                             _ptr(erase, "erase", 1, n), n, _stream(stream)))
+
     # --- queries -----------------------------------------------------------
     def lookup(self, queries, out_values, out_found=None, count: int | None = None, stream=None):
         n = queries.numel() if count is None else count

@@ -1,10 +1,13 @@
 """Serving loop over one LSM dictionary (gpulsm_server_* in include/gpulsm.h).
 
 Continuous batching of mixed lookup / insert / erase / range-sum requests
-with host buffers: a native worker thread coalesces the queue into rounds in
-arrival order, admits updates by a device-memory budget, and pipelines rounds
-through staging slots; results equal applying the requests one at a time in
-submission order.  The reference has no counterpart: GPULSMOpt serialises
+with host buffers: a native worker thread takes the queue, in arrival order,
+into rounds of at most three dictionary calls (the round's inserts and erases
+as one update batch, its lookups, its range sums), admits updates by a
+device-memory budget, and pipelines rounds through staging slots.  Results
+equal applying the rounds in order, each round's updates one at a time in
+submission order before its reads (every request of a round is in flight
+while it runs, so this is a linearization); `Ticket.round` tells the round.  The reference has no counterpart: GPULSMOpt serialises
 every call behind a mutex and an operation event (GPULSMOpt.cuh:6852-6858).
 """
 from __future__ import annotations
@@ -22,10 +25,11 @@ LOOKUP, INSERT, ERASE, RANGE_SUM = 0, 1, 2, 3
 class Ticket:
     """A submitted request; keeps its host buffers alive until collected."""
 
-    __slots__ = ("id", "kind", "bufs", "out", "found", "state")
+    __slots__ = ("id", "kind", "bufs", "out", "found", "state", "round")
 
     def __init__(self, tid, kind, bufs, out, found):
         self.id, self.kind, self.bufs, self.out, self.found, self.state = tid, kind, bufs, out, found, 0
+        self.round = None  # set by wait(): the round that ran the request (0: none)
 
 
 def _u32(a) -> np.ndarray:
@@ -105,8 +109,9 @@ class Server:
     def wait(self, t: Ticket):
         """Block until the request is done; returns its output (lookup values,
         (values, found), range sums, or None for updates)."""
-        st = C.c_int32()
-        N.check(self._lib.gpulsm_server_wait(self._h, t.id, C.byref(st)))
+        st, rd = C.c_int32(), C.c_uint64()
+        N.check(self._lib.gpulsm_server_wait_round(self._h, t.id, C.byref(st), C.byref(rd)))
+        t.round = rd.value
         return self._finish(t, st.value)
 
     def poll(self, t: Ticket) -> bool:

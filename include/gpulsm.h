@@ -93,6 +93,13 @@ int gpulsm_dict_insert(gpulsm_dict *dict, const uint32_t *keys, const uint32_t *
                        uint64_t count, void *stream);
 /* GPULSMOpt::erase(DeviceKeyBatch)  GPULSMOpt.cuh:5843 (tombstones) */
 int gpulsm_dict_erase(gpulsm_dict *dict, const uint32_t *keys, uint64_t count, void *stream);
+/* No GPULSMOpt counterpart (its batches are either inserts or erases): one
+ * batch of both.  Row i erases keys[i] when erase[i] is nonzero, else inserts
+ * (keys[i], values[i]); for a key given more than once the last row wins, as
+ * within an insert or erase batch.  Equals inserting and erasing the rows one
+ * at a time in input order. */
+int gpulsm_dict_update(gpulsm_dict *dict, const uint32_t *keys, const uint32_t *values, const uint8_t *erase,
+                       uint64_t count, void *stream);
 /* GPULSMOpt::lookup(DeviceLookupBatch)  GPULSMOpt.cuh:5850; out_found may be NULL.
  * Miss: out_values = out_found ? 0 : 0xffffffff (GPULSMOpt.cuh:4742-4749). */
 int gpulsm_dict_lookup(gpulsm_dict *dict, const uint32_t *queries, uint64_t count,
@@ -226,13 +233,17 @@ int gpulsm_tenants_resident_bytes(gpulsm_tenants *pool, uint64_t *out_bytes);
  * an operation event (GPULSMOpt.cuh:6852-6858) and leaves batching to the
  * caller.  A server owns one LSM dictionary and serves lookup / insert / erase
  * / range-sum requests submitted from any host thread with HOST buffers
- * (unlike the dict calls): a worker thread coalesces the queue, in arrival
- * order, into rounds (each run of same-kind requests becomes one dictionary
- * call), admits updates while the dictionary's resident bytes plus the
- * rounds in flight fit the device budget (an update that cannot fit fails
- * with GPULSM_ERR_CAPACITY), and pipelines rounds through `depth` staging
- * slots.  Results equal applying the requests one at a time in submission
- * order.  Request buffers stay owned by the caller until the request is done. */
+ * (unlike the dict calls): a worker thread takes what has queued, in arrival
+ * order, into a round of at most three dictionary calls (every insert and
+ * erase of the round as one update batch, then every lookup, then every range
+ * sum), admits updates while the dictionary's resident bytes plus the rounds
+ * in flight fit the device budget (an update that cannot fit fails with
+ * GPULSM_ERR_CAPACITY), and pipelines rounds through `depth` staging slots.
+ * Results equal applying the rounds in order and, inside a round, its updates
+ * one at a time in submission order, then its reads - a linearization, since
+ * every request of a round is in flight while the round runs
+ * (gpulsm_server_wait_round reports each request's round).  Request buffers
+ * stay owned by the caller until the request is done. */
 typedef struct gpulsm_server gpulsm_server;
 
 #define GPULSM_SERVE_LOOKUP 0u    /* keys -> out values (miss 0xffffffff), found flags optional */
@@ -246,10 +257,11 @@ typedef struct gpulsm_serve_stats {
   double mean_round_keys, wall_s;
   double gpu_busy_s, host_launch_s; /* device time of the rounds; worker time staging + launching */
   uint64_t graph_rounds;            /* lookup-only rounds replayed from a captured CUDA graph */
-  double kind_gpu_s[4];             /* device time of each request kind's calls (updates: merges included) */
+  double kind_gpu_s[4];             /* device time of each request kind's calls (updates: merges included;
+                                       a round's update batch counts as insert, or erase when it only erases) */
   double host_copy_s;               /* worker time copying request data into pinned staging */
   double host_scatter_s;            /* completion time copying results into the requests' buffers */
-  uint64_t graph_updates;           /* update runs replayed from a captured CUDA graph (staged admission) */
+  uint64_t graph_updates;           /* update batches replayed from a captured CUDA graph (staged admission) */
   uint64_t stage_flushes;           /* merges of the staged runs into the levels */
 } gpulsm_serve_stats;
 
@@ -282,14 +294,17 @@ int gpulsm_server_submit(gpulsm_server *server, uint32_t kind, const uint32_t *k
 /* *out_state: 0 pending, 1 done, -status failed; a finished ticket is collected by this call. */
 int gpulsm_server_poll(gpulsm_server *server, uint64_t ticket, int32_t *out_state);
 int gpulsm_server_wait(gpulsm_server *server, uint64_t ticket, int32_t *out_state);
+/* As wait; *out_round = the request's round, numbered from 1 in execution
+ * order (0: completed without one - an empty or rejected request). */
+int gpulsm_server_wait_round(gpulsm_server *server, uint64_t ticket, int32_t *out_state, uint64_t *out_round);
 int gpulsm_server_drain(gpulsm_server *server);
 int gpulsm_server_stats(gpulsm_server *server, gpulsm_serve_stats *out);
 int gpulsm_server_reset_stats(gpulsm_server *server);
 int gpulsm_server_run_load(gpulsm_server *server, const gpulsm_load_spec *spec, gpulsm_serve_stats *out);
 int gpulsm_server_resident_bytes(gpulsm_server *server, uint64_t *out_bytes);
 /* How update requests run (no reference counterpart).  0 (the default):
- * direct - each update run is admitted and merged at once and its round waits
- * for the merges.  1: staged - each update run is admitted into a staging run
+ * direct - each round's update batch is admitted and merged at once and the
+ * round waits for the merges.  1: staged - each update batch is admitted into a staging run
  * by one replay of a captured CUDA graph and completes without waiting for
  * merges; the staged runs are the newest levels of point reads and range sums
  * and merge into the levels when the staging slots are full (or before a

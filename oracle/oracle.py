@@ -126,6 +126,19 @@ class OracleLSM:
         k = _u32(keys)
         self._lib.orc_lsm_erase(self._h, k, k.size)
 
+    def update(self, keys, values, erase):
+        """Rows applied one at a time in input order: row i erases keys[i]
+        when erase[i] is nonzero, else inserts (keys[i], values[i]).  Only the
+        last row of each key matters, so those rows are applied as one erase
+        and one insert (their key sets are disjoint)."""
+        k, v, e = _u32(keys), _u32(values), np.asarray(erase, np.uint8)
+        assert k.size == v.size == e.size
+        _, first_from_end = np.unique(k[::-1], return_index=True)
+        last = k.size - 1 - first_from_end
+        er = e[last] != 0
+        self.erase(k[last[er]])
+        self.insert(k[last[~er]], v[last[~er]])
+
     def lookup(self, queries, with_found: bool = False):
         q = _u32(queries)
         out = np.empty(q.size, np.uint32)

@@ -162,6 +162,52 @@ def test_random_updates_match_oracle(gl, cuda, batch_capacity, level_zero, fan_i
     assert t.d.canonical_carry_status() == 0
 
 
+@pytest.mark.parametrize("batch_capacity,level_zero,fan_in", [(256, 512, 4), (1 << 20, 0, 4)])
+def test_mixed_update_batches_match_oracle(gl, cuda, batch_capacity, level_zero, fan_in):
+    """gpulsm_dict_update: inserts and erases in one batch, the last row of a
+    key winning, equal to the oracle applying the rows one at a time; mixed
+    with insert-only and erase-only batches, through level cascades, with
+    inserted values equal to the tombstone sentinel and keys inserted, erased
+    and re-inserted inside one batch (also across a tile boundary of the
+    batch capacity)."""
+    rng = np.random.default_rng(batch_capacity + 5)
+    t = Twin(gl, max_elements=1 << 21, batch_capacity=batch_capacity, level_zero_capacity=level_zero,
+             fan_in=fan_in)
+    universe = rng.integers(0, 1 << 32, 20000, dtype=np.uint64).astype(np.uint32)
+    universe[:6] = [0, 1, 2, 0xFFFFFFFF, 0xFFFFFFFE, 0x80000000]
+    import torch
+    for step in range(30):
+        n = int(rng.choice([1, 2, 100, 4095, 4097, 70000, 300000]))
+        k = universe[rng.integers(0, universe.size, n)]
+        v = rng.integers(0, 1 << 32, n, dtype=np.uint64).astype(np.uint32)
+        v[rng.random(n) < 0.05] = 0xFFFFFFFF  # real values equal to the tombstone sentinel
+        e = (rng.random(n) < rng.choice([0.0, 0.3, 1.0] if step % 4 == 0 else [0.5])).astype(np.uint8)
+        if n >= 3:  # insert, erase, insert the same key inside the batch; and the reverse
+            k[:3] = k[0]
+            e[:3] = [0, 1, 0]
+            k[-2:] = k[-1]
+            e[-2:] = [0, 1]
+        t.d.update(to_dev(k), to_dev(v), torch.from_numpy(e).cuda())
+        t.o.update(k, v, e)
+        if step % 6 == 5:
+            q = np.concatenate([universe, rng.integers(0, 1 << 32, 500, dtype=np.uint64).astype(np.uint32)])
+            t.lookup(q, with_found=True)
+            lo = universe[rng.integers(0, universe.size, 300)]
+            hi = (lo.astype(np.uint64) + rng.integers(0, 1 << 28, 300, dtype=np.uint64)).clip(0, 0xFFFFFFFF)
+            t.ranges(lo, hi.astype(np.uint32))
+            t.successor(q[rng.integers(0, q.size, 3000)])
+        if step % 5 == 2:  # plain batches between mixed ones
+            t.apply(("erase", universe[rng.integers(0, universe.size, 3000)]))
+            kk = universe[rng.integers(0, universe.size, 3000)]
+            t.apply(("insert", kk, rng.integers(0, 1 << 32, kk.size, dtype=np.uint64).astype(np.uint32)))
+    assert t.d.canonical_carry_status() == 0
+    z = torch.empty(0, dtype=torch.int32, device="cuda")
+    t.d.update(z, z, torch.empty(0, dtype=torch.uint8, device="cuda"))  # empty: a no-op
+    kd = to_dev(universe)
+    with pytest.raises(gl.InvalidArgument):  # values and erase marks are required
+        gl._native.check(t.d._lib.gpulsm_dict_update(t.d._h, kd.data_ptr(), None, None, 5, None))
+
+
 def skewed_batches(rng):
     """Update batches shaped to exercise every admission route: batch sizes
     around the 4096-row bucket limit, all-equal keys, few distinct keys

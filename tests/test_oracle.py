@@ -113,6 +113,26 @@ def test_bulk_build_keeps_last_duplicate():
     assert k.tolist() == [3, 7] and v.tolist() == [5, 4]
 
 
+def test_mixed_update_equals_rows_one_at_a_time():
+    rng = np.random.default_rng(9)
+    d, ref = OracleLSM(), {}
+    d.bulk_build(np.arange(0, 200, 2, dtype=np.uint32), np.arange(100, dtype=np.uint32))
+    ref.update({int(k): int(v) for k, v in zip(range(0, 200, 2), range(100))})
+    for _ in range(20):
+        n = int(rng.integers(1, 300))
+        k = rng.integers(0, 220, n).astype(np.uint32)
+        v = rng.integers(0, 1 << 32, n, dtype=np.uint64).astype(np.uint32)
+        e = (rng.random(n) < 0.4).astype(np.uint8)
+        d.update(k, v, e)
+        for ki, vi, ei in zip(k.tolist(), v.tolist(), e.tolist()):
+            if ei:
+                ref.pop(ki, None)
+            else:
+                ref[ki] = vi
+    dk, dv = d.dump()
+    assert dk.tolist() == sorted(ref) and dv.tolist() == [ref[x] for x in sorted(ref)]
+
+
 def test_range_sum_wraps_and_empty_ranges():
     d = OracleLSM()
     d.insert(np.array([10, 11, 12], np.uint32), np.array([0xFFFFFFFF, 0xFFFFFFFF, 3], np.uint32))

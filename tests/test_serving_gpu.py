@@ -1,7 +1,8 @@
 """GPU tests of the serving loop (gpulsm_server_*): continuous batching must
 give every request the result it gets alone, equal to the oracle applied in
-submission order; the device-memory budget must refuse updates it cannot
-hold; the native load generator must report consistent statistics."""
+the server's order (rounds in order; inside a round its updates in submission
+order, then its reads); the device-memory budget must refuse updates it
+cannot hold; the native load generator must report consistent statistics."""
 import threading
 
 import numpy as np
@@ -103,13 +104,23 @@ def test_results_same_alone_and_in_mix(gl, cuda, staged):
     for th in threads:
         th.join()
     flat = sorted((tk.id, tk, req) for lst in submitted for tk, req in lst)
-    mix = [srv.wait(tk) for _, tk, _ in flat]
+    got = {tk.id: srv.wait(tk) for _, tk, _ in flat}
     st = srv.stats()
     assert st["completed"] == len(flat) and st["rejected"] == 0
     assert st["rounds"] < len(flat), "requests that arrived together were not coalesced"
     srv.close()
+    # the server's order: rounds in order, inside a round its updates in
+    # submission order, then its reads
+    assert all(tk.round >= 1 for _, tk, _ in flat)
+    flat.sort(key=lambda x: (x[1].round, x[2][0] not in ("insert", "erase"), x[0]))
+    mix = [got[tk.id] for _, tk, _ in flat]
+    kinds_of_round = {}
+    for _, tk, req in flat:
+        kinds_of_round.setdefault(tk.round, set()).add(req[0])
+    assert any({"insert", "erase"} <= k for k in kinds_of_round.values()), "no round mixed inserts and erases"
+    assert any(len(k) >= 3 for k in kinds_of_round.values()), "no round held three request kinds"
 
-    # alone: one request at a time, in the order the server assigned
+    # alone: one request at a time, in the server's order
     ordered = [req for _, _, req in flat]
     srv = fresh_server(gl, base_k, base_v, staged)
     alone = [srv.wait(submit(srv, req)) for req in ordered]
