@@ -1009,7 +1009,8 @@ void LsmDictionary::range_sum(const uint32_t *lo, const uint32_t *hi, uint64_t n
   } else {
     lsm::LevelSet set;
     live_level_set(&set, s);
-    lsm::range_sum_levels_kernel<<<grid_for(n, 256), 256, 0, s>>>(set, lo, hi, n, out);
+    lsm::range_sum_levels_kernel<<<grid_for(n * lsm::kRangeGroup, lsm::kRangeThreads), lsm::kRangeThreads, 0, s>>>(
+        set, lo, hi, n, out);
     note_launch();
   }
   GPULSM_CUDA(cudaGetLastError());
@@ -1026,7 +1027,8 @@ void LsmDictionary::range_sum_kway(const uint32_t *lo, const uint32_t *hi, uint6
   ensure_models(s);
   lsm::LevelSet set;
   live_level_set(&set, s);
-  lsm::range_sum_levels_kernel<<<grid_for(n, 256), 256, 0, s>>>(set, lo, hi, n, out);
+  lsm::range_sum_levels_kernel<<<grid_for(n * lsm::kRangeGroup, lsm::kRangeThreads), lsm::kRangeThreads, 0, s>>>(
+        set, lo, hi, n, out);
   note_launch();
   GPULSM_CUDA(cudaGetLastError());
   end_op(s);

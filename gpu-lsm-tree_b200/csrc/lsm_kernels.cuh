@@ -743,12 +743,12 @@ __global__ void __launch_bounds__(256) lookup_table_kernel(const LevelSet *__res
                                                            const uint32_t *__restrict__ queries, uint64_t n,
                                                            uint32_t *__restrict__ out_values,
                                                            uint8_t *__restrict__ out_found) {
-  __shared__ LevelSet s_set;
+  __shared__ __align__(16) uint32_t s_words[sizeof(LevelSet) / 4];
   static_assert(sizeof(LevelSet) % 4 == 0, "table copied in words");
   const uint32_t *src = reinterpret_cast<const uint32_t *>(table);
-  uint32_t *dst = reinterpret_cast<uint32_t *>(&s_set);
-  for (uint32_t w = threadIdx.x; w < sizeof(LevelSet) / 4; w += blockDim.x) dst[w] = src[w];
+  for (uint32_t w = threadIdx.x; w < sizeof(LevelSet) / 4; w += blockDim.x) s_words[w] = src[w];
   __syncthreads();
+  const LevelSet &s_set = *reinterpret_cast<const LevelSet *>(s_words);
   const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i < n) lookup_one(s_set, i, queries, out_values, out_found);
 }
@@ -848,46 +848,65 @@ __device__ __forceinline__ uint64_t gallop_lower_bound(const uint32_t *__restric
   return hi;
 }
 
-__global__ void __launch_bounds__(256) range_sum_levels_kernel(LevelSet set, const uint32_t *__restrict__ lo,
-                                                               const uint32_t *__restrict__ hi, uint64_t n,
-                                                               uint32_t *__restrict__ out) {
-  const uint64_t q = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (q >= n) return;
-  const uint32_t a = lo[q], z = hi[q];
-  uint32_t acc = 0;
-  if (a <= z) {
-    uint64_t cur[kMaxLevels], end[kMaxLevels], pos[kMaxLevels];
-    uint32_t lv[kMaxLevels];  // levels with rows in [a, z], newest first
-    uint32_t m = 0;
-    for (uint32_t l = 0; l < set.count; ++l) {
+// One query per group of kRangeGroup lanes: lane t searches the bounds of
+// levels t, t + kRangeGroup, ... (independent loads instead of one thread's
+// chain over every level), the group shares them through shared memory, and
+// the lanes split the rows of the newer levels between them: each row finds
+// the next older version of its key by a directory search of the older
+// levels.  The partial sums (u32, wrapping) meet in a shuffle reduction.
+constexpr uint32_t kRangeGroup = 8;
+constexpr uint32_t kRangeThreads = 256;
+
+__global__ void __launch_bounds__(kRangeThreads) range_sum_levels_kernel(LevelSet set,
+                                                                         const uint32_t *__restrict__ lo,
+                                                                         const uint32_t *__restrict__ hi, uint64_t n,
+                                                                         uint32_t *__restrict__ out) {
+  constexpr uint32_t G = kRangeGroup, kGroups = kRangeThreads / G;
+  __shared__ uint64_t s_b[kGroups][kMaxLevels], s_e[kGroups][kMaxLevels];
+  const uint32_t grp = threadIdx.x / G, t = threadIdx.x % G;
+  const uint64_t q = (uint64_t(blockIdx.x) * kRangeThreads + threadIdx.x) / G;
+  const bool valid = q < n;
+  const uint32_t a = valid ? lo[q] : 1u, z = valid ? hi[q] : 0u;
+  uint32_t acc = 0, has = 0;  // has: levels with rows in [a, z] (bit l = level l of the set)
+  if (a <= z)
+    for (uint32_t l = t; l < set.count; l += G) {
       const LevelDesc d = load_desc(set.lv[l].desc);
       const uint64_t b = level_lower_bound(set.lv[l], d, a), e = level_upper_bound(set.lv[l], d, z);
+      s_b[grp][l] = b;
+      s_e[grp][l] = e;
       if (e > b) {
         acc += set.lv[l].live[e] - set.lv[l].live[b];
-        cur[m] = b;
-        end[m] = e;
-        lv[m++] = l;
+        has |= 1u << l;
       }
     }
-    for (uint32_t i = 0; i + 1 < m; ++i) {
-      const LevelView &N = set.lv[lv[i]];
-      for (uint32_t j = i + 1; j < m; ++j) pos[j] = cur[j];
-      for (uint64_t r = cur[i]; r < end[i]; ++r) {
-        const uint32_t k = N.keys[r];
-        for (uint32_t j = i + 1; j < m; ++j) {
-          const LevelView &O = set.lv[lv[j]];
-          const uint64_t p = gallop_lower_bound(O.keys, pos[j], end[j], k);
-          pos[j] = p;
-          if (p < end[j] && O.keys[p] == k) {
-            const uint32_t v = O.vals[p];
-            if (!row_is_tomb(O, p, v)) acc -= v;
-            break;
-          }
+  // the group's lanes are consecutive lanes of one warp
+  const uint32_t gmask = ((1u << G) - 1u) << ((threadIdx.x & 31u) & ~(G - 1u));
+#pragma unroll
+  for (uint32_t o = 1; o < G; o <<= 1) has |= __shfl_xor_sync(gmask, has, o, G);
+  __syncwarp(gmask);  // the group's bounds are in shared memory
+  // every row of a level but the oldest with rows subtracts the next older
+  // version of its key, when that version is live
+  const uint32_t oldest = has ? 31u - __clz(has) : 0u;
+  for (uint32_t rest = has & ~(1u << oldest); rest; rest &= rest - 1u) {
+    const uint32_t i = __ffs(rest) - 1u;
+    const LevelView &N = set.lv[i];
+    for (uint64_t r = s_b[grp][i] + t; r < s_e[grp][i]; r += G) {
+      const uint32_t k = N.keys[r];
+      for (uint32_t older = has & ~((2u << i) - 1u); older; older &= older - 1u) {
+        const uint32_t j = __ffs(older) - 1u;
+        const LevelView &O = set.lv[j];
+        const uint64_t p = level_lower_bound(O, load_desc(O.desc), k);
+        if (p < s_e[grp][j] && O.keys[p] == k) {
+          const uint32_t v = O.vals[p];
+          if (!row_is_tomb(O, p, v)) acc -= v;
+          break;
         }
       }
     }
   }
-  out[q] = acc;
+#pragma unroll
+  for (uint32_t o = 1; o < G; o <<= 1) acc += __shfl_xor_sync(gmask, acc, o, G);
+  if (valid && t == 0) out[q] = acc;
 }
 
 // ---------------------------------------------------------------------------
