@@ -636,8 +636,9 @@ def serving_leg(args, gl, w, dev):
             "peak_gpu_busy_frac": round(peak["gpu_busy_s"] / max(peak["wall_s"], 1e-9), 3),
             "peak_host_launch_frac": round(peak["host_launch_s"] / max(peak["wall_s"], 1e-9), 3),
             # where a peak round's time goes: device time per request kind (the
-            # merges still running when a round ends are charged to insert),
-            # worker copy into pinned staging, result scatter
+            # merges still running when a round ends are charged to insert;
+            # sampled on every eighth round), the submitting thread's copy into
+            # the server's pinned ring, the completion thread's result scatter
             "peak_kind_gpu_frac": {k: round(v / max(peak["wall_s"], 1e-9), 3)
                                    for k, v in zip(("lookup", "insert", "erase", "range"), peak["kind_gpu_s"])},
             "peak_host_copy_frac": round(peak["host_copy_s"] / max(peak["wall_s"], 1e-9), 3),

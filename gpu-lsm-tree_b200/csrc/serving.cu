@@ -1,5 +1,6 @@
-// Serving loop (serving.h): rounds formed in arrival order, a device-memory
-// budget for admission, pipelined slots, per-request latency.
+// Serving loop (serving.h): requests copied into a pinned ring at submit,
+// rounds formed in arrival order, a device-memory budget for admission,
+// pipelined slots, per-request latency.
 #include "serving.h"
 
 #include <algorithm>
@@ -22,6 +23,53 @@ constexpr uint64_t kUpdateBytesPerKey = 48;
 constexpr size_t kMaxInflight = 2;
 constexpr int kErrCapacity = 2;  // GPULSM_ERR_CAPACITY
 constexpr int kErrCuda = 5;      // GPULSM_ERR_CUDA
+constexpr uint32_t kMaxRoundRequests = 4096;
+// per-call timing events (the kind breakdown of the statistics) are recorded
+// on every kTimedEvery-th round only and scaled up: each pair costs the
+// worker two event records
+constexpr uint64_t kTimedEvery = 8;
+
+// One piece of a round's staging layout: n words of the uploaded span (or its
+// first word repeated, for the padding of a staged update batch) to the keys,
+// values and erase marks of a run.
+struct GatherEntry {
+  unsigned long long src_key;   // word offset in the span
+  unsigned long long src_aux;   // word offset in the span, or kNone: zeros
+  unsigned long long dst_key;   // word offset in the staging input
+  unsigned long long dst_aux;   // word offset, or kNone
+  unsigned long long dst_mark;  // byte offset, or kNone
+  uint32_t n;
+  uint32_t mark;    // the erase mark written (mixed update batches)
+  uint32_t repeat;  // every row copies word 0 of the source
+  uint32_t unused;
+};
+constexpr unsigned long long kNone = ~0ull;
+constexpr size_t kTableHeader = 64;  // the entry count, then the entries
+constexpr size_t kTableBytes = kTableHeader + (kMaxRoundRequests + 1) * sizeof(GatherEntry);
+
+// Lays a round's uploaded span out as its calls read it.  The entry count
+// is read from the table, so a captured graph serves any round of its class.
+__global__ void __launch_bounds__(256) serve_gather_kernel(const uint32_t *__restrict__ span,
+                                                           const unsigned char *__restrict__ table,
+                                                           uint32_t *__restrict__ stage) {
+  const uint32_t count = *reinterpret_cast<const uint32_t *>(table);
+  const GatherEntry *entries = reinterpret_cast<const GatherEntry *>(table + kTableHeader);
+  uint8_t *stage_bytes = reinterpret_cast<uint8_t *>(stage);
+  for (uint32_t r = blockIdx.y; r < count; r += gridDim.y) {
+    const GatherEntry g = entries[r];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
+      const uint32_t j = g.repeat ? 0u : i;
+      stage[g.dst_key + i] = span[g.src_key + j];
+      if (g.dst_aux != kNone) stage[g.dst_aux + i] = g.src_aux != kNone ? span[g.src_aux + j] : 0u;
+      if (g.dst_mark != kNone) stage_bytes[g.dst_mark + i] = uint8_t(g.mark);
+    }
+  }
+}
+
+dim3 gather_grid(uint64_t max_rows, uint32_t entries) {
+  const uint64_t gx = std::min<uint64_t>(32, std::max<uint64_t>(1, (max_rows + 2047) / 2048));
+  return dim3(unsigned(gx), std::max(1u, std::min(entries, 64u)));
+}
 
 int status_of(const std::exception &e) {
   const std::string m = e.what();
@@ -51,13 +99,20 @@ Server::Server(const DictConfig &cfg, uint64_t budget_bytes, uint32_t max_round_
   // inputs: at most two words and an erase mark a key, plus the padding of
   // a staged update batch (form_round checks the exact need)
   in_words_cap_ = 4 * m + 4096;
-  slot_bytes_ = in_words_cap_ * 4 + m * 4 + m;  // inputs, outputs, found flags
+  // a round's span: its requests' data (at most 8 bytes a key), the data of
+  // requests it refused, and a skip to the ring start; the ring holds several
+  span_cap_ = 24 * m + 4096;
+  ring_cap_ = std::max<uint64_t>(uint64_t(depth + 1) * 16 * m, 2 * span_cap_);
+  GPULSM_CUDA(cudaMallocHost(&ring_, ring_cap_));
+  slot_bytes_ = in_words_cap_ * 4 + m * 4 + m + span_cap_ + kTableBytes;  // inputs, outputs, flags, span, table
   slots_.resize(depth);
   for (uint32_t i = 0; i < depth; ++i) {
     Slot &s = slots_[i];
-    GPULSM_CUDA(cudaMallocHost(&s.h_in, in_words_cap_ * 4));
+    GPULSM_CUDA(cudaMallocHost(&s.h_table, kTableBytes));
     GPULSM_CUDA(cudaMallocHost(&s.h_out, m * 4));
     GPULSM_CUDA(cudaMallocHost(&s.h_found, m));
+    GPULSM_CUDA(cudaMalloc(&s.d_span, span_cap_));
+    GPULSM_CUDA(cudaMalloc(&s.d_table, kTableBytes));
     GPULSM_CUDA(cudaMalloc(&s.d_in, in_words_cap_ * 4));
     GPULSM_CUDA(cudaMalloc(&s.d_out, m * 4));
     GPULSM_CUDA(cudaMalloc(&s.d_found, m));
@@ -90,13 +145,16 @@ Server::~Server() {
   }
   cv_work_.notify_all();
   cv_inflight_.notify_all();
+  cv_space_.notify_all();
   if (worker_.joinable()) worker_.join();
   if (completer_.joinable()) completer_.join();
   cudaStreamSynchronize(compute_);
   cudaStreamSynchronize(upload_);
   cudaStreamSynchronize(download_);
   for (Slot &s : slots_) {
-    cudaFreeHost(s.h_in);
+    cudaFreeHost(s.h_table);
+    cudaFree(s.d_span);
+    cudaFree(s.d_table);
     cudaFreeHost(s.h_out);
     cudaFreeHost(s.h_found);
     cudaFree(s.d_in);
@@ -109,6 +167,7 @@ Server::~Server() {
     for (cudaEvent_t e : s.marks) cudaEventDestroy(e);
   }
   for (auto &g : update_graphs_) cudaGraphExecDestroy(g.second);
+  cudaFreeHost(ring_);
   cudaStreamDestroy(capture_);
   cudaStreamDestroy(compute_);
   cudaStreamDestroy(upload_);
@@ -123,17 +182,54 @@ uint64_t Server::submit(uint32_t kind, const uint32_t *keys, const uint32_t *aux
   if (n && has_aux(kind) && !aux) throw std::invalid_argument("null request values / upper bounds");
   if (n && has_out(kind) && !out) throw std::invalid_argument("null request output");
   const double t = now_s();
-  uint64_t tk;
+  const uint64_t key_bytes = n * 4, need = key_bytes * (has_aux(kind) ? 2 : 1);
+  uint64_t tk, pos;
   {
-    std::lock_guard<std::mutex> g(mu_);
-    if (stop_) throw std::runtime_error("server is shutting down");
+    // ring space in submission order: a request never wraps (it starts over
+    // at the ring start when it does not fit before the end)
+    std::unique_lock<std::mutex> lk(mu_);
+    for (;;) {
+      if (stop_) throw std::runtime_error("server is shutting down");
+      pos = ring_head_;
+      if (need && pos % ring_cap_ + need > ring_cap_) pos += ring_cap_ - pos % ring_cap_;
+      if (pos + need - ring_tail_ <= ring_cap_) break;
+      cv_space_.wait(lk);  // the completion of earlier rounds frees their spans
+    }
+    ring_head_ = pos + need;
     tk = next_ticket_++;
-    reqs_[tk] = Req{kind, keys, aux, n, out, found, t, 0};
+    reqs_[tk] = Req{kind, pos, need == 0, n, out, found, t, 0, 0};
     if (st_first_ < 0) st_first_ = t;
     queue_.push_back(tk);
   }
+  if (need) {  // the copy runs outside the lock; the worker takes the request once it is ready
+    const double c0 = now_s();
+    unsigned char *dst = ring_ + pos % ring_cap_;
+    std::memcpy(dst, keys, key_bytes);
+    if (has_aux(kind)) std::memcpy(dst + key_bytes, aux, key_bytes);
+    const double c1 = now_s();
+    std::lock_guard<std::mutex> g(mu_);
+    reqs_.at(tk).ready = true;
+    st_copy_s_ += c1 - c0;
+  }
   cv_work_.notify_one();
   return tk;
+}
+
+uint64_t Server::span_open(uint64_t end) {
+  spans_.emplace_back(end, false);
+  return span_base_ + spans_.size() - 1;
+}
+
+void Server::span_done(uint64_t id) {
+  spans_.at(id - span_base_).second = true;
+  bool freed = false;
+  while (!spans_.empty() && spans_.front().second) {
+    ring_tail_ = std::max(ring_tail_, spans_.front().first);
+    spans_.pop_front();
+    ++span_base_;
+    freed = true;
+  }
+  if (freed) cv_space_.notify_all();
 }
 
 int Server::poll(uint64_t ticket) {
@@ -238,6 +334,8 @@ uint64_t Server::round_words(uint64_t nu, bool mixed, uint64_t nl, uint64_t nr) 
 
 // Called with mu_ held: take requests in arrival order into the round's
 // three runs until the round is full; reject updates the budget cannot hold.
+// The requests taken cover one span of the ring (refused and empty requests
+// included), which the round uploads and releases when it completes.
 bool Server::form_round(Slot &slot) {
   for (Run &r : slot.runs) r = Run{};
   slot.runs[kRunUpdate].kind = kServeInsert;
@@ -248,11 +346,17 @@ bool Server::form_round(Slot &slot) {
   uint64_t keys = 0;
   const uint64_t resident = dict_.resident_bytes();
   const double t = now_s();
-  bool any = false, ins = false, era = false;
+  bool any = false, ins = false, era = false, taken = false;
+  uint64_t begin = 0, end = 0;
+  uint32_t nparts = 0;
   std::vector<Part> parts[kRuns];
   while (!queue_.empty()) {
     const uint64_t tk = queue_.front();
     Req &q = reqs_.at(tk);
+    if (!q.ready) break;  // its data is still being copied into the ring
+    const uint64_t need = q.n * 4 * (has_aux(q.kind) ? 2 : 1);
+    if (taken && q.pos + need - begin > span_cap_) break;
+    if (nparts >= kMaxRoundRequests) break;
     if (keys > 0 && keys + q.n > max_round_keys_) break;
     const int ri = is_update(q.kind) ? kRunUpdate : q.kind == kServeLookup ? kRunLookup : kRunRange;
     if (keys > 0 && q.n) {  // the staging input must hold the round with its padding
@@ -262,6 +366,9 @@ bool Server::form_round(Slot &slot) {
       if (round_words(n[kRunUpdate], mixed, n[kRunLookup], n[kRunRange]) > in_words_cap_) break;
     }
     queue_.pop_front();
+    if (!taken) begin = q.pos;
+    taken = true;
+    end = std::max(end, q.pos + need);
     if (q.n == 0) {  // nothing to do: done at once
       q.state = 1;
       lat_us_.push_back(float((t - q.t_submit) * 1e6));
@@ -282,13 +389,22 @@ bool Server::form_round(Slot &slot) {
       era = era || q.kind == kServeErase;
     }
     Run &r = slot.runs[ri];
-    parts[ri].push_back(Part{tk, q.kind, r.n, q.n, q.keys, q.aux, q.out, q.found});
+    parts[ri].push_back(Part{tk, q.kind, r.n, q.n, (q.pos - begin) / 4, q.out, q.found});
+    ++nparts;
     r.n += q.n;
     keys += q.n;
     any = true;
   }
-  if (!any) return false;
+  if (!taken) return false;
+  if (!any) {  // only refused or empty requests: their data is not read
+    span_done(span_open(end));
+    return false;
+  }
+  slot.span_begin = begin;
+  slot.span_end = end;
+  slot.span_id = span_open(end);
   slot.round = next_round_++;
+  slot.timed_round = slot.round % kTimedEvery == 0;
   // staging layout, runs in execution order: the update batch (keys, values,
   // erase marks), the lookup keys, the range lower then upper bounds
   slot.runs[kRunUpdate].mode = (ins && era) ? kStageMixed : era ? kStageErase : kStageInsert;
@@ -318,10 +434,10 @@ bool Server::form_round(Slot &slot) {
 }
 
 // The graph of a lookup-only round of up to `size_class` keys in this slot:
-// copy the keys in, look them up against the dictionary's device level
-// table, copy values and flags out.  Keys past the round's own are stale
-// staging contents; their answers land past the round's results and are
-// never read.
+// gather the uploaded keys into the staging input, look them up against the
+// dictionary's device level table, copy values and flags out.  Keys past the
+// round's own are stale staging contents; their answers land past the
+// round's results and are never read.
 cudaGraphExec_t Server::lookup_graph(Slot &slot, uint32_t size_class) {
   for (const auto &g : slot.graphs)
     if (g.first == size_class) return g.second;
@@ -329,7 +445,8 @@ cudaGraphExec_t Server::lookup_graph(Slot &slot, uint32_t size_class) {
   cudaGraph_t graph = nullptr;
   GPULSM_CUDA(cudaStreamBeginCapture(capture_, cudaStreamCaptureModeThreadLocal));
   try {
-    GPULSM_CUDA(cudaMemcpyAsync(slot.d_in, slot.h_in, c * 4, cudaMemcpyHostToDevice, capture_));
+    serve_gather_kernel<<<gather_grid(c, 64), 256, 0, capture_>>>(slot.d_span, slot.d_table, slot.d_in);
+    GPULSM_CUDA(cudaGetLastError());
     dict_.enqueue_table_lookup(slot.d_in, c, slot.d_out, slot.d_found, capture_);
     GPULSM_CUDA(cudaMemcpyAsync(slot.h_out, slot.d_out, c * 4, cudaMemcpyDeviceToHost, capture_));
     GPULSM_CUDA(cudaMemcpyAsync(slot.h_found, slot.d_found, c, cudaMemcpyDeviceToHost, capture_));
@@ -393,38 +510,63 @@ cudaGraphExec_t Server::update_graph(int mode, uint32_t size_class, uint32_t sta
 }
 
 void Server::launch_round(Slot &slot) {
-  const double c0 = now_s();
-  for (const Run &r : slot.runs) {
-    if (!r.n) continue;
-    uint32_t *k = slot.h_in + r.in_off;
-    uint8_t *marks = reinterpret_cast<uint8_t *>(k + 2 * r.cls);  // update batch: erase marks
+  // the gather table: where every request's rows go in the staging input
+  Run &ru = slot.runs[kRunUpdate], &rl = slot.runs[kRunLookup], &rr = slot.runs[kRunRange];
+  GatherEntry *tab = reinterpret_cast<GatherEntry *>(slot.h_table + kTableHeader);
+  uint32_t ne = 0;
+  uint64_t max_rows = 0;
+  for (int ri = 0; ri < kRuns; ++ri) {
+    const Run &r = slot.runs[ri];
     for (uint64_t i = 0; i < r.parts; ++i) {
       const Part &p = slot.parts[r.first_part + i];
-      std::memcpy(k + p.off, p.keys, p.n * 4);
-      if (p.aux) std::memcpy(k + r.cls + p.off, p.aux, p.n * 4);
-      else if (r.mode == kStageMixed) std::memset(k + r.cls + p.off, 0, p.n * 4);  // an erase's values: unused
-      if (r.mode == kStageMixed) std::memset(marks + p.off, p.kind == kServeErase ? 1 : 0, p.n);
-    }
-    if (r.cls > r.n) {  // padding of a staged update: repeats of its last row change nothing
-      std::fill(k + r.n, k + r.cls, k[r.n - 1]);
-      if (r.mode != kStageErase) std::fill(k + r.cls + r.n, k + 2 * r.cls, k[r.cls + r.n - 1]);
-      if (r.mode == kStageMixed) std::memset(marks + r.n, marks[r.n - 1], r.cls - r.n);
+      GatherEntry g{p.src, kNone, r.in_off + p.off, kNone, kNone, uint32_t(p.n), 0u, 0u, 0u};
+      if (ri == kRunUpdate) {
+        if (p.kind == kServeInsert) g.src_aux = p.src + p.n;
+        if (r.mode != kStageErase) g.dst_aux = r.in_off + r.cls + p.off;  // an erase's value in a mixed batch: 0
+        if (r.mode == kStageMixed) {
+          g.dst_mark = (r.in_off + 2 * r.cls) * 4 + p.off;
+          g.mark = p.kind == kServeErase ? 1u : 0u;
+        }
+      } else if (ri == kRunRange) {
+        g.src_aux = p.src + p.n;
+        g.dst_aux = r.in_off + r.n + p.off;
+      }
+      tab[ne++] = g;
+      max_rows = std::max<uint64_t>(max_rows, p.n);
     }
   }
-  const double c1 = now_s();
+  if (ru.n && ru.cls > ru.n) {  // padding of a staged update: repeats of its last row change nothing
+    const Part &p = slot.parts[ru.first_part + ru.parts - 1];
+    GatherEntry g{p.src + p.n - 1, kNone, ru.in_off + ru.n, kNone, kNone, uint32_t(ru.cls - ru.n), 0u, 1u, 0u};
+    if (p.kind == kServeInsert) g.src_aux = p.src + 2 * p.n - 1;
+    if (ru.mode != kStageErase) g.dst_aux = ru.in_off + ru.cls + ru.n;
+    if (ru.mode == kStageMixed) {
+      g.dst_mark = (ru.in_off + 2 * ru.cls) * 4 + ru.n;
+      g.mark = p.kind == kServeErase ? 1u : 0u;
+    }
+    tab[ne++] = g;
+    max_rows = std::max<uint64_t>(max_rows, ru.cls - ru.n);
+  }
+  *reinterpret_cast<uint32_t *>(slot.h_table) = ne;
+  slot.entries = ne;
   slot.timed.clear();
-  {
-    std::lock_guard<std::mutex> g(mu_);
-    st_copy_s_ += c1 - c0;
-  }
-  Run &ru = slot.runs[kRunUpdate], &rl = slot.runs[kRunLookup], &rr = slot.runs[kRunRange];
+  // upload: the span (one copy, or two when it wraps the ring end) and the table
+  const uint64_t len = slot.span_end - slot.span_begin, p0 = slot.span_begin % ring_cap_;
+  const uint64_t first = std::min(len, ring_cap_ - p0);
+  if (first) GPULSM_CUDA(cudaMemcpyAsync(slot.d_span, ring_ + p0, first, cudaMemcpyHostToDevice, upload_));
+  if (len > first)
+    GPULSM_CUDA(cudaMemcpyAsync(reinterpret_cast<unsigned char *>(slot.d_span) + first, ring_, len - first,
+                                cudaMemcpyHostToDevice, upload_));
+  GPULSM_CUDA(cudaMemcpyAsync(slot.d_table, slot.h_table, kTableHeader + size_t(ne) * sizeof(GatherEntry),
+                              cudaMemcpyHostToDevice, upload_));
+  GPULSM_CUDA(cudaEventRecord(slot.uploaded, upload_));
+  GPULSM_CUDA(cudaStreamWaitEvent(compute_, slot.uploaded, 0));
   if (!ru.n && !rr.n) {
     // lookup-only round: one graph launch (size classes are powers of two
     // from 1024 keys, the last one the round limit)
     uint64_t c = 1024;
     while (c < rl.n) c <<= 1;
     if (c > max_round_keys_) c = max_round_keys_;
-    GPULSM_CUDA(cudaEventRecord(slot.uploaded, compute_));
     try {
       dict_.launch_read_graph(lookup_graph(slot, uint32_t(c)), compute_);
     } catch (const std::exception &e) {
@@ -436,20 +578,25 @@ void Server::launch_round(Slot &slot) {
     ++st_graph_rounds_;
     return;
   }
-  GPULSM_CUDA(cudaMemcpyAsync(slot.d_in, slot.h_in, slot.in_words * 4, cudaMemcpyHostToDevice, upload_));
-  GPULSM_CUDA(cudaEventRecord(slot.uploaded, upload_));
-  GPULSM_CUDA(cudaStreamWaitEvent(compute_, slot.uploaded, 0));
-  // the calls in execution order; each bracketed by a pair of timing events
+  serve_gather_kernel<<<gather_grid(max_rows, ne), 256, 0, compute_>>>(slot.d_span, slot.d_table, slot.d_in);
+  GPULSM_CUDA(cudaGetLastError());
+  // the calls in execution order; on a timed round each is bracketed by a
+  // pair of timing events
   auto timed_call = [&](Run &r, uint32_t kind, auto &&call) {
-    const uint32_t m = next_mark_pair(slot.marks, slot.timed.size() * 2);
-    GPULSM_CUDA(cudaEventRecord(slot.marks[m], compute_));
+    uint32_t m = 0;
+    if (slot.timed_round) {
+      m = next_mark_pair(slot.marks, slot.timed.size() * 2);
+      GPULSM_CUDA(cudaEventRecord(slot.marks[m], compute_));
+    }
     try {
       call();
     } catch (const std::exception &e) {
       r.status = status_of(e);
     }
-    GPULSM_CUDA(cudaEventRecord(slot.marks[m + 1], compute_));
-    slot.timed.emplace_back(kind, m);
+    if (slot.timed_round) {
+      GPULSM_CUDA(cudaEventRecord(slot.marks[m + 1], compute_));
+      slot.timed.emplace_back(kind, m);
+    }
   };
   // update batches are charged to insert, erase-only batches to erase
   const uint32_t ukind = ru.mode == kStageErase ? kServeErase : kServeInsert;
@@ -509,7 +656,8 @@ void Server::worker() {
     // at most kMaxInflight rounds launched and not yet returned: while the
     // GPU works on them, arrivals accumulate into the next round
     cv_work_.wait(lk, [&] {
-      return stop_ || (!queue_.empty() && !free_slots_.empty() && inflight_.size() < kMaxInflight);
+      return stop_ || (!queue_.empty() && reqs_.at(queue_.front()).ready && !free_slots_.empty() &&
+                       inflight_.size() < kMaxInflight);
     });
     if (stop_) return;
     const uint32_t si = free_slots_.front();
@@ -581,7 +729,8 @@ void Server::completer() {
       }
     const double s1 = now_s();
     lk.lock();
-    for (int k = 0; k < 4; ++k) st_kind_gpu_s_[k] += kind_s[k];
+    for (int k = 0; k < 4; ++k) st_kind_gpu_s_[k] += kind_s[k] * double(kTimedEvery);  // timed rounds only
+    span_done(slot.span_id);  // the round's ring span is no longer read
     st_scatter_s_ += s1 - s0;
     inflight_.pop_front();
     inflight_bytes_ -= slot.bytes;

@@ -9,11 +9,14 @@
 // the round as one mixed update batch, then every lookup as one lookup, then
 // every range sum as one range sum - and admits an update only while the
 // dictionary's resident bytes plus the rounds in flight stay inside a
-// device-memory budget.  Rounds occupy one of `depth` pipeline slots (pinned
-// staging + device buffers): the upload of round r+1 and the host staging of
-// round r+2 overlap the kernels of round r, and a completion thread returns
-// results and records each request's latency (submit to results in the
-// caller's buffers).
+// device-memory budget.  submit() copies the request's keys (and values or
+// upper bounds) into a pinned ring on the caller's thread, so the worker
+// copies nothing: a round uploads the ring span of its requests in one or two
+// copies, and one gather kernel lays the span out as the three calls read
+// it.  Rounds occupy one of `depth` pipeline slots (device buffers): the
+// upload of round r+1 overlaps the kernels of round r, and a completion
+// thread returns results, releases the round's ring span and records each
+// request's latency (submit to results in the caller's buffers).
 //
 // Semantics (linearizable): rounds apply in order; inside a round the updates
 // apply one at a time in submission order (the update batch keeps the last
@@ -58,7 +61,7 @@ struct ServeStats {
   // device time per request kind (updates: merges included; a round's update
   // batch is charged to insert, or to erase when it only erases)
   double kind_gpu_s[4] = {0, 0, 0, 0};
-  double host_copy_s = 0;     // worker time copying request data into pinned staging
+  double host_copy_s = 0;     // submitters' time copying request data into the pinned ring
   double host_scatter_s = 0;  // completion time copying results into the requests' buffers
 };
 
@@ -83,9 +86,11 @@ class Server {
   Server(const Server &) = delete;
   Server &operator=(const Server &) = delete;
 
-  // Host buffers, owned by the caller until the request completes.  keys: the
-  // request keys (range: lower bounds); aux: insert values / range upper
-  // bounds; out: lookup values / range sums; found: optional lookup flags.
+  // Host buffers.  keys: the request keys (range: lower bounds); aux: insert
+  // values / range upper bounds - both copied before submit returns (it
+  // waits while the pinned ring is full); out: lookup values / range sums;
+  // found: optional lookup flags - owned by the caller until the request
+  // completes.
   uint64_t submit(uint32_t kind, const uint32_t *keys, const uint32_t *aux, uint64_t n, uint32_t *out,
                   uint8_t *found);
   int poll(uint64_t ticket);  // 0 pending, 1 done, < 0 failed (negated gpulsm status)
@@ -104,8 +109,8 @@ class Server {
  private:
   struct Req {
     uint32_t kind;
-    const uint32_t *keys;
-    const uint32_t *aux;
+    uint64_t pos;  // ring position (bytes) of its keys, then its values / upper bounds
+    bool ready;    // its data is in the ring
     uint64_t n;
     uint32_t *out;
     uint8_t *found;
@@ -118,8 +123,7 @@ class Server {
     uint32_t kind;
     uint64_t off;  // first key of this request inside its run
     uint64_t n;
-    const uint32_t *keys;
-    const uint32_t *aux;
+    uint64_t src;  // word offset of its keys in the round's uploaded span
     uint32_t *out;
     uint8_t *found;
   };
@@ -138,10 +142,17 @@ class Server {
     int status = 0;        // 0, or the negated gpulsm status of a failed call
   };
   struct Slot {
-    uint32_t *h_in = nullptr, *h_out = nullptr;
+    uint32_t *h_out = nullptr;
     uint8_t *h_found = nullptr;
+    unsigned char *h_table = nullptr;  // gather table (pinned): entry count, then entries
     uint32_t *d_in = nullptr, *d_out = nullptr;
     uint8_t *d_found = nullptr;
+    uint32_t *d_span = nullptr;        // the round's ring span, uploaded
+    unsigned char *d_table = nullptr;
+    uint64_t span_begin = 0, span_end = 0;  // ring positions (bytes)
+    uint64_t span_id = 0;
+    uint32_t entries = 0;
+    bool timed_round = false;          // records the per-call timing events
     cudaEvent_t uploaded = nullptr, computed = nullptr, downloaded = nullptr;
     Run runs[kRuns];
     std::vector<Part> parts;  // grouped by run
@@ -149,7 +160,7 @@ class Server {
     uint64_t in_words = 0, out_words = 0, keys = 0;
     uint64_t bytes = 0;  // device bytes the round's updates may add (admission budget)
     bool launched = false;
-    // lookup-only rounds replay a CUDA graph per size class (copy in, lookup
+    // lookup-only rounds replay a CUDA graph per size class (gather, lookup
     // against the device level table, copy out) captured on first use
     std::vector<std::pair<uint32_t, cudaGraphExec_t>> graphs;
     // device time per run: events bracketing each timed call on the compute
@@ -160,6 +171,10 @@ class Server {
 
   void worker();
   void completer();
+  // with mu_ held: a round's ring span (numbered in formation order) is no
+  // longer read; spans are released (the ring tail advanced) in order
+  uint64_t span_open(uint64_t end);
+  void span_done(uint64_t id);
   bool form_round(Slot &slot);
   void launch_round(Slot &slot);
   cudaGraphExec_t lookup_graph(Slot &slot, uint32_t size_class);
@@ -176,6 +191,12 @@ class Server {
   uint32_t max_round_keys_;
   uint64_t slot_bytes_ = 0;
   uint64_t in_words_cap_ = 0;  // staging input words of a slot
+  // the pinned request ring: positions grow without bound, byte pos % cap
+  unsigned char *ring_ = nullptr;
+  uint64_t ring_cap_ = 0, span_cap_ = 0;
+  uint64_t ring_head_ = 0, ring_tail_ = 0;
+  std::deque<std::pair<uint64_t, bool>> spans_;  // (end, done) of formed rounds, in order
+  uint64_t span_base_ = 0;                       // the number of spans_.front()
   std::vector<Slot> slots_;
   std::deque<uint32_t> free_slots_;
   std::deque<uint32_t> inflight_;
@@ -190,7 +211,7 @@ class Server {
   uint64_t st_graph_updates_ = 0;
 
   std::mutex mu_;
-  std::condition_variable cv_work_, cv_done_, cv_inflight_;
+  std::condition_variable cv_work_, cv_done_, cv_inflight_, cv_space_;
   std::deque<uint64_t> queue_;
   std::unordered_map<uint64_t, Req> reqs_;
   uint64_t next_ticket_ = 1;

@@ -239,11 +239,13 @@ int gpulsm_tenants_resident_bytes(gpulsm_tenants *pool, uint64_t *out_bytes);
  * sum), admits updates while the dictionary's resident bytes plus the rounds
  * in flight fit the device budget (an update that cannot fit fails with
  * GPULSM_ERR_CAPACITY), and pipelines rounds through `depth` staging slots.
+ * Submit copies the request's keys and values / upper bounds into a pinned
+ * ring of the server before it returns (waiting while the ring is full); the
+ * output buffers stay the caller's until the request is done.
  * Results equal applying the rounds in order and, inside a round, its updates
  * one at a time in submission order, then its reads - a linearization, since
  * every request of a round is in flight while the round runs
- * (gpulsm_server_wait_round reports each request's round).  Request buffers
- * stay owned by the caller until the request is done. */
+ * (gpulsm_server_wait_round reports each request's round). */
 typedef struct gpulsm_server gpulsm_server;
 
 #define GPULSM_SERVE_LOOKUP 0u    /* keys -> out values (miss 0xffffffff), found flags optional */
@@ -258,8 +260,9 @@ typedef struct gpulsm_serve_stats {
   double gpu_busy_s, host_launch_s; /* device time of the rounds; worker time staging + launching */
   uint64_t graph_rounds;            /* lookup-only rounds replayed from a captured CUDA graph */
   double kind_gpu_s[4];             /* device time of each request kind's calls (updates: merges included;
-                                       a round's update batch counts as insert, or erase when it only erases) */
-  double host_copy_s;               /* worker time copying request data into pinned staging */
+                                       a round's update batch counts as insert, or erase when it only erases),
+                                       timed on every eighth round and scaled by eight */
+  double host_copy_s;               /* submitters' time copying request data into the server's pinned ring */
   double host_scatter_s;            /* completion time copying results into the requests' buffers */
   uint64_t graph_updates;           /* update batches replayed from a captured CUDA graph (staged admission) */
   uint64_t stage_flushes;           /* merges of the staged runs into the levels */
