@@ -37,10 +37,10 @@ sys.path.insert(0, ROOT)
 
 METRIC = "M lookups/s & M inserted keys/s at 2^26 keys vs plain form; p50/p99 request latency"
 # DRAM bytes (read + write) of merge_kernel per algorithmic byte, from an ncu
-# capture of `bench.py --case merge` (one 17.8M-row merge: 160.3 MB read,
-# 126.5 MB written against 328.6 MB algorithmic; the rest of the writes were
+# capture of `bench.py --case merge` (one 17.8M-row merge: 161.1 MB read,
+# 128.0 MB written against 328.6 MB algorithmic; the rest of the writes were
 # still in L2 when the kernel ended)
-MERGE_TRAFFIC_RATIO = 0.873
+MERGE_TRAFFIC_RATIO = 0.880
 LOOKUP_BYTES = 41  # algorithmic bytes per u32 point lookup (query + value + found + one row sector)
 INSERT_BYTES = 16  # per inserted (key, value): read 8 + write 8 into the structure
 DELETE_BYTES = 12

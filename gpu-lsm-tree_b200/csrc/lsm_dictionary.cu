@@ -111,6 +111,7 @@ RunBuffer *RunPool::acquire(uint64_t min_rows, cudaStream_t stream, bool settled
     if (f->released && f->freed_on != stream) GPULSM_CUDA(cudaStreamWaitEvent(stream, f->freed, 0));
     f->model_ok = false;
     f->model_rows = 0;
+    f->dir_ok = false;
     return f;
   };
   if (best) return take(best, best_i);
@@ -466,6 +467,7 @@ RunBuffer *LsmDictionary::sort_dedup(const uint32_t *keys, const uint32_t *value
       bufs[cur], nn, tombstone ? 1 : 0, carry->keys, carry->vals, carry->flags, carry->desc, carry->dir,
       carry->dir_bits, rows_log2_, lb, counter, dev_status_); note_launch();
   GPULSM_CUDA(cudaGetLastError());
+  carry->dir_ok = true;
   return carry;
 }
 
@@ -516,12 +518,14 @@ void LsmDictionary::bucket_admit_into(const uint32_t *keys, const uint32_t *valu
   launch_chained(ad::admit_bucket_kernel, ad::kBuckets, ad::kThreads, ad::kBucketSmemBytes, s, w1, w0,
                  static_cast<const uint32_t *>(top), nn, src, carry->keys, carry->vals, carry->flags, carry->desc,
                  carry->dir, carry->dir_bits, rows_log2_, lb, counter, dev_status_);
+  carry->dir_ok = true;
 }
 
 RunBuffer *LsmDictionary::merge(RunBuffer *newer, RunBuffer *older, uint64_t out_upper,
                                 bool drop_tombstones, cudaStream_t s, const lsm::ReceiptSrc *rcpt,
                                 bool release_newer, bool release_older) {
   RunBuffer *out = pool_.acquire(out_upper, s);
+  out->dir_ok = merge_dirs_;
   const uint64_t tiles = std::max<uint64_t>(1, (out_upper + lsm::kMergeTile - 1) / lsm::kMergeTile);
   const size_t zero_bytes = merge_scratch_bytes(out_upper);
   const size_t bytes = zero_bytes + align_up((tiles + 2) * 8);
@@ -553,7 +557,7 @@ RunBuffer *LsmDictionary::merge(RunBuffer *newer, RunBuffer *older, uint64_t out
   launch_chained(kernel, unsigned(tiles), lsm::kMergeThreads, lsm::kMergeSmemBytes, s, newer->keys, newer->vals,
                  newer->flags,
                  newer->desc, older->keys, older->vals, older->flags, older->desc, out->keys, out->vals, out->flags,
-                 out->desc, out->dir, out->dir_bits, rows_log2_,
+                 out->desc, merge_dirs_ ? out->dir : nullptr, out->dir_bits, rows_log2_,
                  static_cast<unsigned long long>(std::min<uint64_t>(out_upper, out->cap)),
                  static_cast<unsigned long long>(out->cap), parts, lb, counter, dev_status_, trace,
                  rcpt ? *rcpt : lsm::ReceiptSrc{});
@@ -577,6 +581,15 @@ void LsmDictionary::fit_model(RunBuffer *run, uint64_t upper, cudaStream_t) {
 }
 
 void LsmDictionary::ensure_models(cudaStream_t s) {
+  prev_update_ = false;
+  for (auto &l : levels_)
+    if (l.run && !l.run->dir_ok) {
+      lsm::build_directory_kernel<<<grid_for((l.upper + lsm::kDirRows) / lsm::kDirRows, 256), 256, 0, s>>>(
+          l.run->keys, l.run->desc, l.run->dir);
+      note_launch();
+      GPULSM_CUDA(cudaGetLastError());
+      l.run->dir_ok = true;
+    }
   if (cfg_.search_mode != 1) return;
   for (auto &l : levels_)
     if (l.run && l.run->model_rows && !l.run->model_ok) fit_now(l.run, l.run->model_rows, s);
@@ -871,6 +884,7 @@ void LsmDictionary::clear(cudaStream_t s) {
   failed_ = false;
   failure_.clear();
   receipt_pending_ = false;
+  prev_update_ = false;
   end_op(s);
 }
 
@@ -914,6 +928,8 @@ void LsmDictionary::insert(const uint32_t *keys, const uint32_t *values, uint64_
     begin_op(s);
     flush_staged_locked(s);
   }
+  merge_dirs_ = !prev_update_;  // back-to-back updates leave directories to the reads
+  prev_update_ = true;
   admit(keys, values, nullptr, n, false, s);  // every batch's finishing kernel writes the receipt
   end_op(s);
 }
@@ -930,6 +946,8 @@ void LsmDictionary::erase(const uint32_t *keys, uint64_t n, cudaStream_t s) {
     begin_op(s);
     flush_staged_locked(s);
   }
+  merge_dirs_ = !prev_update_;  // back-to-back updates leave directories to the reads
+  prev_update_ = true;
   admit(keys, nullptr, nullptr, n, true, s);  // every batch's finishing kernel writes the receipt
   end_op(s);
 }
@@ -947,6 +965,8 @@ void LsmDictionary::update(const uint32_t *keys, const uint32_t *values, const u
     begin_op(s);
     flush_staged_locked(s);
   }
+  merge_dirs_ = !prev_update_;  // back-to-back updates leave directories to the reads
+  prev_update_ = true;
   admit(keys, values, erase, n, false, s);  // every batch's finishing kernel writes the receipt
   end_op(s);
 }
@@ -1196,7 +1216,7 @@ void LsmDictionary::kernel_timing(uint64_t *launches, double *total_ms, double *
       float e = 0;
       GPULSM_CUDA(cudaEventElapsedTime(&e, traces_[i].start, traces_[i].stop));
       ms += e;
-      b += 9.0 * double(t[4 * i] + t[4 * i + 1]) + 9.0 * double(t[4 * i + 2]) + 4.0 * double(t[4 * i + 3] + 1);
+      b += 9.0 * double(t[4 * i] + t[4 * i + 1]) + 9.0 * double(t[4 * i + 2]) + 4.0 * double(t[4 * i + 3]);
       spare_events_.push_back(traces_[i].start);
       spare_events_.push_back(traces_[i].stop);
     }
@@ -1230,7 +1250,10 @@ void LsmDictionary::stage_configure(uint32_t slots, uint64_t max_keys, cudaStrea
   for (auto &w : stage_words_) GPULSM_CUDA(cudaMalloc(&w, max_keys * 8));
   GPULSM_CUDA(cudaMalloc(&stage_scratch_, bucket_admit_scratch_bytes(max_keys)));
   staged_.resize(slots);
-  for (Staged &x : staged_) x.run = pool_.acquire(max_keys, s);  // owned by the slot from now on
+  for (Staged &x : staged_) {
+    x.run = pool_.acquire(max_keys, s);  // owned by the slot from now on
+    x.run->dir_ok = true;                // its admissions write the directory
+  }
   end_op(s);
 }
 

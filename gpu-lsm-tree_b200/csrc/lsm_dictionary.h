@@ -50,6 +50,7 @@ struct RunBuffer {
   uint32_t model_segments = 0;
   uint64_t model_rows = 0;  // rows bound of a level that wants a model before its next read (0: none)
   bool model_ok = false;
+  bool dir_ok = false;      // the radix directory matches the rows (merges may leave it to the first read)
   // Last release: an event recorded on the releasing stream after the
   // launches that read the buffer; a reuse on another stream waits for it.
   cudaEvent_t freed = nullptr;
@@ -214,6 +215,9 @@ class LsmDictionary {
   void release_levels(cudaStream_t s);
   void fit_model(RunBuffer *run, uint64_t upper, cudaStream_t s);
   void fit_now(RunBuffer *run, uint64_t upper, cudaStream_t s);
+  // Before every read: the directories a merge left out are built, then the
+  // learned models of search mode 1 (and the next update's merges will write
+  // their directories: a read may follow them again).
   void ensure_models(cudaStream_t s);
   void *scratch(size_t bytes, cudaStream_t s);
   void *admit_scratch(size_t bytes, cudaStream_t s);
@@ -288,6 +292,12 @@ class LsmDictionary {
   cudaEvent_t adm_done_ = nullptr;
   cudaEvent_t merge_done_ = nullptr;
   bool merges_pending_ = false;
+  // Merges write their output's directory unless the operation before this
+  // update was an update too: levels rewritten by back-to-back update batches
+  // are mostly merged again before any read, so their directories are built
+  // by the read that needs them (ensure_models).
+  bool prev_update_ = false;
+  bool merge_dirs_ = true;
   // staged updates (serving): fixed staging runs, newest first by seq
   struct Staged {
     RunBuffer *run = nullptr;

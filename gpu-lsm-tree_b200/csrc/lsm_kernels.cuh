@@ -173,8 +173,49 @@ __device__ __forceinline__ void write_empty_desc(LevelDesc *d, uint32_t *dir) {
   d->kmax = 0u;
   d->shift = 0u;
   d->nbuckets = 1u;
-  dir[0] = 0u;
-  dir[1] = 0u;
+  if (dir) {
+    dir[0] = 0u;
+    dir[1] = 0u;
+  }
+}
+
+// The radix directory of a level whose merge skipped it: entry b is the first
+// row whose key's bucket is at least b (n when none) and entry nbuckets is n -
+// the entries the merge kernel writes when it builds the directory itself.
+// Geometry from the level's descriptor; rows past desc->n are not read.
+// Each thread takes 8 consecutive rows (two 16-byte loads: run buffers are
+// 16-byte aligned) and the key before them.
+constexpr uint32_t kDirRows = 8;
+
+__global__ void __launch_bounds__(256) build_directory_kernel(const uint32_t *__restrict__ keys,
+                                                              const LevelDesc *__restrict__ desc,
+                                                              uint32_t *__restrict__ dir) {
+  const uint64_t n = desc->n;
+  const uint32_t kmin = desc->kmin, shift = desc->shift, nb = desc->nbuckets;
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  const uint64_t t0 = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  // the buckets after the last row's (all of them for an empty level) close at n
+  const int64_t blast = n ? int64_t((keys[n - 1] - kmin) >> shift) : -1;
+  for (uint64_t b = uint64_t(blast + 1) + t0; b <= nb; b += stride) dir[b] = uint32_t(n);
+  for (uint64_t j0 = t0 * kDirRows; j0 < n; j0 += stride * kDirRows) {
+    uint32_t k[kDirRows];
+    if (j0 + kDirRows <= n) {
+      const uint4 *v = reinterpret_cast<const uint4 *>(keys + j0);
+      const uint4 x = __ldg(v), y = __ldg(v + 1);
+      k[0] = x.x, k[1] = x.y, k[2] = x.z, k[3] = x.w, k[4] = y.x, k[5] = y.y, k[6] = y.z, k[7] = y.w;
+    } else {
+#pragma unroll
+      for (uint32_t i = 0; i < kDirRows; ++i) k[i] = j0 + i < n ? keys[j0 + i] : 0u;
+    }
+    int64_t bp = j0 ? int64_t((keys[j0 - 1] - kmin) >> shift) : -1;
+#pragma unroll
+    for (uint32_t i = 0; i < kDirRows; ++i) {
+      if (j0 + i >= n) break;
+      const int64_t bj = int64_t((k[i] - kmin) >> shift);
+      for (int64_t b = bp + 1; b <= bj; ++b) dir[b] = uint32_t(j0 + i);
+      bp = bj;
+    }
+  }
 }
 
 // Keep the LAST word of every equal-key run of a stably sorted batch (the
@@ -585,25 +626,29 @@ __global__ void __launch_bounds__(kMergeThreads, 4) merge_kernel(
   const int32_t bp = has_prev ? int32_t((prev_key - gk) >> gs) : -1;
   const uint32_t g0 = uint32_t(gbase);
   const uint32_t *sout = sm.key + o4;
+  if (odir) {  // null: the directory is built when a read first needs it
 #pragma unroll
-  for (int i = 0; i < kMergeItems; ++i) {
-    const uint32_t j = uint32_t(i) * kMergeThreads + threadIdx.x;
-    // row j - 1 is the previous lane's row of the same item (lane 0: shared memory)
-    uint32_t pk = __shfl_up_sync(0xffffffffu, rk[i], 1);
-    if ((threadIdx.x & 31u) == 0 && j) pk = sout[j - 1];
-    if (j < tile_kept) {
-      const int32_t bj = int32_t((rk[i] - gk) >> gs);
-      const int32_t bprev = j ? int32_t((pk - gk) >> gs) : bp;
-      for (int32_t bb = bprev + 1; bb <= bj; ++bb) odir[bb] = g0 + j;
+    for (int i = 0; i < kMergeItems; ++i) {
+      const uint32_t j = uint32_t(i) * kMergeThreads + threadIdx.x;
+      // row j - 1 is the previous lane's row of the same item (lane 0: shared memory)
+      uint32_t pk = __shfl_up_sync(0xffffffffu, rk[i], 1);
+      if ((threadIdx.x & 31u) == 0 && j) pk = sout[j - 1];
+      if (j < tile_kept) {
+        const int32_t bj = int32_t((rk[i] - gk) >> gs);
+        const int32_t bprev = j ? int32_t((pk - gk) >> gs) : bp;
+        for (int32_t bb = bprev + 1; bb <= bj; ++bb) odir[bb] = g0 + j;
+      }
     }
   }
   const bool last_tile = d1 == total;
   const unsigned long long n_out = gbase + tile_kept;
   if (threadIdx.x == 0) {
-    const int32_t blast = tile_kept ? int32_t((sout[tile_kept - 1] - gk) >> gs) : bp;
-    const int32_t bl = last_tile ? int32_t(geom.nbuckets) - 1 : int32_t((last_key - gk) >> gs);
-    for (int32_t bb = blast + 1; bb <= bl; ++bb) odir[bb] = g0 + tile_kept;
-    if (last_tile) odir[geom.nbuckets] = uint32_t(n_out < out_capacity ? n_out : out_capacity);
+    if (odir) {
+      const int32_t blast = tile_kept ? int32_t((sout[tile_kept - 1] - gk) >> gs) : bp;
+      const int32_t bl = last_tile ? int32_t(geom.nbuckets) - 1 : int32_t((last_key - gk) >> gs);
+      for (int32_t bb = blast + 1; bb <= bl; ++bb) odir[bb] = g0 + tile_kept;
+      if (last_tile) odir[geom.nbuckets] = uint32_t(n_out < out_capacity ? n_out : out_capacity);
+    }
     if (tile == 0) {
       odesc->kmin = geom.kmin;
       odesc->kmax = geom.kmax;
@@ -617,7 +662,7 @@ __global__ void __launch_bounds__(kMergeThreads, 4) merge_kernel(
         trace[0] = na;
         trace[1] = nb;
         trace[2] = n_out < out_capacity ? n_out : out_capacity;
-        trace[3] = geom.nbuckets;
+        trace[3] = odir ? geom.nbuckets + 1u : 0u;  // directory entries written
       }
     }
     // the staged rows have been read out of shared memory before the CTA

@@ -143,7 +143,8 @@ int gpulsm_dict_size(gpulsm_dict *dict, uint64_t *out_rows, uint32_t *out_levels
  * rows it read and wrote.  _read (synchronises) returns, over the merges
  * timed since the previous read, the launch count, the summed device time in
  * ms and the algorithmic bytes (9 B per row read, 9 B per row written, 4 B
- * per directory entry). */
+ * per directory entry written; the merges of an update that follows another
+ * update leave their output's directory to the first read that needs it). */
 int gpulsm_dict_kernel_timing(gpulsm_dict *dict, int enable);
 int gpulsm_dict_kernel_timing_read(gpulsm_dict *dict, uint64_t *out_launches, double *out_ms,
                                    double *out_bytes);
