@@ -201,8 +201,9 @@ __device__ __forceinline__ void write_rows(const At &at, uint32_t cnt, const Row
         out_flags[r] = f;
       }
       // the first element of a run writes the directory entries its row starts
+      // (no directory: it is built when a read first needs it)
       const uint32_t kp = e > 0 ? word_key(at(e - 1)) : 0u;
-      if (e == 0 || kp != k) {
+      if (dir && (e == 0 || kp != k)) {
         const int64_t bprev = e > 0 ? int64_t((kp - g.kmin) >> g.shift) : bp;
         const int64_t bj = int64_t((k - g.kmin) >> g.shift);
         for (int64_t b = bprev + 1; b <= bj; ++b)
@@ -679,8 +680,9 @@ __global__ void __launch_bounds__(kThreads, 2) admit_bucket_kernel(
         out_flags[r] = f;
       }
       // the first element of a run writes the directory entries its row starts
+      // (no directory: it is built when a read first needs it)
       const uint32_t kp = e > 0 ? word_key(w[e - 1]) : 0u;
-      if (e == 0 || kp != k) {
+      if (out_dir && (e == 0 || kp != k)) {
         const int32_t bprev = e > 0 ? int32_t((kp - g.kmin) >> g.shift) : bp;
         const int32_t bj = int32_t((k - g.kmin) >> g.shift);
         for (int32_t bb = bprev + 1; bb <= bj; ++bb)
@@ -697,7 +699,7 @@ __global__ void __launch_bounds__(kThreads, 2) admit_bucket_kernel(
     }
     write_rows(by_array, cnt, src, out_keys, out_vals, out_flags, g0, sm.rank, out_dir, g, int64_t(bp));
   }
-  if (threadIdx.x == 0) {
+  if (out_dir && threadIdx.x == 0) {
     // an empty bucket between the first and the last one only closes its range
     const int32_t blast = cnt ? int32_t((word_key(sorted[cnt - 1]) - g.kmin) >> g.shift) : bp;
     for (int32_t bb = blast + 1; bb <= bl; ++bb)

@@ -441,9 +441,9 @@ void LsmDictionary::release_levels(cudaStream_t s) {
 
 // ----------------------------------------------------------------------------
 RunBuffer *LsmDictionary::sort_dedup(const uint32_t *keys, const uint32_t *values, uint64_t n,
-                                     bool tombstone, cudaStream_t s, const uint8_t *erase) {
+                                     bool tombstone, cudaStream_t s, const uint8_t *erase, bool write_dir) {
   ensure_sort_space(n, s);
-  if (n <= lsm::admit::kMaxKeys) return bucket_admit(keys, values, erase, n, tombstone, s);
+  if (n <= lsm::admit::kMaxKeys) return bucket_admit(keys, values, erase, n, tombstone, s, write_dir);
   // update batches are tiled to at most kMaxBatch = 2^20 rows: only a bulk
   // build (never mixed) takes the four-pass sort
   if (erase) throw std::logic_error("mixed batches are admitted by top-byte buckets only");
@@ -482,11 +482,11 @@ size_t LsmDictionary::bucket_admit_scratch_bytes(uint64_t n) {
 }
 
 RunBuffer *LsmDictionary::bucket_admit(const uint32_t *keys, const uint32_t *values, const uint8_t *erase,
-                                       uint64_t n, bool tombstone, cudaStream_t s) {
+                                       uint64_t n, bool tombstone, cudaStream_t s, bool write_dir) {
   void *scratch = admit_scratch(bucket_admit_scratch_bytes(n), s);
   // before the chain: a fresh buffer is a stream-ordered allocation
   RunBuffer *carry = pool_.acquire(n, s, true);
-  bucket_admit_into(keys, values, erase, n, tombstone, s, carry, words_[0], words_[1], scratch);
+  bucket_admit_into(keys, values, erase, n, tombstone, s, carry, words_[0], words_[1], scratch, write_dir);
   return carry;
 }
 
@@ -495,7 +495,8 @@ RunBuffer *LsmDictionary::bucket_admit(const uint32_t *keys, const uint32_t *val
 // position); its rows take value and flag from the batch by that position.
 void LsmDictionary::bucket_admit_into(const uint32_t *keys, const uint32_t *values, const uint8_t *erase,
                                       uint64_t n, bool tombstone, cudaStream_t s, RunBuffer *carry,
-                                      unsigned long long *w0, unsigned long long *w1, void *scratch) {
+                                      unsigned long long *w0, unsigned long long *w1, void *scratch,
+                                      bool write_dir) {
   namespace ad = lsm::admit;
   const uint32_t nn = uint32_t(n);
   const uint32_t tiles = ad::part_tiles(n);
@@ -517,8 +518,8 @@ void LsmDictionary::bucket_admit_into(const uint32_t *keys, const uint32_t *valu
   const ad::RowSource src{mixed ? values : nullptr, erase, tombstone ? 1 : 0};
   launch_chained(ad::admit_bucket_kernel, ad::kBuckets, ad::kThreads, ad::kBucketSmemBytes, s, w1, w0,
                  static_cast<const uint32_t *>(top), nn, src, carry->keys, carry->vals, carry->flags, carry->desc,
-                 carry->dir, carry->dir_bits, rows_log2_, lb, counter, dev_status_);
-  carry->dir_ok = true;
+                 write_dir ? carry->dir : nullptr, carry->dir_bits, rows_log2_, lb, counter, dev_status_);
+  carry->dir_ok = write_dir;
 }
 
 RunBuffer *LsmDictionary::merge(RunBuffer *newer, RunBuffer *older, uint64_t out_upper,
@@ -848,7 +849,7 @@ void LsmDictionary::admit(const uint32_t *keys, const uint32_t *values, const ui
     // The receipt comes from the merge stream (the final merge, or a receipt
     // kernel when nothing merges), so receipts land in batch order.
     RunBuffer *carry = sort_dedup(keys + off, values ? values + off : nullptr, m, tombstone, s,
-                                  erase ? erase + off : nullptr);
+                                  erase ? erase + off : nullptr, merge_dirs_);
     GPULSM_CUDA(cudaEventRecord(adm_done_, s));
     GPULSM_CUDA(cudaStreamWaitEvent(merge_stream_, adm_done_, 0));
     merges_pending_ = true;

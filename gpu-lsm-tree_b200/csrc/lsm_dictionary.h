@@ -180,13 +180,14 @@ class LsmDictionary {
   // erase: the erase marks of a mixed batch (null for insert / erase batches)
   void admit(const uint32_t *keys, const uint32_t *values, const uint8_t *erase, uint64_t n, bool tombstone,
              cudaStream_t s);
+  // write_dir false: the run's directory is left to the first read (dir_ok)
   RunBuffer *sort_dedup(const uint32_t *keys, const uint32_t *values, uint64_t n, bool tombstone,
-                        cudaStream_t s, const uint8_t *erase = nullptr);
+                        cudaStream_t s, const uint8_t *erase = nullptr, bool write_dir = true);
   RunBuffer *bucket_admit(const uint32_t *keys, const uint32_t *values, const uint8_t *erase, uint64_t n,
-                          bool tombstone, cudaStream_t s);
+                          bool tombstone, cudaStream_t s, bool write_dir);
   void bucket_admit_into(const uint32_t *keys, const uint32_t *values, const uint8_t *erase, uint64_t n,
                          bool tombstone, cudaStream_t s, RunBuffer *out, unsigned long long *w0,
-                         unsigned long long *w1, void *scratch);
+                         unsigned long long *w1, void *scratch, bool write_dir = true);
   static size_t bucket_admit_scratch_bytes(uint64_t n);
   void flush_staged_locked(cudaStream_t s);
   bool stage_seq_pending() const {
