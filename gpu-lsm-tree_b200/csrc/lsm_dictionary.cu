@@ -583,8 +583,10 @@ void LsmDictionary::fit_model(RunBuffer *run, uint64_t upper, cudaStream_t) {
 
 void LsmDictionary::ensure_models(cudaStream_t s) {
   prev_update_ = false;
+  // a level searched by binary search (mode 2) or by its learned model
+  // (mode 1, levels with a model) never reads its directory
   for (auto &l : levels_)
-    if (l.run && !l.run->dir_ok) {
+    if (l.run && !l.run->dir_ok && cfg_.search_mode != 2 && !(cfg_.search_mode == 1 && l.run->model_rows)) {
       lsm::build_directory_kernel<<<grid_for((l.upper + lsm::kDirRows) / lsm::kDirRows, 256), 256, 0, s>>>(
           l.run->keys, l.run->desc, l.run->dir);
       note_launch();
