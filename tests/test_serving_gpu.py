@@ -208,3 +208,49 @@ def test_staged_updates_merge_into_levels_and_stay_exact(gl, cuda):
     st = srv.stats()
     assert st["graph_updates"] == 40 and st["stage_flushes"] >= 5
     srv.close()
+
+
+def test_request_ring_wraps_and_stays_exact(gl, cuda):
+    """Requests are copied into the server's pinned ring at submit.  A small
+    round limit (2^12 keys, a ring of 200 KB) and ~12 MB of requests wrap the
+    ring many times, with requests of the largest size (which start over at
+    the ring's beginning when they do not fit before its end) and empty
+    requests in between; every result still equals the oracle replayed in the
+    server's round order."""
+    rng = np.random.default_rng(31)
+    base_k = rng.integers(0, 1 << 32, 1 << 14, dtype=np.uint64).astype(np.uint32)
+    base_v = np.arange(base_k.size, dtype=np.uint32)
+    universe = np.concatenate([base_k, rng.integers(0, 1 << 32, 1 << 12, dtype=np.uint64).astype(np.uint32)])
+    srv = gl.Server(gl.DictionaryConfig(max_elements=1 << 20, batch_capacity=1 << 12), budget_bytes=4 << 30,
+                    max_round_keys=1 << 12, depth=2)
+    srv.bulk_build(to_dev(base_k), to_dev(base_v))
+    reqs = []
+    for i in range(3000):
+        kind = KINDS[rng.choice(4, p=[0.5, 0.2, 0.15, 0.15])]
+        n = int(rng.choice([0, 1, 17, 300, 4096])) if i % 7 else 4096
+        keys = universe[rng.integers(0, universe.size, n)]
+        if kind == "insert":
+            reqs.append((kind, keys, rng.integers(0, 1 << 32, n, dtype=np.uint64).astype(np.uint32)))
+        elif kind == "range":
+            hi = np.minimum(keys.astype(np.uint64) + (1 << 22), 0xFFFFFFFF).astype(np.uint32)
+            reqs.append((kind, keys, hi))
+        else:
+            reqs.append((kind, keys, None))
+    done = []
+    window = []
+    for req in reqs:  # keep up to 48 requests in flight
+        window.append((submit(srv, req), req))
+        if len(window) >= 48:
+            tk, rq = window.pop(0)
+            done.append((tk, rq, srv.wait(tk)))
+    for tk, rq in window:
+        done.append((tk, rq, srv.wait(tk)))
+    assert srv.stats()["rejected"] == 0
+    srv.close()
+    # empty requests complete without a round (round 0): they change nothing
+    order = sorted(done, key=lambda x: (x[0].round, x[1][0] not in ("insert", "erase"), x[0].id))
+    want = oracle_answers(base_k, base_v, [rq for _, rq, _ in order])
+    for i, ((tk, rq, got), w) in enumerate(zip(order, want)):
+        if rq[1].size == 0:
+            continue
+        assert same(got, w), f"request {tk.id} ({rq[0]}, {rq[1].size} keys, round {tk.round}) differs from the oracle"
