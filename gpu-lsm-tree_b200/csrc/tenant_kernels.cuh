@@ -436,15 +436,24 @@ __device__ __forceinline__ unsigned long long fence_lower_bound(const uint32_t *
     const uint32_t *lv = fences + offs[l];
     const unsigned long long lo = l == int(levels) ? 0ull : b * F;
     const unsigned long long hi = l == int(levels) ? sizes[l] : min(lo + F, sizes[l]);
-    unsigned long long j = lo;
-    // last entry <= q (entries are first keys of their blocks)
-    while (j + 1 < hi && lv[j + 1] <= q) ++j;
-    b = j;
+    // last entry <= q (entries are first keys of their blocks; lo when
+    // none): binary search for the first entry after lo that is > q
+    unsigned long long a = lo + 1, z = hi > lo ? hi : lo + 1;
+    while (a < z) {
+      const unsigned long long mid = (a + z) >> 1;
+      if (lv[mid] <= q) a = mid + 1;
+      else z = mid;
+    }
+    b = a - 1;
   }
-  const unsigned long long lo = b * F, hi = min(lo + F, n);
-  unsigned long long j = lo;
-  while (j < hi && keys[j] < q) ++j;
-  return j;
+  // first key >= q in the chosen block of the run
+  unsigned long long a = b * F, z = min(a + F, n);
+  while (a < z) {
+    const unsigned long long mid = (a + z) >> 1;
+    if (keys[mid] < q) a = mid + 1;
+    else z = mid;
+  }
+  return a;
 }
 
 // Lookups: (tenant, key) -> value / found; delta first (newer), then main.
