@@ -155,6 +155,7 @@ class LsmDictionary {
   void launch_stage_graph(cudaGraphExec_t exec, uint32_t slot, uint64_t n, bool tombs, cudaStream_t s);
   void stage_flush(cudaStream_t s);
   uint64_t stage_flushes() const { return stage_flushes_; }
+  uint32_t stage_slots() const { return uint32_t(staged_.size()); }
 
   // Introspection for tests and benchmarks.
   uint32_t level_count() const { return uint32_t(caps_.size()); }

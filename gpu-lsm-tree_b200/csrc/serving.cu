@@ -130,6 +130,7 @@ Server::Server(const DictConfig &cfg, uint64_t budget_bytes, uint32_t max_round_
     GPULSM_CUDA(cudaStreamSynchronize(compute_));
     stage_ready_ = true;
   }
+  prepare_lookup_graphs();
   worker_ = std::thread(&Server::worker, this);
   completer_ = std::thread(&Server::completer, this);
 }
@@ -266,6 +267,25 @@ void Server::set_staged_updates(bool on) {
     GPULSM_CUDA(cudaStreamSynchronize(compute_));
   }
   staged_updates_ = on;
+  if (on) prepare_update_graphs();
+}
+
+void Server::prepare_lookup_graphs() {
+  for (Slot &slot : slots_)
+    for (uint64_t c = 1024;; c <<= 1) {
+      (void)lookup_graph(slot, uint32_t(std::min<uint64_t>(c, max_round_keys_)));
+      if (c >= max_round_keys_) break;
+    }
+}
+
+void Server::prepare_update_graphs() {
+  const uint32_t stages = dict_.stage_slots();
+  for (uint64_t n = 1; n <= max_round_keys_;) {  // every size class once
+    const uint64_t c = size_class(n);
+    for (int mode = kStageInsert; mode <= kStageMixed; ++mode)
+      for (uint32_t st = 0; st < stages; ++st) (void)update_graph(mode, uint32_t(c), st);
+    n = c + 1;
+  }
 }
 
 void Server::reset_stats() {

@@ -181,6 +181,11 @@ class Server {
   // the graph of a staged update (kStage* mode) of `size_class` keys into staging slot `stage`
   cudaGraphExec_t update_graph(int mode, uint32_t size_class, uint32_t stage);
   uint64_t size_class(uint64_t n) const;
+  // capture and instantiate every graph a round may replay (lookup rounds:
+  // per slot and size class; staged updates: per mode, size class and
+  // staging slot), so that no round pays a first capture
+  void prepare_lookup_graphs();
+  void prepare_update_graphs();
   // staging input words of a round with these update / lookup / range-sum key counts
   uint64_t round_words(uint64_t nu, bool mixed, uint64_t nl, uint64_t nr) const;
   static double now_s();
