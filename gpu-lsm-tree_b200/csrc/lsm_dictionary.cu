@@ -1009,7 +1009,12 @@ void LsmDictionary::lookup(const uint32_t *queries, uint64_t n, uint32_t *out_va
   ensure_models(s);
   lsm::LevelSet set;
   level_set(&set);
-  lsm::lookup_kernel<<<grid_for(n, 256), 256, 0, s>>>(set, queries, n, out_values, out_found); note_launch();
+  if (cfg_.search_mode != 2)
+    lsm::lookup_kernel<true><<<grid_for((n + lsm::kLookupPair - 1) / lsm::kLookupPair, 256), 256, 0, s>>>(
+        set, queries, n, out_values, out_found);
+  else
+    lsm::lookup_kernel<false><<<grid_for(n, 256), 256, 0, s>>>(set, queries, n, out_values, out_found);
+  note_launch();
   GPULSM_CUDA(cudaGetLastError());
   end_op(s);
 }
@@ -1175,8 +1180,12 @@ uint32_t LsmDictionary::status() {
 void LsmDictionary::enqueue_table_lookup(const uint32_t *queries, uint64_t n, uint32_t *out_values,
                                          uint8_t *out_found, cudaStream_t capturing) {
   std::lock_guard<std::mutex> g(mu_);
-  lsm::lookup_table_kernel<<<grid_for(n, 256), 256, 0, capturing>>>(static_cast<const lsm::LevelSet *>(table_dev_),
-                                                                     queries, n, out_values, out_found);
+  const auto *table = static_cast<const lsm::LevelSet *>(table_dev_);
+  if (cfg_.search_mode != 2)
+    lsm::lookup_table_kernel<true><<<grid_for((n + lsm::kLookupPair - 1) / lsm::kLookupPair, 256), 256, 0,
+                                     capturing>>>(table, queries, n, out_values, out_found);
+  else
+    lsm::lookup_table_kernel<false><<<grid_for(n, 256), 256, 0, capturing>>>(table, queries, n, out_values, out_found);
   GPULSM_CUDA(cudaGetLastError());
 }
 

@@ -773,17 +773,129 @@ __device__ __forceinline__ void lookup_one(const LevelSet &set, uint64_t i, cons
   if (out_found) out_found[i] = 0u;
 }
 
+// Two point lookups per thread with their loads interleaved: each level's
+// directory words of both queries are loaded together, then the rows of both
+// buckets (up to kProbeRows rows each, independent loads of one to three
+// sectors), then the values of the hits - two dependent chains in flight per
+// thread instead of one, the same sectors read.  A bucket of more rows (rare:
+// a directory bucket holds about 8) takes bucket_lower_bound; a level
+// searched by its model or by binary search takes level_lower_bound.  Answers
+// equal lookup_one's.  Thread t of a block of B threads takes the queries
+// i0 = block * 2B + t and i0 + B (coalesced for both).
+constexpr uint32_t kProbeRows = 16;
+constexpr uint32_t kLookupPair = 2;
+
+__device__ __forceinline__ void lookup_pair(const LevelSet &set, uint64_t i0, uint64_t n,
+                                            const uint32_t *__restrict__ queries, uint32_t *__restrict__ out_values,
+                                            uint8_t *__restrict__ out_found) {
+  constexpr int Q = int(kLookupPair);
+  const uint64_t idx[Q] = {i0, i0 + blockDim.x};
+  uint32_t q[Q], val[Q];
+  bool done[Q], fnd[Q];
+  const uint32_t miss = out_found ? 0u : kNotFound;
+#pragma unroll
+  for (int j = 0; j < Q; ++j) {
+    done[j] = idx[j] >= n;
+    q[j] = done[j] ? 0u : queries[idx[j]];
+    val[j] = miss;
+    fnd[j] = false;
+  }
+  const uint64_t keep = l2_keep_policy();
+  for (uint32_t l = 0; l < set.count; ++l) {
+    if (done[0] && done[1]) break;
+    const LevelView &L = set.lv[l];
+    const LevelDesc d = load_desc(L.desc);
+    bool act[Q];
+#pragma unroll
+    for (int j = 0; j < Q; ++j) act[j] = !done[j] && q[j] >= d.kmin && q[j] <= d.kmax;
+    uint32_t p[Q];
+    bool hit[Q];
+    if (L.dir && !L.ms) {
+      uint32_t s[Q], e[Q];
+#pragma unroll
+      for (int j = 0; j < Q; ++j) {  // the directory words of both queries
+        s[j] = e[j] = 0;
+        if (act[j]) {
+          const uint32_t b = (q[j] - d.kmin) >> d.shift;
+          s[j] = ld_hint(L.dir + b, keep);
+          e[j] = ld_hint(L.dir + b + 1, keep);
+        }
+      }
+      uint32_t k[Q][kProbeRows];
+#pragma unroll
+      for (int j = 0; j < Q; ++j)  // the rows of both buckets
+#pragma unroll
+        for (uint32_t t = 0; t < kProbeRows; ++t)
+          k[j][t] = (act[j] && e[j] - s[j] <= kProbeRows && s[j] + t < e[j]) ? L.keys[s[j] + t] : 0u;
+#pragma unroll
+      for (int j = 0; j < Q; ++j) {
+        hit[j] = false;
+        p[j] = s[j];
+        if (!act[j]) continue;
+        if (e[j] - s[j] <= kProbeRows) {
+#pragma unroll
+          for (uint32_t t = 0; t < kProbeRows; ++t)
+            if (s[j] + t < e[j]) {
+              p[j] += k[j][t] < q[j] ? 1u : 0u;
+              hit[j] = hit[j] || k[j][t] == q[j];
+            }
+        } else {
+          p[j] = uint32_t(bucket_lower_bound(L.keys, s[j], e[j], q[j]));
+          hit[j] = p[j] < e[j] && L.keys[p[j]] == q[j];
+        }
+      }
+    } else {  // learned model window or binary search
+#pragma unroll
+      for (int j = 0; j < Q; ++j) {
+        hit[j] = false;
+        p[j] = 0;
+        if (!act[j]) continue;
+        const uint64_t pp = level_lower_bound(L, d, q[j]);
+        p[j] = uint32_t(pp);
+        hit[j] = pp < d.n && L.keys[pp] == q[j];
+      }
+    }
+    uint32_t v[Q];
+#pragma unroll
+    for (int j = 0; j < Q; ++j) v[j] = hit[j] ? L.vals[p[j]] : 0u;  // the values of both hits
+#pragma unroll
+    for (int j = 0; j < Q; ++j)
+      if (hit[j]) {
+        const bool live = !row_is_tomb(L, p[j], v[j]);
+        val[j] = live ? v[j] : miss;
+        fnd[j] = live;
+        done[j] = true;
+      }
+  }
+#pragma unroll
+  for (int j = 0; j < Q; ++j)
+    if (idx[j] < n) {
+      out_values[idx[j]] = val[j];
+      if (out_found) out_found[idx[j]] = fnd[j];
+    }
+}
+
+// kPair: two queries per thread (directory and learned levels); without it
+// one query per thread (binary search, whose long per-query chains gain
+// nothing from pairing at the lower occupancy pairing costs).
+template <bool kPair>
 __global__ void __launch_bounds__(256) lookup_kernel(LevelSet set, const uint32_t *__restrict__ queries,
                                                      uint64_t n, uint32_t *__restrict__ out_values,
                                                      uint8_t *__restrict__ out_found) {
-  const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i < n) lookup_one(set, i, queries, out_values, out_found);
+  if (kPair) {
+    const uint64_t i = uint64_t(blockIdx.x) * blockDim.x * kLookupPair + threadIdx.x;
+    if (i < n) lookup_pair(set, i, n, queries, out_values, out_found);
+  } else {
+    const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) lookup_one(set, i, queries, out_values, out_found);
+  }
 }
 
 // The same lookup with the level set read from device memory (a level table
 // the dictionary rewrites when its levels change), so that a captured CUDA
 // graph stays valid across updates; every block copies the table to shared
 // memory first.
+template <bool kPair>
 __global__ void __launch_bounds__(256) lookup_table_kernel(const LevelSet *__restrict__ table,
                                                            const uint32_t *__restrict__ queries, uint64_t n,
                                                            uint32_t *__restrict__ out_values,
@@ -794,8 +906,13 @@ __global__ void __launch_bounds__(256) lookup_table_kernel(const LevelSet *__res
   for (uint32_t w = threadIdx.x; w < sizeof(LevelSet) / 4; w += blockDim.x) s_words[w] = src[w];
   __syncthreads();
   const LevelSet &s_set = *reinterpret_cast<const LevelSet *>(s_words);
-  const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i < n) lookup_one(s_set, i, queries, out_values, out_found);
+  if (kPair) {
+    const uint64_t i = uint64_t(blockIdx.x) * blockDim.x * kLookupPair + threadIdx.x;
+    if (i < n) lookup_pair(s_set, i, n, queries, out_values, out_found);
+  } else {
+    const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) lookup_one(s_set, i, queries, out_values, out_found);
+  }
 }
 
 __global__ void write_table_kernel(LevelSet set, LevelSet *__restrict__ table) {
