@@ -152,13 +152,14 @@ def test_flix_same_answers_as_reference_kernels(gl, cuda, workloads):
     # warm-up on separate small indexes: an insert and a remove are timed once
     # per round (they change the index), so each engine's first-call costs
     # (kernel loading, first stream-ordered allocations) are paid here
-    for eng in (refgpu.RefFlix(32), gl.FlixIndex(key_bits=32, max_elements=1 << 20)):
-        wk = dk(w.build_keys[: 1 << 16])
-        eng.build_bucket_layer_only(wk, 1 << 20) if isinstance(eng, refgpu.RefFlix) else \
-            eng.build_bucket_layer_only(wk, max_size=1 << 20)
-        ins0, vals0, dels0 = rounds[0][0][: 1 << 12], rounds[0][1][: 1 << 12], rounds[0][2][: 1 << 11]
-        eng.insert(ins0, vals0)
-        eng.remove(dels0)
+    # (a round-0-sized insert and remove, so that their workspaces reach full size)
+    warm_keys = np.sort(w.build_keys[: 1 << 18])
+    for eng in (refgpu.RefFlix(32), gl.FlixIndex(key_bits=32, max_elements=1 << 21)):
+        wk = dk(warm_keys)
+        eng.build_bucket_layer_only(wk, 1 << 21) if isinstance(eng, refgpu.RefFlix) else \
+            eng.build_bucket_layer_only(wk, max_size=1 << 21)
+        eng.insert(rounds[0][0], rounds[0][1])
+        eng.remove(dk(warm_keys[::2]))
         torch.cuda.synchronize()
     ref = refgpu.RefFlix(32)
     ours = gl.FlixIndex(key_bits=32, max_elements=max_size)
