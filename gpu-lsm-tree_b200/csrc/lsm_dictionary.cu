@@ -1137,9 +1137,14 @@ void LsmDictionary::range_pairs(const uint32_t *lo, const uint32_t *hi, uint64_t
   const int single = ranges_on_single_level(lo, hi, n, s);
   ensure_models(s);  // a compaction wrote a new level
   if (single >= 0) {
-    const unsigned grid = std::min<unsigned>(grid_for(n * 32, 256), unsigned(num_sms_) * 64u);
+    // resident warps take the query groups from a counter
+    uint32_t *counter = static_cast<uint32_t *>(scratch(sizeof(uint32_t), s));
+    GPULSM_CUDA(cudaMemsetAsync(counter, 0, sizeof(uint32_t), s));
+    const uint64_t groups = (n + lsm::kPairsGroup - 1) / lsm::kPairsGroup;
+    const unsigned grid = std::min<unsigned>(grid_for(groups * 32, 256), unsigned(num_sms_) * 8u);
     lsm::single_level_pairs_kernel<<<grid, 256, 0, s>>>(
-        view_of(single), lo, hi, n, reinterpret_cast<const unsigned long long *>(offsets), out_keys, out_values);
+        view_of(single), lo, hi, n, reinterpret_cast<const unsigned long long *>(offsets), out_keys, out_values,
+        counter);
     note_launch();
   } else {
     lsm::LevelSet set;

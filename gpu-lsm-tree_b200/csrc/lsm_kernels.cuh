@@ -1104,42 +1104,77 @@ __global__ void __launch_bounds__(256) single_level_range_kernel(
   out[q] = r;
 }
 
-// pairs: one warp per query copies its row slice (coalesced, 4 rows in flight per lane)
+// pairs: warps take groups of 32 queries from a counter (a slice may hold
+// tens of thousands of rows, so a fixed share per warp would leave a long
+// tail).  Every lane finds the row slice of one query of the group (the 32
+// searches overlap), a lane whose slice is short copies it alone, then the
+// warp copies each longer slice together (coalesced, 8 rows in flight per
+// lane).  counter starts at zero.
+constexpr uint32_t kPairsShort = 8;  // rows a lane copies alone
+constexpr uint32_t kPairsGroup = 32;
+
 __global__ void __launch_bounds__(256) single_level_pairs_kernel(
     LevelView L, const uint32_t *__restrict__ lo, const uint32_t *__restrict__ hi, uint64_t n,
     const unsigned long long *__restrict__ offsets, uint32_t *__restrict__ out_keys,
-    uint32_t *__restrict__ out_vals) {
+    uint32_t *__restrict__ out_vals, uint32_t *__restrict__ counter) {
   const uint32_t lane = threadIdx.x & 31;
-  const uint64_t warps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
   const LevelDesc d = load_desc(L.desc);
-  for (uint64_t q = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; q < n; q += warps) {
-    const uint32_t a = lo[q], z = hi[q];
-    if (a > z) continue;
-    uint64_t b = 0, e = 0;
-    if (lane == 0) {
-      b = level_lower_bound(L, d, a);
-      e = level_upper_bound(L, d, z);
+  const uint32_t *__restrict__ keys = L.keys;
+  const uint32_t *__restrict__ vals = L.vals;
+  const uint64_t groups = (n + kPairsGroup - 1) / kPairsGroup;
+  for (;;) {
+    uint32_t grp = 0;
+    if (lane == 0) grp = atomicAdd(counter, 1u);
+    grp = __shfl_sync(0xffffffffu, grp, 0);
+    if (grp >= groups) break;  // uniform across the warp
+    const uint64_t q = uint64_t(grp) * kPairsGroup + lane;
+    uint64_t b = 0, len = 0, o = 0;
+    if (q < n) {
+      const uint32_t a = lo[q], z = hi[q];
+      o = offsets[q];
+      if (a <= z) {
+        b = level_lower_bound(L, d, a);
+        const uint64_t e = level_upper_bound(L, d, z);
+        len = e > b ? e - b : 0;
+      }
     }
-    b = __shfl_sync(0xffffffffu, b, 0);
-    e = __shfl_sync(0xffffffffu, e, 0);
-    const unsigned long long o = offsets[q];
-    const uint64_t len = e > b ? e - b : 0;
-    uint64_t j = lane;
-    for (; j + 96 < len; j += 128) {
-      const uint32_t k0 = L.keys[b + j], k1 = L.keys[b + j + 32], k2 = L.keys[b + j + 64], k3 = L.keys[b + j + 96];
-      const uint32_t v0 = L.vals[b + j], v1 = L.vals[b + j + 32], v2 = L.vals[b + j + 64], v3 = L.vals[b + j + 96];
-      out_keys[o + j] = k0;
-      out_keys[o + j + 32] = k1;
-      out_keys[o + j + 64] = k2;
-      out_keys[o + j + 96] = k3;
-      out_vals[o + j] = v0;
-      out_vals[o + j + 32] = v1;
-      out_vals[o + j + 64] = v2;
-      out_vals[o + j + 96] = v3;
+    if (len <= kPairsShort) {
+      uint32_t k[kPairsShort], v[kPairsShort];
+#pragma unroll
+      for (uint32_t i = 0; i < kPairsShort; ++i)
+        if (i < len) {
+          k[i] = keys[b + i];
+          v[i] = vals[b + i];
+        }
+#pragma unroll
+      for (uint32_t i = 0; i < kPairsShort; ++i)
+        if (i < len) {
+          out_keys[o + i] = k[i];
+          out_vals[o + i] = v[i];
+        }
     }
-    for (; j < len; j += 32) {
-      out_keys[o + j] = L.keys[b + j];
-      out_vals[o + j] = L.vals[b + j];
+    for (uint32_t longs = __ballot_sync(0xffffffffu, len > kPairsShort); longs; longs &= longs - 1) {
+      const int src = __ffs(longs) - 1;
+      const uint64_t sb = __shfl_sync(0xffffffffu, b, src), so = __shfl_sync(0xffffffffu, o, src);
+      const uint64_t sl = __shfl_sync(0xffffffffu, len, src);
+      uint64_t j = lane;
+      for (; j + 224 < sl; j += 256) {
+        uint32_t k[8], v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          k[u] = keys[sb + j + 32 * u];
+          v[u] = vals[sb + j + 32 * u];
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          out_keys[so + j + 32 * u] = k[u];
+          out_vals[so + j + 32 * u] = v[u];
+        }
+      }
+      for (; j < sl; j += 32) {
+        out_keys[so + j] = keys[sb + j];
+        out_vals[so + j] = vals[sb + j];
+      }
     }
   }
 }
