@@ -642,6 +642,9 @@ def serving_leg(args, gl, w, dev):
             "mkeys_s": round(half["keys"] / max(half["wall_s"], 1e-9) / 1e6, 1),
             "p50_ms": round(half["p50_us"] / 1e3, 4), "p99_ms": round(half["p99_us"] / 1e3, 4),
             "max_ms": round(half["max_us"] / 1e3, 4),
+            # the worst round at half load: its device time and the worker's launch time
+            "max_round_gpu_ms": round(half["max_round_gpu_us"] / 1e3, 4),
+            "max_launch_ms": round(half["max_launch_us"] / 1e3, 4),
             "peak_p50_ms": round(peak["p50_us"] / 1e3, 4), "peak_p99_ms": round(peak["p99_us"] / 1e3, 4),
             "mean_round_keys": round(half["mean_round_keys"], 1),
             "peak_mean_round_keys": round(peak["mean_round_keys"], 1),

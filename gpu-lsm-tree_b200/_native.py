@@ -122,6 +122,8 @@ class ServeStats(C.Structure):
         ("host_scatter_s", C.c_double),
         ("graph_updates", C.c_uint64),
         ("stage_flushes", C.c_uint64),
+        ("max_round_gpu_us", C.c_double),
+        ("max_launch_us", C.c_double),
     ]
 
 

@@ -148,6 +148,8 @@ void copy_stats(const gpulsm::ServeStats &s, gpulsm_serve_stats *o) {
   o->host_scatter_s = s.host_scatter_s;
   o->graph_updates = s.graph_updates;
   o->stage_flushes = s.stage_flushes;
+  o->max_round_gpu_us = s.max_round_gpu_us;
+  o->max_launch_us = s.max_launch_us;
 }
 }  // namespace
 

@@ -87,6 +87,7 @@ RunPool::~RunPool() {
     if (b->model) cudaFree(b->model);
     if (b->freed) cudaEventDestroy(b->freed);
   }
+  if (trim_pool_) cudaMemPoolTrimTo(trim_pool_, 0);  // freed memory goes back to the driver
 }
 
 RunBuffer *RunPool::acquire(uint64_t min_rows, cudaStream_t stream, bool settled_only) {
@@ -207,6 +208,18 @@ LsmDictionary::LsmDictionary(const DictConfig &config)
   int dev = 0;
   GPULSM_CUDA(cudaGetDevice(&dev));
   GPULSM_CUDA(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, dev));
+  // Runs, prefixes and scratch are stream-ordered allocations from the
+  // device's default pool.  By default the pool returns freed memory to the
+  // driver at every synchronisation, so a buffer allocated again later maps
+  // fresh memory on the calling thread (tens of milliseconds for hundreds of
+  // MB, a stall a serving loop sees in its latency tail).  The pool keeps
+  // freed memory instead (a property of this process's pool; the run pool's
+  // destructor trims what is unused).
+  cudaMemPool_t mem_pool = nullptr;
+  GPULSM_CUDA(cudaDeviceGetDefaultMemPool(&mem_pool, dev));
+  uint64_t keep = ~0ull;
+  GPULSM_CUDA(cudaMemPoolSetAttribute(mem_pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  pool_.trim_on_destroy(mem_pool);
   GPULSM_CUDA(cudaFuncSetAttribute(lsm::admit::admit_bucket_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    int(lsm::admit::kBucketSmemBytes)));
   // two bucket CTAs per SM need nearly all of its shared memory
@@ -226,6 +239,8 @@ LsmDictionary::LsmDictionary(const DictConfig &config)
   GPULSM_CUDA(cudaStreamCreateWithFlags(&merge_stream_, cudaStreamNonBlocking));
   GPULSM_CUDA(cudaEventCreateWithFlags(&adm_done_, cudaEventDisableTiming));
   GPULSM_CUDA(cudaEventCreateWithFlags(&merge_done_, cudaEventDisableTiming));
+  GPULSM_CUDA(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
+  GPULSM_CUDA(cudaEventCreateWithFlags(&side_done_, cudaEventDisableTiming));
 }
 
 LsmDictionary::~LsmDictionary() {
@@ -258,6 +273,8 @@ LsmDictionary::~LsmDictionary() {
   if (op_done_) cudaEventDestroy(op_done_);
   if (adm_done_) cudaEventDestroy(adm_done_);
   if (merge_done_) cudaEventDestroy(merge_done_);
+  if (fork_) cudaEventDestroy(fork_);
+  if (side_done_) cudaEventDestroy(side_done_);
   if (merge_stream_) cudaStreamDestroy(merge_stream_);
 }
 
@@ -331,7 +348,7 @@ void LsmDictionary::ensure_sort_space(uint64_t n, cudaStream_t s) {
     if (w) GPULSM_CUDA(cudaFreeAsync(w, s));
     w = nullptr;
   }
-  uint64_t cap = std::max<uint64_t>(n, batch_capacity_);
+  uint64_t cap = std::max<uint64_t>({n, batch_capacity_, words_cap_ * 3 / 2});
   for (auto &w : words_)
     if (cudaMallocAsync(&w, cap * 8, s) != cudaSuccess) {
       (void)cudaGetLastError();
@@ -783,7 +800,7 @@ void LsmDictionary::live_level_set(void *out, cudaStream_t s) {
   std::sort(st.begin(), st.end(), [&](size_t a, size_t b) { return staged_[a].seq > staged_[b].seq; });
   for (size_t i : st) {
     LivePrefix &lp = live_staged_[i];
-    refresh_live_prefix(lp, staged_[i].run, staged_[i].upper, staged_[i].seq, s);
+    refresh_live_prefix(lp, staged_[i].run, staged_[i].upper, staged_[i].seq, staged_[i].run->cap + 1, s);
     lsm::LevelView v = view_of_run(staged_[i].run);
     v.live = lp.p;
     set->lv[set->count++] = v;
@@ -793,7 +810,9 @@ void LsmDictionary::live_level_set(void *out, cudaStream_t s) {
     const Level &l = levels_[i];
     if (!l.run) continue;
     LivePrefix &lp = live_[i];
-    refresh_live_prefix(lp, l.run, l.upper, l.gen, s);
+    // a level holds at most its capacity (the foundation: at least), so its
+    // prefix is allocated once, at that size
+    refresh_live_prefix(lp, l.run, l.upper, l.gen, caps_[i] + 1, s);
     lsm::LevelView v = view_of(int(i));
     v.live = lp.p;
     set->lv[set->count++] = v;
@@ -802,16 +821,19 @@ void LsmDictionary::live_level_set(void *out, cudaStream_t s) {
 
 // The u32 prefix of live values of a run, rebuilt when its generation changed.
 void LsmDictionary::refresh_live_prefix(LivePrefix &lp, RunBuffer *run, uint64_t upper, uint64_t gen,
-                                        cudaStream_t s) {
+                                        uint64_t min_cap, cudaStream_t s) {
   {
     const uint64_t n = upper;
     if (lp.gen != gen || !lp.p) {
       if (n + 1 > lp.cap) {
+        // at least min_cap (the most rows the slot can hold), and growing by
+        // half when a foundation outgrows it: an allocation here can block the
+        // calling thread while the pool maps new memory
+        const uint64_t cap = std::max<uint64_t>({n + 1, min_cap, lp.cap * 3 / 2, 1024});
         if (lp.p) GPULSM_CUDA(cudaFreeAsync(lp.p, s));
         live_bytes_ -= lp.cap * 4;
         lp.p = nullptr;
         lp.cap = 0;
-        const uint64_t cap = std::max<uint64_t>(n + 1, 1024);
         if (cudaMallocAsync(reinterpret_cast<void **>(&lp.p), cap * 4, s) != cudaSuccess) {
           (void)cudaGetLastError();
           lp.p = nullptr;
@@ -1007,6 +1029,12 @@ void LsmDictionary::lookup(const uint32_t *queries, uint64_t n, uint32_t *out_va
   apply_receipt(false);
   begin_op(s);
   ensure_models(s);
+  launch_lookup(queries, n, out_values, out_found, s);
+  end_op(s);
+}
+
+void LsmDictionary::launch_lookup(const uint32_t *queries, uint64_t n, uint32_t *out_values, uint8_t *out_found,
+                                  cudaStream_t s) {
   lsm::LevelSet set;
   level_set(&set);
   if (cfg_.search_mode != 2)
@@ -1016,7 +1044,6 @@ void LsmDictionary::lookup(const uint32_t *queries, uint64_t n, uint32_t *out_va
     lsm::lookup_kernel<false><<<grid_for(n, 256), 256, 0, s>>>(set, queries, n, out_values, out_found);
   note_launch();
   GPULSM_CUDA(cudaGetLastError());
-  end_op(s);
 }
 
 void LsmDictionary::range_sum(const uint32_t *lo, const uint32_t *hi, uint64_t n, uint32_t *out,
@@ -1059,6 +1086,39 @@ void LsmDictionary::range_sum_kway(const uint32_t *lo, const uint32_t *hi, uint6
         set, lo, hi, n, out);
   note_launch();
   GPULSM_CUDA(cudaGetLastError());
+  end_op(s);
+}
+
+void LsmDictionary::lookup_and_range_sum(const uint32_t *queries, uint64_t nq, uint32_t *out_values,
+                                         uint8_t *out_found, const uint32_t *lo, const uint32_t *hi, uint64_t nr,
+                                         uint32_t *out_sums, cudaStream_t s, cudaStream_t side) {
+  std::lock_guard<std::mutex> g(mu_);
+  if ((nq && (!queries || !out_values)) || (nr && (!lo || !hi || !out_sums)) || !side || side == s)
+    throw std::invalid_argument("invalid GPU dictionary read");
+  if (!nq && !nr) return;
+  apply_receipt(false);
+  begin_op(s);
+  ensure_models(s);  // directories and models before the fork: both reads search the levels
+  if (nq) {
+    GPULSM_CUDA(cudaEventRecord(fork_, s));
+    GPULSM_CUDA(cudaStreamWaitEvent(side, fork_, 0));
+    launch_lookup(queries, nq, out_values, out_found, side);
+    GPULSM_CUDA(cudaEventRecord(side_done_, side));
+  }
+  try {
+    if (nr) {
+      lsm::LevelSet set;
+      live_level_set(&set, s);  // prefix scans of changed levels run beside the lookups
+      lsm::range_sum_levels_kernel<<<grid_for(nr * lsm::kRangeGroup, lsm::kRangeThreads), lsm::kRangeThreads, 0,
+                                     s>>>(set, lo, hi, nr, out_sums);
+      note_launch();
+      GPULSM_CUDA(cudaGetLastError());
+    }
+  } catch (...) {
+    if (nq) (void)cudaStreamWaitEvent(s, side_done_, 0);  // s still covers the lookups
+    throw;
+  }
+  if (nq) GPULSM_CUDA(cudaStreamWaitEvent(s, side_done_, 0));
   end_op(s);
 }
 

@@ -72,9 +72,13 @@ class RunPool {
   void advance() { ++epoch_; }
   size_t bytes() const { return bytes_; }
   void account(int64_t delta) { bytes_ = size_t(int64_t(bytes_) + delta); }
+  // the stream-ordered pool the buffers come from: the destructor, which
+  // runs after every other free of the dictionary, trims it
+  void trim_on_destroy(cudaMemPool_t pool) { trim_pool_ = pool; }
 
  private:
   uint32_t rows_log2_;
+  cudaMemPool_t trim_pool_ = nullptr;
   std::vector<std::unique_ptr<RunBuffer>> all_;
   std::vector<RunBuffer *> free_;
   size_t bytes_ = 0;
@@ -102,6 +106,12 @@ class LsmDictionary {
   // range_sum answered by the per-query merge over the levels, never by a
   // compaction (no host wait: for a serving loop that must not stall)
   void range_sum_kway(const uint32_t *lo, const uint32_t *hi, uint64_t n, uint32_t *out, cudaStream_t s);
+  // lookup and range_sum_kway of the same level state, run concurrently: the
+  // lookups on `side` (forked from s once the levels are ready), the range
+  // sums and the live-value prefixes they need on s, which then joins side.
+  void lookup_and_range_sum(const uint32_t *queries, uint64_t nq, uint32_t *out_values, uint8_t *out_found,
+                            const uint32_t *lo, const uint32_t *hi, uint64_t nr, uint32_t *out_sums,
+                            cudaStream_t s, cudaStream_t side);
   void range_count(const uint32_t *lo, const uint32_t *hi, uint64_t n, uint32_t *out,
                    cudaStream_t s);
   void range_offsets(const uint32_t *lo, const uint32_t *hi, uint64_t n, uint64_t *offsets,
@@ -224,6 +234,9 @@ class LsmDictionary {
   void *scratch(size_t bytes, cudaStream_t s);
   void *admit_scratch(size_t bytes, cudaStream_t s);
   void ensure_sort_space(uint64_t n, cudaStream_t s);
+  // the lookup kernel over the current level set on s (no ordering of its own)
+  void launch_lookup(const uint32_t *queries, uint64_t n, uint32_t *out_values, uint8_t *out_found,
+                     cudaStream_t s);
   void level_set(void *out) const;
   lsm::LevelView view_of(int level) const;
   lsm::LevelView view_of_run(const RunBuffer *r) const;
@@ -268,7 +281,8 @@ class LsmDictionary {
   };
   std::vector<LivePrefix> live_;
   std::vector<LivePrefix> live_staged_;  // one per staging slot (gen = the staged run's seq)
-  void refresh_live_prefix(LivePrefix &lp, RunBuffer *run, uint64_t upper, uint64_t gen, cudaStream_t s);
+  void refresh_live_prefix(LivePrefix &lp, RunBuffer *run, uint64_t upper, uint64_t gen, uint64_t min_cap,
+                           cudaStream_t s);
   uint64_t live_bytes_ = 0;
   unsigned long long *width_ = nullptr;  // device word for the range-width estimate
   unsigned long long *width_host_ = nullptr;
@@ -293,6 +307,7 @@ class LsmDictionary {
   cudaStream_t merge_stream_ = nullptr;
   cudaEvent_t adm_done_ = nullptr;
   cudaEvent_t merge_done_ = nullptr;
+  cudaEvent_t fork_ = nullptr, side_done_ = nullptr;  // lookup_and_range_sum
   bool merges_pending_ = false;
   // Merges write their output's directory unless the operation before this
   // update was an update too: levels rewritten by back-to-back update batches

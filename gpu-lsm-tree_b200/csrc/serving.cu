@@ -95,6 +95,7 @@ Server::Server(const DictConfig &cfg, uint64_t budget_bytes, uint32_t max_round_
   GPULSM_CUDA(cudaStreamCreateWithFlags(&upload_, cudaStreamNonBlocking));
   GPULSM_CUDA(cudaStreamCreateWithFlags(&download_, cudaStreamNonBlocking));
   GPULSM_CUDA(cudaStreamCreateWithFlags(&capture_, cudaStreamNonBlocking));
+  GPULSM_CUDA(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
   const uint64_t m = max_round_keys_;
   // inputs: at most two words and an erase mark a key, plus the padding of
   // a staged update batch (form_round checks the exact need)
@@ -152,6 +153,7 @@ Server::~Server() {
   cudaStreamSynchronize(compute_);
   cudaStreamSynchronize(upload_);
   cudaStreamSynchronize(download_);
+  cudaStreamSynchronize(side_);
   for (Slot &s : slots_) {
     cudaFreeHost(s.h_table);
     cudaFree(s.d_span);
@@ -173,6 +175,7 @@ Server::~Server() {
   cudaStreamDestroy(compute_);
   cudaStreamDestroy(upload_);
   cudaStreamDestroy(download_);
+  cudaStreamDestroy(side_);
 }
 
 uint64_t Server::submit(uint32_t kind, const uint32_t *keys, const uint32_t *aux, uint64_t n, uint32_t *out,
@@ -295,6 +298,7 @@ void Server::reset_stats() {
   st_graph_updates_ = 0;
   st_first_ = -1;
   st_last_ = st_gpu_s_ = st_launch_s_ = 0;
+  st_max_gpu_s_ = st_max_launch_s_ = 0;
   for (double &k : st_kind_gpu_s_) k = 0;
   st_copy_s_ = st_scatter_s_ = 0;
 }
@@ -313,6 +317,8 @@ ServeStats Server::stats() {
     s.wall_s = st_first_ >= 0 ? std::max(0.0, st_last_ - st_first_) : 0.0;
     s.gpu_busy_s = st_gpu_s_;
     s.host_launch_s = st_launch_s_;
+    s.max_round_gpu_us = st_max_gpu_s_ * 1e6;
+    s.max_launch_us = st_max_launch_s_ * 1e6;
     s.graph_rounds = st_graph_rounds_;
     s.graph_updates = st_graph_updates_;
     s.stage_flushes = dict_.stage_flushes();
@@ -645,15 +651,27 @@ void Server::launch_round(Slot &slot) {
       ++st_graph_updates_;
     });
   }
-  if (rl.n)
+  if (rl.n && rr.n) {
+    // both reads see the same levels: the lookups run beside the range sums
+    // (their time is charged to lookup, the kind that also waits for the
+    // round's merges)
+    Run both{};
+    timed_call(both, kServeLookup, [&] {
+      const uint32_t *in = slot.d_in + rr.in_off;
+      dict_.lookup_and_range_sum(slot.d_in + rl.in_off, rl.n, slot.d_out + rl.out_off, slot.d_found + rl.out_off,
+                                 in, in + rr.n, rr.n, slot.d_out + rr.out_off, compute_, side_);
+    });
+    if (both.status) rl.status = rr.status = both.status;
+  } else if (rl.n) {
     timed_call(rl, kServeLookup, [&] {
       dict_.lookup(slot.d_in + rl.in_off, rl.n, slot.d_out + rl.out_off, slot.d_found + rl.out_off, compute_);
     });
-  if (rr.n)
+  } else if (rr.n) {
     timed_call(rr, kServeRangeSum, [&] {
       const uint32_t *in = slot.d_in + rr.in_off;
       dict_.range_sum_kway(in, in + rr.n, rr.n, slot.d_out + rr.out_off, compute_);
     });
+  }
   // an update request completes when its merges have completed
   if (ru.n && !staged_updates_) {
     Run none{};
@@ -703,6 +721,7 @@ void Server::worker() {
     const double t1 = now_s();
     lk.lock();
     st_launch_s_ += t1 - t0;
+    st_max_launch_s_ = std::max(st_max_launch_s_, t1 - t0);
     slot.launched = ok;
     inflight_.push_back(si);
     inflight_bytes_ += slot.bytes;
@@ -766,6 +785,7 @@ void Server::completer() {
     ++st_rounds_;
     st_round_keys_ += slot.keys;
     st_gpu_s_ += double(gpu_ms) * 1e-3;
+    st_max_gpu_s_ = std::max(st_max_gpu_s_, double(gpu_ms) * 1e-3);
     st_last_ = t;
     free_slots_.push_back(si);
     lk.unlock();

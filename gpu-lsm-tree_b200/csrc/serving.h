@@ -63,6 +63,8 @@ struct ServeStats {
   double kind_gpu_s[4] = {0, 0, 0, 0};
   double host_copy_s = 0;     // submitters' time copying request data into the pinned ring
   double host_scatter_s = 0;  // completion time copying results into the requests' buffers
+  double max_round_gpu_us = 0;  // the longest round's device time (upload done -> kernels done)
+  double max_launch_us = 0;     // the worker's longest time staging and launching one round
 };
 
 // Open-loop load: Poisson arrivals, kind mix, log-uniform sizes, Zipf keys.
@@ -207,6 +209,7 @@ class Server {
   std::deque<uint32_t> inflight_;
   cudaStream_t compute_ = nullptr, upload_ = nullptr, download_ = nullptr;
   cudaStream_t capture_ = nullptr;  // graphs are captured here (thread-local mode)
+  cudaStream_t side_ = nullptr;     // a round's lookups beside its range sums
   uint64_t st_graph_rounds_ = 0;
   // staged updates: update runs replayed from captured graphs (admission only;
   // the staged runs merge into the levels when the staging slots are full)
@@ -228,6 +231,7 @@ class Server {
   std::vector<float> lat_us_;
   uint64_t st_completed_ = 0, st_rejected_ = 0, st_rounds_ = 0, st_keys_ = 0, st_round_keys_ = 0;
   double st_first_ = -1, st_last_ = 0, st_gpu_s_ = 0, st_launch_s_ = 0;
+  double st_max_gpu_s_ = 0, st_max_launch_s_ = 0;
   double st_kind_gpu_s_[4] = {0, 0, 0, 0}, st_copy_s_ = 0, st_scatter_s_ = 0;
 
   std::thread worker_, completer_;

@@ -261,12 +261,15 @@ typedef struct gpulsm_serve_stats {
   double gpu_busy_s, host_launch_s; /* device time of the rounds; worker time staging + launching */
   uint64_t graph_rounds;            /* lookup-only rounds replayed from a captured CUDA graph */
   double kind_gpu_s[4];             /* device time of each request kind's calls (updates: merges included;
-                                       a round's update batch counts as insert, or erase when it only erases),
+                                       a round's update batch counts as insert, or erase when it only erases;
+                                       a round's lookups and range sums run concurrently and count as lookup),
                                        timed on every eighth round and scaled by eight */
   double host_copy_s;               /* submitters' time copying request data into the server's pinned ring */
   double host_scatter_s;            /* completion time copying results into the requests' buffers */
   uint64_t graph_updates;           /* update batches replayed from a captured CUDA graph (staged admission) */
   uint64_t stage_flushes;           /* merges of the staged runs into the levels */
+  double max_round_gpu_us;          /* the longest round's device time */
+  double max_launch_us;             /* the worker's longest time staging and launching one round */
 } gpulsm_serve_stats;
 
 /* Open-loop load: Poisson arrivals at rate_per_s (0 = closed loop with

@@ -56,6 +56,32 @@ def test_config_struct_layout_matches_header(gl):
     assert C.sizeof(N.FlixConfig) == 4 * 4 + 8
 
 
+def test_every_ctypes_struct_matches_the_c_header(gl, tmp_path):
+    """Size and every field offset of the ctypes mirrors, against a C program
+    compiled from include/gpulsm.h (a field missing from the header fails the
+    compile)."""
+    N = gl._native
+    pairs = [(N.DictConfig, "gpulsm_dict_config"), (N.FlixConfig, "gpulsm_flix_config"),
+             (N.ServeStats, "gpulsm_serve_stats"), (N.LoadSpec, "gpulsm_load_spec")]
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "gpulsm.h"', "int main(void) {"]
+    for cls, ctype in pairs:
+        lines.append(f'  printf("{ctype} sizeof %zu\\n", sizeof({ctype}));')
+        for name, _ in cls._fields_:
+            lines.append(f'  printf("{ctype} {name} %zu\\n", offsetof({ctype}, {name}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = dict(((a, b), int(c)) for a, b, c in
+               (line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                         check=True).stdout.splitlines()))
+    for cls, ctype in pairs:
+        assert got[(ctype, "sizeof")] == C.sizeof(cls), ctype
+        for name, _ in cls._fields_:
+            assert got[(ctype, name)] == getattr(cls, name).offset, (ctype, name)
+
+
 def test_no_cpu_fallback_when_library_missing(tmp_path):
     """Importing the package from a copy without libgpulsm.so must fail loudly."""
     import shutil
