@@ -6,8 +6,9 @@
 // caller batches by hand.  Here requests are submitted from any host thread
 // with host buffers; a worker thread takes what has queued, in arrival order,
 // into a round of at most three dictionary calls - every insert and erase of
-// the round as one mixed update batch, then every lookup as one lookup, then
-// every range sum as one range sum - and admits an update only while the
+// the round as one mixed update batch, then every lookup as one lookup and
+// every range sum as one range sum, the two reads running concurrently on the
+// same level state - and admits an update only while the
 // dictionary's resident bytes plus the rounds in flight stay inside a
 // device-memory budget.  submit() copies the request's keys (and values or
 // upper bounds) into a pinned ring on the caller's thread, so the worker
