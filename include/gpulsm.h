@@ -238,8 +238,8 @@ int gpulsm_tenants_resident_bytes(gpulsm_tenants *pool, uint64_t *out_bytes);
  * order, into a round of at most three dictionary calls (every insert and
  * erase of the round as one update batch, then every lookup and every range
  * sum, the two reads running concurrently), admits updates while the
- * dictionary's resident bytes plus the rounds
- * in flight fit the device budget (an update that cannot fit fails with
+ * dictionary's resident bytes plus the rounds in flight fit the device
+ * budget (an update that cannot fit fails with
  * GPULSM_ERR_CAPACITY), and pipelines rounds through `depth` staging slots.
  * Submit copies the request's keys and values / upper bounds into a pinned
  * ring of the server before it returns (waiting while the ring is full); the
