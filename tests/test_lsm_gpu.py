@@ -581,3 +581,35 @@ def test_cleanup_keeps_answers_and_leaves_one_level(gl, cuda):
     torch.cuda.synchronize()
     assert np.array_equal(to_host(out)[: q.size], o.lookup(q))
     assert d.cleanup() == len(o)
+
+
+def test_single_level_range_pairs_edges(gl, cuda):
+    """The one-level range-pairs copy (warps take 32-query groups from a
+    counter, slices of up to 8 rows are copied per lane and longer ones by the
+    warp) against the oracle: inverted and empty ranges, single keys present
+    and absent, slices around the 8-row per-lane limit, whole-key-space
+    ranges, the key-space ends, and query counts that are not multiples of
+    the 32-query group."""
+    rng = np.random.default_rng(11)
+    t = Twin(gl, max_elements=1 << 18, batch_capacity=1 << 14)
+    keys = np.unique(rng.integers(0, 1 << 20, 60000, dtype=np.uint64).astype(np.uint32))
+    keys = np.concatenate([keys, np.array([0, 0xFFFFFFFE, 0xFFFFFFFF], np.uint32)])
+    vals = rng.integers(0, 1 << 32, keys.size, dtype=np.uint64).astype(np.uint32)
+    t.apply(("insert", keys, vals))
+    t.apply(("erase", keys[rng.integers(0, keys.size, 3000)]))
+    t.d.cleanup()  # one tombstone-free level: every range read takes the one-level path
+    assert t.d.size()[1] == 1
+    lo, hi = [], []
+    for w in (0, 1, 2, 50, 100, 130, 140, 150, 160, 300, 5000, 1 << 16):  # ~0..3700 rows
+        a = rng.integers(0, 1 << 20, 64, dtype=np.uint64)
+        lo.append(a)
+        hi.append(a + w)
+    present = keys[rng.integers(0, keys.size, 64)].astype(np.uint64)
+    lo += [present, present + 1, np.array([0, 0, 5, 0xFFFFFF00, 0xFFFFFFFF, 0xFFFFFFFF, 100, 1 << 21], np.uint64)]
+    hi += [present, present + 1, np.array([0xFFFFFFFF, 0, 0, 0xFFFFFFFF, 0xFFFFFFFF, 0, 99, 1 << 22], np.uint64)]
+    lo = np.concatenate(lo).clip(0, 0xFFFFFFFF).astype(np.uint32)
+    hi = np.concatenate(hi).clip(0, 0xFFFFFFFF).astype(np.uint32)
+    perm = rng.permutation(lo.size)
+    lo, hi = lo[perm], hi[perm]
+    for n in (1, 31, 33, 100, lo.size):
+        t.ranges(lo[:n], hi[:n])
