@@ -379,9 +379,12 @@ __global__ void __launch_bounds__(256) merge_partition_kernel(const uint32_t *__
 // its chunk); after the gather the same arrays stage the output rows at the
 // alignment of their global position, for bulk stores of the aligned middle.
 struct MergeSmem {
-  uint32_t key[kMergeTile + 16];  // A chunk, then B chunk (each at most slice + 6 keys)
+  // A chunk, then B chunk (each at most slice + 6 keys, + 30 flags); the tails
+  // leave room for the serial merge's reads past a slice's end (up to
+  // kMergeItems + 1 keys past B's slice), whose values it never uses
+  uint32_t key[kMergeTile + 32];
   uint32_t val[kMergeTile + 16];
-  uint8_t flag[kMergeTile + 64];  // A chunk, then B chunk (each at most slice + 30 flags)
+  uint8_t flag[kMergeTile + 80];
   uint16_t src[kMergeTile];       // tile-local source index of each kept row
   uint32_t scan[kMergeThreads / 32];
   uint32_t total;
@@ -520,15 +523,18 @@ __global__ void __launch_bounds__(kMergeThreads, 4) merge_kernel(
   const uint32_t *vA = sm.val + oa, *vB = sm.val + la + ob;
   const uint8_t *gA = sm.flag + fa, *gB = sm.flag + fla + fb;
   // serial merge of this thread's outputs, branch-free: one shared load per
-  // output (the new head of the side that advanced)
+  // output (the new head of the side that advanced).  A head read at or past
+  // its slice's end (ai == alen; bi >= blen) is never used: ka only counts
+  // while ai < alen, kb only while bi < blen, and items past my_n (where bi
+  // may run up to blen + kMergeItems) keep nothing - MergeSmem's padding
+  // keeps those reads inside the arrays.
   const uint32_t my_d = min(uint32_t(threadIdx.x) * kMergeItems, len);
   const uint32_t my_n = min(uint32_t(kMergeItems), len - my_d);
-  const uint32_t amax = alen ? alen - 1 : 0u, bmax = blen ? blen - 1 : 0u;
   uint32_t ai = merge_path32(sA, alen, sB, blen, my_d);
   uint32_t bi = my_d - ai;
   bool hp = ai > 0 ? true : has_prev_a;
   uint32_t prev = ai > 0 ? sA[ai - 1] : prev_a_global;
-  uint32_t ka = sA[min(ai, amax)], kb = sB[min(bi, bmax)];
+  uint32_t ka = sA[ai], kb = sB[bi];
   uint16_t src[kMergeItems];
   uint32_t keep_mask = 0;
 #pragma unroll
@@ -537,12 +543,12 @@ __global__ void __launch_bounds__(kMergeThreads, 4) merge_kernel(
     const uint32_t idx = ta ? ai : alen + bi;
     const bool shadow = !ta && hp && prev == kb;
     bool keep = uint32_t(i) < my_n && !shadow;
-    if (kDropTombstones) keep = keep && !(*(ta ? gA + min(ai, amax) : gB + min(bi, bmax)) & kFlagTomb);
+    if (kDropTombstones) keep = keep && !(*(ta ? gA + ai : gB + bi) & kFlagTomb);
     hp = hp || ta;
     prev = ta ? ka : prev;
     ai += ta ? 1u : 0u;
     bi += ta ? 0u : 1u;
-    const uint32_t nxt = *(ta ? sA + min(ai, amax) : sB + min(bi, bmax));
+    const uint32_t nxt = *(ta ? sA + ai : sB + bi);
     ka = ta ? nxt : ka;
     kb = ta ? kb : nxt;
     src[i] = uint16_t(idx);
